@@ -1,0 +1,135 @@
+/*
+ * pci_gpu.h -- C ABI of the B200 engine for pconf's two hot stages:
+ * the determinant-pair Hamiltonian build (FormH / FormJ) and the Davidson
+ * eigensolver (Diag4).
+ *
+ * Every argument is ISO_C_BINDING-interoperable (int32_t, int64_t, double,
+ * plain pointers).  Index conventions are the Fortran ones: m-state, orbital
+ * and determinant indices are 1-based values, arrays are passed as the
+ * column-major Fortran arrays they are in pconf (Iarr(Ne,Nd) is Ne
+ * consecutive m-states per determinant).  Host arrays are borrowed for the
+ * duration of a call; device buffers (tables, CSR, vectors) belong to the
+ * handle until pci_gpu_destroy.  Calls on one handle must come from one host
+ * thread; all calls are synchronous.
+ *
+ * Every int-returning entry point returns PCI_OK (0) or one of the PCI_E_*
+ * codes below; pci_gpu_last_error() then holds a message.
+ */
+#ifndef PCI_GPU_H
+#define PCI_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PCI_OK                 0
+#define PCI_E_INPUT            1  /* inconsistent sizes or indices (pconf Stop) */
+#define PCI_E_OOM              2  /* device allocation failed */
+#define PCI_E_MISSING_INTEGRAL 3  /* Gint: integral is absent (integrals.f90:256-261) */
+#define PCI_E_ORTHO_FAIL       4  /* Fail of orthogonalization/normalization (davidson.f90:718-737) */
+#define PCI_E_TIMEOUT          5  /* a bounded device wait gave up */
+#define PCI_E_CUDA             6  /* CUDA runtime / library error */
+#define PCI_E_STATE            7  /* call out of order (e.g. davidson before form_h) */
+#define PCI_E_NOT_CONVERGED    8  /* N_it reached with a residual above Crt4 (info only) */
+
+#define PCI_MAT_H   0
+#define PCI_MAT_J2  1
+
+typedef struct pci_gpu pci_gpu_t;
+
+/* Davidson settings.  Field meanings follow CONF.INP / ci.in keys
+ * (conf_init.f90:37-213). */
+typedef struct {
+    int32_t Nlv;        /* number of levels (NLV) */
+    int32_t N_it;       /* iteration limit (N_IT) */
+    int32_t Kl4;        /* 1: initial vectors from the Nd0 block; 2: from X0 (CONF.XIJ) */
+    int32_t Kv;         /* 4: no J selection; 3: select and project on J = XJ_av */
+    int32_t Nc4;        /* configurations eligible for the initial block */
+    int32_t MaxNd0;     /* largest initial block (ci.in MaxNd0, default 3000) */
+    int32_t mode;       /* PCI_DVD_FP64 (reference algorithm) or PCI_DVD_FP32 */
+    int32_t KXIJ;       /* unused by the library; kept for the caller's CONF.XIJ cadence */
+    double  Crt4;       /* residual-norm convergence threshold (CRT4) */
+    double  XJ_av;      /* target J for Kv = 3 */
+    double  admix_crit; /* stop when max admixture <= this (pconf.F90:2015, 1e-6); 0 disables */
+} pci_dvd_params;
+
+#define PCI_DVD_FP64 0
+#define PCI_DVD_FP32 1
+
+/* Replaces: the device has no counterpart in pconf; this opens a handle on
+ * CUDA device `device` (the MPI rank's process is the reference's unit). */
+int pci_gpu_create(int32_t device, pci_gpu_t **h);
+
+/* Replaces: the broadcast of the determinant basis in InitFormH
+ * (pconf.F90:1096-1118) -- Iarr, Nh, Jz, Nn, Kk, Ll, Jj, Ndc, Nc, Ne, Nd,
+ * Nst, Nso, Nx, Mj, Gj.  Nsu is the number of orbitals in Nn/Kk/Ll/Jj.
+ * Determinants must be grouped by configuration in Ndc order and each sorted
+ * ascending (Det_List, determinants.f90:144-183). */
+int pci_gpu_set_basis(pci_gpu_t *h, int32_t Ne, int64_t Nd, int32_t Nst, int32_t Nsu,
+                      int32_t Nso, int32_t Nx, int32_t Mj,
+                      const int32_t *Iarr, const int32_t *Nh, const int32_t *Jz,
+                      const int32_t *Nn, const int32_t *Kk, const int32_t *Ll, const int32_t *Jj,
+                      int32_t Nc, const int32_t *Ndc, double Gj);
+
+/* Replaces: BuildHintLUT, BuildGauntLUT and BuildGintHash
+ * (integrals.f90:604-632, 663-674, 702-715) fed by Rint (integrals.f90:13-120)
+ * and CONF.GNT (pconf.F90:383-406).  HintLUT has Nx*Nx entries, GauntLUT
+ * nGauntLUT entries (index 0..max(In)), Rint2 holds Ngint values (two per
+ * integral, interleaved, when kbrt /= 0) as float (r2_is_f64 = 0, the
+ * reference's default type2_real) or double (USE_DP_INTEGRALS). */
+int pci_gpu_set_integrals(pci_gpu_t *h, const double *HintLUT, int32_t Nlx,
+                          int64_t nGauntLUT, const double *GauntLUT,
+                          int64_t Ngint, int32_t kbrt, int32_t r2_is_f64,
+                          const void *Rint2, const int32_t *Iint2, const int32_t *Iint3);
+
+/* Replaces: Call FormH + RedistributeHamCSR (pconf.F90:217-219).  Builds the
+ * lower triangle (diagonal included, columns ascending, exact zeros dropped:
+ * npes = 1 semantics, pconf.F90:1259) as device-resident CSR with values in
+ * FP64 (value_prec = 64) or FP32 (32).  Returns NumH (stored elements),
+ * numzero (difference <= 2 pairs whose element is exactly 0) and Hmin (the
+ * minimum stored value, Hamil%minval). */
+int pci_gpu_form_h(pci_gpu_t *h, int32_t value_prec, int64_t *NumH, int64_t *numzero, double *Hmin);
+
+/* Replaces: Call FormJ + RedistributeJsqCSR (pconf.F90:224-225).  J^2 in units
+ * of (2j)^2 over pairs inside one configuration block. */
+int pci_gpu_form_j(pci_gpu_t *h, int64_t *NumJ);
+
+/* Sizes of a resident matrix: rows (Nd) and stored elements. */
+int pci_gpu_csr_info(pci_gpu_t *h, int32_t which, int64_t *nrows, int64_t *nnz);
+
+/* Replaces: the Hamil%col/val + HamilCSR_rowptr globals that WriteMatrixCSR
+ * streams to pCONF.HIJ (matrix_io.f90:689-799).  Copies the resident CSR out:
+ * rowptr[Nd+1] 0-based prefix (HamilCSR_rowptr(0:Nd)), col 1-based, val as
+ * double.  Any pointer may be NULL to skip that array. */
+int pci_gpu_get_csr(pci_gpu_t *h, int32_t which, int64_t *rowptr, int32_t *col, double *val);
+
+/* Replaces: ReadMatrixCSR (matrix_io.f90:801-939) for Kl = 1 restarts:
+ * uploads a lower-triangle CSR (same layout as pci_gpu_get_csr) and its Hmin. */
+int pci_gpu_set_csr(pci_gpu_t *h, int32_t which, int64_t Nd, int64_t nnz, const int64_t *rowptr,
+                    const int32_t *col, const double *val, double Hmin);
+
+/* Replaces: Call Diag4 (pconf.F90:238) with Init4, DiagInitApprox, FormB0 and
+ * the Davidson module (davidson.f90).  X0 (Nd x Nlv column-major, Kl4 = 2) may
+ * be NULL.  Outputs: Tk (energies, -(E + Hmin)), Tj (J of each level, J_av),
+ * Iconverge, X (Nd x Nlv column-major eigenvectors, may be NULL), the
+ * iteration count and, if non-NULL, the final residual norms (length Nlv). */
+int pci_gpu_davidson(pci_gpu_t *h, const pci_dvd_params *p, const double *X0,
+                     double *Tk, double *Tj, int32_t *Iconverge, double *X,
+                     int32_t *iters, double *resid);
+
+/* Per-stage device times (milliseconds) of the last calls: [0] FormH total,
+ * [1] FormH count pass, [2] FormH fill pass, [3] FormJ, [4] Davidson total,
+ * [5] SpMM total in the last Davidson, [6] number of SpMM launches,
+ * [7] Init4 + DiagInitApprox.  n is the capacity of `out`; returns the
+ * number written. */
+int32_t pci_gpu_stats(pci_gpu_t *h, double *out, int32_t n);
+
+const char *pci_gpu_last_error(pci_gpu_t *h);
+void pci_gpu_destroy(pci_gpu_t *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PCI_GPU_H */

@@ -1,0 +1,181 @@
+"""ctypes binding of libpci_gpu.so (include/pci_gpu.h).
+
+This is the same boundary a Fortran ``pconf`` binds through ISO_C_BINDING:
+plain pointers and sizes, 1-based Fortran indices.  There is no fallback: if
+the library is missing or fails to load, importing the binding raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .build import LIB
+
+PCI_OK = 0
+ERRORS = {1: "PCI_E_INPUT", 2: "PCI_E_OOM", 3: "PCI_E_MISSING_INTEGRAL", 4: "PCI_E_ORTHO_FAIL",
+          5: "PCI_E_TIMEOUT", 6: "PCI_E_CUDA", 7: "PCI_E_STATE", 8: "PCI_E_NOT_CONVERGED"}
+PCI_MAT_H, PCI_MAT_J2 = 0, 1
+PCI_DVD_FP64, PCI_DVD_FP32 = 0, 1
+
+EXPORTS = ["pci_gpu_create", "pci_gpu_set_basis", "pci_gpu_set_integrals", "pci_gpu_form_h",
+           "pci_gpu_form_j", "pci_gpu_csr_info", "pci_gpu_get_csr", "pci_gpu_set_csr",
+           "pci_gpu_davidson", "pci_gpu_stats", "pci_gpu_last_error", "pci_gpu_destroy"]
+
+
+class PciError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class DvdParams(C.Structure):
+    _fields_ = [("Nlv", C.c_int32), ("N_it", C.c_int32), ("Kl4", C.c_int32), ("Kv", C.c_int32),
+                ("Nc4", C.c_int32), ("MaxNd0", C.c_int32), ("mode", C.c_int32), ("KXIJ", C.c_int32),
+                ("Crt4", C.c_double), ("XJ_av", C.c_double), ("admix_crit", C.c_double)]
+
+
+_lib = None
+
+
+def load(path: str = LIB):
+    """Load the library (raises if it is absent: build it with pci_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"libpci_gpu.so not found at {path}; run `python -m pci_b200.build`")
+    L = C.CDLL(path)
+    P = C.c_void_p
+    i32, i64, f64 = C.c_int32, C.c_int64, C.c_double
+    L.pci_gpu_create.argtypes = [i32, C.POINTER(P)]
+    L.pci_gpu_set_basis.argtypes = [P, i32, i64, i32, i32, i32, i32, i32, P, P, P, P, P, P, P, i32, P, f64]
+    L.pci_gpu_set_integrals.argtypes = [P, P, i32, i64, P, i64, i32, i32, P, P, P]
+    L.pci_gpu_form_h.argtypes = [P, i32, C.POINTER(i64), C.POINTER(i64), C.POINTER(f64)]
+    L.pci_gpu_form_j.argtypes = [P, C.POINTER(i64)]
+    L.pci_gpu_csr_info.argtypes = [P, i32, C.POINTER(i64), C.POINTER(i64)]
+    L.pci_gpu_get_csr.argtypes = [P, i32, P, P, P]
+    L.pci_gpu_set_csr.argtypes = [P, i32, i64, i64, P, P, P, f64]
+    L.pci_gpu_davidson.argtypes = [P, C.POINTER(DvdParams), P, P, P, P, P, C.POINTER(i32), P]
+    L.pci_gpu_stats.argtypes = [P, P, i32]
+    L.pci_gpu_stats.restype = i32
+    L.pci_gpu_last_error.argtypes = [P]
+    L.pci_gpu_last_error.restype = C.c_char_p
+    L.pci_gpu_destroy.argtypes = [P]
+    L.pci_gpu_destroy.restype = None
+    _lib = L
+    return L
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Engine:
+    """One device handle: the drop-in for pconf's FormH, FormJ and Diag4 calls."""
+
+    def __init__(self, device: int = 0):
+        self.L = load()
+        self.h = C.c_void_p()
+        rc = self.L.pci_gpu_create(device, C.byref(self.h))
+        self._check(rc)
+
+    def _check(self, rc):
+        if rc != PCI_OK:
+            msg = self.L.pci_gpu_last_error(self.h).decode() if self.h else ""
+            raise PciError(rc, msg)
+
+    def close(self):
+        if self.h:
+            self.L.pci_gpu_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # --- inputs ---------------------------------------------------------
+    def set_basis(self, sysm):
+        b = sysm.basis
+        nsu = sysm.nsu
+        arr = lambda x: np.ascontiguousarray(x, dtype=np.int32)
+        self._basis = dict(iarr=arr(sysm.iarr), nh=arr(sysm.nh), jz=arr(sysm.jz), nn=arr(b.nn[:nsu]),
+                           kk=arr(b.kk[:nsu]), ll=arr(b.ll[:nsu]), jj=arr(b.jj[:nsu]), ndc=arr(sysm.ndc))
+        k = self._basis
+        rc = self.L.pci_gpu_set_basis(self.h, sysm.ne, sysm.nd, sysm.nst, nsu, b.nso, sysm.nx, sysm.mj,
+                                      _p(k["iarr"]), _p(k["nh"]), _p(k["jz"]), _p(k["nn"]), _p(k["kk"]),
+                                      _p(k["ll"]), _p(k["jj"]), sysm.nc, _p(k["ndc"]), float(sysm.gj))
+        self._check(rc)
+
+    def set_integrals(self, sysm):
+        hl = np.ascontiguousarray(sysm.hint_lut, np.float64)
+        gl = np.ascontiguousarray(sysm.gaunt_lut, np.float64)
+        r2 = np.ascontiguousarray(sysm.rint2)
+        i2 = np.ascontiguousarray(sysm.iint2, np.int32)
+        i3 = np.ascontiguousarray(sysm.iint3, np.int32)
+        rc = self.L.pci_gpu_set_integrals(self.h, _p(hl), sysm.nlx, gl.size, _p(gl), sysm.ngint, sysm.kbrt,
+                                          1 if r2.dtype == np.float64 else 0, _p(r2), _p(i2), _p(i3))
+        self._check(rc)
+
+    def load_system(self, sysm):
+        self.set_basis(sysm)
+        self.set_integrals(sysm)
+
+    # --- FormH / FormJ --------------------------------------------------
+    def form_h(self, value_prec: int = 64):
+        numh, nz, hmin = C.c_int64(), C.c_int64(), C.c_double()
+        self._check(self.L.pci_gpu_form_h(self.h, value_prec, C.byref(numh), C.byref(nz), C.byref(hmin)))
+        return numh.value, nz.value, hmin.value
+
+    def form_j(self):
+        n = C.c_int64()
+        self._check(self.L.pci_gpu_form_j(self.h, C.byref(n)))
+        return n.value
+
+    def get_csr(self, which: int = PCI_MAT_H):
+        nrows, nnz = C.c_int64(), C.c_int64()
+        self._check(self.L.pci_gpu_csr_info(self.h, which, C.byref(nrows), C.byref(nnz)))
+        rowptr = np.zeros(nrows.value + 1, np.int64)
+        col = np.zeros(nnz.value, np.int32)
+        val = np.zeros(nnz.value, np.float64)
+        self._check(self.L.pci_gpu_get_csr(self.h, which, _p(rowptr), _p(col), _p(val)))
+        return rowptr, col, val
+
+    def set_csr(self, which, rowptr, col, val, hmin=0.0):
+        rowptr = np.ascontiguousarray(rowptr, np.int64)
+        col = np.ascontiguousarray(col, np.int32)
+        val = np.ascontiguousarray(val, np.float64)
+        self._check(self.L.pci_gpu_set_csr(self.h, which, rowptr.size - 1, col.size, _p(rowptr), _p(col),
+                                           _p(val), float(hmin)))
+
+    # --- Diag4 ----------------------------------------------------------
+    def davidson(self, nd: int, Nlv: int, N_it: int = 200, Crt4: float = 1e-8, Kl4: int = 1, Kv: int = 4,
+                 Nc4: int = 0, MaxNd0: int = 3000, mode: int = PCI_DVD_FP64, XJ_av: float = 0.0,
+                 admix_crit: float = 1e-6, X0=None, want_vectors: bool = True):
+        p = DvdParams(Nlv, N_it, Kl4, Kv, Nc4, MaxNd0, mode, 0, Crt4, XJ_av, admix_crit)
+        Tk = np.zeros(Nlv)
+        Tj = np.zeros(Nlv)
+        ic = np.zeros(Nlv, np.int32)
+        res = np.zeros(Nlv)
+        X = np.zeros((Nlv, nd)) if want_vectors else None   # column-major Nd x Nlv == row-major Nlv x Nd
+        x0 = None if X0 is None else np.ascontiguousarray(np.asarray(X0).T, np.float64)
+        iters = C.c_int32()
+        self._check(self.L.pci_gpu_davidson(self.h, C.byref(p), _p(x0), _p(Tk), _p(Tj), _p(ic), _p(X),
+                                            C.byref(iters), _p(res)))
+        return dict(Tk=Tk, Tj=Tj, Iconverge=ic, X=None if X is None else X.T, iterations=iters.value, resid=res)
+
+    def stats(self):
+        out = np.zeros(8)
+        n = self.L.pci_gpu_stats(self.h, _p(out), 8)
+        keys = ["formh_ms", "formh_count_ms", "formh_fill_ms", "formj_ms", "davidson_ms", "spmm_ms",
+                "spmm_calls", "init_ms"]
+        return dict(zip(keys[:n], out[:n].tolist()))

@@ -1,0 +1,377 @@
+// C ABI of libpci_gpu.so: handle lifecycle, input validation and upload,
+// CSR copy-out, and dispatch to the H-build, SpMM and Davidson units.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pci_internal.h"
+
+// ------------------------------------------------------------ helpers ---
+
+int set_err(pci_gpu *h, int code, const std::string &msg)
+{
+    if (h) h->err = msg;
+    return code;
+}
+
+int cuda_err(pci_gpu *h, cudaError_t e, const char *what)
+{
+    std::string m = std::string("CUDA error ") + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ") in " + what;
+    return set_err(h, e == cudaErrorMemoryAllocation ? PCI_E_OOM : PCI_E_CUDA, m);
+}
+
+void *dev_alloc(pci_gpu *h, size_t bytes, int *rc)
+{
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *rc = set_err(h, PCI_E_OOM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+        return nullptr;
+    }
+    *rc = PCI_OK;
+    return p;
+}
+
+void dev_free(void *p)
+{
+    if (p) cudaFree(p);
+}
+
+int ensure_tmp(pci_gpu *h, size_t bytes)
+{
+    if (h->tmp_bytes >= bytes && h->d_tmp) return PCI_OK;
+    cudaStreamSynchronize(h->st);
+    dev_free(h->d_tmp);
+    h->d_tmp = nullptr;
+    h->tmp_bytes = 0;
+    int rc = 0;
+    h->d_tmp = dev_alloc(h, bytes, &rc);
+    if (rc) return rc;
+    h->tmp_bytes = bytes;
+    return PCI_OK;
+}
+
+DevSys make_devsys(const pci_gpu *h)
+{
+    DevSys S;
+    memset(&S, 0, sizeof(S));
+    S.ne = h->ne; S.nst = h->nst; S.nsu = h->nsu; S.nso = h->nso; S.nx = h->nx; S.mj = h->mj; S.nc = h->nc;
+    S.nlx = h->nlx; S.kbrt = h->kbrt; S.kdim = h->kdim; S.ntype = h->ntype;
+    S.nd = h->nd; S.gj = h->gj;
+    S.occ = h->d_occ; S.conf_of = h->d_conf_of; S.conf_start = h->d_conf_start; S.conf_orb = h->d_conf_orb;
+    S.adj_ptr = h->d_adj_ptr; S.adj = h->d_adj;
+    S.ms_orb = h->d_ms_orb; S.ms_jz = h->d_ms_jz; S.ms_type = h->d_ms_type;
+    S.orb_l = h->d_orb_l; S.orb_j = h->d_orb_j;
+    S.h1 = h->d_h1; S.gaunt = h->d_gaunt; S.hkey = h->d_hkey; S.hval = h->d_hval;
+    S.hmask = h->hcap ? h->hcap - 1 : 0;
+    S.err = h->d_err;
+    return S;
+}
+
+static int type_offset(int j2) { return ((j2 - 1) / 2) * ((j2 + 1) / 2); }
+
+template <typename T>
+static int upload(pci_gpu *h, T **dst, const std::vector<T> &src)
+{
+    int rc = 0;
+    dev_free(*dst);
+    *dst = (T *)dev_alloc(h, std::max<size_t>(src.size(), 1) * sizeof(T), &rc);
+    if (rc) return rc;
+    if (!src.empty()) PCI_CUDA(h, cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, h->st));
+    return PCI_OK;
+}
+
+static void free_basis(pci_gpu *h)
+{
+    dev_free(h->d_occ); dev_free(h->d_conf_of); dev_free(h->d_conf_start); dev_free(h->d_conf_orb);
+    dev_free(h->d_adj_ptr); dev_free(h->d_adj); dev_free(h->d_ms_orb); dev_free(h->d_ms_jz);
+    dev_free(h->d_ms_type); dev_free(h->d_orb_l); dev_free(h->d_orb_j);
+    h->d_occ = nullptr; h->d_conf_of = nullptr; h->d_conf_start = nullptr; h->d_conf_orb = nullptr;
+    h->d_adj_ptr = nullptr; h->d_adj = nullptr; h->d_ms_orb = nullptr; h->d_ms_jz = nullptr;
+    h->d_ms_type = nullptr; h->d_orb_l = nullptr; h->d_orb_j = nullptr;
+    h->have_basis = false;
+}
+
+// Gaunt table over (k, (j1,m1) type, (j2,m2) type) and the compact one-electron
+// table need both the basis and the integrals; rebuilt whenever either changes.
+static int build_tables(pci_gpu *h, const double *hint_lut, int nlx, int64_t nglut, const double *glut)
+{
+    int jmax2 = 1;
+    for (int o = 0; o < h->nsu; o++) jmax2 = std::max(jmax2, h->h_orb_j[o]);
+    h->kdim = jmax2 + 1;
+    h->ntype = type_offset(jmax2 + 2);
+    h->nlx = nlx;
+    std::vector<double> g((size_t)h->kdim * h->ntype * h->ntype, 0.0);
+    for (int k = 0; k < h->kdim; k++)
+        for (int j1 = 1; j1 <= jmax2; j1 += 2)
+            for (int m1 = -j1; m1 <= j1; m1 += 2)
+                for (int j2 = 1; j2 <= jmax2; j2 += 2)
+                    for (int m2 = -j2; m2 <= j2; m2 += 2) {
+                        int t1 = type_offset(j1) + (m1 + j1) / 2, t2 = type_offset(j2) + (m2 + j2) / 2;
+                        g[((size_t)k * h->ntype + t1) * h->ntype + t2] =
+                            host_gaunt(nlx, glut, nglut, k, j1 * 0.5, m1 * 0.5, j2 * 0.5, m2 * 0.5);
+                    }
+    int rc = upload(h, &h->d_gaunt, g);
+    if (rc) return rc;
+    std::vector<double> h1((size_t)h->nsu * h->nsu, 0.0);
+    for (int a = 0; a < h->nsu; a++)
+        for (int b = 0; b < h->nsu; b++) {
+            if (h->h_orb_k[a] != h->h_orb_k[b]) continue;
+            int na = std::min(a, b) + 1, nb = std::max(a, b) + 1;  // 1-based, na <= nb
+            int64_t ind = (int64_t)h->nx * (na - h->nso - 1) + (nb - h->nso);
+            if (ind >= 1 && ind <= (int64_t)h->nx * h->nx) h1[(size_t)a * h->nsu + b] = hint_lut[ind - 1];
+        }
+    return upload(h, &h->d_h1, h1);
+}
+
+// ---------------------------------------------------------------- ABI ---
+
+extern "C" {
+
+int pci_gpu_create(int32_t device, pci_gpu_t **out)
+{
+    if (!out) return PCI_E_INPUT;
+    *out = nullptr;
+    pci_gpu *h = new pci_gpu();
+    h->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        int rc = cuda_err(h, e, "cudaSetDevice");
+        *out = h;  // keep the handle so the caller can read the message
+        return rc;
+    }
+    e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { *out = h; return cuda_err(h, e, "cudaStreamCreate"); }
+    int rc = 0;
+    h->d_err = (unsigned int *)dev_alloc(h, 16, &rc);
+    if (rc) { *out = h; return rc; }
+    cudaMemset(h->d_err, 0, 16);
+    *out = h;
+    return PCI_OK;
+}
+
+int pci_gpu_set_basis(pci_gpu_t *h, int32_t Ne, int64_t Nd, int32_t Nst, int32_t Nsu, int32_t Nso, int32_t Nx,
+                      int32_t Mj, const int32_t *Iarr, const int32_t *Nh, const int32_t *Jz, const int32_t *Nn,
+                      const int32_t *Kk, const int32_t *Ll, const int32_t *Jj, int32_t Nc, const int32_t *Ndc,
+                      double Gj)
+{
+    if (!h) return PCI_E_INPUT;
+    cudaSetDevice(h->device);
+    if (Ne < 1 || Ne > PCI_NE_MAX) return set_err(h, PCI_E_INPUT, "Ne must be 1..8");
+    if (Nd < 1 || Nd >= (1LL << 31)) return set_err(h, PCI_E_INPUT, "Nd out of range");
+    if (Nst < 1 || Nst > 65000) return set_err(h, PCI_E_INPUT, "Nst out of range");
+    if (Nsu < 1 || Nc < 1 || Nx < 1 || Nso < 0) return set_err(h, PCI_E_INPUT, "bad Nsu/Nc/Nx/Nso");
+    if (!Iarr || !Nh || !Jz || !Kk || !Ll || !Jj || !Ndc) return set_err(h, PCI_E_INPUT, "null array");
+    (void)Nn;
+    int64_t sum = 0;
+    for (int c = 0; c < Nc; c++) {
+        if (Ndc[c] < 0) return set_err(h, PCI_E_INPUT, "negative Ndc");
+        sum += Ndc[c];
+    }
+    if (sum != Nd) return set_err(h, PCI_E_INPUT, "sum(Ndc) /= Nd");
+    for (int i = 0; i < Nst; i++) {
+        if (Nh[i] < 1 || Nh[i] > Nsu) return set_err(h, PCI_E_INPUT, "Nh outside 1..Nsu");
+        int j2 = Jj[Nh[i] - 1];
+        if (j2 < 1 || j2 > 63 || (j2 & 1) == 0 || Jz[i] < -j2 || Jz[i] > j2 || ((Jz[i] + j2) & 1))
+            return set_err(h, PCI_E_INPUT, "Jz inconsistent with Jj");
+    }
+    if (Nsu - Nso > Nx) return set_err(h, PCI_E_INPUT, "Nsu - Nso exceeds Nx");
+    free_basis(h);
+    csr_free(h->H); csr_free(h->J); csr_free(h->Hfull);
+    h->ne = Ne; h->nd = Nd; h->nst = Nst; h->nsu = Nsu; h->nso = Nso; h->nx = Nx; h->mj = Mj; h->nc = Nc; h->gj = Gj;
+    h->h_ndc.assign(Ndc, Ndc + Nc);
+    h->h_orb_j.assign(Jj, Jj + Nsu);
+    h->h_orb_l.assign(Ll, Ll + Nsu);
+    h->h_orb_k.assign(Kk, Kk + Nsu);
+    h->h_nh.assign(Nh, Nh + Nst);
+    h->h_jz.assign(Jz, Jz + Nst);
+    // determinants: 0-based uint16, validated sorted and configuration-consistent
+    std::vector<uint16_t> occ((size_t)Nd * Ne);
+    std::vector<int32_t> conf_of(Nd);
+    std::vector<int64_t> conf_start(Nc + 1);
+    std::vector<uint16_t> conf_orb((size_t)Nc * Ne, 0);
+    conf_start[0] = 0;
+    for (int c = 0; c < Nc; c++) conf_start[c + 1] = conf_start[c] + Ndc[c];
+    for (int c = 0; c < Nc; c++) {
+        for (int64_t n = conf_start[c]; n < conf_start[c + 1]; n++) {
+            conf_of[n] = c;
+            for (int e = 0; e < Ne; e++) {
+                int32_t m = Iarr[n * Ne + e];
+                if (m < 1 || m > Nst) return set_err(h, PCI_E_INPUT, "Iarr entry outside 1..Nst at det " + std::to_string(n + 1));
+                if (e > 0 && m <= Iarr[n * Ne + e - 1])
+                    return set_err(h, PCI_E_INPUT, "RSPQ: determinant not sorted ascending at det " + std::to_string(n + 1));
+                occ[n * Ne + e] = (uint16_t)(m - 1);
+                uint16_t o = (uint16_t)(Nh[m - 1] - 1);
+                if (n == conf_start[c]) conf_orb[(size_t)c * Ne + e] = o;
+                else if (conf_orb[(size_t)c * Ne + e] != o)
+                    return set_err(h, PCI_E_INPUT, "determinant " + std::to_string(n + 1) + " does not belong to its configuration block");
+            }
+        }
+    }
+    std::vector<int16_t> ms_orb(Nst);
+    std::vector<int8_t> ms_jz(Nst), orb_l(Nsu), orb_j(Nsu);
+    std::vector<uint8_t> ms_type(Nst);
+    for (int i = 0; i < Nst; i++) {
+        ms_orb[i] = (int16_t)(Nh[i] - 1);
+        ms_jz[i] = (int8_t)Jz[i];
+        int j2 = Jj[Nh[i] - 1];
+        ms_type[i] = (uint8_t)(type_offset(j2) + (Jz[i] + j2) / 2);
+    }
+    for (int o = 0; o < Nsu; o++) { orb_l[o] = (int8_t)Ll[o]; orb_j[o] = (int8_t)Jj[o]; }
+    int rc;
+    if ((rc = upload(h, &h->d_occ, occ))) return rc;
+    if ((rc = upload(h, &h->d_conf_of, conf_of))) return rc;
+    if ((rc = upload(h, &h->d_conf_start, conf_start))) return rc;
+    if ((rc = upload(h, &h->d_conf_orb, conf_orb))) return rc;
+    if ((rc = upload(h, &h->d_ms_orb, ms_orb))) return rc;
+    if ((rc = upload(h, &h->d_ms_jz, ms_jz))) return rc;
+    if ((rc = upload(h, &h->d_ms_type, ms_type))) return rc;
+    if ((rc = upload(h, &h->d_orb_l, orb_l))) return rc;
+    if ((rc = upload(h, &h->d_orb_j, orb_j))) return rc;
+    PCI_CUDA(h, cudaStreamSynchronize(h->st));
+    h->have_basis = true;
+    h->have_ints = false;  // tables depend on the basis; integrals must be set again
+    return PCI_OK;
+}
+
+int pci_gpu_set_integrals(pci_gpu_t *h, const double *HintLUT, int32_t Nlx, int64_t nGauntLUT, const double *GauntLUT,
+                          int64_t Ngint, int32_t kbrt, int32_t r2_is_f64, const void *Rint2, const int32_t *Iint2,
+                          const int32_t *Iint3)
+{
+    if (!h) return PCI_E_INPUT;
+    cudaSetDevice(h->device);
+    if (!h->have_basis) return set_err(h, PCI_E_STATE, "set_integrals before set_basis");
+    if (!HintLUT || !GauntLUT || !Rint2 || !Iint2 || !Iint3) return set_err(h, PCI_E_INPUT, "null array");
+    if (Nlx < 0 || nGauntLUT < 1) return set_err(h, PCI_E_INPUT, "bad Gaunt table");
+    int rc;
+    if ((rc = build_tables(h, HintLUT, Nlx, nGauntLUT, GauntLUT))) return rc;
+    if ((rc = hb_build_hash(h, Ngint, kbrt, r2_is_f64, Rint2, Iint2, Iint3))) return rc;
+    csr_free(h->H); csr_free(h->J); csr_free(h->Hfull);
+    h->have_ints = true;
+    return PCI_OK;
+}
+
+int pci_gpu_form_h(pci_gpu_t *h, int32_t value_prec, int64_t *NumH, int64_t *numzero, double *Hmin)
+{
+    if (!h) return PCI_E_INPUT;
+    cudaSetDevice(h->device);
+    return hb_form_h(h, value_prec, NumH, numzero, Hmin);
+}
+
+int pci_gpu_form_j(pci_gpu_t *h, int64_t *NumJ)
+{
+    if (!h) return PCI_E_INPUT;
+    cudaSetDevice(h->device);
+    return hb_form_j(h, NumJ);
+}
+
+int pci_gpu_csr_info(pci_gpu_t *h, int32_t which, int64_t *nrows, int64_t *nnz)
+{
+    if (!h) return PCI_E_INPUT;
+    const Csr &c = which == PCI_MAT_J2 ? h->J : h->H;
+    if (!c.rowptr) return set_err(h, PCI_E_STATE, "matrix not formed");
+    if (nrows) *nrows = c.nrows;
+    if (nnz) *nnz = c.nnz;
+    return PCI_OK;
+}
+
+int pci_gpu_get_csr(pci_gpu_t *h, int32_t which, int64_t *rowptr, int32_t *col, double *val)
+{
+    if (!h) return PCI_E_INPUT;
+    cudaSetDevice(h->device);
+    const Csr &c = which == PCI_MAT_J2 ? h->J : h->H;
+    if (!c.rowptr) return set_err(h, PCI_E_STATE, "matrix not formed");
+    if (rowptr) PCI_CUDA(h, cudaMemcpy(rowptr, c.rowptr, (c.nrows + 1) * 8, cudaMemcpyDeviceToHost));
+    if (col) {
+        PCI_CUDA(h, cudaMemcpy(col, c.col, c.nnz * 4, cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < c.nnz; i++) col[i] += 1;  // Fortran 1-based columns
+    }
+    if (val) {
+        if (c.val_f32) {
+            std::vector<float> tmp(c.nnz);
+            PCI_CUDA(h, cudaMemcpy(tmp.data(), c.val, c.nnz * 4, cudaMemcpyDeviceToHost));
+            for (int64_t i = 0; i < c.nnz; i++) val[i] = tmp[i];
+        } else {
+            PCI_CUDA(h, cudaMemcpy(val, c.val, c.nnz * 8, cudaMemcpyDeviceToHost));
+        }
+    }
+    return PCI_OK;
+}
+
+int pci_gpu_set_csr(pci_gpu_t *h, int32_t which, int64_t Nd, int64_t nnz, const int64_t *rowptr, const int32_t *col,
+                    const double *val, double Hmin)
+{
+    if (!h) return PCI_E_INPUT;
+    cudaSetDevice(h->device);
+    if (!rowptr || !col || !val || Nd < 1 || nnz < 0) return set_err(h, PCI_E_INPUT, "bad CSR");
+    if (h->have_basis && Nd != h->nd) return set_err(h, PCI_E_INPUT, "CSR rows differ from Nd");
+    if (rowptr[0] != 0 || rowptr[Nd] != nnz) return set_err(h, PCI_E_INPUT, "rowptr inconsistent with nnz");
+    Csr &c = which == PCI_MAT_J2 ? h->J : h->H;
+    csr_free(c);
+    if (which != PCI_MAT_J2) csr_free(h->Hfull);
+    int rc = 0;
+    c.nrows = Nd;
+    c.nnz = nnz;
+    c.val_f32 = 0;
+    c.rowptr = (int64_t *)dev_alloc(h, (Nd + 1) * 8, &rc);
+    if (rc) return rc;
+    c.col = (int32_t *)dev_alloc(h, std::max<int64_t>(nnz, 1) * 4, &rc);
+    if (rc) return rc;
+    c.val = dev_alloc(h, std::max<int64_t>(nnz, 1) * 8, &rc);
+    if (rc) return rc;
+    std::vector<int32_t> c0(nnz);
+    for (int64_t i = 0; i < nnz; i++) {
+        if (col[i] < 1 || col[i] > Nd) return set_err(h, PCI_E_INPUT, "column outside 1..Nd");
+        c0[i] = col[i] - 1;
+    }
+    PCI_CUDA(h, cudaMemcpy(c.rowptr, rowptr, (Nd + 1) * 8, cudaMemcpyHostToDevice));
+    PCI_CUDA(h, cudaMemcpy(c.col, c0.data(), nnz * 4, cudaMemcpyHostToDevice));
+    PCI_CUDA(h, cudaMemcpy(c.val, val, nnz * 8, cudaMemcpyHostToDevice));
+    if (which != PCI_MAT_J2) {
+        h->hmin = Hmin;
+        h->numh = nnz;
+        if (!h->have_basis) h->nd = Nd;
+    }
+    return PCI_OK;
+}
+
+int pci_gpu_davidson(pci_gpu_t *h, const pci_dvd_params *p, const double *X0, double *Tk, double *Tj,
+                     int32_t *Iconverge, double *X, int32_t *iters, double *resid)
+{
+    if (!h || !p) return PCI_E_INPUT;
+    cudaSetDevice(h->device);
+    return dv_run(h, p, X0, Tk, Tj, Iconverge, X, iters, resid);
+}
+
+int32_t pci_gpu_stats(pci_gpu_t *h, double *out, int32_t n)
+{
+    if (!h || !out) return 0;
+    double v[8] = {h->st_formh, h->st_formh_count, h->st_formh_fill, h->st_formj,
+                   h->st_dvd, h->st_spmm, h->st_spmm_calls, h->st_init};
+    int32_t m = std::min<int32_t>(n, 8);
+    for (int i = 0; i < m; i++) out[i] = v[i];
+    return m;
+}
+
+const char *pci_gpu_last_error(pci_gpu_t *h)
+{
+    return h ? h->err.c_str() : "null handle";
+}
+
+void pci_gpu_destroy(pci_gpu_t *h)
+{
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->st) cudaStreamSynchronize(h->st);
+    free_basis(h);
+    csr_free(h->H); csr_free(h->J); csr_free(h->Hfull);
+    dev_free(h->d_h1); dev_free(h->d_gaunt); dev_free(h->d_hkey); dev_free(h->d_hval);
+    dev_free(h->d_err); dev_free(h->d_tmp);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+}
+
+}  // extern "C"

@@ -1,0 +1,128 @@
+// Internal declarations shared by the translation units of libpci_gpu.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/pci_gpu.h"
+
+#define PCI_NE_MAX 8
+#define PCI_MAX_PROBE 4096
+
+// Device error bits (OR-ed into Handle::d_err by kernels)
+#define DERR_MISSING_INTEGRAL 1u
+#define DERR_M_NOT_CONSERVED  2u
+#define DERR_BAD_INDEX        4u
+
+struct Csr {
+    int64_t nrows = 0, nnz = 0;
+    int64_t *rowptr = nullptr;   // [nrows+1], 0-based prefix
+    int32_t *col = nullptr;      // 0-based column
+    void *val = nullptr;         // double or float
+    int val_f32 = 0;
+};
+
+// Everything the H-build kernels read; plain pointers so it can be passed by value.
+struct DevSys {
+    int ne, nst, nsu, nso, nx, mj, nc, nlx, kbrt, kdim, ntype;
+    int64_t nd;
+    double gj;
+    const uint16_t *occ;        // [nd*ne] 0-based m-state, ascending per determinant
+    const int32_t *conf_of;     // [nd]
+    const int64_t *conf_start;  // [nc+1]
+    const uint16_t *conf_orb;   // [nc*ne] 0-based orbitals of the configuration, ascending
+    const int64_t *adj_ptr;     // [nc+1]
+    const int32_t *adj;         // connected configurations c2 <= c1, ascending
+    const int16_t *ms_orb;      // [nst] orbital (0-based) of each m-state
+    const int8_t *ms_jz;        // [nst] 2m
+    const uint8_t *ms_type;     // [nst] (j,m) type index into the Gaunt table
+    const int8_t *orb_l;        // [nsu]
+    const int8_t *orb_j;        // [nsu] 2j
+    const double *h1;           // [nsu*nsu] one-electron integrals, 0 unless kappa equal
+    const double *gaunt;        // [kdim][ntype][ntype]
+    const unsigned long long *hkey;  // [hcap] 0 = empty
+    const double *hval;         // [hcap*(kbrt?2:1)]
+    unsigned long long hmask;
+    unsigned int *err;
+};
+
+struct pci_gpu {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    std::string err;
+    // basis
+    int ne = 0, nst = 0, nsu = 0, nso = 0, nx = 0, mj = 0, nc = 0;
+    int64_t nd = 0;
+    double gj = 0.0;
+    bool have_basis = false, have_ints = false;
+    std::vector<int32_t> h_ndc;       // host copy of Ndc
+    std::vector<int32_t> h_orb_j, h_orb_l, h_orb_k;
+    std::vector<int32_t> h_nh, h_jz;
+    uint16_t *d_occ = nullptr;
+    int32_t *d_conf_of = nullptr;
+    int64_t *d_conf_start = nullptr;
+    uint16_t *d_conf_orb = nullptr;
+    int64_t *d_adj_ptr = nullptr;
+    int32_t *d_adj = nullptr;
+    int64_t n_adj = 0;
+    int16_t *d_ms_orb = nullptr;
+    int8_t *d_ms_jz = nullptr;
+    uint8_t *d_ms_type = nullptr;
+    int8_t *d_orb_l = nullptr, *d_orb_j = nullptr;
+    // integrals
+    double *d_h1 = nullptr;
+    double *d_gaunt = nullptr;
+    int kdim = 0, ntype = 0, nlx = 0, kbrt = 0;
+    unsigned long long *d_hkey = nullptr;
+    double *d_hval = nullptr;
+    unsigned long long hcap = 0;
+    // matrices
+    Csr H, J, Hfull;
+    double hmin = 0.0;
+    int64_t numh = 0, numzero = 0, numj = 0;
+    unsigned int *d_err = nullptr;
+    // scratch
+    void *d_tmp = nullptr;
+    size_t tmp_bytes = 0;
+    // stats (ms)
+    double st_formh = 0, st_formh_count = 0, st_formh_fill = 0, st_formj = 0;
+    double st_dvd = 0, st_spmm = 0, st_spmm_calls = 0, st_init = 0;
+};
+
+// error helpers
+int set_err(pci_gpu *h, int code, const std::string &msg);
+int cuda_err(pci_gpu *h, cudaError_t e, const char *what);
+#define PCI_CUDA(h, call)                                         \
+    do {                                                          \
+        cudaError_t _e = (call);                                  \
+        if (_e != cudaSuccess) return cuda_err((h), _e, #call);   \
+    } while (0)
+
+void *dev_alloc(pci_gpu *h, size_t bytes, int *rc);
+void dev_free(void *p);
+int ensure_tmp(pci_gpu *h, size_t bytes);
+DevSys make_devsys(const pci_gpu *h);
+
+// hbuild.cu
+int hb_build_hash(pci_gpu *h, int64_t ngint, int kbrt, int r2_is_f64, const void *rint2,
+                  const int32_t *iint2, const int32_t *iint3);
+int hb_build_adjacency(pci_gpu *h);
+int hb_form_h(pci_gpu *h, int value_prec, int64_t *numh, int64_t *numzero, double *hmin);
+int hb_form_j(pci_gpu *h, int64_t *numj);
+double host_gaunt(int nlx, const double *lut, int64_t nlut, int k, double xj1, double xm1,
+                  double xj2, double xm2);
+
+// spmm.cu
+int sp_build_full(pci_gpu *h);
+// Y = (H - hmin I) X on row-major blocks: X[n*ldx + v], Y[n*ldy + v], v < nv
+int sp_spmm(pci_gpu *h, const double *X, int ldx, double *Y, int ldy, int nv, cudaStream_t st);
+int sp_spmm_f32(pci_gpu *h, const float *X, int ldx, float *Y, int ldy, int nv, cudaStream_t st);
+// y = J x restricted to rows/cols < nlim, returned as <x|J|x>
+int sp_jav(pci_gpu *h, const double *X, int ldx, int nv, int64_t nlim, double *out_host);
+void csr_free(Csr &c);
+
+// davidson.cu
+int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk, double *Tj,
+           int32_t *Iconverge, double *X, int32_t *iters, double *resid);

@@ -1,0 +1,249 @@
+// Sparse products of the Davidson loop: Y = (H - Hmin I) X over a block of
+// vectors (Mxmpy, src/davidson.f90:572-647) and <x|J^2|x> (J_av,
+// src/formj2.f90:355-387).
+//
+// The reference stores the lower triangle and scatters the transpose part
+// (y_k += H_nk x_n) one vector at a time, with an Allreduce per vector.  Here
+// the SpMM works on all Nlv vectors at once from a full symmetric CSR built
+// once on the device from the lower triangle, so each output row is one
+// warp-private gather with no atomics: a group of NV lanes owns one stored
+// element, lane v multiplies x_k[v] (one coalesced read of the NV-wide row of
+// X), and the groups are reduced with shuffles at the end of the row.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+
+#include "pci_internal.h"
+
+#define FULL_MASK 0xffffffffu
+
+void csr_free(Csr &c)
+{
+    dev_free(c.rowptr);
+    dev_free(c.col);
+    dev_free(c.val);
+    c.rowptr = nullptr;
+    c.col = nullptr;
+    c.val = nullptr;
+    c.nrows = c.nnz = 0;
+}
+
+// --------------------------------------------------------- full CSR ---
+
+__global__ void k_count_upper(const int64_t *rowptr, const int32_t *col, int64_t nd, unsigned int *cntU)
+{
+    int lane = threadIdx.x & 31;
+    int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t n = warp; n < nd; n += nwarps) {
+        for (int64_t l = rowptr[n] + lane; l < rowptr[n + 1]; l += 32) {
+            int k = col[l];
+            if (k != n) atomicAdd(&cntU[k], 1u);
+        }
+    }
+}
+
+__global__ void k_full_counts(const int64_t *rowptr, const unsigned int *cntU, int64_t nd, int64_t *fullcnt)
+{
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nd; n += (int64_t)gridDim.x * blockDim.x)
+        fullcnt[n] = (rowptr[n + 1] - rowptr[n]) + cntU[n];
+}
+
+template <typename VT>
+__global__ void k_full_fill(const int64_t *rowptr, const int32_t *col, const VT *val, int64_t nd,
+                            const int64_t *frow, unsigned int *cursor, int32_t *fcol, VT *fval)
+{
+    int lane = threadIdx.x & 31;
+    int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t n = warp; n < nd; n += nwarps) {
+        int64_t r0 = rowptr[n], r1 = rowptr[n + 1];
+        int64_t f0 = frow[n];
+        for (int64_t l = r0 + lane; l < r1; l += 32) {
+            int k = col[l];
+            VT v = val[l];
+            fcol[f0 + (l - r0)] = k;   // lower part keeps its order
+            fval[f0 + (l - r0)] = v;
+            if (k != n) {
+                int64_t lowk = rowptr[k + 1] - rowptr[k];
+                int64_t p = frow[k] + lowk + atomicAdd(&cursor[k], 1u);
+                fcol[p] = (int32_t)n;
+                fval[p] = v;
+            }
+        }
+    }
+}
+
+int sp_build_full(pci_gpu *h)
+{
+    if (h->Hfull.rowptr) return PCI_OK;
+    Csr &L = h->H;
+    if (!L.rowptr) return set_err(h, PCI_E_STATE, "no Hamiltonian resident");
+    int rc = 0;
+    const int64_t nd = L.nrows;
+    unsigned int *cntU = (unsigned int *)dev_alloc(h, nd * 4 + 16, &rc);
+    if (rc) return rc;
+    int64_t *fullcnt = (int64_t *)dev_alloc(h, (nd + 1) * 8, &rc);
+    if (rc) return rc;
+    PCI_CUDA(h, cudaMemsetAsync(cntU, 0, nd * 4, h->st));
+    k_count_upper<<<148 * 16, 256, 0, h->st>>>(L.rowptr, L.col, nd, cntU);
+    k_full_counts<<<148 * 4, 256, 0, h->st>>>(L.rowptr, cntU, nd, fullcnt);
+    Csr &F = h->Hfull;
+    F.nrows = nd;
+    F.val_f32 = L.val_f32;
+    F.rowptr = (int64_t *)dev_alloc(h, (nd + 1) * 8, &rc);
+    if (rc) return rc;
+    PCI_CUDA(h, cudaMemsetAsync(F.rowptr, 0, 8, h->st));
+    size_t tb = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, tb, fullcnt, F.rowptr + 1, nd, h->st);
+    if ((rc = ensure_tmp(h, tb))) return rc;
+    cub::DeviceScan::InclusiveSum(h->d_tmp, tb, fullcnt, F.rowptr + 1, nd, h->st);
+    PCI_CUDA(h, cudaMemcpyAsync(&F.nnz, F.rowptr + nd, 8, cudaMemcpyDeviceToHost, h->st));
+    PCI_CUDA(h, cudaStreamSynchronize(h->st));
+    size_t vs = F.val_f32 ? 4 : 8;
+    F.col = (int32_t *)dev_alloc(h, F.nnz * 4, &rc);
+    if (rc) return rc;
+    F.val = dev_alloc(h, F.nnz * vs, &rc);
+    if (rc) return rc;
+    PCI_CUDA(h, cudaMemsetAsync(cntU, 0, nd * 4, h->st));
+    if (F.val_f32) {
+        k_full_fill<float><<<148 * 16, 256, 0, h->st>>>(L.rowptr, L.col, (const float *)L.val, nd, F.rowptr, cntU,
+                                                        F.col, (float *)F.val);
+    } else {
+        k_full_fill<double><<<148 * 16, 256, 0, h->st>>>(L.rowptr, L.col, (const double *)L.val, nd, F.rowptr, cntU,
+                                                         F.col, (double *)F.val);
+    }
+    PCI_CUDA(h, cudaGetLastError());
+    PCI_CUDA(h, cudaStreamSynchronize(h->st));
+    dev_free(cntU);
+    dev_free(fullcnt);
+    return PCI_OK;
+}
+
+// ------------------------------------------------------------- SpMM ---
+
+// One warp per row; NV lanes per stored element, 32/NV elements per step.
+template <int NV, typename VT, typename XT>
+__global__ void __launch_bounds__(256) k_spmm(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ col,
+                                               const VT *__restrict__ val, int64_t nd, double hmin,
+                                               const XT *__restrict__ X, int ldx, XT *__restrict__ Y, int ldy)
+{
+    constexpr int G = 32 / NV;
+    const int lane = threadIdx.x & 31;
+    const int g = lane / NV, v = lane - g * NV;
+    const bool active = g < G;
+    int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t n = warp; n < nd; n += nwarps) {
+        const int64_t r0 = rowptr[n], r1 = rowptr[n + 1];
+        XT acc = 0;
+        if (active) {
+            int64_t l = r0 + g;
+            for (; l + 3 * G < r1; l += 4 * G) {
+                int k0 = __ldg(&col[l]), k1 = __ldg(&col[l + G]), k2 = __ldg(&col[l + 2 * G]), k3 = __ldg(&col[l + 3 * G]);
+                XT t0 = (XT)__ldg(&val[l]), t1 = (XT)__ldg(&val[l + G]), t2 = (XT)__ldg(&val[l + 2 * G]),
+                   t3 = (XT)__ldg(&val[l + 3 * G]);
+                if (k0 == n) t0 -= (XT)hmin;
+                if (k1 == n) t1 -= (XT)hmin;
+                if (k2 == n) t2 -= (XT)hmin;
+                if (k3 == n) t3 -= (XT)hmin;
+                XT x0 = __ldg(&X[(int64_t)k0 * ldx + v]), x1 = __ldg(&X[(int64_t)k1 * ldx + v]);
+                XT x2 = __ldg(&X[(int64_t)k2 * ldx + v]), x3 = __ldg(&X[(int64_t)k3 * ldx + v]);
+                acc += t0 * x0;
+                acc += t1 * x1;
+                acc += t2 * x2;
+                acc += t3 * x3;
+            }
+            for (; l < r1; l += G) {
+                int k = __ldg(&col[l]);
+                XT t = (XT)__ldg(&val[l]);
+                if (k == n) t -= (XT)hmin;
+                acc += t * __ldg(&X[(int64_t)k * ldx + v]);
+            }
+        }
+#pragma unroll
+        for (int gg = 1; gg < G; gg++) {
+            XT o = __shfl_sync(FULL_MASK, acc, (lane + gg * NV) & 31);
+            if (g == 0) acc += o;
+        }
+        if (g == 0) Y[n * (int64_t)ldy + v] = acc;
+    }
+}
+
+template <typename VT, typename XT>
+static int spmm_dispatch(pci_gpu *h, const XT *X, int ldx, XT *Y, int ldy, int nv, cudaStream_t st)
+{
+    Csr &F = h->Hfull;
+    const VT *val = (const VT *)F.val;
+    int blocks = 148 * 16;
+    double hm = h->hmin;
+#define CASE(N) \
+    case N: k_spmm<N, VT, XT><<<blocks, 256, 0, st>>>(F.rowptr, F.col, val, F.nrows, hm, X, ldx, Y, ldy); break;
+    switch (nv) {
+        CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8)
+        CASE(9) CASE(10) CASE(11) CASE(12) CASE(13) CASE(14) CASE(15) CASE(16)
+    default: return set_err(h, PCI_E_INPUT, "SpMM supports 1..16 vectors");
+    }
+#undef CASE
+    PCI_CUDA(h, cudaGetLastError());
+    return PCI_OK;
+}
+
+int sp_spmm(pci_gpu *h, const double *X, int ldx, double *Y, int ldy, int nv, cudaStream_t st)
+{
+    int rc = sp_build_full(h);
+    if (rc) return rc;
+    if (h->Hfull.val_f32) return spmm_dispatch<float, double>(h, X, ldx, Y, ldy, nv, st);
+    return spmm_dispatch<double, double>(h, X, ldx, Y, ldy, nv, st);
+}
+
+int sp_spmm_f32(pci_gpu *h, const float *X, int ldx, float *Y, int ldy, int nv, cudaStream_t st)
+{
+    int rc = sp_build_full(h);
+    if (rc) return rc;
+    if (h->Hfull.val_f32) return spmm_dispatch<float, float>(h, X, ldx, Y, ldy, nv, st);
+    return spmm_dispatch<double, float>(h, X, ldx, Y, ldy, nv, st);
+}
+
+// ------------------------------------------------------------- J_av ---
+
+// sums[v] += sum over stored (n, k), n,k < nlim, of t x_k x_n (doubled off the diagonal)
+__global__ void k_jav(const int64_t *rowptr, const int32_t *col, const double *val, int64_t nlim,
+                      const double *X, int ldx, int nv, double *sums)
+{
+    int lane = threadIdx.x & 31;
+    int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int v = 0; v < nv; v++) {
+        double acc = 0.0;
+        for (int64_t n = warp; n < nlim; n += nwarps) {
+            double xn = X[n * ldx + v];
+            for (int64_t l = rowptr[n] + lane; l < rowptr[n + 1]; l += 32) {
+                int k = col[l];
+                if (k < nlim) {
+                    double r = val[l] * X[(int64_t)k * ldx + v] * xn;
+                    if (k != n) r = r + r;
+                    acc += r;
+                }
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(FULL_MASK, acc, o);
+        if (lane == 0) atomicAdd(&sums[v], acc);
+    }
+}
+
+int sp_jav(pci_gpu *h, const double *X, int ldx, int nv, int64_t nlim, double *out_host)
+{
+    if (!h->J.rowptr) return set_err(h, PCI_E_STATE, "J^2 not formed");
+    int rc = 0;
+    if ((rc = ensure_tmp(h, 8 * 64))) return rc;
+    double *sums = (double *)h->d_tmp;
+    PCI_CUDA(h, cudaMemsetAsync(sums, 0, 8 * nv, h->st));
+    k_jav<<<148 * 4, 256, 0, h->st>>>(h->J.rowptr, h->J.col, (const double *)h->J.val, nlim, X, ldx, nv, sums);
+    PCI_CUDA(h, cudaGetLastError());
+    std::vector<double> s(nv);
+    PCI_CUDA(h, cudaMemcpyAsync(s.data(), sums, 8 * nv, cudaMemcpyDeviceToHost, h->st));
+    PCI_CUDA(h, cudaStreamSynchronize(h->st));
+    for (int v = 0; v < nv; v++) out_host[v] = 0.5 * (sqrt(1.0 + s[v]) - 1.0);
+    return PCI_OK;
+}

@@ -1,0 +1,52 @@
+"""The C-ABI library loads without a GPU and exports every entry point
+declared in include/pci_gpu.h; the Python binding mirrors the header."""
+import ctypes as C
+import os
+import re
+
+from conftest import ROOT
+
+
+def declared_symbols():
+    hdr = open(os.path.join(ROOT, "include", "pci_gpu.h")).read()
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    return sorted(set(re.findall(r"\b(pci_gpu_\w+)\s*\(", hdr)))
+
+
+def test_library_exports_header_symbols():
+    from pci_b200 import build
+    lib = build.build()
+    L = C.CDLL(lib)
+    syms = declared_symbols()
+    assert len(syms) >= 10
+    for name in syms:
+        assert hasattr(L, name), name
+
+
+def test_binding_covers_header():
+    from pci_b200 import capi
+    assert sorted(capi.EXPORTS) == declared_symbols()
+
+
+def test_dvd_params_layout():
+    """pci_dvd_params: 8 int32 then 3 doubles, no padding (ISO_C_BINDING friendly)."""
+    from pci_b200.capi import DvdParams
+    assert C.sizeof(DvdParams) == 8 * 4 + 3 * 8
+    hdr = open(os.path.join(ROOT, "include", "pci_gpu.h")).read()
+    body = hdr[hdr.index("typedef struct {"):hdr.index("} pci_dvd_params;")]
+    fields = re.findall(r"(int32_t|double)\s+(\w+);", body)
+    assert [f for _, f in fields] == [f for f, _ in DvdParams._fields_]
+
+
+def test_no_device_is_reported_not_crashing():
+    """Without a GPU (this container) creating a handle fails with PCI_E_CUDA and a message."""
+    import torch
+    if torch.cuda.is_available():
+        return
+    from pci_b200 import capi
+    L = capi.load()
+    h = C.c_void_p()
+    rc = L.pci_gpu_create(0, C.byref(h))
+    assert rc == 6
+    assert b"CUDA" in L.pci_gpu_last_error(h)
+    L.pci_gpu_destroy(h)

@@ -1,0 +1,163 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle.
+
+Bar: the non-zero pattern (row pointers and 1-based columns), numzero and Hmin
+are identical; FP64 values are bit-identical (both sides evaluate Hmltn/Gint
+in the reference's operation order without fused multiply-adds); FP32 storage
+equals the FP64 oracle value rounded to float32.  Davidson eigenvalues agree
+with the oracle's restatement of Diag4 to 1e-8 Ha (|delta E| <= 1e-8).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import get_system, oracle_h
+from pci_b200 import system as S
+
+pytestmark = pytest.mark.gpu
+
+SYSTEMS = ["tiny", "small3", "small4", "cfg1"]
+
+
+@pytest.fixture(scope="module")
+def engine():
+    from pci_b200.capi import Engine
+    e = Engine(0)
+    yield e
+    e.close()
+
+
+def _load(engine, s):
+    engine.load_system(s)
+
+
+@pytest.mark.parametrize("name", SYSTEMS)
+def test_form_h_bit_exact(engine, name):
+    s = get_system(name)
+    (rp, col, val, nz, hmin, pairs), _ = oracle_h(name)
+    _load(engine, s)
+    numh, numzero, ghmin = engine.form_h(64)
+    grp, gcol, gval = engine.get_csr(0)
+    assert numh == rp[-1]
+    assert numzero == nz
+    assert ghmin == hmin
+    assert np.array_equal(grp, rp)
+    assert np.array_equal(gcol, col)
+    assert np.array_equal(gval.view(np.int64), val.view(np.int64))   # bit-identical
+
+
+@pytest.mark.parametrize("name", ["small3", "small4"])
+def test_form_h_fp32_storage(engine, name):
+    s = get_system(name)
+    (rp, col, val, nz, hmin, pairs), _ = oracle_h(name)
+    _load(engine, s)
+    numh, numzero, ghmin = engine.form_h(32)
+    grp, gcol, gval = engine.get_csr(0)
+    assert np.array_equal(grp, rp) and np.array_equal(gcol, col)
+    assert np.array_equal(gval, val.astype(np.float32).astype(np.float64))
+    assert ghmin == float(np.float32(hmin))
+
+
+@pytest.mark.parametrize("name", SYSTEMS)
+def test_form_j_bit_exact(engine, name):
+    s = get_system(name)
+    _, (jr, jc, jv) = oracle_h(name)
+    _load(engine, s)
+    numj = engine.form_j()
+    grp, gcol, gval = engine.get_csr(1)
+    assert numj == jr[-1]
+    assert np.array_equal(grp, jr) and np.array_equal(gcol, jc)
+    assert np.array_equal(gval, jv)
+
+
+def test_breit_and_gj_paths(engine):
+    """kbrt = 1 (two radial values per key, Breit phase is_br) and Gj /= 0
+    (the J^2 penalty inside Hmltn) on a small system."""
+    kw = S.CONFIGS["small3"]()
+    kw.update(kbrt=1, gj=0.05)
+    s = S.make_system(**kw)
+    rp, col, val, nz, hmin, pairs = O.Oracle(s).form_h()
+    _load(engine, s)
+    numh, numzero, ghmin = engine.form_h(64)
+    grp, gcol, gval = engine.get_csr(0)
+    assert np.array_equal(grp, rp) and np.array_equal(gcol, col)
+    assert np.array_equal(gval.view(np.int64), val.view(np.int64))
+    assert numzero == nz and ghmin == hmin
+
+
+def test_fp32_integrals(engine):
+    """Rint2 as float32 (the reference's default type2_real)."""
+    kw = S.CONFIGS["small4"]()
+    kw.update(r2_dtype=np.float32)
+    s = S.make_system(**kw)
+    rp, col, val, nz, hmin, pairs = O.Oracle(s).form_h()
+    _load(engine, s)
+    engine.form_h(64)
+    grp, gcol, gval = engine.get_csr(0)
+    assert np.array_equal(grp, rp) and np.array_equal(gcol, col)
+    assert np.array_equal(gval.view(np.int64), val.view(np.int64))
+
+
+@pytest.mark.parametrize("name", ["tiny", "cfg1"])
+def test_davidson_converged_levels(engine, name):
+    s = get_system(name)
+    (rp, col, val, nz, hmin, pairs), (jr, jc, jv) = oracle_h(name)
+    p = dict(s.params)
+    ref = O.diag4(s.nd, (rp, col, val), hmin, (jr, jc, jv), p, s.ndc)
+    _load(engine, s)
+    engine.form_h(64)
+    engine.form_j()
+    res = engine.davidson(s.nd, Nlv=p["Nlv"], N_it=p["N_it"], Crt4=p["Crt4"], MaxNd0=p["MaxNd0"],
+                          admix_crit=p["admix_crit"])
+    assert res["iterations"] == ref["iterations"]
+    assert np.max(np.abs(res["Tk"] - ref["Tk"])) <= 1e-8
+    assert np.allclose(res["Tj"], ref["Tj"], atol=1e-6)
+    # eigenvectors agree up to sign
+    ov = np.abs(np.sum(res["X"] * ref["X"], axis=0))
+    assert np.all(ov > 1 - 1e-6)
+
+
+def test_davidson_trajectory_small3(engine):
+    """A slowly converging case: after the same number of iterations of the same
+    algorithm both sides hold the same Ritz values."""
+    name = "small3"
+    s = get_system(name)
+    (rp, col, val, nz, hmin, pairs), (jr, jc, jv) = oracle_h(name)
+    p = dict(s.params)
+    p.update(N_it=25, admix_crit=0.0)
+    ref = O.diag4(s.nd, (rp, col, val), hmin, (jr, jc, jv), p, s.ndc)
+    _load(engine, s)
+    engine.form_h(64)
+    engine.form_j()
+    res = engine.davidson(s.nd, Nlv=p["Nlv"], N_it=25, Crt4=p["Crt4"], MaxNd0=p["MaxNd0"], admix_crit=0.0)
+    assert res["iterations"] == ref["iterations"] == 25
+    assert np.max(np.abs(res["Tk"] - ref["Tk"])) <= 1e-8
+    assert np.allclose(res["resid"], ref["cnorm"], rtol=1e-5, atol=1e-9)
+
+
+def test_missing_integral_is_reported(engine):
+    from pci_b200.capi import PciError
+    kw = S.CONFIGS["tiny"]()
+    s = S.make_system(**kw)
+    # drop R^0(3s 3s; 3s 3s), which every 3s^2 diagonal element needs
+    keep = ~((s.iint2 == 1) & (s.iint3 == 1))
+    assert keep.sum() == s.ngint - 1
+    s.rint2 = s.rint2[keep]
+    s.iint2 = s.iint2[keep]
+    s.iint3 = s.iint3[keep]
+    _load(engine, s)
+    with pytest.raises(PciError) as ei:
+        engine.form_h(64)
+    assert ei.value.code == 3
+
+
+def test_bad_determinant_order_is_reported(engine):
+    from pci_b200.capi import PciError
+    s = get_system("tiny")
+    bad = S.make_system(**S.CONFIGS["tiny"]())
+    bad.iarr = bad.iarr.copy()
+    bad.iarr[5] = bad.iarr[5][::-1]
+    with pytest.raises(PciError) as ei:
+        engine.set_basis(bad)
+    assert ei.value.code == 1
+    _load(engine, s)   # the handle stays usable
+    engine.form_h(64)
