@@ -1,0 +1,284 @@
+#!/usr/bin/env python
+"""Benchmark of pconf's Hamiltonian build on one B200 (or N independent replicas).
+
+Workload: the config-2 system (3 valence electrons, 120 relativistic orbitals
+n <= 20, l <= 4, odd parity, M_J = 1/2, singles + doubles from 20 reference
+configurations, seeded synthetic integrals, FP64 values).  One step = one
+FormH: configuration adjacency, count pass, scan and fill pass, from the
+device-resident determinant list and integral tables to the device-resident
+lower-triangle CSR (NumH non-zeros).  Metric: H-build nnz/s.
+
+  value  -- NumH / device time of FormH (CUDA events on the library stream),
+            inputs resident in HBM; L2 flushed (512 MiB write) before each step.
+  e2e    -- the same metric through the C ABI from pinned host arrays:
+            set_basis + set_integrals (host->device) + form_h + NumH/Hmin back.
+  --impl reference -- the oracle (C restatement of the reference's FormH) on
+            the host cores, rows sampled per step.
+
+Multi-GPU: replicas only (the build of one system does not shard across GPUs
+in this engine); every rank builds the same system, value = total NumH / max
+time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MEASURED_PEAK_FALLBACK = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="cfg2")
+    ap.add_argument("--cpu-rows", type=int, default=2000, help="rows per CPU sample step")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d.get("hbm_gbs", MEASURED_PEAK_FALLBACK)), "measured"
+    return MEASURED_PEAK_FALLBACK, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def algorithmic_bytes_fill(sysm, numh, value_bytes=8):
+    """Bytes the fill pass must move: CSR out (col + value), row pointers in,
+    determinant occupation lists in, the radial-integral table read once."""
+    return (numh * (value_bytes + 4) + (sysm.nd + 1) * 8 + sysm.nd * sysm.ne * 2
+            + sysm.ngint * 8 + sysm.hint_lut.nbytes)
+
+
+def cpu_sample(sysm, nrows, seed, threads=0):
+    """Oracle FormH over `nrows` random rows (count pass: every element evaluated,
+    zeros dropped); returns (seconds, nnz)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    o = O.Oracle(sysm)
+    rng = np.random.default_rng(seed)
+    rows = np.sort(rng.choice(np.arange(1, sysm.nd + 1), size=min(nrows, sysm.nd), replace=False))
+    t, nnz, _ = o.form_h_timed_sample([(int(r), int(r)) for r in rows], threads=threads)
+    return t, nnz, rows.size
+
+
+def dist_setup(backend):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws == 1:
+        return 0, 1, 0, None
+    import torch.distributed as dist
+    from datetime import timedelta
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group(backend, timeout=timedelta(seconds=600))
+    return dist.get_rank(), dist.get_world_size(), int(os.environ.get("LOCAL_RANK", "0")), dist
+
+
+def max_over_ranks(x, dist, device=None):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_reference(args):
+    rank, world, local, dist = dist_setup("gloo")
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+    from pci_b200 import system as S
+    sysm = S.make_system(**S.CONFIGS[args.config]())
+    threads = os.cpu_count() or 1
+    for w in range(args.warmup):
+        cpu_sample(sysm, max(args.cpu_rows // 4, 8), 1000 + w, threads)
+    tot_t = tot_n = tot_rows = 0
+    for k in range(args.steps):
+        t, n, r = cpu_sample(sysm, args.cpu_rows, 2000 + k, threads)
+        tot_t += t
+        tot_n += n
+        tot_rows += r
+    value = tot_n / tot_t
+    line = {
+        "metric": f"H-build nnz/s ({args.config})", "value": value, "unit": "nnz/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot_t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": f"{args.config}: FormH of Nd={sysm.nd} determinants", "Nd": sysm.nd,
+                   "rows_per_step": args.cpu_rows},
+        "cpu_baseline": {"value": value, "unit": "nnz/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.cpu_rows} random rows of FormH per step (oracle restatement "
+                                   f"of src/pconf.F90:1227-1290, OpenMP over rows)"},
+        "e2e": {"value": value, "unit": "nnz/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def pinned(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+
+
+def run_ours(args):
+    import torch
+    rank, world, local, dist = dist_setup("nccl")
+    torch.cuda.set_device(local)
+    from pci_b200 import system as S
+    from pci_b200.capi import Engine
+    sysm = S.make_system(**S.CONFIGS[args.config]())
+    # host inputs in pinned memory (the e2e leg copies from these every step)
+    for name in ("iarr", "nh", "jz", "ndc", "hint_lut", "gaunt_lut", "rint2", "iint2", "iint3"):
+        setattr(sysm, name, pinned(getattr(sysm, name)))
+    h2d = sum(getattr(sysm, n).nbytes for n in ("iarr", "nh", "jz", "ndc", "hint_lut", "gaunt_lut",
+                                                  "rint2", "iint2", "iint3"))
+    h2d += 4 * 4 * sysm.nsu
+    eng = Engine(local)
+    eng.load_system(sysm)
+    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
+    for _ in range(args.warmup):
+        eng.form_h(64)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    t_dev, t_fill, t_count, t_adj = [], [], [], []
+    launches = 0
+    numh = 0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        numh, numzero, hmin = eng.form_h(64)
+        st = eng.stats()
+        t_dev.append(st["formh_ms"])
+        t_fill.append(st["formh_fill_ms"])
+        t_count.append(st["formh_count_ms"])
+        t_adj.append(st["adjacency_ms"])
+        launches += int(st["formh_launches"]) + 1
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if dist is not None:
+        dist.barrier()
+    ms = float(np.mean(t_dev))
+    ms_max = max_over_ranks(ms, dist, device=f"cuda:{local}")
+    value = world * numh / (ms_max * 1e-3)
+    # e2e through the C ABI from pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        te = []
+        for _ in range(max(1, min(args.steps, 2))):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            eng.load_system(sysm)
+            n2, z2, hm2 = eng.form_h(64)
+            te.append(time.perf_counter() - t0)
+        e_s = max_over_ranks(float(np.mean(te)), dist, device=f"cuda:{local}")
+        e2e = {"value": world * numh / e_s, "unit": "nnz/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": 24, "seconds_per_step": e_s}
+    peak, peak_kind = peaks()
+    fill_bytes = algorithmic_bytes_fill(sysm, numh)
+    achieved = fill_bytes / (float(np.mean(t_fill)) * 1e-3) / 1e9
+    line = {
+        "metric": f"H-build nnz/s ({args.config})", "value": value, "unit": "nnz/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": f"{args.config}: FormH of Nd={sysm.nd} determinants, Ne={sysm.ne}, "
+                               f"Nc={sysm.nc}, Ngint={sysm.ngint}",
+                   "Nd": sysm.nd, "NumH": int(numh), "numzero": int(numzero), "Hmin": hmin,
+                   "l2": "flushed (512 MiB write) before every step; CSR output 12 B x NumH >> L2",
+                   "parallelism": f"replicas x{world}"},
+        "breakdown_ms": {"adjacency": float(np.mean(t_adj)), "count": float(np.mean(t_count)),
+                         "fill": float(np.mean(t_fill))},
+        "roofline": {"bound": "hbm", "kernel": "k_rows fill pass", "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "algorithmic_bytes": int(fill_bytes)},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "e2e": e2e,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        t, n, r = cpu_sample(sysm, args.cpu_rows, 7, os.cpu_count() or 1)
+        line["cpu_baseline"] = {"value": n / t, "unit": "nnz/s", "cores": os.cpu_count() or 1, "kind": "port",
+                                "sample": f"{r} random rows of FormH ({n} non-zeros, {t:.1f} s), oracle "
+                                          f"restatement of src/pconf.F90:1227-1290 with OpenMP"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

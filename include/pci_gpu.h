@@ -119,11 +119,13 @@ int pci_gpu_davidson(pci_gpu_t *h, const pci_dvd_params *p, const double *X0,
                      double *Tk, double *Tj, int32_t *Iconverge, double *X,
                      int32_t *iters, double *resid);
 
-/* Per-stage device times (milliseconds) of the last calls: [0] FormH total,
- * [1] FormH count pass, [2] FormH fill pass, [3] FormJ, [4] Davidson total,
- * [5] SpMM total in the last Davidson, [6] number of SpMM launches,
- * [7] Init4 + DiagInitApprox.  n is the capacity of `out`; returns the
- * number written. */
+/* Per-stage device times (milliseconds) and counters of the last calls:
+ * [0] FormH total (adjacency + count + fill), [1] FormH count pass,
+ * [2] FormH fill pass, [3] FormJ, [4] Davidson total, [5] SpMM total in the
+ * last Davidson, [6] number of SpMM launches, [7] Init4 + DiagInitApprox,
+ * [8] configuration adjacency build, [9] determinant pairs with difference
+ * <= 2, [10] determinant pairs compared, [11] kernel launches of the last
+ * FormH.  n is the capacity of `out`; returns the number written. */
 int32_t pci_gpu_stats(pci_gpu_t *h, double *out, int32_t n);
 
 const char *pci_gpu_last_error(pci_gpu_t *h);

@@ -174,8 +174,8 @@ class Engine:
         return dict(Tk=Tk, Tj=Tj, Iconverge=ic, X=None if X is None else X.T, iterations=iters.value, resid=res)
 
     def stats(self):
-        out = np.zeros(8)
-        n = self.L.pci_gpu_stats(self.h, _p(out), 8)
+        out = np.zeros(12)
+        n = self.L.pci_gpu_stats(self.h, _p(out), 12)
         keys = ["formh_ms", "formh_count_ms", "formh_fill_ms", "formj_ms", "davidson_ms", "spmm_ms",
-                "spmm_calls", "init_ms"]
+                "spmm_calls", "init_ms", "adjacency_ms", "pairs", "scanned", "formh_launches"]
         return dict(zip(keys[:n], out[:n].tolist()))

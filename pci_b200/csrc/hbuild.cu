@@ -645,9 +645,23 @@ int hb_form_h(pci_gpu *h, int value_prec, int64_t *numh, int64_t *numzero, doubl
     if (!h->have_basis || !h->have_ints) return set_err(h, PCI_E_STATE, "form_h before set_basis/set_integrals");
     if (value_prec != 64 && value_prec != 32) return set_err(h, PCI_E_INPUT, "value_prec must be 64 or 32");
     int rc;
-    if (!h->d_adj && (rc = hb_build_adjacency(h))) return rc;
+    cudaEvent_t a0, a1;
+    cudaEventCreate(&a0); cudaEventCreate(&a1);
+    cudaEventRecord(a0, h->st);
+    if ((rc = hb_build_adjacency(h))) return rc;
+    cudaEventRecord(a1, h->st);
+    cudaEventSynchronize(a1);
+    float tadj = 0;
+    cudaEventElapsedTime(&tadj, a0, a1);
+    cudaEventDestroy(a0); cudaEventDestroy(a1);
     RowStats hs;
     if ((rc = rows_dispatch<0>(h, value_prec, h->H, &hs))) return rc;
+    h->st_adj = tadj;
+    h->st_formh += tadj;
+    h->st_pairs = (double)hs.pairs;
+    h->st_scanned = (double)hs.scanned;
+    // adjacency: 2 passes + scan (2 kernels) + memset; rows: 2 passes + scan (2) + 2 memsets
+    h->st_launches = 11;
     csr_free(h->Hfull);
     h->numh = h->H.nnz;
     h->numzero = (int64_t)hs.numzero;

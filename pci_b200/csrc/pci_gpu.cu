@@ -349,9 +349,10 @@ int pci_gpu_davidson(pci_gpu_t *h, const pci_dvd_params *p, const double *X0, do
 int32_t pci_gpu_stats(pci_gpu_t *h, double *out, int32_t n)
 {
     if (!h || !out) return 0;
-    double v[8] = {h->st_formh, h->st_formh_count, h->st_formh_fill, h->st_formj,
-                   h->st_dvd, h->st_spmm, h->st_spmm_calls, h->st_init};
-    int32_t m = std::min<int32_t>(n, 8);
+    double v[12] = {h->st_formh, h->st_formh_count, h->st_formh_fill, h->st_formj,
+                    h->st_dvd, h->st_spmm, h->st_spmm_calls, h->st_init,
+                    h->st_adj, h->st_pairs, h->st_scanned, h->st_launches};
+    int32_t m = std::min<int32_t>(n, 12);
     for (int i = 0; i < m; i++) out[i] = v[i];
     return m;
 }

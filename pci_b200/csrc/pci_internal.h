@@ -89,6 +89,7 @@ struct pci_gpu {
     // stats (ms)
     double st_formh = 0, st_formh_count = 0, st_formh_fill = 0, st_formj = 0;
     double st_dvd = 0, st_spmm = 0, st_spmm_calls = 0, st_init = 0;
+    double st_adj = 0, st_pairs = 0, st_scanned = 0, st_launches = 0;
 };
 
 // error helpers

@@ -426,3 +426,13 @@ def cfg2(seed=2):
     refs = _random_refs(shells, 3, 1, 20, 28, seed)
     return dict(name="cfg2", shells=shells, ne=3, mj=1, parity=1, refs=refs, seed=seed,
                 params=dict(Nlv=10, MaxNd0=3000))
+
+
+@_register
+def mid(seed=2):
+    """A config-2-like system at about 1/12 the size (3 electrons, 71 orbitals,
+    ~86k determinants); used for profiling captures."""
+    shells = _shells({0: (3, 12), 1: (3, 10), 2: (3, 9), 3: (4, 8), 4: (5, 7)})
+    refs = _random_refs(shells, 3, 1, 6, 12, seed)
+    return dict(name="mid", shells=shells, ne=3, mj=1, parity=1, refs=refs, seed=seed,
+                params=dict(Nlv=10, MaxNd0=3000))
