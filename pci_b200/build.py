@@ -2,13 +2,16 @@
 
 The library is plain CUDA C++ behind the C ABI of include/pci_gpu.h; it does
 not link against libtorch or Python.  Objects go to pci_b200/_build/, the
-shared library to pci_b200/lib/libpci_gpu.so.
+shared library to pci_b200/lib/libpci_gpu.so.  Translation units compile in
+parallel; the Hamiltonian-build kernels are instantiated once per electron
+count (hbuild_ne.cu with -DPCI_NE=1..8).
 """
 from __future__ import annotations
 
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(PKG, "csrc")
@@ -21,41 +24,46 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
                  "--expt-relaxed-constexpr"]
-# Per-unit extra flags.  The H-build keeps the reference's operation order with
-# separately rounded multiplies and adds (no fused multiply-add contraction).
-UNITS = {
-    "hbuild.cu": ["-fmad=false"],
-    "spmm.cu": [],
-    "davidson.cu": [],
-    "pci_gpu.cu": [],
-}
-HEADERS = ["pci_internal.h", os.path.join("..", "..", "include", "pci_gpu.h")]
+# The Hamiltonian build keeps the reference's operation order with separately
+# rounded multiplies and adds (no fused multiply-add contraction).
+NOFMA = ["-fmad=false"]
+NE_MAX = 8
+
+# (object name, source, extra flags)
+UNITS = [("hbuild", "hbuild.cu", NOFMA)] + \
+    [(f"hbuild_ne{n}", "hbuild_ne.cu", NOFMA + [f"-DPCI_NE={n}"]) for n in range(1, NE_MAX + 1)] + \
+    [("spmm", "spmm.cu", []), ("davidson", "davidson.cu", []), ("pci_gpu", "pci_gpu.cu", [])]
+HEADERS = ["pci_internal.h", "hbuild_impl.cuh", os.path.join("..", "..", "include", "pci_gpu.h")]
 
 
 def _mtime(p):
     return os.path.getmtime(p) if os.path.exists(p) else 0.0
 
 
-def build(verbose: bool = False, force: bool = False, extra: list | None = None) -> str:
+def build(verbose: bool = False, force: bool = False, extra: list | None = None, jobs: int = 0) -> str:
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
     hdr_t = max(_mtime(os.path.join(SRC, hh)) for hh in HEADERS)
-    objs = []
-    for unit, flags in UNITS.items():
+    todo, objs = [], []
+    for name, unit, flags in UNITS:
         src = os.path.join(SRC, unit)
-        obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
+        obj = os.path.join(BUILD, name + ".o")
         objs.append(obj)
         if force or _mtime(obj) < max(_mtime(src), hdr_t):
-            cmd = [NVCC] + COMMON + flags + (extra or []) + ["-c", src, "-o", obj]
-            if verbose:
-                print(" ".join(cmd), flush=True)
-            subprocess.check_call(cmd)
-    if force or _mtime(LIB) < max(_mtime(o) for o in objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + [
-            "-lcusolver", "-lcublas", "-Xlinker", f"-rpath,{CUDA_HOME}/lib64"]
+            todo.append([NVCC] + COMMON + flags + (extra or []) + ["-c", src, "-o", obj])
+
+    def run(cmd):
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)
+
+    if todo:
+        with ThreadPoolExecutor(max_workers=jobs or max(1, os.cpu_count() or 1)) as ex:
+            for f in [ex.submit(run, c) for c in todo]:
+                f.result()
+    if force or _mtime(LIB) < max(_mtime(o) for o in objs):
+        run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs +
+            ["-lcusolver", "-lcublas", "-Xlinker", f"-rpath,{CUDA_HOME}/lib64"])
     return LIB
 
 

@@ -477,7 +477,7 @@ int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out
     cublasSetStream(d.cub, d.st);
     if (cusolverDnCreate(&d.sol) != CUSOLVER_STATUS_SUCCESS) { free_dvd(d); return set_err(h, PCI_E_CUDA, "cusolverDnCreate failed"); }
     cusolverDnSetStream(d.sol, d.st);
-    if ((rc = sp_build_full(h))) { free_dvd(d); return rc; }
+    // the SpMM picks the full symmetric copy or the lower-triangle kernel by free memory
     PCI_CUDA(h, cudaMemsetAsync(d.A, 0, (size_t)nd * d.ld * 8, d.st));
     PCI_CUDA(h, cudaMemsetAsync(d.iconv_d, 0, 16 * 4, d.st));
     PCI_CUDA(h, cudaMemsetAsync(d.ost, 0, sizeof(OrtnState), d.st));

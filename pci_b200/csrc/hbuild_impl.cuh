@@ -1,0 +1,898 @@
+// Device code of the Hamiltonian / J^2 build, shared by the per-Ne
+// translation units (hbuild_ne.cu compiled once per electron count) and the
+// host entry points in hbuild.cu.  Compiled with -fmad=false (see hbuild.cu).
+#pragma once
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "pci_internal.h"
+
+#define FULL_MASK 0xffffffffu
+
+// ------------------------------------------------------------- hashing ---
+
+__host__ __device__ __forceinline__ unsigned long long hmix(unsigned long long x)
+{
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdULL;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ULL;
+    x ^= x >> 33;
+    return x;
+}
+
+__host__ __device__ __forceinline__ unsigned long long hkey(int iac, int ibd)
+{
+    return ((unsigned long long)(unsigned)iac << 32) | (unsigned long long)(unsigned)ibd;
+}
+
+// ------------------------------------------------------- device physics ---
+
+__device__ __forceinline__ double d_lookup(const DevSys &S, int iac, int ibd, int comp)
+{
+    unsigned long long key = hkey(iac, ibd);
+    unsigned long long s = hmix(key) & S.hmask;
+    int stride = S.kbrt ? 2 : 1;
+    for (int p = 0; p < PCI_MAX_PROBE; p++) {
+        unsigned long long k = __ldg(&S.hkey[s]);
+        if (k == key) return __ldg(&S.hval[s * stride + comp]);
+        if (k == 0ULL) break;
+        s = (s + 1) & S.hmask;
+    }
+    atomicOr(S.err, DERR_MISSING_INTEGRAL);
+    return 0.0;
+}
+
+// Per-warp cache of the radial integrals one configuration tile needs,
+// direct-mapped by the same key hash; filled warp-synchronously at tile start
+// (one writer per slot), read-only while the tile's pairs are evaluated.
+constexpr int CACHE_SLOTS = 128;
+struct TileCache {
+    unsigned long long key[CACHE_SLOTS];
+    double val[CACHE_SLOTS * 2];
+};
+
+__device__ __forceinline__ int cache_slot(unsigned long long key)
+{
+    const unsigned a = (unsigned)(key >> 32), b = (unsigned)key;
+    return (int)((a * 0x9E3779B1u + b * 0x85EBCA77u) >> 25) & (CACHE_SLOTS - 1);
+}
+
+// Term lists of a tile whose two configurations differ by two orbitals
+// (A -> B): every candidate pair there is an nf = 2 element
+// Gint(q1,q2,p1,p2) with argument orbitals (B0,B1,A0,A1), so the allowed k
+// values and radial integrals of its direct and exchange sums are the same
+// for the whole tile.
+constexpr int KLIST = 16;
+struct TilePlan {
+    int kind;   // 2: two-orbital tile with lists below; -1: evaluate generically
+    int nd, nx;
+    int kd[KLIST], kx[KLIST];
+    double rd[KLIST], rx[KLIST];
+};
+
+__device__ __forceinline__ double d_lookup_c(const DevSys &S, const TileCache *tc, int iac, int ibd, int comp)
+{
+    if (tc) {
+        unsigned long long key = hkey(iac, ibd);
+        int s = cache_slot(key);
+        if (tc->key[s] == key) return tc->val[2 * s + comp];
+    }
+    return d_lookup(S, iac, ibd, comp);
+}
+
+// Packed per-m-state descriptor (built by pci_gpu_set_basis): orbital
+// (bits 0-9), (j,m) type of the Gaunt table (10-15), 2m + 128 (16-23),
+// l (24-27), (2j-1)/2 (28-31).
+struct Ms {
+    int orb, type, jz, l, j2;
+};
+
+__device__ __forceinline__ Ms ms_get(const DevSys &S, int i)
+{
+    uint32_t w = __ldg(&S.msd[i]);
+    Ms m;
+    m.orb = (int)(w & 1023u);
+    m.type = (int)((w >> 10) & 63u);
+    m.jz = (int)((w >> 16) & 255u) - 128;
+    m.l = (int)((w >> 24) & 15u);
+    m.j2 = 2 * (int)(w >> 28) + 1;
+    return m;
+}
+
+// Hint (src/integrals.f90:122-151); m-states are 0-based.
+__device__ __forceinline__ double d_hint(const DevSys &S, const Ms &a, const Ms &b)
+{
+    if (a.jz != b.jz) return 0.0;
+    return __ldg(&S.h1[a.orb * S.nsu + b.orb]);
+}
+
+__device__ __forceinline__ double d_gaunt(const DevSys &S, int k, int t1, int t2)
+{
+    return __ldg(&S.gaunt[((size_t)k * S.ntype + t1) * S.ntype + t2]);
+}
+
+// Gint (src/integrals.f90:153-293) with Ksig < 2 and no SMS term.  Orbital
+// indices are 0-based here, so the 1-based na-Nso-1 of the key becomes oa-Nso.
+static __device__ double d_gint(const DevSys &S, const TileCache *cache, const Ms &m1, const Ms &m2, const Ms &m3,
+                         const Ms &m4)
+{
+    const bool l_br = S.kbrt != 0;
+    double e = 0.0;
+    int is = 1;
+#pragma unroll
+    for (int ii = 0; ii < 2; ii++) {
+        const Ms &A = m1, &B = m2, &Cc = ii ? m4 : m3, &D = ii ? m3 : m4;
+        if (A.jz + B.jz != Cc.jz + D.jz) { atomicOr(S.err, DERR_M_NOT_CONSERVED); return 0.0; }
+        int na = A.orb, nb = B.orb, nc = Cc.orb, nd = D.orb;
+        int la = A.l, lc = Cc.l;
+        if (((la + B.l + lc + D.l) & 1) == 0) {
+            int ja = A.j2, jb = B.j2, jc = Cc.j2, jd = D.j2;
+            int ibr = 0, k;
+            if (na > nc) { k = na; na = nc; nc = k; ibr++; }
+            if (nb > nd) { k = nb; nb = nd; nd = k; ibr++; }
+            if (na > nb) { k = na; na = nb; nb = k; k = nc; nc = nd; nd = k; }
+            if (na == nb && nc > nd) { k = nc; nc = nd; nd = k; }
+            ibr = (ibr == 1) ? -1 : 1;
+            int iac0 = S.nx * (na - S.nso) + (nc + 1 - S.nso);
+            int ibd0 = S.nx * (nb - S.nso) + (nd + 1 - S.nso);
+            int kmin = max(abs(ja - jc) / 2, abs(jb - jd) / 2);
+            int kmax = min((ja + jc) / 2, (jb + jd) / 2);
+            int is_br = ((la + lc + kmin) & 1) ? ibr : 1;
+            for (k = kmin; k <= kmax; k++) {
+                bool l_pr = ((k + la + lc) & 1) == 0;
+                if (l_pr || l_br) {
+                    is_br = is_br * ibr;
+                    int iac = S.nx * S.nx * k + iac0;
+                    double rabcd = d_lookup_c(S, cache, iac, ibd0, 0);
+                    if (l_br) rabcd = rabcd + is_br * d_lookup_c(S, cache, iac, ibd0, 1);
+                    double g1 = d_gaunt(S, k, A.type, Cc.type);
+                    double g2 = d_gaunt(S, k, D.type, B.type);
+                    e = e + ((is * g1) * g2) * rabcd;
+                }
+            }
+        }
+        is = -is;
+    }
+    return e;
+}
+
+// Plj (src/formj2.f90:48-67)
+__device__ __forceinline__ double d_plj(const Ms &a, const Ms &b)
+{
+    if (a.orb == b.orb && a.jz == b.jz + 2) return sqrt((double)(a.j2 * (a.j2 + 2) - a.jz * b.jz));
+    return 0.0;
+}
+
+// F_J2, nf = 0 (src/formj2.f90:23-38)
+template <int NE>
+__device__ double d_fj2_diag(const DevSys &S, const uint16_t *d)
+{
+    double t = (double)(S.mj * S.mj);
+#pragma unroll
+    for (int iq = 0; iq < NE; iq++) {
+        Ms a = ms_get(S, d[iq]);
+        t = t + (double)(a.j2 * (a.j2 + 2) - a.jz * a.jz);
+#pragma unroll
+        for (int jq = iq + 1; jq < NE; jq++) {
+            Ms b = ms_get(S, d[jq]);
+            double p1 = d_plj(a, b), p2 = d_plj(b, a);
+            t = t - p1 * p1 - p2 * p2;
+        }
+    }
+    return t;
+}
+
+// F_J2, nf = 2 (src/formj2.f90:39-41), arguments (ia, ic, ib, id)
+__device__ __forceinline__ double d_fj2_two(const DevSys &S, int is, int ia, int ic, int ib, int id)
+{
+    Ms A = ms_get(S, ia), Cc = ms_get(S, ic), B = ms_get(S, ib), D = ms_get(S, id);
+    return is * (d_plj(A, Cc) * d_plj(D, B) + d_plj(Cc, A) * d_plj(B, D)
+                 - d_plj(A, D) * d_plj(Cc, B) - d_plj(D, A) * d_plj(B, Cc));
+}
+
+// Difference of two sorted occupation lists.  Positions of the differing
+// m-states are list positions, so the fermion sign of Rspq_phase2
+// (src/determinants.f90:709-724), (-1)^(|j2-i2| + |j3-i3|), is the parity of
+// the sum of the four positions.
+template <int NE>
+struct Diff {
+    int nf;
+    int p1, p2, q1, q2;  // m-states: det1 (row) earlier/later, det2 (column) earlier/later
+    int is;
+};
+
+template <int NE>
+__device__ __forceinline__ Diff<NE> d_diff(const uint16_t *d1, const uint16_t *d2)
+{
+    unsigned ma = 0, mb = 0;
+#pragma unroll
+    for (int i = 0; i < NE; i++)
+#pragma unroll
+        for (int j = 0; j < NE; j++)
+            if (d1[i] == d2[j]) { ma |= 1u << i; mb |= 1u << j; }
+    Diff<NE> r;
+    r.nf = NE - __popc(ma);
+    r.p1 = r.p2 = r.q1 = r.q2 = -1;
+    r.is = 1;
+    if (r.nf == 1 || r.nf == 2) {
+        unsigned ua = (~ma) & ((1u << NE) - 1), ub = (~mb) & ((1u << NE) - 1);
+        int ip1 = __ffs(ua) - 1, jp1 = __ffs(ub) - 1;
+        int par = ip1 + jp1;
+        r.p1 = d1[ip1];
+        r.q1 = d2[jp1];
+        if (r.nf == 2) {
+            int ip2 = 31 - __clz(ua), jp2 = 31 - __clz(ub);
+            par += ip2 + jp2;
+            r.p2 = d1[ip2];
+            r.q2 = d2[jp2];
+        }
+        r.is = (par & 1) ? -1 : 1;
+    }
+    return r;
+}
+
+// Hmltn (src/pconf.F90:1653-1692) as called from FormH with
+// (i2, i1, j2, j1) = (jIndexes(3), iIndexes(3), jIndexes(2), iIndexes(2)).
+template <int NE>
+__device__ double d_hmltn(const DevSys &S, const TileCache *tc, const uint16_t *d1, const Diff<NE> &df)
+{
+    double t = 0.0;
+    if (df.nf == 2) {
+        // Gint(i2, j2, i1, j1) = Gint(q1, q2, p1, p2)
+        Ms q1 = ms_get(S, df.q1), q2 = ms_get(S, df.q2), p1 = ms_get(S, df.p1), p2 = ms_get(S, df.p2);
+        t = t + d_gint(S, tc, q1, q2, p1, p2) * df.is;
+        if (S.gj != 0.0) t = t + S.gj * d_fj2_two(S, df.is, df.q1, df.p1, df.q2, df.p2);
+    } else if (df.nf == 1) {
+        // j2 = q (det2), j1 = p (det1)
+        Ms q = ms_get(S, df.q1), p = ms_get(S, df.p1);
+#pragma unroll
+        for (int iq = 0; iq < NE; iq++) {
+            int a = d1[iq];
+            if (a != df.p1) {
+                Ms x = ms_get(S, a);
+                t = t + d_gint(S, tc, q, x, p, x) * df.is;
+            }
+        }
+        t = t + d_hint(S, q, p) * df.is;
+    } else {
+        Ms m[NE];
+#pragma unroll
+        for (int iq = 0; iq < NE; iq++) m[iq] = ms_get(S, d1[iq]);
+#pragma unroll
+        for (int iq = 0; iq < NE; iq++) {
+#pragma unroll
+            for (int jq = iq + 1; jq < NE; jq++) t = t + d_gint(S, tc, m[iq], m[jq], m[iq], m[jq]) * 1;
+            t = t + d_hint(S, m[iq], m[iq]) * 1;
+        }
+        if (S.gj != 0.0) t = t + S.gj * d_fj2_diag<NE>(S, d1);
+    }
+    return t;
+}
+
+// ---------------------------------------------------------- adjacency ---
+
+// CompD (src/determinants.f90:748-779) on sorted orbital lists.
+template <int NE>
+__device__ __forceinline__ int d_compd(const uint16_t *a, const uint16_t *b)
+{
+    int ni = 0, nj = 0, i = 0, j = 0;
+    while (i < NE && j < NE) {
+        int l1 = a[i], l2 = b[j];
+        if (l1 == l2) { i++; j++; }
+        else if (l1 > l2) { if (++nj > 2) return 3; j++; }
+        else { if (++ni > 2) return 3; i++; }
+    }
+    return ni > nj ? ni : nj;
+}
+
+// One warp per configuration c1: list c2 <= c1 (non-empty) with CompD <= 2.
+// The count pass also records the work of c1 (pairs its rows will visit).
+template <int NE, int FILL>
+__global__ void __launch_bounds__(256) k_adjacency(DevSys S, const int32_t *ndc, int64_t *cnt, int32_t *adj,
+                                                   unsigned long long *work)
+{
+    int lane = threadIdx.x & 31;
+    int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t c1 = warp; c1 < S.nc; c1 += nwarps) {
+        if (ndc[c1] == 0) {
+            if (!FILL && lane == 0) { cnt[c1] = 0; work[c1] = 0; }
+            continue;
+        }
+        uint16_t a[NE];
+#pragma unroll
+        for (int e = 0; e < NE; e++) a[e] = S.conf_orb[c1 * NE + e];
+        int64_t base = FILL ? cnt[c1] : 0, c = 0;
+        unsigned long long wsum = 0;
+        for (int64_t c2b = 0; c2b <= c1; c2b += 32) {
+            int64_t c2 = c2b + lane;
+            bool ok = false;
+            if (c2 <= c1 && ndc[c2] > 0) {
+                uint16_t b[NE];
+#pragma unroll
+                for (int e = 0; e < NE; e++) b[e] = S.conf_orb[c2 * NE + e];
+                ok = d_compd<NE>(a, b) <= 2;
+                if (ok) wsum += ndc[c2];
+            }
+            unsigned m = __ballot_sync(FULL_MASK, ok);
+            if (FILL && ok) adj[base + c + __popc(m & ((1u << lane) - 1))] = (int32_t)c2;
+            c += __popc(m);
+        }
+        if (!FILL) {
+            for (int o = 16; o > 0; o >>= 1) wsum += __shfl_down_sync(FULL_MASK, wsum, o);
+            if (lane == 0) {
+                cnt[c1] = c;
+                work[c1] = wsum;   // determinant pairs per row of c1
+            }
+        }
+    }
+}
+
+template <int NE>
+static int adjacency_impl(pci_gpu *h, DevSys S, const int32_t *d_ndc)
+{
+    int rc = 0;
+    int64_t nc = h->nc;
+    int64_t *cnt = (int64_t *)dev_alloc(h, (nc + 1) * 8, &rc);
+    if (rc) return rc;
+    unsigned long long *work = (unsigned long long *)dev_alloc(h, (nc + 1) * 8, &rc);
+    if (rc) { dev_free(cnt); return rc; }
+    k_adjacency<NE, 0><<<148 * 8, 256, 0, h->st>>>(S, d_ndc, cnt, nullptr, work);
+    PCI_CUDA(h, cudaGetLastError());
+    dev_free(h->d_adj_ptr);
+    h->d_adj_ptr = (int64_t *)dev_alloc(h, (nc + 1) * 8, &rc);
+    if (rc) { dev_free(cnt); dev_free(work); return rc; }
+    PCI_CUDA(h, cudaMemsetAsync(h->d_adj_ptr, 0, 8, h->st));
+    size_t tb = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, tb, cnt, h->d_adj_ptr + 1, nc, h->st);
+    if ((rc = ensure_tmp(h, tb))) { dev_free(cnt); dev_free(work); return rc; }
+    cub::DeviceScan::InclusiveSum(h->d_tmp, tb, cnt, h->d_adj_ptr + 1, nc, h->st);
+    int64_t nadj = 0;
+    h->h_rowwork.resize(nc);
+    PCI_CUDA(h, cudaMemcpyAsync(h->h_rowwork.data(), work, nc * 8, cudaMemcpyDeviceToHost, h->st));
+    PCI_CUDA(h, cudaMemcpyAsync(&nadj, h->d_adj_ptr + nc, 8, cudaMemcpyDeviceToHost, h->st));
+    PCI_CUDA(h, cudaStreamSynchronize(h->st));
+    dev_free(h->d_adj);
+    h->d_adj = (int32_t *)dev_alloc(h, std::max<int64_t>(nadj, 1) * 4, &rc);
+    if (rc) { dev_free(cnt); dev_free(work); return rc; }
+    S.adj_ptr = h->d_adj_ptr;
+    k_adjacency<NE, 1><<<148 * 8, 256, 0, h->st>>>(S, d_ndc, h->d_adj_ptr, h->d_adj, nullptr);
+    PCI_CUDA(h, cudaGetLastError());
+    PCI_CUDA(h, cudaStreamSynchronize(h->st));
+    dev_free(cnt);
+    dev_free(work);
+    h->n_adj = nadj;
+    return PCI_OK;
+}
+
+// ---------------------------------------------------------- tile cache ---
+
+// Radial keys Gint visits for the argument orbitals (na, nb, nc, nd), both
+// terms (direct, then c<->d exchange), exactly as d_gint computes them.
+static __device__ int quad_keys(const DevSys &S, int na, int nb, int nc, int nd, unsigned long long *out, int cap)
+{
+    int n = 0;
+    for (int ii = 0; ii < 2; ii++) {
+        int a = na, b = nb, c = ii ? nd : nc, d = ii ? nc : nd;
+        int la = S.orb_l[a], lb = S.orb_l[b], lc = S.orb_l[c], ld = S.orb_l[d];
+        if (((la + lb + lc + ld) & 1) == 0) {
+            int ja = S.orb_j[a], jb = S.orb_j[b], jc = S.orb_j[c], jd = S.orb_j[d];
+            int k;
+            if (a > c) { k = a; a = c; c = k; }
+            if (b > d) { k = b; b = d; d = k; }
+            if (a > b) { k = a; a = b; b = k; k = c; c = d; d = k; }
+            if (a == b && c > d) { k = c; c = d; d = k; }
+            int iac0 = S.nx * (a - S.nso) + (c + 1 - S.nso);
+            int ibd0 = S.nx * (b - S.nso) + (d + 1 - S.nso);
+            int kmin = max(abs(ja - jc) / 2, abs(jb - jd) / 2);
+            int kmax = min((ja + jc) / 2, (jb + jd) / 2);
+            for (k = kmin; k <= kmax; k++) {
+                bool l_pr = ((k + la + lc) & 1) == 0;
+                if ((l_pr || S.kbrt) && n < cap) out[n++] = hkey(S.nx * S.nx * k + iac0, ibd0);
+            }
+        }
+    }
+    return n;
+}
+
+constexpr int TILE_KEYS = 160;
+
+// Warp-synchronous fill of the tile cache for configurations with sorted
+// orbital lists o1 (rows) and o2 (columns), CompD(o1, o2) <= 2.  The keys are
+// those of every Gint call an element of the tile can make:
+//   CompD 2: Gint(q1,q2,p1,p2) with orbitals (b1,b2,a1,a2);
+//   CompD 1: Gint(q,x,p,x) and the two-m-state case with a spectator s:
+//            orbitals (c,s,a,s) for every spectator orbital s;
+//   CompD 0: Gint(x,y,x,y) and same-configuration doubles: (s,t,s,t) for every
+//            orbital pair of the configuration.
+// Keys that miss the cache fall back to the global table, so a dropped or
+// evicted key costs time, never correctness.
+// Lane-parallel term list of a two-orbital tile: lanes 0-15 take the direct
+// sum's k = kmin + lane, lanes 16-31 the exchange sum's; valid terms are
+// compacted in ascending k.  False if a needed integral is absent or a k
+// range does not fit, so the caller falls back to the generic evaluation.
+static __device__ bool plan_two_orbital(const DevSys &S, TilePlan *plan, int A0, int A1, int B0, int B1, int lane)
+{
+    const int ii = lane >> 4, kk = lane & 15;
+    int a = B0, b = B1, c = ii ? A1 : A0, d = ii ? A0 : A1;
+    const int la = S.orb_l[a], lb = S.orb_l[b], lc = S.orb_l[c], ld = S.orb_l[d];
+    const int ja = S.orb_j[a], jb = S.orb_j[b], jc = S.orb_j[c], jd = S.orb_j[d];
+    int t;
+    if (a > c) { t = a; a = c; c = t; }
+    if (b > d) { t = b; b = d; d = t; }
+    if (a > b) { t = a; a = b; b = t; t = c; c = d; d = t; }
+    if (a == b && c > d) { t = c; c = d; d = t; }
+    const int kmin = max(abs(ja - jc) / 2, abs(jb - jd) / 2);
+    const int kmax = min((ja + jc) / 2, (jb + jd) / 2);
+    const int k = kmin + kk;
+    const bool par = ((la + lb + lc + ld) & 1) == 0;
+    const bool valid = par && k <= kmax && ((k + la + lc) & 1) == 0;
+    bool found = true;
+    double r = 0.0;
+    if (valid) {
+        const unsigned long long key = hkey(S.nx * S.nx * k + S.nx * (a - S.nso) + (c + 1 - S.nso),
+                                            S.nx * (b - S.nso) + (d + 1 - S.nso));
+        unsigned long long s = hmix(key) & S.hmask;
+        found = false;
+        for (int p = 0; p < PCI_MAX_PROBE; p++) {
+            const unsigned long long kq = __ldg(&S.hkey[s]);
+            if (kq == key) { r = __ldg(&S.hval[s]); found = true; break; }
+            if (kq == 0ULL) break;
+            s = (s + 1) & S.hmask;
+        }
+    }
+    const unsigned vm = __ballot_sync(FULL_MASK, valid);
+    const unsigned bad = __ballot_sync(FULL_MASK, (valid && !found) || (par && kk == 15 && k < kmax));
+    const unsigned half = ii ? 0xffff0000u : 0x0000ffffu;
+    const int pos = __popc(vm & half & ((1u << lane) - 1));
+    if (valid) {
+        if (ii == 0) { plan->kd[pos] = k; plan->rd[pos] = r; }
+        else { plan->kx[pos] = k; plan->rx[pos] = r; }
+    }
+    if (lane == 0) {
+        plan->nd = __popc(vm & 0x0000ffffu);
+        plan->nx = __popc(vm & 0xffff0000u);
+        plan->kind = bad ? -1 : 2;
+    }
+    __syncwarp();
+    return bad == 0;
+}
+
+template <int NE>
+__device__ void fill_tile_cache(const DevSys &S, TileCache *tc, TilePlan *plan, unsigned long long *keys,
+                                const uint16_t *o1, const uint16_t *o2, int lane)
+{
+    // multiset differences of the two orbital lists (every lane; NE <= 8)
+    int A[NE], B[NE], common[NE], na = 0, nb = 0, ncommon = 0;
+    {
+        int i = 0, j = 0;
+        while (i < NE && j < NE) {
+            if (o1[i] == o2[j]) { common[ncommon++] = o1[i]; i++; j++; }
+            else if (o1[i] < o2[j]) A[na++] = o1[i++];
+            else B[nb++] = o2[j++];
+        }
+        while (i < NE) A[na++] = o1[i++];
+        while (j < NE) B[nb++] = o2[j++];
+    }
+    if (na == 2 && !S.kbrt) {
+        if (plan_two_orbital(S, plan, A[0], A[1], B[0], B[1], lane)) return;
+    } else if (lane == 0) {
+        plan->kind = -1;
+    }
+    int nkeys = 0;
+    if (lane == 0) {
+        if (na == 2) {
+            nkeys += quad_keys(S, B[0], B[1], A[0], A[1], keys + nkeys, TILE_KEYS - nkeys);
+        } else if (na == 1) {
+            int prev = -1;
+            for (int s = 0; s < ncommon; s++) {
+                if (common[s] == prev) continue;
+                prev = common[s];
+                nkeys += quad_keys(S, B[0], common[s], A[0], common[s], keys + nkeys, TILE_KEYS - nkeys);
+            }
+        } else if (na == 0) {
+            for (int x = 0; x < NE; x++)
+                for (int y = x + 1; y < NE; y++) {
+                    bool seen = false;
+                    for (int x2 = 0; x2 <= x && !seen; x2++)
+                        for (int y2 = x2 + 1; y2 < NE && !seen; y2++)
+                            if ((x2 < x || y2 < y) && o1[x2] == o1[x] && o1[y2] == o1[y]) seen = true;
+                    if (!seen) nkeys += quad_keys(S, o1[x], o1[y], o1[x], o1[y], keys + nkeys, TILE_KEYS - nkeys);
+                }
+        }
+    }
+    nkeys = __shfl_sync(FULL_MASK, nkeys, 0);
+    __syncwarp();
+    const int stride = S.kbrt ? 2 : 1;
+    for (int base = 0; base < nkeys; base += 32) {
+        int idx = base + lane;
+        unsigned long long key = idx < nkeys ? keys[idx] : 0ULL;
+        int slot = idx < nkeys ? cache_slot(key) : -1 - lane;
+        unsigned same = __match_any_sync(FULL_MASK, slot);
+        bool writer = idx < nkeys && (__ffs(same) - 1) == lane;
+        if (writer) {
+            // prefetch only: a key absent from the table is left out of the
+            // cache, so the element that needs it reports the missing integral
+            unsigned long long s = hmix(key) & S.hmask;
+            for (int p = 0; p < PCI_MAX_PROBE; p++) {
+                unsigned long long kk = __ldg(&S.hkey[s]);
+                if (kk == key) {
+                    tc->key[slot] = key;
+                    tc->val[2 * slot] = __ldg(&S.hval[s * stride]);
+                    tc->val[2 * slot + 1] = stride == 2 ? __ldg(&S.hval[s * stride + 1]) : 0.0;
+                    break;
+                }
+                if (kk == 0ULL) break;
+                s = (s + 1) & S.hmask;
+            }
+        }
+        __syncwarp();
+    }
+    if (lane == 0) plan->kind = -1;
+    __syncwarp();
+}
+
+// ------------------------------------------------------------ tile pass ---
+
+struct RowStats {
+    unsigned long long numzero, pairs, scanned;
+    long long hmin_key;  // order-preserving integer image of the minimum value
+};
+
+__device__ __forceinline__ long long dkey(double x)
+{
+    long long b = __double_as_longlong(x);
+    return b >= 0 ? b : (b ^ 0x7fffffffffffffffLL);
+}
+
+static inline double key_to_double(long long k)
+{
+    long long b = k >= 0 ? k : (k ^ 0x7fffffffffffffffLL);
+    double x;
+    memcpy(&x, &b, 8);
+    return x;
+}
+
+constexpr int TR = 64;   // rows of c1 per chunk
+constexpr int TK = 64;   // columns of c2 per chunk
+constexpr int WARPS = 8;
+constexpr int QCAP = 64;
+
+struct WarpSmem {
+    TileCache tc;
+    TilePlan plan;
+    unsigned long long keys[TILE_KEYS];
+    int64_t rowbase[TR];
+    int32_t rowcnt[TR];
+    uint32_t queue[QCAP];   // candidate pairs (row << 16 | column) in tile order
+    uint16_t drow[TR * PCI_NE_MAX];
+    uint16_t dcol[TK * PCI_NE_MAX];
+};
+
+struct Tally {
+    unsigned long long nzero, npairs, nscan;
+    double hmin;
+};
+
+// Evaluate the first `cnt` queued pairs (one per lane) and write or count the
+// non-zeros.  Rows receive their columns in queue order, which is ascending.
+template <int NE, int KIND, int FILL, typename VT>
+__device__ __forceinline__ void eval_queue(const DevSys &S, WarpSmem *ws, const TileCache *tc, int cnt,
+                                           int64_t rabs0, int64_t kabs0, int32_t *col, VT *val, Tally &ty,
+                                           int lane)
+{
+    const unsigned lt = (1u << lane) - 1;
+    int r = TR + lane;
+    bool nz = false;
+    double v = 0.0;
+    int64_t k = 0;
+    if (lane < cnt) {
+        uint32_t e = ws->queue[lane];
+        r = (int)(e >> 16);
+        const int kk = (int)(e & 0xffffu);
+        k = kabs0 + kk;
+        uint16_t d1[NE], d2[NE];
+#pragma unroll
+        for (int q = 0; q < NE; q++) { d1[q] = ws->drow[r * NE + q]; d2[q] = ws->dcol[kk * NE + q]; }
+        Diff<NE> df = d_diff<NE>(d1, d2);
+        if (KIND == 0) {
+            ty.npairs++;
+            if (ws->plan.kind == 2) {
+                // Gint(q1,q2,p1,p2) from the tile's term lists, same operation order as d_gint
+                const int tq1 = (int)((__ldg(&S.msd[df.q1]) >> 10) & 63u), tq2 = (int)((__ldg(&S.msd[df.q2]) >> 10) & 63u);
+                const int tp1 = (int)((__ldg(&S.msd[df.p1]) >> 10) & 63u), tp2 = (int)((__ldg(&S.msd[df.p2]) >> 10) & 63u);
+                const TilePlan &P = ws->plan;
+                double e = 0.0;
+                for (int i = 0; i < P.nd; i++) {
+                    const int kq = P.kd[i];
+                    const double g1 = d_gaunt(S, kq, tq1, tp1), g2 = d_gaunt(S, kq, tp2, tq2);
+                    e = e + ((1 * g1) * g2) * P.rd[i];
+                }
+                for (int i = 0; i < P.nx; i++) {
+                    const int kq = P.kx[i];
+                    const double g1 = d_gaunt(S, kq, tq1, tp2), g2 = d_gaunt(S, kq, tp1, tq2);
+                    e = e + ((-1 * g1) * g2) * P.rx[i];
+                }
+                v = 0.0 + e * df.is;
+                if (S.gj != 0.0) v = v + S.gj * d_fj2_two(S, df.is, df.q1, df.p1, df.q2, df.p2);
+            } else {
+                v = d_hmltn<NE>(S, tc, d1, df);
+            }
+            if (v != 0.0) nz = true; else ty.nzero++;
+        } else {
+            v = df.nf == 0 ? d_fj2_diag<NE>(S, d1) : d_fj2_two(S, df.is, df.q1, df.p1, df.q2, df.p2);
+            nz = v != 0.0;
+        }
+    }
+    const unsigned nzm = __ballot_sync(FULL_MASK, nz);
+    if (nzm) {
+        const unsigned same = __match_any_sync(FULL_MASK, r) & nzm;
+        int cur = 0;
+        if (nz) cur = ws->rowcnt[r];
+        __syncwarp();
+        if (nz) {
+            VT vs = (VT)v;
+            double vd = (double)vs;
+            if (vd < ty.hmin) ty.hmin = vd;
+            if (FILL) {
+                int64_t pos = ws->rowbase[r] + cur + __popc(same & lt);
+                col[pos] = (int32_t)k;
+                val[pos] = vs;
+            }
+            if ((same & lt) == 0) ws->rowcnt[r] = cur + __popc(same);
+        }
+    }
+    __syncwarp();
+    (void)rabs0;
+}
+
+// One warp per work item (row configuration c1, a chunk of its rows), items
+// taken heaviest first.  For each adjacent configuration c2 (ascending) the
+// warp fills the tile cache and stages the column determinants; lanes compare
+// 32 pairs at a time and push the pairs with difference <= 2 into a FIFO;
+// every 32 queued pairs are evaluated together, so the Slater-Condon work
+// runs with full warps.  Non-zeros are compacted per row with
+// __match_any_sync + __ballot_sync, every row receiving its columns in
+// ascending order.
+// KIND 0: Hamiltonian; KIND 1: J^2 (diagonal tile only, nf in {0, 2}).
+// FILL 0: per-row counts into rowinfo; FILL 1: rowinfo is the CSR rowptr.
+template <int NE, int KIND, int FILL, typename VT>
+__global__ void __launch_bounds__(WARPS * 32) k_tiles(DevSys S, const int4 *items, int64_t nitems,
+                                                      unsigned long long *counter, int64_t *rowinfo, int32_t *col,
+                                                      VT *val, RowStats *stats)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    WarpSmem *ws = reinterpret_cast<WarpSmem *>(smem_raw) + (threadIdx.x >> 5);
+    const TileCache *tc = KIND == 0 ? &ws->tc : nullptr;
+    if (KIND == 0)
+        for (int i = lane; i < CACHE_SLOTS; i += 32) ws->tc.key[i] = 0ULL;
+    __syncwarp();
+    Tally ty = {0, 0, 0, INFINITY};
+    const unsigned lt = (1u << lane) - 1;
+    while (true) {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(counter, 1ULL);
+        t = __shfl_sync(FULL_MASK, t, 0);
+        if (t >= (unsigned long long)nitems) break;
+        const int4 it = items[t];
+        const int c1 = it.x;
+        const int64_t cs1 = S.conf_start[c1];
+        const int64_t r0 = cs1 + it.y;
+        const int nr = it.z;
+        uint16_t o1[NE];
+#pragma unroll
+        for (int e = 0; e < NE; e++) o1[e] = S.conf_orb[(int64_t)c1 * NE + e];
+        const int64_t a0 = KIND == 0 ? S.adj_ptr[c1] : 0, a1 = KIND == 0 ? S.adj_ptr[c1 + 1] : 1;
+        for (int rc = 0; rc < nr; rc += TR) {
+            const int nrc = min(TR, nr - rc);
+            const int64_t rb = r0 + rc;   // absolute index of the chunk's first row
+            for (int i = lane; i < nrc * NE; i += 32) ws->drow[i] = S.occ[rb * NE + i];
+            for (int i = lane; i < nrc; i += 32) {
+                ws->rowcnt[i] = 0;
+                ws->rowbase[i] = FILL ? rowinfo[rb + i] : 0;
+            }
+            __syncwarp();
+            for (int64_t a = a0; a < a1; a++) {
+                const int c2 = KIND == 0 ? S.adj[a] : c1;
+                const int64_t k0 = S.conf_start[c2];
+                const int nk = (int)(S.conf_start[c2 + 1] - k0);
+                const bool diag = c2 == c1;
+                if (KIND == 0) {
+                    uint16_t o2[NE];
+#pragma unroll
+                    for (int e = 0; e < NE; e++) o2[e] = S.conf_orb[(int64_t)c2 * NE + e];
+                    fill_tile_cache<NE>(S, &ws->tc, &ws->plan, ws->keys, o1, o2, lane);
+                }
+                for (int kc = 0; kc < nk; kc += TK) {
+                    const int nkc = min(TK, nk - kc);
+                    if (diag && k0 + kc > rb + nrc - 1) break;  // whole chunk above the diagonal
+                    __syncwarp();
+                    for (int i = lane; i < nkc * NE; i += 32) ws->dcol[i] = S.occ[(k0 + kc) * NE + i];
+                    __syncwarp();
+                    const int np = nrc * nkc;
+                    int qn = 0;
+                    for (int base = 0; base < np; base += 32) {
+                        const int idx = base + lane;
+                        const int r = idx / nkc;
+                        const int kk = idx - r * nkc;
+                        bool cand = false;
+                        if (idx < np && !(diag && k0 + kc + kk > rb + r)) {
+                            ty.nscan++;
+                            uint16_t d1[NE], d2[NE];
+#pragma unroll
+                            for (int e = 0; e < NE; e++) { d1[e] = ws->drow[r * NE + e]; d2[e] = ws->dcol[kk * NE + e]; }
+                            unsigned ma = 0;
+#pragma unroll
+                            for (int i = 0; i < NE; i++)
+#pragma unroll
+                                for (int j = 0; j < NE; j++)
+                                    if (d1[i] == d2[j]) ma |= 1u << i;
+                            const int nf = NE - __popc(ma);
+                            cand = KIND == 0 ? nf <= 2 : (nf == 0 || nf == 2);
+                        }
+                        const unsigned cm = __ballot_sync(FULL_MASK, cand);
+                        if (cand) ws->queue[qn + __popc(cm & lt)] = ((uint32_t)r << 16) | (uint32_t)kk;
+                        qn += __popc(cm);
+                        __syncwarp();
+                        if (qn >= 32) {
+                            eval_queue<NE, KIND, FILL, VT>(S, ws, tc, 32, rb, k0 + kc, col, val, ty, lane);
+                            if (lane < qn - 32) ws->queue[lane] = ws->queue[32 + lane];
+                            qn -= 32;
+                            __syncwarp();
+                        }
+                    }
+                    if (qn > 0) eval_queue<NE, KIND, FILL, VT>(S, ws, tc, qn, rb, k0 + kc, col, val, ty, lane);
+                }
+            }
+            __syncwarp();
+            if (!FILL)
+                for (int i = lane; i < nrc; i += 32) rowinfo[rb + i] = ws->rowcnt[i];
+            __syncwarp();
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        ty.nzero += __shfl_down_sync(FULL_MASK, ty.nzero, o);
+        ty.npairs += __shfl_down_sync(FULL_MASK, ty.npairs, o);
+        ty.nscan += __shfl_down_sync(FULL_MASK, ty.nscan, o);
+        ty.hmin = fmin(ty.hmin, __shfl_down_sync(FULL_MASK, ty.hmin, o));
+    }
+    if (lane == 0 && stats) {
+        atomicAdd(&stats->numzero, ty.nzero);
+        atomicAdd(&stats->pairs, ty.npairs);
+        atomicAdd(&stats->scanned, ty.nscan);
+        if (ty.hmin < INFINITY) atomicMin(&stats->hmin_key, dkey(ty.hmin));
+    }
+}
+
+// Work items (configuration, first row, row count), heaviest first.  A
+// configuration's rows are split so that no item holds much more than
+// `target` determinant pairs; for J^2 every configuration is one item.
+static inline void make_items(const pci_gpu *h, const std::vector<unsigned long long> &rowwork, int kind, int nwarps,
+                       std::vector<int4> &items)
+{
+    items.clear();
+    const int nc = h->nc;
+    if (kind == 1) {
+        for (int c = 0; c < nc; c++)
+            if (h->h_ndc[c] > 0) items.push_back(make_int4(c, 0, h->h_ndc[c], 0));
+        return;
+    }
+    double total = 0.0;
+    for (int c = 0; c < nc; c++) total += (double)rowwork[c] * h->h_ndc[c];
+    const double target = std::max(1.0, total / (6.0 * nwarps));
+    std::vector<std::pair<double, int4>> tmp;
+    for (int c = 0; c < nc; c++) {
+        int nr = h->h_ndc[c];
+        if (nr == 0) continue;
+        double w = std::max(1.0, (double)rowwork[c]);
+        int R = (int)std::max(1.0, std::min((double)TR, std::floor(target / w)));
+        for (int r = 0; r < nr; r += R) {
+            int cnt = std::min(R, nr - r);
+            tmp.push_back({w * cnt, make_int4(c, r, cnt, 0)});
+        }
+    }
+    std::stable_sort(tmp.begin(), tmp.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+    items.reserve(tmp.size());
+    for (auto &p : tmp) items.push_back(p.second);
+}
+
+template <int NE, int KIND>
+static int rows_impl(pci_gpu *h, int value_prec, Csr &out, RowStats *hs)
+{
+    int rc = 0;
+    DevSys S = make_devsys(h);
+    const int64_t nd = h->nd;
+    csr_free(out);
+    out.nrows = nd;
+    out.rowptr = (int64_t *)dev_alloc(h, (nd + 1) * 8, &rc);
+    if (rc) return rc;
+    int64_t *cnt = (int64_t *)dev_alloc(h, (nd + 1) * 8, &rc);
+    if (rc) return rc;
+    RowStats *d_stats = (RowStats *)dev_alloc(h, sizeof(RowStats) + 16, &rc);
+    if (rc) { dev_free(cnt); return rc; }
+    unsigned long long *d_counter = (unsigned long long *)((char *)d_stats + sizeof(RowStats));
+    RowStats init = {0, 0, 0, 0x7fffffffffffffffLL};
+    PCI_CUDA(h, cudaMemcpyAsync(d_stats, &init, sizeof(RowStats), cudaMemcpyHostToDevice, h->st));
+    PCI_CUDA(h, cudaMemsetAsync(d_counter, 0, 8, h->st));
+    PCI_CUDA(h, cudaMemsetAsync(cnt, 0, (nd + 1) * 8, h->st));
+    const size_t smem = sizeof(WarpSmem) * WARPS;
+    auto kc64 = k_tiles<NE, KIND, 0, double>;
+    auto kc32 = k_tiles<NE, KIND, 0, float>;
+    auto kf64 = k_tiles<NE, KIND, 1, double>;
+    auto kf32 = k_tiles<NE, KIND, 1, float>;
+    cudaFuncSetAttribute(kc64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(kc32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(kf64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(kf32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kc64, WARPS * 32, smem);
+    int dev_sms = 148;
+    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, h->device);
+    const int blocks = dev_sms * std::max(per_sm, 1);
+    std::vector<int4> items;
+    make_items(h, h->h_rowwork, KIND, blocks * WARPS, items);
+    int4 *d_items = (int4 *)dev_alloc(h, std::max<size_t>(items.size(), 1) * sizeof(int4), &rc);
+    if (rc) { dev_free(cnt); dev_free(d_stats); return rc; }
+    PCI_CUDA(h, cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, h->st));
+    const int64_t nit = (int64_t)items.size();
+    cudaEvent_t e0, e1, e2;
+    cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2);
+    cudaEventRecord(e0, h->st);
+    if (value_prec == 32) kc32<<<blocks, WARPS * 32, smem, h->st>>>(S, d_items, nit, d_counter, cnt, nullptr, nullptr, d_stats);
+    else kc64<<<blocks, WARPS * 32, smem, h->st>>>(S, d_items, nit, d_counter, cnt, nullptr, nullptr, d_stats);
+    PCI_CUDA(h, cudaGetLastError());
+    PCI_CUDA(h, cudaMemsetAsync(out.rowptr, 0, 8, h->st));
+    size_t tb = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, tb, cnt, out.rowptr + 1, nd, h->st);
+    if ((rc = ensure_tmp(h, tb))) return rc;
+    cub::DeviceScan::InclusiveSum(h->d_tmp, tb, cnt, out.rowptr + 1, nd, h->st);
+    int64_t nnz = 0;
+    PCI_CUDA(h, cudaMemcpyAsync(&nnz, out.rowptr + nd, 8, cudaMemcpyDeviceToHost, h->st));
+    cudaEventRecord(e1, h->st);
+    PCI_CUDA(h, cudaStreamSynchronize(h->st));
+    unsigned int derr = 0;
+    PCI_CUDA(h, cudaMemcpy(&derr, h->d_err, 4, cudaMemcpyDeviceToHost));
+    if (derr) {
+        dev_free(cnt); dev_free(d_stats); dev_free(d_items);
+        PCI_CUDA(h, cudaMemset(h->d_err, 0, 4));
+        if (derr & DERR_MISSING_INTEGRAL) return set_err(h, PCI_E_MISSING_INTEGRAL, "Gint: integral is absent");
+        return set_err(h, PCI_E_INPUT, "Gint error: ma+mb /= mc+md (determinant list inconsistent)");
+    }
+    out.nnz = nnz;
+    out.val_f32 = value_prec == 32;
+    out.col = (int32_t *)dev_alloc(h, std::max<int64_t>(nnz, 1) * 4, &rc);
+    if (rc) return rc;
+    out.val = dev_alloc(h, std::max<int64_t>(nnz, 1) * (out.val_f32 ? 4 : 8), &rc);
+    if (rc) return rc;
+    PCI_CUDA(h, cudaMemsetAsync(d_counter, 0, 8, h->st));
+    if (value_prec == 32)
+        kf32<<<blocks, WARPS * 32, smem, h->st>>>(S, d_items, nit, d_counter, out.rowptr, out.col, (float *)out.val, nullptr);
+    else
+        kf64<<<blocks, WARPS * 32, smem, h->st>>>(S, d_items, nit, d_counter, out.rowptr, out.col, (double *)out.val, nullptr);
+    PCI_CUDA(h, cudaGetLastError());
+    cudaEventRecord(e2, h->st);
+    PCI_CUDA(h, cudaMemcpyAsync(hs, d_stats, sizeof(RowStats), cudaMemcpyDeviceToHost, h->st));
+    PCI_CUDA(h, cudaStreamSynchronize(h->st));
+    float t01 = 0, t12 = 0;
+    cudaEventElapsedTime(&t01, e0, e1);
+    cudaEventElapsedTime(&t12, e1, e2);
+    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
+    if (KIND == 0) {
+        h->st_formh_count = t01;
+        h->st_formh_fill = t12;
+        h->st_formh = t01 + t12;
+    } else {
+        h->st_formj = t01 + t12;
+    }
+    dev_free(cnt);
+    dev_free(d_stats);
+    dev_free(d_items);
+    return PCI_OK;
+}
+

@@ -2,6 +2,7 @@
 // CSR copy-out, and dispatch to the H-build, SpMM and Davidson units.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -63,7 +64,7 @@ DevSys make_devsys(const pci_gpu *h)
     S.nd = h->nd; S.gj = h->gj;
     S.occ = h->d_occ; S.conf_of = h->d_conf_of; S.conf_start = h->d_conf_start; S.conf_orb = h->d_conf_orb;
     S.adj_ptr = h->d_adj_ptr; S.adj = h->d_adj;
-    S.ms_orb = h->d_ms_orb; S.ms_jz = h->d_ms_jz; S.ms_type = h->d_ms_type;
+    S.ms_orb = h->d_ms_orb; S.ms_jz = h->d_ms_jz; S.ms_type = h->d_ms_type; S.msd = h->d_msd;
     S.orb_l = h->d_orb_l; S.orb_j = h->d_orb_j;
     S.h1 = h->d_h1; S.gaunt = h->d_gaunt; S.hkey = h->d_hkey; S.hval = h->d_hval;
     S.hmask = h->hcap ? h->hcap - 1 : 0;
@@ -88,7 +89,8 @@ static void free_basis(pci_gpu *h)
 {
     dev_free(h->d_occ); dev_free(h->d_conf_of); dev_free(h->d_conf_start); dev_free(h->d_conf_orb);
     dev_free(h->d_adj_ptr); dev_free(h->d_adj); dev_free(h->d_ms_orb); dev_free(h->d_ms_jz);
-    dev_free(h->d_ms_type); dev_free(h->d_orb_l); dev_free(h->d_orb_j);
+    dev_free(h->d_ms_type); dev_free(h->d_orb_l); dev_free(h->d_orb_j); dev_free(h->d_msd);
+    h->d_msd = nullptr;
     h->d_occ = nullptr; h->d_conf_of = nullptr; h->d_conf_start = nullptr; h->d_conf_orb = nullptr;
     h->d_adj_ptr = nullptr; h->d_adj = nullptr; h->d_ms_orb = nullptr; h->d_ms_jz = nullptr;
     h->d_ms_type = nullptr; h->d_orb_l = nullptr; h->d_orb_j = nullptr;
@@ -148,6 +150,10 @@ int pci_gpu_create(int32_t device, pci_gpu_t **out)
     int rc = 0;
     h->d_err = (unsigned int *)dev_alloc(h, 16, &rc);
     if (rc) { *out = h; return rc; }
+    if (const char *m = getenv("PCI_SPMM")) {
+        if (!strcmp(m, "full")) h->spmm_mode = 1;
+        else if (!strcmp(m, "lower")) h->spmm_mode = 2;
+    }
     cudaMemset(h->d_err, 0, 16);
     *out = h;
     return PCI_OK;
@@ -214,11 +220,18 @@ int pci_gpu_set_basis(pci_gpu_t *h, int32_t Ne, int64_t Nd, int32_t Nst, int32_t
     std::vector<int16_t> ms_orb(Nst);
     std::vector<int8_t> ms_jz(Nst), orb_l(Nsu), orb_j(Nsu);
     std::vector<uint8_t> ms_type(Nst);
+    std::vector<uint32_t> msd(Nst);
+    if (Nsu > 1024) return set_err(h, PCI_E_INPUT, "Nsu above 1024");
     for (int i = 0; i < Nst; i++) {
         ms_orb[i] = (int16_t)(Nh[i] - 1);
         ms_jz[i] = (int8_t)Jz[i];
         int j2 = Jj[Nh[i] - 1];
-        ms_type[i] = (uint8_t)(type_offset(j2) + (Jz[i] + j2) / 2);
+        int l = Ll[Nh[i] - 1];
+        int type = type_offset(j2) + (Jz[i] + j2) / 2;
+        if (j2 > 31 || l > 15 || type > 63) return set_err(h, PCI_E_INPUT, "orbital j or l out of range (2j <= 31, l <= 15)");
+        ms_type[i] = (uint8_t)type;
+        msd[i] = (uint32_t)(Nh[i] - 1) | ((uint32_t)type << 10) | ((uint32_t)(Jz[i] + 128) << 16) |
+                 ((uint32_t)l << 24) | ((uint32_t)((j2 - 1) / 2) << 28);
     }
     for (int o = 0; o < Nsu; o++) { orb_l[o] = (int8_t)Ll[o]; orb_j[o] = (int8_t)Jj[o]; }
     int rc;
@@ -229,6 +242,7 @@ int pci_gpu_set_basis(pci_gpu_t *h, int32_t Ne, int64_t Nd, int32_t Nst, int32_t
     if ((rc = upload(h, &h->d_ms_orb, ms_orb))) return rc;
     if ((rc = upload(h, &h->d_ms_jz, ms_jz))) return rc;
     if ((rc = upload(h, &h->d_ms_type, ms_type))) return rc;
+    if ((rc = upload(h, &h->d_msd, msd))) return rc;
     if ((rc = upload(h, &h->d_orb_l, orb_l))) return rc;
     if ((rc = upload(h, &h->d_orb_j, orb_j))) return rc;
     PCI_CUDA(h, cudaStreamSynchronize(h->st));

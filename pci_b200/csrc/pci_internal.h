@@ -38,6 +38,7 @@ struct DevSys {
     const int16_t *ms_orb;      // [nst] orbital (0-based) of each m-state
     const int8_t *ms_jz;        // [nst] 2m
     const uint8_t *ms_type;     // [nst] (j,m) type index into the Gaunt table
+    const uint32_t *msd;        // [nst] packed: orbital, type, 2m+128, l, (2j-1)/2
     const int8_t *orb_l;        // [nsu]
     const int8_t *orb_j;        // [nsu] 2j
     const double *h1;           // [nsu*nsu] one-electron integrals, 0 unless kappa equal
@@ -60,6 +61,8 @@ struct pci_gpu {
     std::vector<int32_t> h_ndc;       // host copy of Ndc
     std::vector<int32_t> h_orb_j, h_orb_l, h_orb_k;
     std::vector<int32_t> h_nh, h_jz;
+    std::vector<unsigned long long> h_rowwork;   // determinant pairs per row, per configuration
+    uint32_t *d_msd = nullptr;                   // packed m-state descriptors
     uint16_t *d_occ = nullptr;
     int32_t *d_conf_of = nullptr;
     int64_t *d_conf_start = nullptr;
@@ -90,6 +93,8 @@ struct pci_gpu {
     double st_formh = 0, st_formh_count = 0, st_formh_fill = 0, st_formj = 0;
     double st_dvd = 0, st_spmm = 0, st_spmm_calls = 0, st_init = 0;
     double st_adj = 0, st_pairs = 0, st_scanned = 0, st_launches = 0;
+    int spmm_mode = 0;        // 0 auto, 1 full symmetric copy, 2 lower triangle (env PCI_SPMM)
+    int spmm_lower_used = 0;
 };
 
 // error helpers
@@ -107,6 +112,10 @@ int ensure_tmp(pci_gpu *h, size_t bytes);
 DevSys make_devsys(const pci_gpu *h);
 
 // hbuild.cu
+struct RowStatsOut {
+    unsigned long long numzero = 0, pairs = 0, scanned = 0;
+    double hmin = 0.0;
+};
 int hb_build_hash(pci_gpu *h, int64_t ngint, int kbrt, int r2_is_f64, const void *rint2,
                   const int32_t *iint2, const int32_t *iint3);
 int hb_build_adjacency(pci_gpu *h);

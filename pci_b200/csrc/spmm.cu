@@ -12,6 +12,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <climits>
 
 #include "pci_internal.h"
 
@@ -170,6 +171,124 @@ __global__ void __launch_bounds__(256) k_spmm(const int64_t *__restrict__ rowptr
     }
 }
 
+// --------------------------------------------- lower-triangle SpMM ---
+//
+// Y += (H - hmin I) X from the stored lower triangle alone, for matrices too
+// large to hold twice.  One warp owns 32 consecutive rows (lane = row) and
+// walks the union of their sorted column lists in windows of WIN columns:
+// each lane consumes its row's entries inside the window, adding h x_k to a
+// register accumulator (row part) and h x_n into a shared-memory window
+// buffer (transpose part, k != n).  At the end of a window the buffer goes to
+// Y with one global atomic per (column, vector); the row accumulators go to Y
+// once at the end.  Rows of one configuration share their column structure,
+// so a window collects many transpose contributions per atomic.  Y must be
+// zero on entry.
+constexpr int LW_ROWS = 32;
+constexpr int LW_WIN = 32;
+constexpr int LW_WARPS = 4;
+
+// Transpose contributions inside a window are summed in shared memory as
+// 64-bit fixed point (scale 2^55, |window sum| < 256): integer atomics are
+// exact, so the window sums do not depend on the order lanes arrive in.
+constexpr double LW_SCALE = 36028797018963968.0;  // 2^55
+
+template <int NV, typename VT>
+__global__ void __launch_bounds__(LW_WARPS * 32) k_spmm_lower(const int64_t *__restrict__ rowptr,
+                                                               const int32_t *__restrict__ col,
+                                                               const VT *__restrict__ val, int64_t nd, double hmin,
+                                                               const double *__restrict__ X, int ldx, double *Y,
+                                                               int ldy, unsigned long long *counter)
+{
+    __shared__ unsigned long long tbuf[LW_WARPS][LW_WIN * NV];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned long long *tb = tbuf[w];
+    const int64_t nitems = (nd + LW_ROWS - 1) / LW_ROWS;
+    for (int i = lane; i < LW_WIN * NV; i += 32) tb[i] = 0ULL;
+    __syncwarp();
+    while (true) {
+        unsigned long long it = 0;
+        if (lane == 0) it = atomicAdd(counter, 1ULL);
+        it = __shfl_sync(FULL_MASK, it, 0);
+        if (it >= (unsigned long long)nitems) break;
+        const int64_t n = (int64_t)it * LW_ROWS + lane;
+        const bool mine = n < nd;
+        int64_t cur = mine ? rowptr[n] : 0, end = mine ? rowptr[n + 1] : 0;
+        double xn[NV], acc[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            xn[v] = mine ? X[n * ldx + v] : 0.0;
+            acc[v] = 0.0;
+        }
+        int ck = cur < end ? __ldg(&col[cur]) : INT_MAX;
+        while (true) {
+            int wmin = ck;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) wmin = min(wmin, __shfl_xor_sync(FULL_MASK, wmin, o));
+            if (wmin == INT_MAX) break;
+            const int wend = wmin + LW_WIN;
+            while (ck < wend) {
+                const double h0 = (double)__ldg(&val[cur]);
+                const double h = ck == n ? h0 - hmin : h0;
+                const double *xk = X + (int64_t)ck * ldx;
+#pragma unroll
+                for (int v = 0; v < NV; v++) acc[v] += h * __ldg(&xk[v]);
+                if (ck != n) {
+                    unsigned long long *t = tb + (ck - wmin) * NV;
+#pragma unroll
+                    for (int v = 0; v < NV; v++) atomicAdd(&t[v], (unsigned long long)__double2ll_rn(h * xn[v] * LW_SCALE));
+                }
+                cur++;
+                ck = cur < end ? __ldg(&col[cur]) : INT_MAX;
+            }
+            __syncwarp();
+            for (int i = lane; i < LW_WIN * NV; i += 32) {
+                const long long q = (long long)tb[i];
+                if (q != 0) {
+                    const int64_t k = wmin + i / NV;
+                    atomicAdd(&Y[k * ldy + (i % NV)], (double)q / LW_SCALE);
+                    tb[i] = 0ULL;
+                }
+            }
+            __syncwarp();
+        }
+        if (mine)
+#pragma unroll
+            for (int v = 0; v < NV; v++) atomicAdd(&Y[n * ldy + v], acc[v]);
+    }
+}
+
+__global__ void k_zero_block(double *Y, int ldy, int64_t nd, int nv)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nd * nv; i += (int64_t)gridDim.x * blockDim.x)
+        Y[(i / nv) * ldy + (i % nv)] = 0.0;
+}
+
+template <typename VT>
+static int spmm_lower_dispatch(pci_gpu *h, const double *X, int ldx, double *Y, int ldy, int nv, cudaStream_t st)
+{
+    const Csr &L = h->H;
+    int rc = 0;
+    if ((rc = ensure_tmp(h, 64))) return rc;
+    unsigned long long *counter = (unsigned long long *)h->d_tmp;
+    PCI_CUDA(h, cudaMemsetAsync(counter, 0, 8, st));
+    k_zero_block<<<148 * 8, 256, 0, st>>>(Y, ldy, L.nrows, nv);
+    const int blocks = 148 * 8;
+    const VT *val = (const VT *)L.val;
+#define CASE(N)                                                                                           \
+    case N:                                                                                               \
+        k_spmm_lower<N, VT><<<blocks, LW_WARPS * 32, 0, st>>>(L.rowptr, L.col, val, L.nrows, h->hmin, \
+                                                                      X, ldx, Y, ldy, counter);           \
+        break;
+    switch (nv) {
+        CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8)
+        CASE(9) CASE(10) CASE(11) CASE(12) CASE(13) CASE(14) CASE(15) CASE(16)
+    default: return set_err(h, PCI_E_INPUT, "SpMM supports 1..16 vectors");
+    }
+#undef CASE
+    PCI_CUDA(h, cudaGetLastError());
+    return PCI_OK;
+}
+
 template <typename VT, typename XT>
 static int spmm_dispatch(pci_gpu *h, const XT *X, int ldx, XT *Y, int ldy, int nv, cudaStream_t st)
 {
@@ -189,8 +308,27 @@ static int spmm_dispatch(pci_gpu *h, const XT *X, int ldx, XT *Y, int ldy, int n
     return PCI_OK;
 }
 
+// The full symmetric copy is used when it fits beside everything else on the
+// device (or PCI_SPMM=full); otherwise the lower-triangle kernel (or PCI_SPMM=lower).
+static bool use_lower(pci_gpu *h)
+{
+    if (h->spmm_mode == 2) return true;
+    if (h->spmm_mode == 1 || h->Hfull.rowptr) return false;
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    const size_t vs = h->H.val_f32 ? 4 : 8;
+    const size_t need = (size_t)(2 * h->H.nnz) * (4 + vs) + (size_t)(h->H.nrows + 1) * 16;
+    return need + ((size_t)2 << 30) > fr;
+}
+
 int sp_spmm(pci_gpu *h, const double *X, int ldx, double *Y, int ldy, int nv, cudaStream_t st)
 {
+    if (use_lower(h)) {
+        h->spmm_lower_used = 1;
+        return h->H.val_f32 ? spmm_lower_dispatch<float>(h, X, ldx, Y, ldy, nv, st)
+                            : spmm_lower_dispatch<double>(h, X, ldx, Y, ldy, nv, st);
+    }
+    h->spmm_lower_used = 0;
     int rc = sp_build_full(h);
     if (rc) return rc;
     if (h->Hfull.val_f32) return spmm_dispatch<float, double>(h, X, ldx, Y, ldy, nv, st);

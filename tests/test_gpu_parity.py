@@ -161,3 +161,23 @@ def test_bad_determinant_order_is_reported(engine):
     assert ei.value.code == 1
     _load(engine, s)   # the handle stays usable
     engine.form_h(64)
+
+
+@pytest.mark.parametrize("mode", ["lower", "full"])
+def test_davidson_spmm_paths(mode, monkeypatch):
+    """The lower-triangle SpMM (transpose part through shared-memory windows and
+    atomics) and the full symmetric copy give the same Davidson levels."""
+    from pci_b200.capi import Engine
+    monkeypatch.setenv("PCI_SPMM", mode)
+    name = "small3"
+    s = get_system(name)
+    (rp, col, val, nz, hmin, pairs), (jr, jc, jv) = oracle_h(name)
+    p = dict(s.params)
+    p.update(N_it=25, admix_crit=0.0)
+    ref = O.diag4(s.nd, (rp, col, val), hmin, (jr, jc, jv), p, s.ndc)
+    with Engine(0) as e:
+        e.load_system(s)
+        e.form_h(64)
+        e.form_j()
+        res = e.davidson(s.nd, Nlv=p["Nlv"], N_it=25, Crt4=p["Crt4"], MaxNd0=p["MaxNd0"], admix_crit=0.0)
+    assert np.max(np.abs(res["Tk"] - ref["Tk"])) <= 1e-8
