@@ -119,6 +119,13 @@ int pci_gpu_davidson(pci_gpu_t *h, const pci_dvd_params *p, const double *X0,
                      double *Tk, double *Tj, int32_t *Iconverge, double *X,
                      int32_t *iters, double *resid);
 
+/* Replaces: J_av (formj2.f90:355-387), the J of each vector from
+ * <x|J^2|x> over rows and columns 1..nlim of the resident J^2 matrix, as
+ * WriteFinalXIJ (pconf.F90:2566-2602) and FormB0 (davidson.f90:107-135) use
+ * it.  X is Nd x nv column-major on the host (1 <= nv <= 64); Tj[nv] receives
+ * J = (sqrt(1 + <x|J^2|x>) - 1) / 2. */
+int pci_gpu_j_av(pci_gpu_t *h, const double *X, int32_t nv, int64_t nlim, double *Tj);
+
 /* Per-stage device times (milliseconds) and counters of the last calls:
  * [0] FormH total (adjacency + count + fill), [1] FormH count pass,
  * [2] FormH fill pass, [3] FormJ, [4] Davidson total, [5] SpMM total in the

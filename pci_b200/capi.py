@@ -21,7 +21,7 @@ PCI_DVD_FP64, PCI_DVD_FP32 = 0, 1
 
 EXPORTS = ["pci_gpu_create", "pci_gpu_set_basis", "pci_gpu_set_integrals", "pci_gpu_form_h",
            "pci_gpu_form_j", "pci_gpu_csr_info", "pci_gpu_get_csr", "pci_gpu_set_csr",
-           "pci_gpu_davidson", "pci_gpu_stats", "pci_gpu_last_error", "pci_gpu_destroy"]
+           "pci_gpu_davidson", "pci_gpu_j_av", "pci_gpu_stats", "pci_gpu_last_error", "pci_gpu_destroy"]
 
 
 class PciError(RuntimeError):
@@ -58,6 +58,7 @@ def load(path: str = LIB):
     L.pci_gpu_get_csr.argtypes = [P, i32, P, P, P]
     L.pci_gpu_set_csr.argtypes = [P, i32, i64, i64, P, P, P, f64]
     L.pci_gpu_davidson.argtypes = [P, C.POINTER(DvdParams), P, P, P, P, P, C.POINTER(i32), P]
+    L.pci_gpu_j_av.argtypes = [P, P, i32, i64, P]
     L.pci_gpu_stats.argtypes = [P, P, i32]
     L.pci_gpu_stats.restype = i32
     L.pci_gpu_last_error.argtypes = [P]
@@ -172,6 +173,17 @@ class Engine:
         self._check(self.L.pci_gpu_davidson(self.h, C.byref(p), _p(x0), _p(Tk), _p(Tj), _p(ic), _p(X),
                                             C.byref(iters), _p(res)))
         return dict(Tk=Tk, Tj=Tj, Iconverge=ic, X=None if X is None else X.T, iterations=iters.value, resid=res)
+
+    def j_av(self, X, nlim=None):
+        """J of each column of X (Nd x nv) from <x|J^2|x> over rows/columns <= nlim."""
+        X = np.asarray(X, np.float64)
+        if X.ndim == 1:
+            X = X[:, None]
+        nd, nv = X.shape
+        xc = np.ascontiguousarray(X.T)        # column-major Nd x nv
+        out = np.zeros(nv)
+        self._check(self.L.pci_gpu_j_av(self.h, _p(xc), nv, nd if nlim is None else nlim, _p(out)))
+        return out
 
     def stats(self):
         out = np.zeros(12)

@@ -360,6 +360,25 @@ int pci_gpu_davidson(pci_gpu_t *h, const pci_dvd_params *p, const double *X0, do
     return dv_run(h, p, X0, Tk, Tj, Iconverge, X, iters, resid);
 }
 
+int pci_gpu_j_av(pci_gpu_t *h, const double *X, int32_t nv, int64_t nlim, double *Tj)
+{
+    if (!h) return PCI_E_INPUT;
+    cudaSetDevice(h->device);
+    if (!X || !Tj) return set_err(h, PCI_E_INPUT, "null array");
+    if (!h->J.rowptr) return set_err(h, PCI_E_STATE, "J_av before form_j");
+    if (nv < 1 || nv > 64) return set_err(h, PCI_E_INPUT, "J_av: nv must be 1..64");
+    const int64_t nd = h->J.nrows;
+    int rc = 0;
+    double *d = (double *)dev_alloc(h, (size_t)nd * nv * 8, &rc);
+    if (rc) return rc;
+    cudaError_t e = cudaMemcpyAsync(d, X, (size_t)nd * nv * 8, cudaMemcpyHostToDevice, h->st);
+    if (e != cudaSuccess) { dev_free(d); return cuda_err(h, e, "cudaMemcpyAsync"); }
+    rc = sp_jav_strided(h, d, 1, nd, nv, nlim, Tj);
+    cudaStreamSynchronize(h->st);
+    dev_free(d);
+    return rc;
+}
+
 int32_t pci_gpu_stats(pci_gpu_t *h, double *out, int32_t n)
 {
     if (!h || !out) return 0;

@@ -131,6 +131,7 @@ int sp_spmm(pci_gpu *h, const double *X, int ldx, double *Y, int ldy, int nv, cu
 int sp_spmm_f32(pci_gpu *h, const float *X, int ldx, float *Y, int ldy, int nv, cudaStream_t st);
 // y = J x restricted to rows/cols < nlim, returned as <x|J|x>
 int sp_jav(pci_gpu *h, const double *X, int ldx, int nv, int64_t nlim, double *out_host);
+int sp_jav_strided(pci_gpu *h, const double *X, int64_t sn, int64_t sv, int nv, int64_t nlim, double *out_host);
 void csr_free(Csr &c);
 
 // davidson.cu

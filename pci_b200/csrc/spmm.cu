@@ -345,9 +345,10 @@ int sp_spmm_f32(pci_gpu *h, const float *X, int ldx, float *Y, int ldy, int nv, 
 
 // ------------------------------------------------------------- J_av ---
 
-// sums[v] += sum over stored (n, k), n,k < nlim, of t x_k x_n (doubled off the diagonal)
+// sums[v] += sum over stored (n, k), n,k < nlim, of t x_k x_n (doubled off the
+// diagonal); element (n, v) of X is X[n*sn + v*sv].
 __global__ void k_jav(const int64_t *rowptr, const int32_t *col, const double *val, int64_t nlim,
-                      const double *X, int ldx, int nv, double *sums)
+                      const double *X, int64_t sn, int64_t sv, int nv, double *sums)
 {
     int lane = threadIdx.x & 31;
     int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -355,11 +356,11 @@ __global__ void k_jav(const int64_t *rowptr, const int32_t *col, const double *v
     for (int v = 0; v < nv; v++) {
         double acc = 0.0;
         for (int64_t n = warp; n < nlim; n += nwarps) {
-            double xn = X[n * ldx + v];
+            double xn = X[n * sn + v * sv];
             for (int64_t l = rowptr[n] + lane; l < rowptr[n + 1]; l += 32) {
                 int k = col[l];
                 if (k < nlim) {
-                    double r = val[l] * X[(int64_t)k * ldx + v] * xn;
+                    double r = val[l] * X[(int64_t)k * sn + v * sv] * xn;
                     if (k != n) r = r + r;
                     acc += r;
                 }
@@ -370,18 +371,25 @@ __global__ void k_jav(const int64_t *rowptr, const int32_t *col, const double *v
     }
 }
 
-int sp_jav(pci_gpu *h, const double *X, int ldx, int nv, int64_t nlim, double *out_host)
+int sp_jav_strided(pci_gpu *h, const double *X, int64_t sn, int64_t sv, int nv, int64_t nlim, double *out_host)
 {
     if (!h->J.rowptr) return set_err(h, PCI_E_STATE, "J^2 not formed");
+    if (nv < 1 || nv > 64) return set_err(h, PCI_E_INPUT, "J_av: nv must be 1..64");
+    if (nlim < 0 || nlim > h->J.nrows) return set_err(h, PCI_E_INPUT, "J_av: nlim outside 0..Nd");
     int rc = 0;
     if ((rc = ensure_tmp(h, 8 * 64))) return rc;
     double *sums = (double *)h->d_tmp;
     PCI_CUDA(h, cudaMemsetAsync(sums, 0, 8 * nv, h->st));
-    k_jav<<<148 * 4, 256, 0, h->st>>>(h->J.rowptr, h->J.col, (const double *)h->J.val, nlim, X, ldx, nv, sums);
+    k_jav<<<148 * 4, 256, 0, h->st>>>(h->J.rowptr, h->J.col, (const double *)h->J.val, nlim, X, sn, sv, nv, sums);
     PCI_CUDA(h, cudaGetLastError());
     std::vector<double> s(nv);
     PCI_CUDA(h, cudaMemcpyAsync(s.data(), sums, 8 * nv, cudaMemcpyDeviceToHost, h->st));
     PCI_CUDA(h, cudaStreamSynchronize(h->st));
     for (int v = 0; v < nv; v++) out_host[v] = 0.5 * (sqrt(1.0 + s[v]) - 1.0);
     return PCI_OK;
+}
+
+int sp_jav(pci_gpu *h, const double *X, int ldx, int nv, int64_t nlim, double *out_host)
+{
+    return sp_jav_strided(h, X, ldx, 1, nv, nlim, out_host);
 }

@@ -181,3 +181,20 @@ def test_davidson_spmm_paths(mode, monkeypatch):
         e.form_j()
         res = e.davidson(s.nd, Nlv=p["Nlv"], N_it=25, Crt4=p["Crt4"], MaxNd0=p["MaxNd0"], admix_crit=0.0)
     assert np.max(np.abs(res["Tk"] - ref["Tk"])) <= 1e-8
+
+
+@pytest.mark.parametrize("name", ["tiny", "small3"])
+def test_j_av_matches_oracle(engine, name):
+    """J_av over the resident J^2 against the oracle's restatement, full length and
+    restricted to the first rows (the FormB0 use on the initial block)."""
+    s = get_system(name)
+    _, (jr, jc, jv) = oracle_h(name)
+    _load(engine, s)
+    engine.form_j()
+    rng = np.random.default_rng(3)
+    X = rng.standard_normal((s.nd, 5))
+    X /= np.linalg.norm(X, axis=0)
+    for nlim in (s.nd, s.nd // 3):
+        got = engine.j_av(X, nlim)
+        ref = np.array([O.j_av(jr, jc, jv, X[:, v], nlim) for v in range(5)])
+        assert np.allclose(got, ref, rtol=1e-12, atol=1e-12)
