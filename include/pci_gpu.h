@@ -126,6 +126,24 @@ int pci_gpu_davidson(pci_gpu_t *h, const pci_dvd_params *p, const double *X0,
  * J = (sqrt(1 + <x|J^2|x>) - 1) / 2. */
 int pci_gpu_j_av(pci_gpu_t *h, const double *X, int32_t nv, int64_t nlim, double *Tj);
 
+/* No counterpart in the reference.  The J_av of pci_gpu_j_av for callers that
+ * cannot allocate device memory (a host that owns all device memory through
+ * its own pool or a framework's caching allocator, or a path where
+ * cudaMalloc's implicit synchronisation is not acceptable).  Every array is
+ * device memory the caller already holds: the J^2 matrix in the
+ * pci_gpu_get_csr layout (rowptr[nrows+1] 0-based prefix, col 1-based, val),
+ * X column-major with leading dimension ldx >= nrows, and Tj[nv] for the
+ * result.  No handle and no allocation: the only scratch is a static device
+ * array of 64 doubles, so nv is limited to 1..64 (larger nv returns
+ * PCI_E_INPUT).  Work is enqueued on `stream` (NULL = default stream) and not
+ * waited for.  All calls on a device share the scratch; calls that overlap on
+ * the GPU race.  The first call on a device resolves the scratch address and
+ * should come before any stream capture.  On error, errbuf (errlen bytes, may
+ * be NULL) receives a message. */
+int pci_gpu_j_av_noalloc(const int64_t *rowptr, const int32_t *col, const double *val, int64_t nrows,
+                         const double *X, int64_t ldx, int32_t nv, int64_t nlim, double *Tj,
+                         void *stream, char *errbuf, int32_t errlen);
+
 /* Per-stage device times (milliseconds) and counters of the last calls:
  * [0] FormH total (adjacency + count + fill), [1] FormH count pass,
  * [2] FormH fill pass, [3] FormJ, [4] Davidson total, [5] SpMM total in the
