@@ -1,0 +1,57 @@
+! ISO_C_BINDING interface to libpci_gpu.so (include/pci_gpu.h) for pconf.
+! Use it under #ifdef PCI_GPU in place of the FormH / FormJ / Diag4 calls at
+! pconf.F90:217-238 (see INTEGRATION.md for the call sites).  Indices and
+! arrays are passed exactly as pconf holds them (1-based, column-major).
+module pci_gpu_mod
+  use, intrinsic :: iso_c_binding
+  implicit none
+  type, bind(C) :: pci_dvd_params
+     integer(c_int32_t) :: Nlv, N_it, Kl4, Kv, Nc4, MaxNd0, mode, KXIJ
+     real(c_double)     :: Crt4, XJ_av, admix_crit
+  end type
+  interface
+     integer(c_int) function pci_gpu_create(device, h) bind(C)
+       import; integer(c_int32_t), value :: device; type(c_ptr) :: h
+     end function
+     integer(c_int) function pci_gpu_set_basis(h, Ne, Nd, Nst, Nsu, Nso, Nx, Mj, Iarr, Nh, Jz, &
+                                               Nn, Kk, Ll, Jj, Nc, Ndc, Gj) bind(C)
+       import; type(c_ptr), value :: h
+       integer(c_int32_t), value :: Ne, Nst, Nsu, Nso, Nx, Mj, Nc
+       integer(c_int64_t), value :: Nd
+       integer(c_int32_t) :: Iarr(*), Nh(*), Jz(*), Nn(*), Kk(*), Ll(*), Jj(*), Ndc(*)
+       real(c_double), value :: Gj
+     end function
+     integer(c_int) function pci_gpu_set_integrals(h, HintLUT, Nlx, nGauntLUT, GauntLUT, Ngint, kbrt, &
+                                                   r2_is_f64, Rint2, Iint2, Iint3) bind(C)
+       import; type(c_ptr), value :: h
+       real(c_double) :: HintLUT(*), GauntLUT(*)
+       integer(c_int32_t), value :: Nlx, kbrt, r2_is_f64
+       integer(c_int64_t), value :: nGauntLUT, Ngint
+       type(c_ptr), value :: Rint2
+       integer(c_int32_t) :: Iint2(*), Iint3(*)
+     end function
+     integer(c_int) function pci_gpu_form_h(h, value_prec, NumH, numzero, Hmin) bind(C)
+       import; type(c_ptr), value :: h; integer(c_int32_t), value :: value_prec
+       integer(c_int64_t) :: NumH, numzero; real(c_double) :: Hmin
+     end function
+     integer(c_int) function pci_gpu_form_j(h, NumJ) bind(C)
+       import; type(c_ptr), value :: h; integer(c_int64_t) :: NumJ
+     end function
+     integer(c_int) function pci_gpu_davidson(h, p, X0, Tk, Tj, Iconverge, X, iters, resid) bind(C)
+       import; type(c_ptr), value :: h; type(pci_dvd_params) :: p
+       type(c_ptr), value :: X0
+       real(c_double) :: Tk(*), Tj(*), X(*), resid(*)
+       integer(c_int32_t) :: Iconverge(*), iters
+     end function
+     integer(c_int) function pci_gpu_j_av(h, X, nv, nlim, Tj) bind(C)
+       import; type(c_ptr), value :: h; real(c_double) :: X(*), Tj(*)
+       integer(c_int32_t), value :: nv; integer(c_int64_t), value :: nlim
+     end function
+     type(c_ptr) function pci_gpu_last_error(h) bind(C)
+       import; type(c_ptr), value :: h
+     end function
+     subroutine pci_gpu_destroy(h) bind(C)
+       import; type(c_ptr), value :: h
+     end subroutine
+  end interface
+end module
