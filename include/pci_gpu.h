@@ -145,12 +145,15 @@ int pci_gpu_j_av_noalloc(const int64_t *rowptr, const int32_t *col, const double
                          void *stream, char *errbuf, int32_t errlen);
 
 /* Per-stage device times (milliseconds) and counters of the last calls:
- * [0] FormH total (adjacency + count + fill), [1] FormH count pass,
- * [2] FormH fill pass, [3] FormJ, [4] Davidson total, [5] SpMM total in the
- * last Davidson, [6] number of SpMM launches, [7] Init4 + DiagInitApprox,
- * [8] configuration adjacency build, [9] determinant pairs with difference
- * <= 2, [10] determinant pairs compared, [11] kernel launches of the last
- * FormH.  n is the capacity of `out`; returns the number written. */
+ * [0] FormH total (adjacency + count + fill + compaction), [1] FormH count
+ * pass (candidate bound in the single-evaluation build), [2] FormH fill
+ * pass, [3] FormJ, [4] Davidson total, [5] SpMM total in the last Davidson,
+ * [6] number of SpMM launches, [7] Init4 + DiagInitApprox, [8] configuration
+ * adjacency build, [9] determinant pairs with difference <= 2, [10]
+ * determinant pairs compared, [11] kernel launches of the last FormH,
+ * [12] FormH compaction, [13] 1 when the last FormH took the single-
+ * evaluation build, 0 for the two-pass build.  n is the capacity of `out`;
+ * returns the number written. */
 int32_t pci_gpu_stats(pci_gpu_t *h, double *out, int32_t n);
 
 const char *pci_gpu_last_error(pci_gpu_t *h);

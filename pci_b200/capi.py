@@ -188,8 +188,9 @@ class Engine:
         return out
 
     def stats(self):
-        out = np.zeros(12)
-        n = self.L.pci_gpu_stats(self.h, _p(out), 12)
+        out = np.zeros(14)
+        n = self.L.pci_gpu_stats(self.h, _p(out), 14)
         keys = ["formh_ms", "formh_count_ms", "formh_fill_ms", "formj_ms", "davidson_ms", "spmm_ms",
-                "spmm_calls", "init_ms", "adjacency_ms", "pairs", "scanned", "formh_launches"]
+                "spmm_calls", "init_ms", "adjacency_ms", "pairs", "scanned", "formh_launches",
+                "formh_compact_ms", "formh_single_eval"]
         return dict(zip(keys[:n], out[:n].tolist()))

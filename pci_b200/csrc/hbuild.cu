@@ -16,8 +16,11 @@
 // the warp looks them up once per tile into a shared-memory cache.  Pairs are
 // compared on occupation lists (Ne <= 8 m-states as uint16); non-zeros are
 // compacted per row with __match_any_sync/__ballot_sync/__popc so each row's
-// columns stay ascending.  Two passes: count (values evaluated, zeros
-// dropped) and, after a scan, fill straight into CSR.
+// columns stay ascending.  Two builds: single evaluation (count the
+// candidate pairs per row without evaluating them, evaluate once into
+// rows padded to that bound, squeeze the rows into CSR), taken when the
+// padded rows fit in device memory; otherwise two passes (count with values
+// evaluated and zeros dropped, then, after a scan, fill straight into CSR).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -138,6 +141,70 @@ int hb_build_hash(pci_gpu *h, int64_t ngint, int kbrt, int r2_is_f64, const void
     return PCI_OK;
 }
 
+// ----------------------------------------------------------- compaction ---
+
+// One warp per row: copy the row's entries from its padded slot to its CSR
+// position, relative to the chunk's first CSR position qa.
+template <typename VT>
+__global__ void k_compact_gather(const int64_t *pptr, const int64_t *rowptr, int64_t ra, int64_t rb, int64_t qa,
+                                 const int32_t *col, const VT *val, int32_t *tcol, VT *tval)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = ra + w; r < rb; r += nw) {
+        const int64_t src = pptr[r], dst = rowptr[r] - qa, n = rowptr[r + 1] - rowptr[r];
+        for (int64_t i = lane; i < n; i += 32) {
+            tcol[dst + i] = col[src + i];
+            tval[dst + i] = val[src + i];
+        }
+    }
+}
+
+int hb_compact(pci_gpu *h, const int64_t *pptr, const int64_t *rowptr, int64_t nrows, int32_t *col, void *val,
+               int vbytes, int64_t chunk)
+{
+    std::vector<int64_t> p(nrows + 1), q(nrows + 1);
+    PCI_CUDA(h, cudaMemcpyAsync(p.data(), pptr, (nrows + 1) * 8, cudaMemcpyDeviceToHost, h->st));
+    PCI_CUDA(h, cudaMemcpyAsync(q.data(), rowptr, (nrows + 1) * 8, cudaMemcpyDeviceToHost, h->st));
+    PCI_CUDA(h, cudaStreamSynchronize(h->st));
+    // rows that start where their padded slot starts are already in place
+    int64_t ra = 0;
+    while (ra < nrows && p[ra] == q[ra]) ra++;
+    if (q[nrows] == p[nrows]) return PCI_OK;
+    int64_t maxrow = 0;
+    for (int64_t r = ra; r < nrows; r++) maxrow = std::max(maxrow, q[r + 1] - q[r]);
+    chunk = std::max(chunk, maxrow);
+    int rc = 0;
+    int32_t *tcol = (int32_t *)dev_alloc(h, std::max<int64_t>(chunk, 1) * 4, &rc);
+    if (rc) return rc;
+    void *tval = dev_alloc(h, std::max<int64_t>(chunk, 1) * vbytes, &rc);
+    if (rc) { dev_free(tcol); return rc; }
+    while (ra < nrows) {
+        // largest rb with q[rb] - q[ra] <= chunk (at least one row)
+        int64_t rb = std::upper_bound(q.begin() + ra + 1, q.end(), q[ra] + chunk) - q.begin() - 1;
+        rb = std::max(rb, ra + 1);
+        const int64_t n = q[rb] - q[ra];
+        if (n > 0) {
+            if (vbytes == 4)
+                k_compact_gather<float><<<148 * 8, 256, 0, h->st>>>(pptr, rowptr, ra, rb, q[ra], col, (const float *)val,
+                                                                     tcol, (float *)tval);
+            else
+                k_compact_gather<double><<<148 * 8, 256, 0, h->st>>>(pptr, rowptr, ra, rb, q[ra], col,
+                                                                      (const double *)val, tcol, (double *)tval);
+            PCI_CUDA(h, cudaGetLastError());
+            h->st_formh_compact_launches += 1;
+            PCI_CUDA(h, cudaMemcpyAsync(col + q[ra], tcol, n * 4, cudaMemcpyDeviceToDevice, h->st));
+            PCI_CUDA(h, cudaMemcpyAsync((char *)val + q[ra] * vbytes, tval, n * vbytes, cudaMemcpyDeviceToDevice, h->st));
+        }
+        ra = rb;
+    }
+    PCI_CUDA(h, cudaStreamSynchronize(h->st));
+    dev_free(tcol);
+    dev_free(tval);
+    return PCI_OK;
+}
+
 // ------------------------------------------------------ per-Ne dispatch ---
 
 #define PCI_DECL_NE(n)                                                                   \
@@ -203,8 +270,9 @@ int hb_form_h(pci_gpu *h, int value_prec, int64_t *numh, int64_t *numzero, doubl
     h->st_formh += tadj;
     h->st_pairs = (double)hs.pairs;
     h->st_scanned = (double)hs.scanned;
-    // adjacency: 2 passes + scan (2 kernels); tiles: 2 passes + scan (2)
-    h->st_launches = 8;
+    // adjacency: 2 passes + scan (2 kernels); tiles: 2 passes + scan (2);
+    // the single-evaluation build adds a second scan and its compaction
+    h->st_launches = h->st_formh_padded ? 10 + h->st_formh_compact_launches : 8;
     csr_free(h->Hfull);
     h->numh = h->H.nnz;
     h->numzero = (int64_t)hs.numzero;

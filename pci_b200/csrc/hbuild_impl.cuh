@@ -660,11 +660,15 @@ __device__ __forceinline__ void eval_queue(const DevSys &S, WarpSmem *ws, const 
 // __match_any_sync + __ballot_sync, every row receiving its columns in
 // ascending order.
 // KIND 0: Hamiltonian; KIND 1: J^2 (diagonal tile only, nf in {0, 2}).
-// FILL 0: per-row counts into rowinfo; FILL 1: rowinfo is the CSR rowptr.
+// FILL 0: per-row non-zero counts into rowinfo (values evaluated).
+// FILL 1: rowinfo holds each row's first slot; non-zeros are written there
+//         and, when rowcnt_out is given, each row's count goes to rowcnt_out.
+// FILL 2: per-row candidate counts (difference <= 2) into rowinfo, nothing
+//         evaluated: the slot bound of the single-evaluation build.
 template <int NE, int KIND, int FILL, typename VT>
 __global__ void __launch_bounds__(WARPS * 32) k_tiles(DevSys S, const int4 *items, int64_t nitems,
                                                       unsigned long long *counter, int64_t *rowinfo, int32_t *col,
-                                                      VT *val, RowStats *stats)
+                                                      VT *val, RowStats *stats, int64_t *rowcnt_out)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
@@ -695,7 +699,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_tiles(DevSys S, const int4 *item
             for (int i = lane; i < nrc * NE; i += 32) ws->drow[i] = S.occ[rb * NE + i];
             for (int i = lane; i < nrc; i += 32) {
                 ws->rowcnt[i] = 0;
-                ws->rowbase[i] = FILL ? rowinfo[rb + i] : 0;
+                ws->rowbase[i] = FILL == 1 ? rowinfo[rb + i] : 0;
             }
             __syncwarp();
             for (int64_t a = a0; a < a1; a++) {
@@ -703,7 +707,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_tiles(DevSys S, const int4 *item
                 const int64_t k0 = S.conf_start[c2];
                 const int nk = (int)(S.conf_start[c2 + 1] - k0);
                 const bool diag = c2 == c1;
-                if (KIND == 0) {
+                if (KIND == 0 && FILL != 2) {
                     uint16_t o2[NE];
 #pragma unroll
                     for (int e = 0; e < NE; e++) o2[e] = S.conf_orb[(int64_t)c2 * NE + e];
@@ -737,6 +741,18 @@ __global__ void __launch_bounds__(WARPS * 32) k_tiles(DevSys S, const int4 *item
                             cand = KIND == 0 ? nf <= 2 : (nf == 0 || nf == 2);
                         }
                         const unsigned cm = __ballot_sync(FULL_MASK, cand);
+                        if (FILL == 2) {
+                            // the lanes of one row are a contiguous run; its first lane adds the run's count
+                            if (idx < np) {
+                                const int lo = max(r * nkc - base, 0), hi = min((r + 1) * nkc - base, 32);
+                                if (lane == lo) {
+                                    const unsigned run = (hi == 32 ? FULL_MASK : ((1u << hi) - 1u)) & ~((1u << lo) - 1u);
+                                    ws->rowcnt[r] += __popc(cm & run);
+                                }
+                            }
+                            __syncwarp();
+                            continue;
+                        }
                         if (cand) ws->queue[qn + __popc(cm & lt)] = ((uint32_t)r << 16) | (uint32_t)kk;
                         qn += __popc(cm);
                         __syncwarp();
@@ -751,8 +767,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_tiles(DevSys S, const int4 *item
                 }
             }
             __syncwarp();
-            if (!FILL)
+            if (FILL != 1)
                 for (int i = lane; i < nrc; i += 32) rowinfo[rb + i] = ws->rowcnt[i];
+            else if (rowcnt_out)
+                for (int i = lane; i < nrc; i += 32) rowcnt_out[rb + i] = ws->rowcnt[i];
             __syncwarp();
         }
     }
@@ -802,20 +820,51 @@ static inline void make_items(const pci_gpu *h, const std::vector<unsigned long 
     for (auto &p : tmp) items.push_back(p.second);
 }
 
+// Which FormH layout to build: the single-evaluation build (candidate
+// bound per row, values evaluated once into padded rows, then compacted)
+// needs slots for every candidate pair; the two-pass build (count, then
+// fill) needs exactly NumH slots but evaluates every value twice.
+// PCI_FORMH=exact|padded forces one; by default padded is taken when its
+// slots and the compaction buffer fit in free device memory.
+static inline int formh_mode_env()
+{
+    const char *e = getenv("PCI_FORMH");
+    if (!e) return -1;
+    if (!strcmp(e, "exact")) return 0;
+    if (!strcmp(e, "padded")) return 1;
+    return -1;
+}
+
+// Compaction buffer of the padded build, in entries.
+constexpr int64_t COMPACT_CHUNK = 1LL << 28;
+
 template <int NE, int KIND>
 static int rows_impl(pci_gpu *h, int value_prec, Csr &out, RowStats *hs)
 {
     int rc = 0;
     DevSys S = make_devsys(h);
     const int64_t nd = h->nd;
+    const int vb = value_prec == 32 ? 4 : 8;
     csr_free(out);
     out.nrows = nd;
+    int64_t *cnt = nullptr, *pptr = nullptr;
+    RowStats *d_stats = nullptr;
+    int4 *d_items = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
+    auto cleanup = [&](int code) {
+        dev_free(cnt); dev_free(pptr); dev_free(d_stats); dev_free(d_items);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (e2) cudaEventDestroy(e2);
+        if (e3) cudaEventDestroy(e3);
+        return code;
+    };
     out.rowptr = (int64_t *)dev_alloc(h, (nd + 1) * 8, &rc);
-    if (rc) return rc;
-    int64_t *cnt = (int64_t *)dev_alloc(h, (nd + 1) * 8, &rc);
-    if (rc) return rc;
-    RowStats *d_stats = (RowStats *)dev_alloc(h, sizeof(RowStats) + 16, &rc);
-    if (rc) { dev_free(cnt); return rc; }
+    if (rc) return cleanup(rc);
+    cnt = (int64_t *)dev_alloc(h, (nd + 1) * 8, &rc);
+    if (rc) return cleanup(rc);
+    d_stats = (RowStats *)dev_alloc(h, sizeof(RowStats) + 16, &rc);
+    if (rc) return cleanup(rc);
     unsigned long long *d_counter = (unsigned long long *)((char *)d_stats + sizeof(RowStats));
     RowStats init = {0, 0, 0, 0x7fffffffffffffffLL};
     PCI_CUDA(h, cudaMemcpyAsync(d_stats, &init, sizeof(RowStats), cudaMemcpyHostToDevice, h->st));
@@ -826,10 +875,12 @@ static int rows_impl(pci_gpu *h, int value_prec, Csr &out, RowStats *hs)
     auto kc32 = k_tiles<NE, KIND, 0, float>;
     auto kf64 = k_tiles<NE, KIND, 1, double>;
     auto kf32 = k_tiles<NE, KIND, 1, float>;
+    auto ksc = k_tiles<NE, KIND, 2, double>;
     cudaFuncSetAttribute(kc64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(kc32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(kf64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(kf32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(ksc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kc64, WARPS * 32, smem);
     int dev_sms = 148;
@@ -837,62 +888,122 @@ static int rows_impl(pci_gpu *h, int value_prec, Csr &out, RowStats *hs)
     const int blocks = dev_sms * std::max(per_sm, 1);
     std::vector<int4> items;
     make_items(h, h->h_rowwork, KIND, blocks * WARPS, items);
-    int4 *d_items = (int4 *)dev_alloc(h, std::max<size_t>(items.size(), 1) * sizeof(int4), &rc);
-    if (rc) { dev_free(cnt); dev_free(d_stats); return rc; }
+    d_items = (int4 *)dev_alloc(h, std::max<size_t>(items.size(), 1) * sizeof(int4), &rc);
+    if (rc) return cleanup(rc);
     PCI_CUDA(h, cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, h->st));
     const int64_t nit = (int64_t)items.size();
-    cudaEvent_t e0, e1, e2;
-    cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2);
-    cudaEventRecord(e0, h->st);
-    if (value_prec == 32) kc32<<<blocks, WARPS * 32, smem, h->st>>>(S, d_items, nit, d_counter, cnt, nullptr, nullptr, d_stats);
-    else kc64<<<blocks, WARPS * 32, smem, h->st>>>(S, d_items, nit, d_counter, cnt, nullptr, nullptr, d_stats);
-    PCI_CUDA(h, cudaGetLastError());
-    PCI_CUDA(h, cudaMemsetAsync(out.rowptr, 0, 8, h->st));
+    cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2); cudaEventCreate(&e3);
     size_t tb = 0;
     cub::DeviceScan::InclusiveSum(nullptr, tb, cnt, out.rowptr + 1, nd, h->st);
-    if ((rc = ensure_tmp(h, tb))) return rc;
-    cub::DeviceScan::InclusiveSum(h->d_tmp, tb, cnt, out.rowptr + 1, nd, h->st);
-    int64_t nnz = 0;
-    PCI_CUDA(h, cudaMemcpyAsync(&nnz, out.rowptr + nd, 8, cudaMemcpyDeviceToHost, h->st));
-    cudaEventRecord(e1, h->st);
-    PCI_CUDA(h, cudaStreamSynchronize(h->st));
-    unsigned int derr = 0;
-    PCI_CUDA(h, cudaMemcpy(&derr, h->d_err, 4, cudaMemcpyDeviceToHost));
-    if (derr) {
-        dev_free(cnt); dev_free(d_stats); dev_free(d_items);
+    if ((rc = ensure_tmp(h, tb))) return cleanup(rc);
+    auto check_derr = [&]() -> int {
+        unsigned int derr = 0;
+        PCI_CUDA(h, cudaMemcpy(&derr, h->d_err, 4, cudaMemcpyDeviceToHost));
+        if (!derr) return PCI_OK;
         PCI_CUDA(h, cudaMemset(h->d_err, 0, 4));
         if (derr & DERR_MISSING_INTEGRAL) return set_err(h, PCI_E_MISSING_INTEGRAL, "Gint: integral is absent");
         return set_err(h, PCI_E_INPUT, "Gint error: ma+mb /= mc+md (determinant list inconsistent)");
+    };
+    auto launch_fill = [&](int64_t *rowinfo, int64_t *rowcnt_out, RowStats *st) {
+        PCI_CUDA(h, cudaMemsetAsync(d_counter, 0, 8, h->st));
+        if (value_prec == 32)
+            kf32<<<blocks, WARPS * 32, smem, h->st>>>(S, d_items, nit, d_counter, rowinfo, out.col, (float *)out.val, st,
+                                                      rowcnt_out);
+        else
+            kf64<<<blocks, WARPS * 32, smem, h->st>>>(S, d_items, nit, d_counter, rowinfo, out.col, (double *)out.val, st,
+                                                      rowcnt_out);
+        PCI_CUDA(h, cudaGetLastError());
+        return PCI_OK;
+    };
+    const int forced = KIND == 0 ? formh_mode_env() : 0;
+    if (KIND == 0) {
+        h->st_formh_padded = 0;
+        h->st_formh_compact = 0;
+        h->st_formh_compact_launches = 0;
     }
-    out.nnz = nnz;
-    out.val_f32 = value_prec == 32;
-    out.col = (int32_t *)dev_alloc(h, std::max<int64_t>(nnz, 1) * 4, &rc);
-    if (rc) return rc;
-    out.val = dev_alloc(h, std::max<int64_t>(nnz, 1) * (out.val_f32 ? 4 : 8), &rc);
-    if (rc) return rc;
-    PCI_CUDA(h, cudaMemsetAsync(d_counter, 0, 8, h->st));
-    if (value_prec == 32)
-        kf32<<<blocks, WARPS * 32, smem, h->st>>>(S, d_items, nit, d_counter, out.rowptr, out.col, (float *)out.val, nullptr);
-    else
-        kf64<<<blocks, WARPS * 32, smem, h->st>>>(S, d_items, nit, d_counter, out.rowptr, out.col, (double *)out.val, nullptr);
-    PCI_CUDA(h, cudaGetLastError());
-    cudaEventRecord(e2, h->st);
+    float t01 = 0, t12 = 0, t23 = 0;
+    bool done = false;
+    cudaEventRecord(e0, h->st);
+    if (KIND == 0 && forced != 0) {
+        // Single evaluation: candidate bound per row, padded fill, compaction.
+        ksc<<<blocks, WARPS * 32, smem, h->st>>>(S, d_items, nit, d_counter, cnt, nullptr, nullptr, nullptr, nullptr);
+        PCI_CUDA(h, cudaGetLastError());
+        pptr = (int64_t *)dev_alloc(h, (nd + 1) * 8, &rc);
+        if (rc) return cleanup(rc);
+        PCI_CUDA(h, cudaMemsetAsync(pptr, 0, 8, h->st));
+        cub::DeviceScan::InclusiveSum(h->d_tmp, tb, cnt, pptr + 1, nd, h->st);
+        int64_t ncand = 0;
+        PCI_CUDA(h, cudaMemcpyAsync(&ncand, pptr + nd, 8, cudaMemcpyDeviceToHost, h->st));
+        PCI_CUDA(h, cudaStreamSynchronize(h->st));
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        const int64_t chunk = std::min<int64_t>(COMPACT_CHUNK, std::max<int64_t>(ncand, 1));
+        const double need = (double)(ncand + chunk) * (4 + vb) + (double)(nd + 1) * 8 + (512.0 * (1 << 20));
+        if (forced == 1 || need <= (double)fr) {
+            out.nnz = ncand;
+            out.val_f32 = value_prec == 32;
+            out.col = (int32_t *)dev_alloc(h, std::max<int64_t>(ncand, 1) * 4, &rc);
+            if (rc) return cleanup(rc);
+            out.val = dev_alloc(h, std::max<int64_t>(ncand, 1) * vb, &rc);
+            if (rc) return cleanup(rc);
+            cudaEventRecord(e1, h->st);
+            if ((rc = launch_fill(pptr, cnt, d_stats))) return cleanup(rc);
+            cudaEventRecord(e2, h->st);
+            cub::DeviceScan::InclusiveSum(h->d_tmp, tb, cnt, out.rowptr + 1, nd, h->st);
+            PCI_CUDA(h, cudaMemsetAsync(out.rowptr, 0, 8, h->st));
+            PCI_CUDA(h, cudaStreamSynchronize(h->st));
+            if ((rc = check_derr())) return cleanup(rc);
+            if ((rc = hb_compact(h, pptr, out.rowptr, nd, out.col, out.val, vb, chunk))) return cleanup(rc);
+            PCI_CUDA(h, cudaMemcpyAsync(&out.nnz, out.rowptr + nd, 8, cudaMemcpyDeviceToHost, h->st));
+            cudaEventRecord(e3, h->st);
+            PCI_CUDA(h, cudaStreamSynchronize(h->st));
+            cudaEventElapsedTime(&t01, e0, e1);
+            cudaEventElapsedTime(&t12, e1, e2);
+            cudaEventElapsedTime(&t23, e2, e3);
+            h->st_formh_padded = 1;
+            h->st_formh_compact = t23;
+            done = true;
+        } else {
+            // does not fit: the two-pass build below (the scan time is kept in the count figure)
+            dev_free(pptr);
+            pptr = nullptr;
+            PCI_CUDA(h, cudaMemsetAsync(d_counter, 0, 8, h->st));
+            PCI_CUDA(h, cudaMemcpyAsync(d_stats, &init, sizeof(RowStats), cudaMemcpyHostToDevice, h->st));
+        }
+    }
+    if (!done) {
+        if (value_prec == 32)
+            kc32<<<blocks, WARPS * 32, smem, h->st>>>(S, d_items, nit, d_counter, cnt, nullptr, nullptr, d_stats, nullptr);
+        else
+            kc64<<<blocks, WARPS * 32, smem, h->st>>>(S, d_items, nit, d_counter, cnt, nullptr, nullptr, d_stats, nullptr);
+        PCI_CUDA(h, cudaGetLastError());
+        PCI_CUDA(h, cudaMemsetAsync(out.rowptr, 0, 8, h->st));
+        cub::DeviceScan::InclusiveSum(h->d_tmp, tb, cnt, out.rowptr + 1, nd, h->st);
+        int64_t nnz = 0;
+        PCI_CUDA(h, cudaMemcpyAsync(&nnz, out.rowptr + nd, 8, cudaMemcpyDeviceToHost, h->st));
+        cudaEventRecord(e1, h->st);
+        PCI_CUDA(h, cudaStreamSynchronize(h->st));
+        if ((rc = check_derr())) return cleanup(rc);
+        out.nnz = nnz;
+        out.val_f32 = value_prec == 32;
+        out.col = (int32_t *)dev_alloc(h, std::max<int64_t>(nnz, 1) * 4, &rc);
+        if (rc) return cleanup(rc);
+        out.val = dev_alloc(h, std::max<int64_t>(nnz, 1) * vb, &rc);
+        if (rc) return cleanup(rc);
+        if ((rc = launch_fill(out.rowptr, nullptr, nullptr))) return cleanup(rc);
+        cudaEventRecord(e2, h->st);
+        PCI_CUDA(h, cudaStreamSynchronize(h->st));
+        cudaEventElapsedTime(&t01, e0, e1);
+        cudaEventElapsedTime(&t12, e1, e2);
+    }
     PCI_CUDA(h, cudaMemcpyAsync(hs, d_stats, sizeof(RowStats), cudaMemcpyDeviceToHost, h->st));
     PCI_CUDA(h, cudaStreamSynchronize(h->st));
-    float t01 = 0, t12 = 0;
-    cudaEventElapsedTime(&t01, e0, e1);
-    cudaEventElapsedTime(&t12, e1, e2);
-    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
     if (KIND == 0) {
         h->st_formh_count = t01;
         h->st_formh_fill = t12;
-        h->st_formh = t01 + t12;
+        h->st_formh = t01 + t12 + t23;
     } else {
         h->st_formj = t01 + t12;
     }
-    dev_free(cnt);
-    dev_free(d_stats);
-    dev_free(d_items);
-    return PCI_OK;
+    return cleanup(PCI_OK);
 }
-

@@ -93,6 +93,7 @@ struct pci_gpu {
     double st_formh = 0, st_formh_count = 0, st_formh_fill = 0, st_formj = 0;
     double st_dvd = 0, st_spmm = 0, st_spmm_calls = 0, st_init = 0;
     double st_adj = 0, st_pairs = 0, st_scanned = 0, st_launches = 0;
+    double st_formh_compact = 0, st_formh_padded = 0, st_formh_compact_launches = 0;
     int spmm_mode = 0;        // 0 auto, 1 full symmetric copy, 2 lower triangle (env PCI_SPMM)
     int spmm_lower_used = 0;
 };
@@ -119,6 +120,11 @@ struct RowStatsOut {
 int hb_build_hash(pci_gpu *h, int64_t ngint, int kbrt, int r2_is_f64, const void *rint2,
                   const int32_t *iint2, const int32_t *iint3);
 int hb_build_adjacency(pci_gpu *h);
+// Squeeze the padded rows of the single-evaluation FormH (row r's entries at
+// pptr[r], rowptr[r+1]-rowptr[r] of them) into plain CSR order in place,
+// through a buffer of `chunk` entries.
+int hb_compact(pci_gpu *h, const int64_t *pptr, const int64_t *rowptr, int64_t nrows, int32_t *col, void *val,
+               int vbytes, int64_t chunk);
 int hb_form_h(pci_gpu *h, int value_prec, int64_t *numh, int64_t *numzero, double *hmin);
 int hb_form_j(pci_gpu *h, int64_t *numj);
 double host_gaunt(int nlx, const double *lut, int64_t nlut, int k, double xj1, double xm1,

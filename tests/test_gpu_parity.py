@@ -30,12 +30,17 @@ def _load(engine, s):
     engine.load_system(s)
 
 
+@pytest.mark.parametrize("build", ["padded", "exact"])
 @pytest.mark.parametrize("name", SYSTEMS)
-def test_form_h_bit_exact(engine, name):
+def test_form_h_bit_exact(engine, name, build, monkeypatch):
+    """Both FormH builds: single evaluation into padded rows + compaction,
+    and the two-pass count/fill build."""
     s = get_system(name)
     (rp, col, val, nz, hmin, pairs), _ = oracle_h(name)
     _load(engine, s)
+    monkeypatch.setenv("PCI_FORMH", build)
     numh, numzero, ghmin = engine.form_h(64)
+    assert engine.stats()["formh_single_eval"] == (1.0 if build == "padded" else 0.0)
     grp, gcol, gval = engine.get_csr(0)
     assert numh == rp[-1]
     assert numzero == nz
@@ -45,11 +50,13 @@ def test_form_h_bit_exact(engine, name):
     assert np.array_equal(gval.view(np.int64), val.view(np.int64))   # bit-identical
 
 
+@pytest.mark.parametrize("build", ["padded", "exact"])
 @pytest.mark.parametrize("name", ["small3", "small4"])
-def test_form_h_fp32_storage(engine, name):
+def test_form_h_fp32_storage(engine, name, build, monkeypatch):
     s = get_system(name)
     (rp, col, val, nz, hmin, pairs), _ = oracle_h(name)
     _load(engine, s)
+    monkeypatch.setenv("PCI_FORMH", build)
     numh, numzero, ghmin = engine.form_h(32)
     grp, gcol, gval = engine.get_csr(0)
     assert np.array_equal(grp, rp) and np.array_equal(gcol, col)
