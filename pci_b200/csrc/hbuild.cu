@@ -143,8 +143,15 @@ int hb_build_hash(pci_gpu *h, int64_t ngint, int kbrt, int r2_is_f64, const void
 
 // ----------------------------------------------------------- compaction ---
 
+// Smallest gap (entries) worth a direct in-place move; below it rows go
+// through the buffer.  Zeros are spread over the rows, so the gap grows with
+// the position and only the first rows need the buffer.
+constexpr int64_t COMPACT_DIRECT_MIN = 1LL << 20;
+
 // One warp per row: copy the row's entries from its padded slot to its CSR
-// position, relative to the chunk's first CSR position qa.
+// position, relative to the chunk's first CSR position qa.  The source and
+// destination may be the same arrays as long as the chunk's destination
+// range ends before its source range starts.
 template <typename VT>
 __global__ void k_compact_gather(const int64_t *pptr, const int64_t *rowptr, int64_t ra, int64_t rb, int64_t qa,
                                  const int32_t *col, const VT *val, int32_t *tcol, VT *tval)
@@ -154,7 +161,17 @@ __global__ void k_compact_gather(const int64_t *pptr, const int64_t *rowptr, int
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t r = ra + w; r < rb; r += nw) {
         const int64_t src = pptr[r], dst = rowptr[r] - qa, n = rowptr[r + 1] - rowptr[r];
-        for (int64_t i = lane; i < n; i += 32) {
+        int64_t i = lane;
+        // four loads of each array in flight per lane before the stores
+        for (; i + 96 < n; i += 128) {
+            int32_t c[4];
+            VT v[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) { c[u] = col[src + i + 32 * u]; v[u] = val[src + i + 32 * u]; }
+#pragma unroll
+            for (int u = 0; u < 4; u++) { tcol[dst + i + 32 * u] = c[u]; tval[dst + i + 32 * u] = v[u]; }
+        }
+        for (; i < n; i += 32) {
             tcol[dst + i] = col[src + i];
             tval[dst + i] = val[src + i];
         }
@@ -175,12 +192,32 @@ int hb_compact(pci_gpu *h, const int64_t *pptr, const int64_t *rowptr, int64_t n
     int64_t maxrow = 0;
     for (int64_t r = ra; r < nrows; r++) maxrow = std::max(maxrow, q[r + 1] - q[r]);
     chunk = std::max(chunk, maxrow);
+    // the buffer lives in the handle's scratch (kept across calls); values
+    // first so both arrays stay aligned
     int rc = 0;
-    int32_t *tcol = (int32_t *)dev_alloc(h, std::max<int64_t>(chunk, 1) * 4, &rc);
-    if (rc) return rc;
-    void *tval = dev_alloc(h, std::max<int64_t>(chunk, 1) * vbytes, &rc);
-    if (rc) { dev_free(tcol); return rc; }
+    if ((rc = ensure_tmp(h, (size_t)chunk * (vbytes + 4) + 256))) return rc;
+    void *tval = h->d_tmp;
+    int32_t *tcol = (int32_t *)((char *)h->d_tmp + (((size_t)chunk * vbytes + 255) & ~(size_t)255));
     while (ra < nrows) {
+        // Direct move: once the gap p[ra] - q[ra] left by the zeros dropped
+        // so far covers a whole run of rows, their CSR range ends before
+        // their padded range starts and they move in place without a buffer.
+        const int64_t gap = p[ra] - q[ra];
+        if (gap >= COMPACT_DIRECT_MIN) {
+            int64_t rb = std::upper_bound(q.begin() + ra + 1, q.end(), q[ra] + gap) - q.begin() - 1;
+            if (rb > ra) {
+                if (vbytes == 4)
+                    k_compact_gather<float><<<148 * 8, 256, 0, h->st>>>(pptr, rowptr, ra, rb, 0, col, (const float *)val,
+                                                                         col, (float *)val);
+                else
+                    k_compact_gather<double><<<148 * 8, 256, 0, h->st>>>(pptr, rowptr, ra, rb, 0, col,
+                                                                          (const double *)val, col, (double *)val);
+                PCI_CUDA(h, cudaGetLastError());
+                h->st_formh_compact_launches += 1;
+                ra = rb;
+                continue;
+            }
+        }
         // largest rb with q[rb] - q[ra] <= chunk (at least one row)
         int64_t rb = std::upper_bound(q.begin() + ra + 1, q.end(), q[ra] + chunk) - q.begin() - 1;
         rb = std::max(rb, ra + 1);
@@ -200,8 +237,6 @@ int hb_compact(pci_gpu *h, const int64_t *pptr, const int64_t *rowptr, int64_t n
         ra = rb;
     }
     PCI_CUDA(h, cudaStreamSynchronize(h->st));
-    dev_free(tcol);
-    dev_free(tval);
     return PCI_OK;
 }
 

@@ -47,10 +47,13 @@ __device__ __forceinline__ double d_lookup(const DevSys &S, int iac, int ibd, in
     return 0.0;
 }
 
-// Per-warp cache of the radial integrals one configuration tile needs,
-// direct-mapped by the same key hash; filled warp-synchronously at tile start
-// (one writer per slot), read-only while the tile's pairs are evaluated.
-constexpr int CACHE_SLOTS = 128;
+// Per-warp cache of the radial integrals one generic configuration tile
+// needs, direct-mapped by the key hash; cleared and filled warp-synchronously
+// at tile start (one writer per slot), read-only while the tile's pairs are
+// evaluated.  A key that lost its slot is looked up in the global table, so
+// a collision costs time, never correctness.
+constexpr int CACHE_SLOTS_LOG2 = 6;
+constexpr int CACHE_SLOTS = 1 << CACHE_SLOTS_LOG2;
 struct TileCache {
     unsigned long long key[CACHE_SLOTS];
     double val[CACHE_SLOTS * 2];
@@ -59,21 +62,8 @@ struct TileCache {
 __device__ __forceinline__ int cache_slot(unsigned long long key)
 {
     const unsigned a = (unsigned)(key >> 32), b = (unsigned)key;
-    return (int)((a * 0x9E3779B1u + b * 0x85EBCA77u) >> 25) & (CACHE_SLOTS - 1);
+    return (int)((a * 0x9E3779B1u + b * 0x85EBCA77u) >> (32 - CACHE_SLOTS_LOG2)) & (CACHE_SLOTS - 1);
 }
-
-// Term lists of a tile whose two configurations differ by two orbitals
-// (A -> B): every candidate pair there is an nf = 2 element
-// Gint(q1,q2,p1,p2) with argument orbitals (B0,B1,A0,A1), so the allowed k
-// values and radial integrals of its direct and exchange sums are the same
-// for the whole tile.
-constexpr int KLIST = 16;
-struct TilePlan {
-    int kind;   // 2: two-orbital tile with lists below; -1: evaluate generically
-    int nd, nx;
-    int kd[KLIST], kx[KLIST];
-    double rd[KLIST], rx[KLIST];
-};
 
 __device__ __forceinline__ double d_lookup_c(const DevSys &S, const TileCache *tc, int iac, int ibd, int comp)
 {
@@ -84,6 +74,34 @@ __device__ __forceinline__ double d_lookup_c(const DevSys &S, const TileCache *t
     }
     return d_lookup(S, iac, ibd, comp);
 }
+
+// Term lists of one Gint(a,b,c,d) orbital quadruple: the k values of its
+// direct (a,b,c,d) and exchange (a,b,d,c) sums that pass the parity rules, in
+// ascending k, with the Gaunt-table block offset k * ntype^2 of each term and
+// its radial integral.  Everything Gint sums except the two Gaunt factors
+// depends only on the four orbitals, so a tile evaluates every element of a
+// quadruple from these lists.
+constexpr int KTERMS = 8;
+struct QuadTerms {
+    int nd, nx;
+    int god[KTERMS], gox[KTERMS];
+    double rd[KTERMS], rx[KTERMS];
+};
+
+// Tile kinds.  TILE_TWO: the configurations differ by two orbitals
+// (A0,A1 -> B0,B1), every candidate is an nf = 2 element with orbitals
+// (B0,B1,A0,A1), t[0].  TILE_ONE: they differ by one orbital (A0 -> B0); for
+// each distinct spectator orbital s (spec[i]) t[2i] serves the nf = 1 terms
+// Gint(q,x,p,x) with orbitals (B0,s,A0,s) and t[2i+1] the nf = 2 elements
+// with orbitals (sorted(B0,s), sorted(A0,s)).  TILE_GENERIC: per-element
+// Gint through the tile cache.
+constexpr int TILE_GENERIC = -1, TILE_ONE = 1, TILE_TWO = 2;
+constexpr int MAXSPEC = 3;
+struct TilePlan {
+    int nspec, a0, b0;
+    int spec[MAXSPEC];
+    QuadTerms t[2 * MAXSPEC];
+};
 
 // Packed per-m-state descriptor (built by pci_gpu_set_basis): orbital
 // (bits 0-9), (j,m) type of the Gaunt table (10-15), 2m + 128 (16-23),
@@ -203,6 +221,7 @@ template <int NE>
 struct Diff {
     int nf;
     int p1, p2, q1, q2;  // m-states: det1 (row) earlier/later, det2 (column) earlier/later
+    int ip1, ip2, jp1, jp2;  // their positions in the two occupation lists
     int is;
 };
 
@@ -218,6 +237,7 @@ __device__ __forceinline__ Diff<NE> d_diff(const uint16_t *d1, const uint16_t *d
     Diff<NE> r;
     r.nf = NE - __popc(ma);
     r.p1 = r.p2 = r.q1 = r.q2 = -1;
+    r.ip1 = r.ip2 = r.jp1 = r.jp2 = 0;
     r.is = 1;
     if (r.nf == 1 || r.nf == 2) {
         unsigned ua = (~ma) & ((1u << NE) - 1), ub = (~mb) & ((1u << NE) - 1);
@@ -225,11 +245,15 @@ __device__ __forceinline__ Diff<NE> d_diff(const uint16_t *d1, const uint16_t *d
         int par = ip1 + jp1;
         r.p1 = d1[ip1];
         r.q1 = d2[jp1];
+        r.ip1 = ip1;
+        r.jp1 = jp1;
         if (r.nf == 2) {
             int ip2 = 31 - __clz(ua), jp2 = 31 - __clz(ub);
             par += ip2 + jp2;
             r.p2 = d1[ip2];
             r.q2 = d2[jp2];
+            r.ip2 = ip2;
+            r.jp2 = jp2;
         }
         r.is = (par & 1) ? -1 : 1;
     }
@@ -400,7 +424,7 @@ static __device__ int quad_keys(const DevSys &S, int na, int nb, int nc, int nd,
     return n;
 }
 
-constexpr int TILE_KEYS = 160;
+constexpr int TILE_KEYS = 96;
 
 // Warp-synchronous fill of the tile cache for configurations with sorted
 // orbital lists o1 (rows) and o2 (columns), CompD(o1, o2) <= 2.  The keys are
@@ -412,14 +436,16 @@ constexpr int TILE_KEYS = 160;
 //            orbital pair of the configuration.
 // Keys that miss the cache fall back to the global table, so a dropped or
 // evicted key costs time, never correctness.
-// Lane-parallel term list of a two-orbital tile: lanes 0-15 take the direct
-// sum's k = kmin + lane, lanes 16-31 the exchange sum's; valid terms are
-// compacted in ascending k.  False if a needed integral is absent or a k
-// range does not fit, so the caller falls back to the generic evaluation.
-static __device__ bool plan_two_orbital(const DevSys &S, TilePlan *plan, int A0, int A1, int B0, int B1, int lane)
+// Lane-parallel term lists of one orbital quadruple (a,b,c,d), built by the
+// 16 lanes [base, base+16): lanes base..base+7 take the direct sum's k values
+// kmin', kmin'+2, ... (kmin' the first k with the parity of la+lc), lanes
+// base+8..base+15 the exchange sum's.  Returns (warp-uniformly) false if a
+// needed integral is absent or a sum has more than KTERMS terms.
+static __device__ bool plan_quad(const DevSys &S, QuadTerms *P, int qa, int qb, int qc, int qd, int base, int lane)
 {
-    const int ii = lane >> 4, kk = lane & 15;
-    int a = B0, b = B1, c = ii ? A1 : A0, d = ii ? A0 : A1;
+    const bool mine = lane >= base && lane < base + 16;
+    const int ii = (lane >> 3) & 1, kk = lane & 7;
+    int a = qa, b = qb, c = ii ? qd : qc, d = ii ? qc : qd;
     const int la = S.orb_l[a], lb = S.orb_l[b], lc = S.orb_l[c], ld = S.orb_l[d];
     const int ja = S.orb_j[a], jb = S.orb_j[b], jc = S.orb_j[c], jd = S.orb_j[d];
     int t;
@@ -429,9 +455,10 @@ static __device__ bool plan_two_orbital(const DevSys &S, TilePlan *plan, int A0,
     if (a == b && c > d) { t = c; c = d; d = t; }
     const int kmin = max(abs(ja - jc) / 2, abs(jb - jd) / 2);
     const int kmax = min((ja + jc) / 2, (jb + jd) / 2);
-    const int k = kmin + kk;
+    const int k0 = kmin + ((kmin + la + lc) & 1);
+    const int k = k0 + 2 * kk;
     const bool par = ((la + lb + lc + ld) & 1) == 0;
-    const bool valid = par && k <= kmax && ((k + la + lc) & 1) == 0;
+    const bool valid = mine && par && k <= kmax;
     bool found = true;
     double r = 0.0;
     if (valid) {
@@ -447,25 +474,70 @@ static __device__ bool plan_two_orbital(const DevSys &S, TilePlan *plan, int A0,
         }
     }
     const unsigned vm = __ballot_sync(FULL_MASK, valid);
-    const unsigned bad = __ballot_sync(FULL_MASK, (valid && !found) || (par && kk == 15 && k < kmax));
-    const unsigned half = ii ? 0xffff0000u : 0x0000ffffu;
-    const int pos = __popc(vm & half & ((1u << lane) - 1));
+    const unsigned bad = __ballot_sync(FULL_MASK, (valid && !found) ||
+                                                  (mine && par && kk == KTERMS - 1 && k + 2 <= kmax));
+    const unsigned grp = 0xffu << (lane & ~7);
+    const int pos = __popc(vm & grp & ((1u << lane) - 1));
     if (valid) {
-        if (ii == 0) { plan->kd[pos] = k; plan->rd[pos] = r; }
-        else { plan->kx[pos] = k; plan->rx[pos] = r; }
+        if (ii == 0) { P->god[pos] = k * S.ntype * S.ntype; P->rd[pos] = r; }
+        else { P->gox[pos] = k * S.ntype * S.ntype; P->rx[pos] = r; }
     }
-    if (lane == 0) {
-        plan->nd = __popc(vm & 0x0000ffffu);
-        plan->nx = __popc(vm & 0xffff0000u);
-        plan->kind = bad ? -1 : 2;
+    if (lane == base) {
+        P->nd = __popc(vm & (0xffu << base));
+        P->nx = __popc(vm & (0xffu << (base + 8)));
     }
     __syncwarp();
     return bad == 0;
 }
 
+// Gint(a,b,c,d) of m-states with Gaunt types (ta,tb,tc,td) from the term
+// lists of their orbital quadruple, in d_gint's operation order: direct terms
+// e + ((1*G(k,ta,tc))*G(k,td,tb))*R, then exchange terms
+// e + ((-1*G(k,ta,td))*G(k,tc,tb))*R.  The Gaunt factors of the first four
+// terms of both sums are loaded before any is used.
+__device__ __forceinline__ double plan_gint(const DevSys &S, const QuadTerms &P, int ta, int tb, int tc, int td)
+{
+    const int nt = S.ntype;
+    const int oac = ta * nt + tc, odb = td * nt + tb, oad = ta * nt + td, ocb = tc * nt + tb;
+    const double *G = S.gaunt;
+    double a1[4], a2[4], b1[4], b2[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        a1[u] = a2[u] = b1[u] = b2[u] = 0.0;
+        if (u < P.nd) { a1[u] = __ldg(G + P.god[u] + oac); a2[u] = __ldg(G + P.god[u] + odb); }
+        if (u < P.nx) { b1[u] = __ldg(G + P.gox[u] + oad); b2[u] = __ldg(G + P.gox[u] + ocb); }
+    }
+    double e = 0.0;
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+        if (u < P.nd) e = e + ((1 * a1[u]) * a2[u]) * P.rd[u];
+    for (int i = 4; i < P.nd; i++) {
+        const double g1 = __ldg(G + P.god[i] + oac), g2 = __ldg(G + P.god[i] + odb);
+        e = e + ((1 * g1) * g2) * P.rd[i];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+        if (u < P.nx) e = e + ((-1 * b1[u]) * b2[u]) * P.rx[u];
+    for (int i = 4; i < P.nx; i++) {
+        const double g1 = __ldg(G + P.gox[i] + oad), g2 = __ldg(G + P.gox[i] + ocb);
+        e = e + ((-1 * g1) * g2) * P.rx[i];
+    }
+    return e;
+}
+
+// Prepare a tile for configurations with sorted orbital lists o1 (rows) and
+// o2 (columns), CompD(o1, o2) <= 2: term lists for two- and one-orbital
+// tiles (without the Breit term), otherwise the tile cache holding the keys
+// of every Gint call an element of the tile can make:
+//   CompD 2: Gint(q1,q2,p1,p2) with orbitals (b1,b2,a1,a2);
+//   CompD 1: Gint(q,x,p,x) and the two-m-state case with a spectator s:
+//            orbitals (c,s,a,s) for every spectator orbital s;
+//   CompD 0: Gint(x,y,x,y) and same-configuration doubles: (s,t,s,t) for every
+//            orbital pair of the configuration.
+// Returns the tile kind (warp-uniform).
 template <int NE>
-__device__ void fill_tile_cache(const DevSys &S, TileCache *tc, TilePlan *plan, unsigned long long *keys,
-                                const uint16_t *o1, const uint16_t *o2, int lane)
+__device__ int prepare_tile(const DevSys &S, TileCache *tc, TilePlan *plan, unsigned long long *keys,
+                            const uint16_t *o1, const uint16_t *o2, int lane)
 {
     // multiset differences of the two orbital lists (every lane; NE <= 8)
     int A[NE], B[NE], common[NE], na = 0, nb = 0, ncommon = 0;
@@ -479,11 +551,42 @@ __device__ void fill_tile_cache(const DevSys &S, TileCache *tc, TilePlan *plan, 
         while (i < NE) A[na++] = o1[i++];
         while (j < NE) B[nb++] = o2[j++];
     }
-    if (na == 2 && !S.kbrt) {
-        if (plan_two_orbital(S, plan, A[0], A[1], B[0], B[1], lane)) return;
-    } else if (lane == 0) {
-        plan->kind = -1;
+    if (S.plans && na == 2) {
+        if (plan_quad(S, &plan->t[0], B[0], B[1], A[0], A[1], 0, lane)) return TILE_TWO;
+    } else if (S.plans && na == 1) {
+        int spec[MAXSPEC], ns = 0;
+        bool fits = true;
+        for (int x = 0; x < ncommon; x++) {
+            if (ns > 0 && spec[ns - 1] == common[x]) continue;   // common is sorted
+            if (ns == MAXSPEC) { fits = false; break; }
+            spec[ns++] = common[x];
+        }
+        if (fits) {
+            const int a0 = A[0], b0 = B[0];
+            bool ok = true;
+            for (int x = 0; x < ns; x++) {
+                // one pass per spectator: lanes 0-15 build the one-m-state lists
+                // (B0,s,A0,s), lanes 16-31 the two-m-state lists
+                const int sp = spec[x];
+                const bool lo = lane < 16;
+                const int qa = lo ? b0 : min(b0, sp), qb = lo ? sp : max(b0, sp);
+                const int qc = lo ? a0 : min(a0, sp), qd = lo ? sp : max(a0, sp);
+                ok = plan_quad(S, &plan->t[2 * x + (lo ? 0 : 1)], qa, qb, qc, qd, lo ? 0 : 16, lane) && ok;
+            }
+            if (ok) {
+                if (lane == 0) {
+                    plan->nspec = ns;
+                    plan->a0 = a0;
+                    plan->b0 = b0;
+                    for (int x = 0; x < ns; x++) plan->spec[x] = spec[x];
+                }
+                __syncwarp();
+                return TILE_ONE;
+            }
+        }
     }
+    // generic tile: clear the cache (term lists may have overwritten it), list the keys, fill
+    for (int t = lane; t < CACHE_SLOTS; t += 32) tc->key[t] = 0ULL;
     int nkeys = 0;
     if (lane == 0) {
         if (na == 2) {
@@ -533,8 +636,7 @@ __device__ void fill_tile_cache(const DevSys &S, TileCache *tc, TilePlan *plan, 
         }
         __syncwarp();
     }
-    if (lane == 0) plan->kind = -1;
-    __syncwarp();
+    return TILE_GENERIC;
 }
 
 // ------------------------------------------------------------ tile pass ---
@@ -561,17 +663,35 @@ static inline double key_to_double(long long k)
 constexpr int TR = 64;   // rows of c1 per chunk
 constexpr int TK = 64;   // columns of c2 per chunk
 constexpr int WARPS = 8;
+// Resident blocks per SM the tile kernel is compiled for (caps registers at
+// 65536 / (256 * blocks)).
+#ifndef PCI_TILES_MIN_BLOCKS
+#define PCI_TILES_MIN_BLOCKS 3
+#endif
 constexpr int QCAP = 64;
 
+// Per-warp shared memory, occupation lists sized for NE electrons.
+template <int NE>
 struct WarpSmem {
-    TileCache tc;
-    TilePlan plan;
-    unsigned long long keys[TILE_KEYS];
+    union {
+        TileCache tc;    // generic tiles
+        TilePlan plan;   // one- and two-orbital tiles
+    } c;
     int64_t rowbase[TR];
     int32_t rowcnt[TR];
-    uint32_t queue[QCAP];   // candidate pairs (row << 16 | column) in tile order
-    uint16_t drow[TR * PCI_NE_MAX];
-    uint16_t dcol[TK * PCI_NE_MAX];
+    uint16_t drow[TR * NE];
+    uint16_t orow[TR * NE];  // orbital of each row m-state
+    uint8_t trow[TR * NE];   // Gaunt-table type of each row m-state
+    union {
+        // radial keys of a generic tile: used only while its cache is
+        // filled, before its columns are staged
+        unsigned long long keys[TILE_KEYS];
+        struct {
+            uint32_t queue[QCAP];   // candidate pairs (row << 16 | column) in tile order
+            uint16_t dcol[TK * NE];
+            uint8_t tcol[TK * NE];
+        } t;
+    } u;
 };
 
 struct Tally {
@@ -582,7 +702,7 @@ struct Tally {
 // Evaluate the first `cnt` queued pairs (one per lane) and write or count the
 // non-zeros.  Rows receive their columns in queue order, which is ascending.
 template <int NE, int KIND, int FILL, typename VT>
-__device__ __forceinline__ void eval_queue(const DevSys &S, WarpSmem *ws, const TileCache *tc, int cnt,
+__device__ __forceinline__ void eval_queue(const DevSys &S, WarpSmem<NE> *ws, int tkind, int cnt,
                                            int64_t rabs0, int64_t kabs0, int32_t *col, VT *val, Tally &ty,
                                            int lane)
 {
@@ -592,36 +712,51 @@ __device__ __forceinline__ void eval_queue(const DevSys &S, WarpSmem *ws, const 
     double v = 0.0;
     int64_t k = 0;
     if (lane < cnt) {
-        uint32_t e = ws->queue[lane];
+        uint32_t e = ws->u.t.queue[lane];
         r = (int)(e >> 16);
         const int kk = (int)(e & 0xffffu);
         k = kabs0 + kk;
         uint16_t d1[NE], d2[NE];
 #pragma unroll
-        for (int q = 0; q < NE; q++) { d1[q] = ws->drow[r * NE + q]; d2[q] = ws->dcol[kk * NE + q]; }
+        for (int q = 0; q < NE; q++) { d1[q] = ws->drow[r * NE + q]; d2[q] = ws->u.t.dcol[kk * NE + q]; }
         Diff<NE> df = d_diff<NE>(d1, d2);
         if (KIND == 0) {
             ty.npairs++;
-            if (ws->plan.kind == 2) {
-                // Gint(q1,q2,p1,p2) from the tile's term lists, same operation order as d_gint
-                const int tq1 = (int)((__ldg(&S.msd[df.q1]) >> 10) & 63u), tq2 = (int)((__ldg(&S.msd[df.q2]) >> 10) & 63u);
-                const int tp1 = (int)((__ldg(&S.msd[df.p1]) >> 10) & 63u), tp2 = (int)((__ldg(&S.msd[df.p2]) >> 10) & 63u);
-                const TilePlan &P = ws->plan;
-                double e = 0.0;
-                for (int i = 0; i < P.nd; i++) {
-                    const int kq = P.kd[i];
-                    const double g1 = d_gaunt(S, kq, tq1, tp1), g2 = d_gaunt(S, kq, tp2, tq2);
-                    e = e + ((1 * g1) * g2) * P.rd[i];
-                }
-                for (int i = 0; i < P.nx; i++) {
-                    const int kq = P.kx[i];
-                    const double g1 = d_gaunt(S, kq, tq1, tp2), g2 = d_gaunt(S, kq, tp1, tq2);
-                    e = e + ((-1 * g1) * g2) * P.rx[i];
-                }
-                v = 0.0 + e * df.is;
+            if (tkind == TILE_TWO) {
+                // Gint(q1,q2,p1,p2), orbitals (B0,B1,A0,A1)
+                const int tq1 = ws->u.t.tcol[kk * NE + df.jp1], tq2 = ws->u.t.tcol[kk * NE + df.jp2];
+                const int tp1 = ws->trow[r * NE + df.ip1], tp2 = ws->trow[r * NE + df.ip2];
+                v = 0.0 + plan_gint(S, ws->c.plan.t[0], tq1, tq2, tp1, tp2) * df.is;
                 if (S.gj != 0.0) v = v + S.gj * d_fj2_two(S, df.is, df.q1, df.p1, df.q2, df.p2);
+            } else if (tkind == TILE_ONE) {
+                const TilePlan &P = ws->c.plan;
+                if (df.nf == 2) {
+                    // Gint(q1,q2,p1,p2): one electron moved A0 -> B0, one changed m in spectator orbital s
+                    const int s2 = ws->orow[r * NE + df.ip1] + ws->orow[r * NE + df.ip2] - P.a0;
+                    int x = 0;
+                    while (x + 1 < P.nspec && P.spec[x] != s2) x++;
+                    const int tq1 = ws->u.t.tcol[kk * NE + df.jp1], tq2 = ws->u.t.tcol[kk * NE + df.jp2];
+                    const int tp1 = ws->trow[r * NE + df.ip1], tp2 = ws->trow[r * NE + df.ip2];
+                    v = 0.0 + plan_gint(S, P.t[2 * x + 1], tq1, tq2, tp1, tp2) * df.is;
+                    if (S.gj != 0.0) v = v + S.gj * d_fj2_two(S, df.is, df.q1, df.p1, df.q2, df.p2);
+                } else {
+                    // nf = 1: sum of Gint(q,x,p,x) over the spectators x of det1, then Hint(q,p)
+                    const int tq = ws->u.t.tcol[kk * NE + df.jp1], tp = ws->trow[r * NE + df.ip1];
+                    double t = 0.0;
+#pragma unroll
+                    for (int iq = 0; iq < NE; iq++) {
+                        if (iq != df.ip1) {
+                            const int so = ws->orow[r * NE + iq];
+                            int x = 0;
+                            while (x + 1 < P.nspec && P.spec[x] != so) x++;
+                            const int tx = ws->trow[r * NE + iq];
+                            t = t + plan_gint(S, P.t[2 * x], tq, tx, tp, tx) * df.is;
+                        }
+                    }
+                    v = t + d_hint(S, ms_get(S, df.q1), ms_get(S, df.p1)) * df.is;
+                }
             } else {
-                v = d_hmltn<NE>(S, tc, d1, df);
+                v = d_hmltn<NE>(S, &ws->c.tc, d1, df);
             }
             if (v != 0.0) nz = true; else ty.nzero++;
         } else {
@@ -666,16 +801,15 @@ __device__ __forceinline__ void eval_queue(const DevSys &S, WarpSmem *ws, const 
 // FILL 2: per-row candidate counts (difference <= 2) into rowinfo, nothing
 //         evaluated: the slot bound of the single-evaluation build.
 template <int NE, int KIND, int FILL, typename VT>
-__global__ void __launch_bounds__(WARPS * 32) k_tiles(DevSys S, const int4 *items, int64_t nitems,
+__global__ void __launch_bounds__(WARPS * 32, PCI_TILES_MIN_BLOCKS) k_tiles(DevSys S, const int4 *items, int64_t nitems,
                                                       unsigned long long *counter, int64_t *rowinfo, int32_t *col,
                                                       VT *val, RowStats *stats, int64_t *rowcnt_out)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
-    WarpSmem *ws = reinterpret_cast<WarpSmem *>(smem_raw) + (threadIdx.x >> 5);
-    const TileCache *tc = KIND == 0 ? &ws->tc : nullptr;
+    WarpSmem<NE> *ws = reinterpret_cast<WarpSmem<NE> *>(smem_raw) + (threadIdx.x >> 5);
     if (KIND == 0)
-        for (int i = lane; i < CACHE_SLOTS; i += 32) ws->tc.key[i] = 0ULL;
+        for (int i = lane; i < CACHE_SLOTS; i += 32) ws->c.tc.key[i] = 0ULL;
     __syncwarp();
     Tally ty = {0, 0, 0, INFINITY};
     const unsigned lt = (1u << lane) - 1;
@@ -696,7 +830,15 @@ __global__ void __launch_bounds__(WARPS * 32) k_tiles(DevSys S, const int4 *item
         for (int rc = 0; rc < nr; rc += TR) {
             const int nrc = min(TR, nr - rc);
             const int64_t rb = r0 + rc;   // absolute index of the chunk's first row
-            for (int i = lane; i < nrc * NE; i += 32) ws->drow[i] = S.occ[rb * NE + i];
+            for (int i = lane; i < nrc * NE; i += 32) {
+                const uint16_t m = S.occ[rb * NE + i];
+                ws->drow[i] = m;
+                if (FILL != 2) {
+                    const uint32_t w = __ldg(&S.msd[m]);
+                    ws->trow[i] = (uint8_t)((w >> 10) & 63u);
+                    ws->orow[i] = (uint16_t)(w & 1023u);
+                }
+            }
             for (int i = lane; i < nrc; i += 32) {
                 ws->rowcnt[i] = 0;
                 ws->rowbase[i] = FILL == 1 ? rowinfo[rb + i] : 0;
@@ -707,17 +849,22 @@ __global__ void __launch_bounds__(WARPS * 32) k_tiles(DevSys S, const int4 *item
                 const int64_t k0 = S.conf_start[c2];
                 const int nk = (int)(S.conf_start[c2 + 1] - k0);
                 const bool diag = c2 == c1;
+                int tkind = TILE_GENERIC;
                 if (KIND == 0 && FILL != 2) {
                     uint16_t o2[NE];
 #pragma unroll
                     for (int e = 0; e < NE; e++) o2[e] = S.conf_orb[(int64_t)c2 * NE + e];
-                    fill_tile_cache<NE>(S, &ws->tc, &ws->plan, ws->keys, o1, o2, lane);
+                    tkind = prepare_tile<NE>(S, &ws->c.tc, &ws->c.plan, ws->u.keys, o1, o2, lane);
                 }
                 for (int kc = 0; kc < nk; kc += TK) {
                     const int nkc = min(TK, nk - kc);
                     if (diag && k0 + kc > rb + nrc - 1) break;  // whole chunk above the diagonal
                     __syncwarp();
-                    for (int i = lane; i < nkc * NE; i += 32) ws->dcol[i] = S.occ[(k0 + kc) * NE + i];
+                    for (int i = lane; i < nkc * NE; i += 32) {
+                        const uint16_t m = S.occ[(k0 + kc) * NE + i];
+                        ws->u.t.dcol[i] = m;
+                        if (FILL != 2) ws->u.t.tcol[i] = (uint8_t)((__ldg(&S.msd[m]) >> 10) & 63u);
+                    }
                     __syncwarp();
                     const int np = nrc * nkc;
                     int qn = 0;
@@ -730,7 +877,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_tiles(DevSys S, const int4 *item
                             ty.nscan++;
                             uint16_t d1[NE], d2[NE];
 #pragma unroll
-                            for (int e = 0; e < NE; e++) { d1[e] = ws->drow[r * NE + e]; d2[e] = ws->dcol[kk * NE + e]; }
+                            for (int e = 0; e < NE; e++) { d1[e] = ws->drow[r * NE + e]; d2[e] = ws->u.t.dcol[kk * NE + e]; }
                             unsigned ma = 0;
 #pragma unroll
                             for (int i = 0; i < NE; i++)
@@ -753,17 +900,17 @@ __global__ void __launch_bounds__(WARPS * 32) k_tiles(DevSys S, const int4 *item
                             __syncwarp();
                             continue;
                         }
-                        if (cand) ws->queue[qn + __popc(cm & lt)] = ((uint32_t)r << 16) | (uint32_t)kk;
+                        if (cand) ws->u.t.queue[qn + __popc(cm & lt)] = ((uint32_t)r << 16) | (uint32_t)kk;
                         qn += __popc(cm);
                         __syncwarp();
                         if (qn >= 32) {
-                            eval_queue<NE, KIND, FILL, VT>(S, ws, tc, 32, rb, k0 + kc, col, val, ty, lane);
-                            if (lane < qn - 32) ws->queue[lane] = ws->queue[32 + lane];
+                            eval_queue<NE, KIND, FILL, VT>(S, ws, tkind, 32, rb, k0 + kc, col, val, ty, lane);
+                            if (lane < qn - 32) ws->u.t.queue[lane] = ws->u.t.queue[32 + lane];
                             qn -= 32;
                             __syncwarp();
                         }
                     }
-                    if (qn > 0) eval_queue<NE, KIND, FILL, VT>(S, ws, tc, qn, rb, k0 + kc, col, val, ty, lane);
+                    if (qn > 0) eval_queue<NE, KIND, FILL, VT>(S, ws, tkind, qn, rb, k0 + kc, col, val, ty, lane);
                 }
             }
             __syncwarp();
@@ -836,7 +983,7 @@ static inline int formh_mode_env()
 }
 
 // Compaction buffer of the padded build, in entries.
-constexpr int64_t COMPACT_CHUNK = 1LL << 28;
+constexpr int64_t COMPACT_CHUNK = 1LL << 24;
 
 template <int NE, int KIND>
 static int rows_impl(pci_gpu *h, int value_prec, Csr &out, RowStats *hs)
@@ -870,7 +1017,7 @@ static int rows_impl(pci_gpu *h, int value_prec, Csr &out, RowStats *hs)
     PCI_CUDA(h, cudaMemcpyAsync(d_stats, &init, sizeof(RowStats), cudaMemcpyHostToDevice, h->st));
     PCI_CUDA(h, cudaMemsetAsync(d_counter, 0, 8, h->st));
     PCI_CUDA(h, cudaMemsetAsync(cnt, 0, (nd + 1) * 8, h->st));
-    const size_t smem = sizeof(WarpSmem) * WARPS;
+    const size_t smem = sizeof(WarpSmem<NE>) * WARPS;
     auto kc64 = k_tiles<NE, KIND, 0, double>;
     auto kc32 = k_tiles<NE, KIND, 0, float>;
     auto kf64 = k_tiles<NE, KIND, 1, double>;

@@ -61,6 +61,9 @@ DevSys make_devsys(const pci_gpu *h)
     memset(&S, 0, sizeof(S));
     S.ne = h->ne; S.nst = h->nst; S.nsu = h->nsu; S.nso = h->nso; S.nx = h->nx; S.mj = h->mj; S.nc = h->nc;
     S.nlx = h->nlx; S.kbrt = h->kbrt; S.kdim = h->kdim; S.ntype = h->ntype;
+    // per-tile term lists take the m-states of one orbital to precede those of
+    // every later orbital (Nh non-decreasing) and carry no Breit term
+    S.plans = (h->kbrt == 0 && std::is_sorted(h->h_nh.begin(), h->h_nh.end())) ? 1 : 0;
     S.nd = h->nd; S.gj = h->gj;
     S.occ = h->d_occ; S.conf_of = h->d_conf_of; S.conf_start = h->d_conf_start; S.conf_orb = h->d_conf_orb;
     S.adj_ptr = h->d_adj_ptr; S.adj = h->d_adj;

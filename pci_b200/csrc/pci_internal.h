@@ -27,6 +27,7 @@ struct Csr {
 // Everything the H-build kernels read; plain pointers so it can be passed by value.
 struct DevSys {
     int ne, nst, nsu, nso, nx, mj, nc, nlx, kbrt, kdim, ntype;
+    int plans;   // per-tile term lists allowed: no Breit term, m-states numbered orbital by orbital
     int64_t nd;
     double gj;
     const uint16_t *occ;        // [nd*ne] 0-based m-state, ascending per determinant
