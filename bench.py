@@ -52,6 +52,13 @@ def parse():
     return ap.parse_args()
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) the fill kernel
+# moves per stored element, from an ncu capture of the same kernel on the mid
+# system (NumH 1.64e8: 358 MB read + 1985 MB written); the full-size launch
+# is too large to capture and its traffic grows with the stored elements.
+FILL_DRAM_BYTES_PER_NNZ = (358.172416e6 + 1985.190e6) / 164067833
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -261,7 +268,9 @@ def run_ours(args):
         "formh_build": "single evaluation (candidate bound, padded fill, compaction)" if single
                        else "two passes (count, fill)",
         "roofline": {"bound": "hbm", "kernel": "k_tiles fill pass", "achieved": achieved, "peak": peak,
-                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": FILL_DRAM_BYTES_PER_NNZ * numh, "traffic_note": "ncu DRAM bytes per stored element "
+                     "of the fill kernel on the mid system, scaled by NumH",
                      "algorithmic_bytes": int(fill_bytes)},
         "gpu_launches": launches,
         "clocks": clk,
