@@ -114,7 +114,12 @@ int pci_gpu_set_csr(pci_gpu_t *h, int32_t which, int64_t Nd, int64_t nnz, const 
  * the Davidson module (davidson.f90).  X0 (Nd x Nlv column-major, Kl4 = 2) may
  * be NULL.  Outputs: Tk (energies, -(E + Hmin)), Tj (J of each level, J_av),
  * Iconverge, X (Nd x Nlv column-major eigenvectors, may be NULL), the
- * iteration count and, if non-NULL, the final residual norms (length Nlv). */
+ * iteration count and, if non-NULL, the final residual norms (length Nlv).
+ * Kv = 3 selects initial vectors with J = XJ_av, averages the diagonal over
+ * configurations (AvgDiag) and filters new vectors onto J = XJ_av (Prj_J with
+ * the terms of pci_gpu_jterms); if fewer than Nlv initial vectors have that
+ * J, the reference lowers Nlv, and the levels past that number come back with
+ * Iconverge = -1 and zero Tk, Tj and X. */
 int pci_gpu_davidson(pci_gpu_t *h, const pci_dvd_params *p, const double *X0,
                      double *Tk, double *Tj, int32_t *Iconverge, double *X,
                      int32_t *iters, double *resid);
@@ -143,6 +148,13 @@ int pci_gpu_j_av(pci_gpu_t *h, const double *X, int32_t nv, int64_t nlim, double
 int pci_gpu_j_av_noalloc(const int64_t *rowptr, const int32_t *col, const double *val, int64_t nrows,
                          const double *X, int64_t ldx, int32_t nv, int64_t nlim, double *Tj,
                          void *stream, char *errbuf, int32_t errlen);
+
+/* Jt(1:Njd) of the basis set by pci_gpu_set_basis: the sorted 2J values of
+ * the terms its configurations hold, as Dinit lists them
+ * (src/determinants.f90:227-325); Prj_J of the Kv = 3 Davidson filters
+ * them.  Copies up to cap values into out (may be NULL) and returns Njd, or
+ * -1 before set_basis. */
+int32_t pci_gpu_jterms(pci_gpu_t *h, int32_t *out, int32_t cap);
 
 /* Per-stage device times (milliseconds) and counters of the last calls:
  * [0] FormH total (adjacency + count + fill + compaction), [1] FormH count

@@ -220,6 +220,49 @@ def j_av(rowptr, col, val, x, nx):
     return lib().orc_j_av(rowptr.size - 1, _ptr(rowptr), _ptr(col), _ptr(val), _ptr(x), nx)
 
 
+def j_terms(basis, configs, mj):
+    """Jt(1:Njd), the sorted 2J values of the terms present, as Dinit finds
+    them (src/determinants.f90:227-325): for every configuration that has
+    determinants with 2M = mj, count its determinants nmj(im) with
+    2M = mj + 2(im-1) >= mj, peel terms off from the largest im down, and keep
+    each new 2J = mj + 2(im-1) once.  ``configs`` as in
+    pci_b200.system.enumerate_determinants; determinants are enumerated
+    explicitly (small systems only)."""
+    import itertools
+    jt = []
+    for conf in configs:
+        shells = [(ni, nq) for ni, nq in conf if nq > 0]
+        per_shell = []
+        for ni, nq in shells:
+            j2 = int(basis.jj[ni - 1])
+            ms = list(range(-j2, j2 + 1, 2))
+            per_shell.append([sum(c) for c in itertools.combinations(ms, nq)])
+        nmj = {}
+        ndi = 0
+        for combo in itertools.product(*per_shell):
+            m = sum(combo)
+            if m == mj:
+                ndi += 1
+            if m >= mj:
+                im = (m - mj) // 2 + 1
+                nmj[im] = nmj.get(im, 0) + 1
+        if ndi == 0:
+            continue
+        imax = max(nmj)
+        cnt = [0] * (imax + 1)
+        for im, c in nmj.items():
+            cnt[im] = c
+        for im in range(imax, 0, -1):
+            n = cnt[im]
+            if n != 0:
+                mt = (im - 1) * 2 + mj
+                for j in range(1, im + 1):
+                    cnt[j] -= n
+                if mt not in jt:
+                    jt.append(mt)
+    return sorted(jt)
+
+
 def calc_nd0(ndc, nc4, max_nd0):
     """calcNd0, src/determinants.f90:22-45 (kCSF = 0)."""
     ic1, n2, n1, n0 = 0, 0, 0, max_nd0 + 1
@@ -237,11 +280,12 @@ class DavidsonResult(dict):
     pass
 
 
-def diag4(nd, H, hmin, J, params, ndc, mxmpy_threads=1, log=None, timing=None):
+def diag4(nd, H, hmin, J, params, ndc, mxmpy_threads=1, log=None, timing=None, jt=None):
     """Restatement of Diag4 (src/pconf.F90:1993-2264) with Init4, DiagInitApprox,
     FormB0, Ortn, Mxmpy, FormP, Dvdsn, FormB/FormBskip and WriteFinalXIJ from
-    src/davidson.f90 (npes = 1, Kv = 4 or 3 without Prj_J filtering of new
-    vectors).  H and J are (rowptr, col, val) lower-triangle CSR with 1-based
+    src/davidson.f90 (npes = 1).  Kv = 3 (K_prj = 1) adds the J selection of
+    FormB0, AvgDiag in the first iteration and Prj_J on the new vectors, which
+    needs the term list ``jt`` (j_terms).  H and J are (rowptr, col, val) lower-triangle CSR with 1-based
     columns.  Returns energies Tk (binding-energy convention, -(E+Hmin)),
     Tj, eigenvectors X[nd, Nlv], iterations and the residual norms."""
     rowptr, col, val = H
@@ -390,6 +434,59 @@ def diag4(nd, H, hmin, J, params, ndc, mxmpy_threads=1, log=None, timing=None):
         ArrB[:Nd0, j1 - 1] = b1 * s
         ArrB[Nd0:, j1 - 1] = b_loc * s
 
+    def avg_diag():  # src/davidson.f90:371-434
+        id0 = 0
+        for c in ndc:
+            c = int(c)
+            if c > 0:
+                s = 0.0
+                for i in range(id0, id0 + c):
+                    s += diag[i]
+                diag[id0:id0 + c] = s / c
+                id0 += c
+
+    if K_prj == 1:
+        if jt is None:
+            raise ValueError("Kv = 3 needs the term list jt")
+        if 0 in jt and int(2 * XJ_av + 0.1) != 0:
+            # the filter factor 1/(jx(jx+2)) of src/davidson.f90:808 is 1/0 for
+            # a J = 0 term, which the reference applies when XJ_av /= 0
+            raise ValueError("Prj_J: a J = 0 term with XJ_av /= 0 divides by zero")
+
+    def prj_j(lin, num, lout, trsd):  # src/davidson.f90:743-884, lin/lout 1-based
+        jav = int(2 * XJ_av + 0.1)
+        col_in = np.array(ArrB[:, lin - 1:lin - 1 + num])
+        col_out = np.zeros_like(col_in)
+        go = [Iconverge[i] == 0 for i in range(num)]
+        njd = len(jt)
+        jx, f = 0, 0.0
+        for itr in range(1, njd + 2):
+            itj = njd + 1 - itr
+            if itj != 0:
+                jx = int(jt[itj - 1])
+                f = 1.0 / (jx * (jx + 2)) if jx != 0 else float("inf")   # IEEE 1/0 of the reference
+            if jx != jav or itj == 0:
+                col_out[:] = 0.0
+                for i in range(num):
+                    if go[i]:
+                        x = np.ascontiguousarray(col_in[:, i])
+                        L.orc_mxmpy(nd, _ptr(jrow), _ptr(jcol), _ptr(jval), 0.0, _ptr(x), _ptr(y_tmp), None)
+                        col_out[:, i] = y_tmp
+                ArrB[:, lout - 1:lout - 1 + num] = col_out
+                err1 = 0.0
+                for i in range(num):
+                    if go[i]:
+                        sj = float(col_in[:, i] @ col_out[:, i])
+                        err1 = max(err1, abs(np.sqrt(1 + sj) - 1 - jav))
+                if err1 < trsd:
+                    return
+                if itj != 0:
+                    for i in range(num):
+                        if go[i]:
+                            a = col_in[:, i] - f * col_out[:, i]
+                            col_in[:, i] = a / np.sqrt(float(a @ a))
+                            ArrB[:, lin - 1 + i] = col_in[:, i]
+
     hist = []
     for it in range(1, N_it + 1):
         if not (ax > crit):
@@ -399,11 +496,18 @@ def diag4(nd, H, hmin, J, params, ndc, mxmpy_threads=1, log=None, timing=None):
             ortn(i)
         mxmpy(1)
         formp(1)
+        if it == 1 and K_prj == 1:
+            avg_diag()
         cnx = 0.0
         for i in range(1, Nlv + 1):
             dvdsn(i)
             if Iconverge[i - 1] == 0:
                 ortn(i + Nlv)
+        if K_prj == 1:
+            prj_j(Nlv + 1, Nlv, 2 * Nlv + 1, 1e-5)
+            for i in range(Nlv + 1, 2 * Nlv + 1):
+                if Iconverge[i - Nlv - 1] == 0:
+                    ortn(i)
         hist.append(cnorms.copy())
         if cnx > Crt4:
             mxmpy(2)

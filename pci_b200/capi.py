@@ -21,8 +21,8 @@ PCI_DVD_FP64, PCI_DVD_FP32 = 0, 1
 
 EXPORTS = ["pci_gpu_create", "pci_gpu_set_basis", "pci_gpu_set_integrals", "pci_gpu_form_h",
            "pci_gpu_form_j", "pci_gpu_csr_info", "pci_gpu_get_csr", "pci_gpu_set_csr",
-           "pci_gpu_davidson", "pci_gpu_j_av", "pci_gpu_j_av_noalloc", "pci_gpu_stats", "pci_gpu_last_error",
-           "pci_gpu_destroy"]
+           "pci_gpu_davidson", "pci_gpu_j_av", "pci_gpu_j_av_noalloc", "pci_gpu_jterms", "pci_gpu_stats",
+           "pci_gpu_last_error", "pci_gpu_destroy"]
 
 
 class PciError(RuntimeError):
@@ -61,6 +61,8 @@ def load(path: str = LIB):
     L.pci_gpu_davidson.argtypes = [P, C.POINTER(DvdParams), P, P, P, P, P, C.POINTER(i32), P]
     L.pci_gpu_j_av.argtypes = [P, P, i32, i64, P]
     L.pci_gpu_j_av_noalloc.argtypes = [P, P, P, i64, P, i64, i32, i64, P, P, C.c_char_p, i32]
+    L.pci_gpu_jterms.argtypes = [P, P, i32]
+    L.pci_gpu_jterms.restype = i32
     L.pci_gpu_stats.argtypes = [P, P, i32]
     L.pci_gpu_stats.restype = i32
     L.pci_gpu_last_error.argtypes = [P]
@@ -186,6 +188,15 @@ class Engine:
         out = np.zeros(nv)
         self._check(self.L.pci_gpu_j_av(self.h, _p(xc), nv, nd if nlim is None else nlim, _p(out)))
         return out
+
+    def jterms(self):
+        """Jt(1:Njd) of the current basis (sorted 2J of the terms present)."""
+        n = self.L.pci_gpu_jterms(self.h, None, 0)
+        if n < 0:
+            raise PciError(7, "jterms before set_basis")
+        out = np.zeros(max(n, 1), np.int32)
+        self.L.pci_gpu_jterms(self.h, _p(out), n)
+        return out[:n].tolist()
 
     def stats(self):
         out = np.zeros(14)

@@ -338,6 +338,56 @@ __global__ void k_get_cols(const double *A, int ld, int64_t nd, double *dst, int
         for (int c = 0; c < ncol; c++) dst[n + (int64_t)c * nd] = A[n * ld + c];
 }
 
+// ----------------------------------------------------------- Kv = 3 ---
+
+// AvgDiag (src/davidson.f90:371-434): each configuration's diagonal entries
+// replaced by their average (sequential sum, as the reference).
+__global__ void k_avg_diag(double *D, const int64_t *conf_start, int nc)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+        const int64_t a = conf_start[c], b = conf_start[c + 1];
+        if (b > a) {
+            double s = 0.0;
+            for (int64_t i = a; i < b; i++) s += D[i];
+            const double v = s / (double)(b - a);
+            for (int64_t i = a; i < b; i++) D[i] = v;
+        }
+    }
+}
+
+// J^2 (lower-triangle CSR, 0-based columns) applied to the probe vectors of
+// unconverged levels, columns cin.. -> cout.. (zeroed before), with the
+// symmetric scatter of Prj_J (src/davidson.f90:811-826).
+__global__ void k_jsq_apply(const int64_t *rowptr, const int32_t *col, const double *val, int64_t nd, double *A,
+                            int ld, int cin, int cout, int nv, const int *iconv)
+{
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nd; n += (int64_t)gridDim.x * blockDim.x)
+        for (int64_t l = rowptr[n]; l < rowptr[n + 1]; l++) {
+            const int64_t k = col[l];
+            const double t = val[l];
+            for (int v = 0; v < nv; v++) {
+                if (iconv[v]) continue;
+                atomicAdd(&A[n * ld + cout + v], t * A[k * ld + cin + v]);
+                if (k != n) atomicAdd(&A[k * ld + cout + v], t * A[n * ld + cin + v]);
+            }
+        }
+}
+
+// Prj_J filter step a = x - f * J^2 x on unconverged levels
+__global__ void k_prj_update(double *A, int ld, int64_t nd, int cin, int cout, int nv, double f, const int *iconv)
+{
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nd; n += (int64_t)gridDim.x * blockDim.x)
+        for (int v = 0; v < nv; v++)
+            if (!iconv[v]) A[n * ld + cin + v] = A[n * ld + cin + v] - f * A[n * ld + cout + v];
+}
+
+__global__ void k_prj_scale(double *A, int ld, int64_t nd, int cin, int nv, const double *inv, const int *iconv)
+{
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nd; n += (int64_t)gridDim.x * blockDim.x)
+        for (int v = 0; v < nv; v++)
+            if (!iconv[v]) A[n * ld + cin + v] *= inv[v];
+}
+
 // ------------------------------------------------------------ driver ---
 
 struct Dvd {
@@ -429,7 +479,11 @@ int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out
     if (!h->J.rowptr) return set_err(h, PCI_E_STATE, "davidson before form_j");
     if (p->Nlv < 1 || p->Nlv > 16) return set_err(h, PCI_E_INPUT, "Nlv must be 1..16");
     if (p->mode != PCI_DVD_FP64) return set_err(h, PCI_E_INPUT, "only the FP64 Davidson form is built");
-    if (p->Kv == 3) return set_err(h, PCI_E_INPUT, "Kv = 3 (J projection) is not built");
+    if (p->Kv != 3 && p->Kv != 4) return set_err(h, PCI_E_INPUT, "Kv must be 4 or 3");
+    const int jav = (int)(2 * p->XJ_av + 0.1);
+    if (p->Kv == 3 && jav != 0 && std::find(h->h_jterms.begin(), h->h_jterms.end(), 0) != h->h_jterms.end())
+        // the filter factor 1/(jx(jx+2)) of Prj_J (src/davidson.f90:808) is 1/0 for a J = 0 term
+        return set_err(h, PCI_E_INPUT, "Prj_J: a J = 0 term with XJ_av /= 0 divides by zero");
     Dvd d;
     d.h = h;
     d.st = h->st;
@@ -506,7 +560,27 @@ int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out
         if (cs != CUSOLVER_STATUS_SUCCESS || hinfo != 0) { free_dvd(d); return set_err(h, PCI_E_CUDA, "DSYEVD of the initial block failed"); }
     }
     cudaEventRecord(t1, d.st);
-    // FormB0 (src/davidson.f90:75-193)
+    // FormB0 (src/davidson.f90:75-193): initial vectors from the Nd0 block;
+    // with Kv = 3 only eigenvectors with |J - XJ_av| <= 0.1 (J from J_av on
+    // the first Nd0 rows) are taken, and Nlv becomes the number taken
+    std::vector<int> acc;
+    if (p->Kl4 != 2) {
+        if (p->Kv == 3) {
+            for (int j0 = 0; j0 < nd0 && (int)acc.size() < Nlv; j0 += 64) {
+                const int nv = std::min(64, nd0 - j0);
+                std::vector<double> xj(nv);
+                if ((rc = sp_jav_strided(h, d.Z1 + (size_t)j0 * nd0, 1, nd0, nv, nd0, xj.data()))) { free_dvd(d); return rc; }
+                for (int q = 0; q < nv && (int)acc.size() < Nlv; q++)
+                    if (!(fabs(xj[q] - p->XJ_av) > 1e-1)) acc.push_back(j0 + q);
+            }
+            if (acc.empty()) { free_dvd(d); return set_err(h, PCI_E_INPUT, "FormB0: no initial vector has J = XJ_av"); }
+        } else {
+            for (int j = 0; j < Nlv; j++) acc.push_back(j);
+        }
+        Nlv = (int)acc.size();
+        d.nlv = Nlv;
+        d.ld = 3 * Nlv;
+    }
     std::vector<double> E(2 * Nlv, 0.0), Tj(Nlv, 0.0), Tk(Nlv, 0.0);
     if (p->Kl4 == 2) {
         if (!X0) { free_dvd(d); return set_err(h, PCI_E_INPUT, "Kl4 = 2 needs X0"); }
@@ -517,9 +591,10 @@ int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out
         PCI_CUDA(h, cudaStreamSynchronize(d.st));
         dev_free(tmp);
     } else {
-        // Kv = 4: the first Nlv eigenvectors of the initial block
-        k_put_cols<<<d.blocks, 256, 0, d.st>>>(d.A, d.ld, nd, d.Z1, nd0, nd0, 0, Nlv);
-        for (int j = 0; j < Nlv; j++) E[j] = -(E1[j] + h->hmin);
+        for (int q = 0; q < Nlv; q++) {
+            k_put_cols<<<d.blocks, 256, 0, d.st>>>(d.A, d.ld, nd, d.Z1 + (size_t)acc[q] * nd0, nd0, nd0, q, 1);
+            E[q] = -(E1[acc[q]] + h->hmin);
+        }
     }
     // Davidson loop
     std::vector<double> P((size_t)4 * Nlv * Nlv, 0.0), Pt((size_t)2 * Nlv * Nlv), cn(Nlv, 0.0);
@@ -549,6 +624,8 @@ int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out
                 P[i + (size_t)k * n1] = v;
                 P[k + (size_t)i * n1] = v;
             }
+        if (it == 1 && p->Kv == 3)
+            k_avg_diag<<<(h->nc + 255) / 256, 256, 0, d.st>>>(d.D, h->d_conf_start, h->nc);
         // Dvdsn for all levels: residual norms first
         std::vector<double> theta(Nlv);
         for (int j = 0; j < Nlv; j++) theta[j] = P[j + (size_t)j * n1];
@@ -601,6 +678,47 @@ int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out
             for (int q = 0; q < nj; q++) {
                 if ((rc = ortn(d, Nlv + jsel[q] + 1))) { free_dvd(d); return rc; }
             }
+            if ((rc = check_ortn(d))) { free_dvd(d); return rc; }
+        }
+        if (p->Kv == 3) {
+            // Prj_J(Nlv+1, Nlv, 2Nlv+1, 1e-5) (src/davidson.f90:743-884), then Ortn of the new vectors
+            const std::vector<int32_t> &jt = h->h_jterms;
+            const int njd = (int)jt.size();
+            int jx = 0;
+            double f = 0.0;
+            std::vector<double> G((size_t)Nlv * Nlv), inv(Nlv, 1.0);
+            const Csr &J = h->J;
+            for (int iter = 1; iter <= njd + 1; iter++) {
+                const int itj = njd + 1 - iter;
+                if (itj != 0) {
+                    jx = jt[itj - 1];
+                    f = jx != 0 ? 1.0 / (double)(jx * (jx + 2)) : 0.0;   // jx = 0 is used only when J = 0 is the target
+                }
+                if (!(jx != jav || itj == 0)) continue;
+                for (int v = 0; v < Nlv; v++) k_zero_col<<<d.blocks, 256, 0, d.st>>>(d.A, d.ld, nd, 2 * Nlv + v);
+                k_jsq_apply<<<d.blocks, 256, 0, d.st>>>(J.rowptr, J.col, (const double *)J.val, nd, d.A, d.ld, Nlv,
+                                                        2 * Nlv, Nlv, d.iconv_d);
+                PCI_CUDA(h, cudaGetLastError());
+                if ((rc = gram(d, Nlv, Nlv, 2 * Nlv, Nlv, d.small + SM_GRAM))) { free_dvd(d); return rc; }
+                PCI_CUDA(h, cudaMemcpyAsync(G.data(), d.small + SM_GRAM, G.size() * 8, cudaMemcpyDeviceToHost, d.st));
+                PCI_CUDA(h, cudaStreamSynchronize(d.st));
+                double err1 = 0.0;
+                for (int v = 0; v < Nlv; v++)
+                    if (!d.iconv[v]) err1 = std::max(err1, fabs(sqrt(1.0 + G[(size_t)v * Nlv + v]) - 1.0 - jav));
+                if (err1 < 1e-5) break;
+                if (itj != 0) {
+                    k_prj_update<<<d.blocks, 256, 0, d.st>>>(d.A, d.ld, nd, Nlv, 2 * Nlv, Nlv, f, d.iconv_d);
+                    if ((rc = gram(d, Nlv, Nlv, Nlv, Nlv, d.small + SM_GRAM))) { free_dvd(d); return rc; }
+                    PCI_CUDA(h, cudaMemcpyAsync(G.data(), d.small + SM_GRAM, G.size() * 8, cudaMemcpyDeviceToHost, d.st));
+                    PCI_CUDA(h, cudaStreamSynchronize(d.st));
+                    for (int v = 0; v < Nlv; v++) inv[v] = d.iconv[v] ? 1.0 : 1.0 / sqrt(G[(size_t)v * Nlv + v]);
+                    PCI_CUDA(h, cudaMemcpyAsync(d.small + SM_TSEL, inv.data(), Nlv * 8, cudaMemcpyHostToDevice, d.st));
+                    k_prj_scale<<<d.blocks, 256, 0, d.st>>>(d.A, d.ld, nd, Nlv, Nlv, d.small + SM_TSEL, d.iconv_d);
+                    PCI_CUDA(h, cudaGetLastError());
+                }
+            }
+            for (int i = Nlv + 1; i <= 2 * Nlv; i++)
+                if (!d.iconv[i - Nlv - 1] && (rc = ortn(d, i))) { free_dvd(d); return rc; }
             if ((rc = check_ortn(d))) { free_dvd(d); return rc; }
         }
         if (cnx > p->Crt4) {
@@ -678,6 +796,14 @@ int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out
         if (Tj_out) Tj_out[k] = Tj[k];
         if (Iconverge_out) Iconverge_out[k] = d.iconv[k];
         if (resid_out) resid_out[k] = cn[k];
+    }
+    // levels FormB0 could not seed (Kv = 3: fewer initial vectors with J = XJ_av)
+    for (int k = Nlv; k < p->Nlv; k++) {
+        if (Tk_out) Tk_out[k] = 0.0;
+        if (Tj_out) Tj_out[k] = 0.0;
+        if (Iconverge_out) Iconverge_out[k] = -1;
+        if (resid_out) resid_out[k] = 0.0;
+        if (X_out) memset(X_out + (size_t)k * nd, 0, (size_t)nd * 8);
     }
     if (iters_out) *iters_out = it_done;
     free_dvd(d);

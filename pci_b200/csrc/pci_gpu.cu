@@ -162,6 +162,71 @@ int pci_gpu_create(int32_t device, pci_gpu_t **out)
     return PCI_OK;
 }
 
+// Jt(1:Njd), the sorted 2J values of the terms the configurations hold, as
+// Dinit finds them (src/determinants.f90:227-325): per configuration with
+// determinants at 2M = Mj, the number of its determinants at each
+// 2M = Mj + 2(im-1) >= Mj; terms are peeled off from the largest im down.
+// The counts come from the m-value distribution of each orbital's
+// occupation (subsets of its 2j+1 m values) convolved over the orbitals,
+// instead of enumerating the determinants.
+static std::vector<int32_t> compute_jterms(int Ne, int Nc, const int32_t *Ndc, const std::vector<uint16_t> &conf_orb,
+                                           const int32_t *Jj, int Nsu, int Mj)
+{
+    std::vector<int32_t> jt;
+    int jmax = 1;
+    for (int o = 0; o < Nsu; o++) jmax = std::max(jmax, (int)Jj[o]);
+    const int OFF = Ne * jmax;  // |2M| <= Ne * max(2j)
+    for (int c = 0; c < Nc; c++) {
+        if (Ndc[c] == 0) continue;
+        std::vector<int> orbs(conf_orb.begin() + (size_t)c * Ne, conf_orb.begin() + (size_t)(c + 1) * Ne);
+        std::sort(orbs.begin(), orbs.end());
+        std::vector<int64_t> dist(2 * OFF + 1, 0);
+        dist[OFF] = 1;
+        for (size_t i = 0; i < orbs.size();) {
+            size_t j = i;
+            while (j < orbs.size() && orbs[j] == orbs[i]) j++;
+            const int q = (int)(j - i), j2 = Jj[orbs[i]];
+            // ways[k][s]: k of the m values -j2, -j2+2, ..., j2 chosen with 2M sum s
+            std::vector<std::vector<int64_t>> ways(q + 1, std::vector<int64_t>(2 * OFF + 1, 0));
+            ways[0][OFF] = 1;
+            for (int m = -j2; m <= j2; m += 2)
+                for (int k = q; k >= 1; k--)
+                    for (int sidx = 0; sidx <= 2 * OFF; sidx++)
+                        if (ways[k - 1][sidx] && sidx + m >= 0 && sidx + m <= 2 * OFF) ways[k][sidx + m] += ways[k - 1][sidx];
+            std::vector<int64_t> nd2(2 * OFF + 1, 0);
+            for (int a = 0; a <= 2 * OFF; a++)
+                if (dist[a])
+                    for (int b = 0; b <= 2 * OFF; b++)
+                        if (ways[q][b] && a + b - OFF >= 0 && a + b - OFF <= 2 * OFF) nd2[a + b - OFF] += dist[a] * ways[q][b];
+            dist.swap(nd2);
+            i = j;
+        }
+        if (Mj + OFF < 0 || Mj + OFF > 2 * OFF || dist[Mj + OFF] == 0) continue;
+        std::vector<int64_t> nmj(1, 0);   // nmj[im], im >= 1
+        for (int m2 = Mj; m2 + OFF <= 2 * OFF; m2 += 2) nmj.push_back(dist[m2 + OFF]);
+        int imax = (int)nmj.size() - 1;
+        while (imax > 1 && nmj[imax] == 0) imax--;
+        for (int im = imax; im >= 1; im--) {
+            const int64_t n = nmj[im];
+            if (n != 0) {
+                const int mt = (im - 1) * 2 + Mj;
+                for (int k = 1; k <= im; k++) nmj[k] -= n;
+                if (std::find(jt.begin(), jt.end(), mt) == jt.end()) jt.push_back(mt);
+            }
+        }
+    }
+    std::sort(jt.begin(), jt.end());
+    return jt;
+}
+
+int pci_gpu_jterms(pci_gpu_t *h, int32_t *out, int32_t cap)
+{
+    if (!h || !h->have_basis) return -1;
+    const int32_t n = (int32_t)h->h_jterms.size();
+    for (int32_t i = 0; i < n && out && i < cap; i++) out[i] = h->h_jterms[(size_t)i];
+    return n;
+}
+
 int pci_gpu_set_basis(pci_gpu_t *h, int32_t Ne, int64_t Nd, int32_t Nst, int32_t Nsu, int32_t Nso, int32_t Nx,
                       int32_t Mj, const int32_t *Iarr, const int32_t *Nh, const int32_t *Jz, const int32_t *Nn,
                       const int32_t *Kk, const int32_t *Ll, const int32_t *Jj, int32_t Nc, const int32_t *Ndc,
@@ -220,6 +285,7 @@ int pci_gpu_set_basis(pci_gpu_t *h, int32_t Ne, int64_t Nd, int32_t Nst, int32_t
             }
         }
     }
+    h->h_jterms = compute_jterms(Ne, Nc, Ndc, conf_orb, Jj, Nsu, Mj);
     std::vector<int16_t> ms_orb(Nst);
     std::vector<int8_t> ms_jz(Nst), orb_l(Nsu), orb_j(Nsu);
     std::vector<uint8_t> ms_type(Nst);

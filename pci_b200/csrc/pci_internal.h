@@ -62,6 +62,7 @@ struct pci_gpu {
     std::vector<int32_t> h_ndc;       // host copy of Ndc
     std::vector<int32_t> h_orb_j, h_orb_l, h_orb_k;
     std::vector<int32_t> h_nh, h_jz;
+    std::vector<int32_t> h_jterms;    // Jt(1:Njd): sorted 2J of the terms present
     std::vector<unsigned long long> h_rowwork;   // determinant pairs per row, per configuration
     uint32_t *d_msd = nullptr;                   // packed m-state descriptors
     uint16_t *d_occ = nullptr;

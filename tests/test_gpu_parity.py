@@ -141,6 +141,46 @@ def test_davidson_trajectory_small3(engine):
     assert np.allclose(res["resid"], ref["cnorm"], rtol=1e-5, atol=1e-9)
 
 
+@pytest.mark.parametrize("name", ["tiny", "small3", "small4", "cfg1"])
+def test_jterms_match_oracle(engine, name):
+    """Jt computed in set_basis from the configurations' M distributions
+    equals the oracle's enumeration of Dinit's term analysis."""
+    s = get_system(name)
+    _load(engine, s)
+    assert engine.jterms() == O.j_terms(s.basis, s.configs, s.mj)
+
+
+@pytest.mark.parametrize("name,xj,nlv,n_it", [("tiny", 0.0, 3, 200), ("small3", 1.5, 6, 20)])
+def test_davidson_kv3(engine, name, xj, nlv, n_it):
+    """Kv = 3 against the oracle: the same iterations of J-selected FormB0,
+    AvgDiag and Prj_J give the same Ritz values (1e-8) and J = XJ_av."""
+    s = get_system(name)
+    (rp, col, val, nz, hmin, pairs), (jr, jc, jv) = oracle_h(name)
+    p = dict(s.params, Kv=3, XJ_av=xj, Nlv=nlv, N_it=n_it, admix_crit=0.0)
+    ref = O.diag4(s.nd, (rp, col, val), hmin, (jr, jc, jv), p, s.ndc, jt=O.j_terms(s.basis, s.configs, s.mj))
+    _load(engine, s)
+    engine.form_h(64)
+    engine.form_j()
+    res = engine.davidson(s.nd, Nlv=nlv, N_it=n_it, Crt4=p["Crt4"], Kv=3, XJ_av=xj, MaxNd0=p["MaxNd0"],
+                          admix_crit=0.0)
+    n = ref["Tk"].size
+    assert res["iterations"] == ref["iterations"]
+    assert np.max(np.abs(res["Tk"][:n] - ref["Tk"])) <= 1e-8
+    assert np.allclose(res["Tj"][:n], xj, atol=1e-6)
+    assert np.all(res["Iconverge"][n:] == -1)
+
+
+def test_davidson_kv3_zero_term_is_rejected(engine):
+    from pci_b200.capi import PciError
+    s = get_system("tiny")
+    _load(engine, s)
+    engine.form_h(64)
+    engine.form_j()
+    with pytest.raises(PciError) as ei:
+        engine.davidson(s.nd, Nlv=3, Kv=3, XJ_av=1.0)
+    assert ei.value.code == 1 and "divides by zero" in str(ei.value)
+
+
 def test_missing_integral_is_reported(engine):
     from pci_b200.capi import PciError
     kw = S.CONFIGS["tiny"]()

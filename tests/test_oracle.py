@@ -314,3 +314,39 @@ def test_rspq_vs_bit_path():
                 assert all(m in occ for m in range(first, lo))
     assert stats[2][0] == stats[2][1] > 500
     assert stats[1][0] >= 0.99 * stats[1][1]
+
+
+@pytest.mark.parametrize("name", ["tiny", "small3", "cfg1"])
+def test_j_terms_match_j2_spectrum(name):
+    """Jt of Dinit's term analysis = the 2J values in the J^2 spectrum."""
+    s = get_system(name)
+    _, (jr, jc, jv) = oracle_h(name)
+    w = np.linalg.eigvalsh(O.csr_to_dense(s.nd, jr, jc, jv))
+    two_j = sorted(set(np.round(np.sqrt(1 + w) - 1).astype(int).tolist()))
+    assert O.j_terms(s.basis, s.configs, s.mj) == two_j
+
+
+def test_davidson_kv3_matches_j_subspace():
+    """Kv = 3 (J-selected FormB0, AvgDiag, Prj_J) converges to the lowest
+    levels of H inside the J = XJ_av subspace, with J exact."""
+    name, xj = "tiny", 0.0
+    s = get_system(name)
+    (rp, col, val, nz, hmin, pairs), (jr, jc, jv) = oracle_h(name)
+    A = O.csr_to_dense(s.nd, rp, col, val)
+    wj, vj = np.linalg.eigh(O.csr_to_dense(s.nd, jr, jc, jv))
+    P = vj[:, np.abs(np.sqrt(1 + wj) - 1 - 2 * xj) < 1e-6]
+    exact = np.linalg.eigvalsh(P.T @ A @ P)
+    p = dict(s.params, Kv=3, XJ_av=xj, Nlv=3, admix_crit=0.0)
+    res = O.diag4(s.nd, (rp, col, val), hmin, (jr, jc, jv), p, s.ndc, jt=O.j_terms(s.basis, s.configs, s.mj))
+    assert res["converged"]
+    assert np.allclose(np.sort(-res["Tk"]), exact[:3], atol=1e-9)
+    assert np.allclose(res["Tj"], xj, atol=1e-8)
+
+
+def test_davidson_kv3_rejects_zero_term_filter():
+    """A J = 0 term with XJ_av /= 0 makes Prj_J divide by zero in the reference."""
+    s = get_system("tiny")
+    (rp, col, val, nz, hmin, pairs), (jr, jc, jv) = oracle_h("tiny")
+    p = dict(s.params, Kv=3, XJ_av=1.0, Nlv=3)
+    with pytest.raises(ValueError, match="divides by zero"):
+        O.diag4(s.nd, (rp, col, val), hmin, (jr, jc, jv), p, s.ndc, jt=O.j_terms(s.basis, s.configs, s.mj))
