@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--cpu-rows", type=int, default=2000, help="rows per CPU sample step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp32-form", action="store_true", help="skip the FP32 Davidson form")
     ap.add_argument("--davidson-iters", type=int, default=2,
                     help="plain FP64 Davidson iterations timed after the H-build (0 skips)")
     return ap.parse_args()
@@ -298,6 +299,26 @@ def run_ours(args):
                               if os.environ.get("PCI_SPMM") == "lower" or numh * 24 > 100e9
                               else "full symmetric copy"},
         }
+        if not args.no_fp32_form:
+            # precision form: H re-formed in FP32, FP32 SpMM, the same iterations;
+            # eigenvalue difference from the FP64 form after them, per level
+            eng.form_h(32)
+            r32 = eng.davidson(sysm.nd, Nlv=nlv, N_it=args.davidson_iters, Crt4=1e-8, mode=1,
+                               MaxNd0=int(sysm.params["MaxNd0"]), admix_crit=0.0, want_vectors=False)
+            s32 = eng.stats()
+            c32 = max(1.0, s32["spmm_calls"])
+            sp32 = s32["spmm_ms"] / c32
+            b32 = numh * 8 + (sysm.nd + 1) * 8 + 2 * sysm.nd * nlv * 4
+            a32 = b32 / (sp32 * 1e-3) / 1e9
+            line["davidson_fp32"] = {
+                "form": "FP32 H and SpMM (FP32 accumulate); FP64 projections, eigensolve, residuals",
+                "iterations": r32["iterations"],
+                "ms_per_iteration": (s32["davidson_ms"] - s32["init_ms"]) / max(1, r32["iterations"]),
+                "spmm_ms_per_call": sp32,
+                "abs_dE_vs_fp64_per_level": [float(x) for x in np.abs(r32["Tk"] - res["Tk"])],
+                "spmm_roofline": {"bound": "hbm", "achieved": a32, "peak": peak, "unit": "GB/s",
+                                  "frac": a32 / peak, "algorithmic_bytes": int(b32)},
+            }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         t, n, r = cpu_sample(sysm, args.cpu_rows, 7, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": n / t, "unit": "nnz/s", "cores": os.cpu_count() or 1, "kind": "port",

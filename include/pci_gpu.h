@@ -48,7 +48,10 @@ typedef struct {
     int32_t Kv;         /* 4: no J selection; 3: select and project on J = XJ_av */
     int32_t Nc4;        /* configurations eligible for the initial block */
     int32_t MaxNd0;     /* largest initial block (ci.in MaxNd0, default 3000) */
-    int32_t mode;       /* PCI_DVD_FP64 (reference algorithm) or PCI_DVD_FP32 */
+    int32_t mode;       /* PCI_DVD_FP64 (reference algorithm) or PCI_DVD_FP32: H stored in FP32
+                           (form_h value_prec 32), SpMM on float vectors with FP32 accumulation;
+                           orthogonalisation, projections, Rayleigh quotients, residual norms and
+                           the projected eigensolve stay FP64 */
     int32_t KXIJ;       /* unused by the library; kept for the caller's CONF.XIJ cadence */
     double  Crt4;       /* residual-norm convergence threshold (CRT4) */
     double  XJ_av;      /* target J for Kv = 3 */

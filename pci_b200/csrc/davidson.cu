@@ -388,6 +388,26 @@ __global__ void k_prj_scale(double *A, int ld, int64_t nd, int cin, int nv, cons
             if (!iconv[v]) A[n * ld + cin + v] *= inv[v];
 }
 
+// -------------------------------------------------- SpMM block packing ---
+
+// The probe block goes to the SpMM as a contiguous Nd x nv array (the basis
+// rows hold 3 Nlv columns), so the column gathers of the SpMM touch nv
+// values per determinant instead of whole basis rows; in the FP32 form the
+// packed block is float.
+template <typename T>
+__global__ void k_pack(const double *A, int ld, int64_t nd, int c0, int nv, T *P)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nd * nv; i += (int64_t)gridDim.x * blockDim.x)
+        P[i] = (T)A[(i / nv) * ld + c0 + (i % nv)];
+}
+
+template <typename T>
+__global__ void k_unpack(const T *P, int64_t nd, int nv, double *A, int ld, int c0)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nd * nv; i += (int64_t)gridDim.x * blockDim.x)
+        A[(i / nv) * ld + c0 + (i % nv)] = (double)P[i];
+}
+
 // ------------------------------------------------------------ driver ---
 
 struct Dvd {
@@ -397,6 +417,8 @@ struct Dvd {
     int nlv, ld, nd0;
     double *A = nullptr, *D = nullptr, *Z1 = nullptr, *E1 = nullptr, *C = nullptr, *Bz = nullptr, *Sz = nullptr;
     double *part = nullptr, *small = nullptr;  // small: scratch scalars
+    void *xp = nullptr, *yp = nullptr;         // packed SpMM input / output blocks
+    bool fp32 = false;                         // FP32 form: float blocks, FP32 SpMM
     OrtnState *ost = nullptr;
     int *iconv_d = nullptr, *jsel_d = nullptr;
     std::vector<int> iconv;
@@ -450,7 +472,16 @@ int mxmpy(Dvd &d, int ip)
 {
     int i2 = ip * d.nlv, i1 = i2 - d.nlv;
     cudaEventRecord(d.ea, d.st);
-    int rc = sp_spmm(d.h, d.A + i1, d.ld, d.A + i2, d.ld, d.nlv, d.st);
+    int rc;
+    if (d.fp32) {
+        k_pack<float><<<d.blocks, 256, 0, d.st>>>(d.A, d.ld, d.nd, i1, d.nlv, (float *)d.xp);
+        rc = sp_spmm_f32(d.h, (const float *)d.xp, d.nlv, (float *)d.yp, d.nlv, d.nlv, d.st);
+        if (!rc) k_unpack<float><<<d.blocks, 256, 0, d.st>>>((const float *)d.yp, d.nd, d.nlv, d.A, d.ld, i2);
+    } else {
+        k_pack<double><<<d.blocks, 256, 0, d.st>>>(d.A, d.ld, d.nd, i1, d.nlv, (double *)d.xp);
+        rc = sp_spmm(d.h, (const double *)d.xp, d.nlv, (double *)d.yp, d.nlv, d.nlv, d.st);
+        if (!rc) k_unpack<double><<<d.blocks, 256, 0, d.st>>>((const double *)d.yp, d.nd, d.nlv, d.A, d.ld, i2);
+    }
     cudaEventRecord(d.eb, d.st);
     cudaEventSynchronize(d.eb);
     float ms = 0;
@@ -464,6 +495,7 @@ void free_dvd(Dvd &d)
 {
     dev_free(d.A); dev_free(d.D); dev_free(d.Z1); dev_free(d.E1); dev_free(d.C); dev_free(d.Bz); dev_free(d.Sz);
     dev_free(d.part); dev_free(d.small); dev_free(d.ost); dev_free(d.iconv_d); dev_free(d.jsel_d);
+    dev_free(d.xp); dev_free(d.yp);
     if (d.cub) cublasDestroy(d.cub);
     if (d.sol) cusolverDnDestroy(d.sol);
     if (d.ea) cudaEventDestroy(d.ea);
@@ -478,7 +510,9 @@ int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out
     if (!h->H.rowptr) return set_err(h, PCI_E_STATE, "davidson before form_h");
     if (!h->J.rowptr) return set_err(h, PCI_E_STATE, "davidson before form_j");
     if (p->Nlv < 1 || p->Nlv > 16) return set_err(h, PCI_E_INPUT, "Nlv must be 1..16");
-    if (p->mode != PCI_DVD_FP64) return set_err(h, PCI_E_INPUT, "only the FP64 Davidson form is built");
+    if (p->mode != PCI_DVD_FP64 && p->mode != PCI_DVD_FP32) return set_err(h, PCI_E_INPUT, "mode must be FP64 or FP32");
+    if (p->mode == PCI_DVD_FP32 && !h->H.val_f32)
+        return set_err(h, PCI_E_INPUT, "the FP32 form needs H stored in FP32 (form_h with value_prec 32)");
     if (p->Kv != 3 && p->Kv != 4) return set_err(h, PCI_E_INPUT, "Kv must be 4 or 3");
     const int jav = (int)(2 * p->XJ_av + 0.1);
     if (p->Kv == 3 && jav != 0 && std::find(h->h_jterms.begin(), h->h_jterms.end(), 0) != h->h_jterms.end())
@@ -526,6 +560,9 @@ int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out
     ALLOC(d.ost, OrtnState, 1);
     ALLOC(d.iconv_d, int, 16);
     ALLOC(d.jsel_d, int, 16);
+    d.fp32 = p->mode == PCI_DVD_FP32;
+    ALLOC(d.xp, double, nd * Nlv);
+    ALLOC(d.yp, double, nd * Nlv);
 #undef ALLOC
     if (cublasCreate(&d.cub) != CUBLAS_STATUS_SUCCESS) { free_dvd(d); return set_err(h, PCI_E_CUDA, "cublasCreate failed"); }
     cublasSetStream(d.cub, d.st);

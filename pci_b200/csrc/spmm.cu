@@ -192,11 +192,11 @@ constexpr int LW_WARPS = 4;
 // exact, so the window sums do not depend on the order lanes arrive in.
 constexpr double LW_SCALE = 36028797018963968.0;  // 2^55
 
-template <int NV, typename VT>
+template <int NV, typename VT, typename XT>
 __global__ void __launch_bounds__(LW_WARPS * 32) k_spmm_lower(const int64_t *__restrict__ rowptr,
                                                                const int32_t *__restrict__ col,
                                                                const VT *__restrict__ val, int64_t nd, double hmin,
-                                                               const double *__restrict__ X, int ldx, double *Y,
+                                                               const XT *__restrict__ X, int ldx, XT *Y,
                                                                int ldy, unsigned long long *counter)
 {
     __shared__ unsigned long long tbuf[LW_WARPS][LW_WIN * NV];
@@ -213,11 +213,11 @@ __global__ void __launch_bounds__(LW_WARPS * 32) k_spmm_lower(const int64_t *__r
         const int64_t n = (int64_t)it * LW_ROWS + lane;
         const bool mine = n < nd;
         int64_t cur = mine ? rowptr[n] : 0, end = mine ? rowptr[n + 1] : 0;
-        double xn[NV], acc[NV];
+        XT xn[NV], acc[NV];
 #pragma unroll
         for (int v = 0; v < NV; v++) {
-            xn[v] = mine ? X[n * ldx + v] : 0.0;
-            acc[v] = 0.0;
+            xn[v] = mine ? X[n * ldx + v] : (XT)0;
+            acc[v] = (XT)0;
         }
         int ck = cur < end ? __ldg(&col[cur]) : INT_MAX;
         while (true) {
@@ -227,15 +227,16 @@ __global__ void __launch_bounds__(LW_WARPS * 32) k_spmm_lower(const int64_t *__r
             if (wmin == INT_MAX) break;
             const int wend = wmin + LW_WIN;
             while (ck < wend) {
-                const double h0 = (double)__ldg(&val[cur]);
-                const double h = ck == n ? h0 - hmin : h0;
-                const double *xk = X + (int64_t)ck * ldx;
+                const XT h0 = (XT)__ldg(&val[cur]);
+                const XT h = ck == n ? h0 - (XT)hmin : h0;
+                const XT *xk = X + (int64_t)ck * ldx;
 #pragma unroll
                 for (int v = 0; v < NV; v++) acc[v] += h * __ldg(&xk[v]);
                 if (ck != n) {
                     unsigned long long *t = tb + (ck - wmin) * NV;
 #pragma unroll
-                    for (int v = 0; v < NV; v++) atomicAdd(&t[v], (unsigned long long)__double2ll_rn(h * xn[v] * LW_SCALE));
+                    for (int v = 0; v < NV; v++)
+                        atomicAdd(&t[v], (unsigned long long)__double2ll_rn((double)(h * xn[v]) * LW_SCALE));
                 }
                 cur++;
                 ck = cur < end ? __ldg(&col[cur]) : INT_MAX;
@@ -245,7 +246,7 @@ __global__ void __launch_bounds__(LW_WARPS * 32) k_spmm_lower(const int64_t *__r
                 const long long q = (long long)tb[i];
                 if (q != 0) {
                     const int64_t k = wmin + i / NV;
-                    atomicAdd(&Y[k * ldy + (i % NV)], (double)q / LW_SCALE);
+                    atomicAdd(&Y[k * ldy + (i % NV)], (XT)((double)q / LW_SCALE));
                     tb[i] = 0ULL;
                 }
             }
@@ -257,14 +258,15 @@ __global__ void __launch_bounds__(LW_WARPS * 32) k_spmm_lower(const int64_t *__r
     }
 }
 
-__global__ void k_zero_block(double *Y, int ldy, int64_t nd, int nv)
+template <typename XT>
+__global__ void k_zero_block(XT *Y, int ldy, int64_t nd, int nv)
 {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nd * nv; i += (int64_t)gridDim.x * blockDim.x)
-        Y[(i / nv) * ldy + (i % nv)] = 0.0;
+        Y[(i / nv) * ldy + (i % nv)] = (XT)0;
 }
 
-template <typename VT>
-static int spmm_lower_dispatch(pci_gpu *h, const double *X, int ldx, double *Y, int ldy, int nv, cudaStream_t st)
+template <typename VT, typename XT>
+static int spmm_lower_dispatch(pci_gpu *h, const XT *X, int ldx, XT *Y, int ldy, int nv, cudaStream_t st)
 {
     const Csr &L = h->H;
     int rc = 0;
@@ -276,7 +278,7 @@ static int spmm_lower_dispatch(pci_gpu *h, const double *X, int ldx, double *Y, 
     const VT *val = (const VT *)L.val;
 #define CASE(N)                                                                                           \
     case N:                                                                                               \
-        k_spmm_lower<N, VT><<<blocks, LW_WARPS * 32, 0, st>>>(L.rowptr, L.col, val, L.nrows, h->hmin, \
+        k_spmm_lower<N, VT, XT><<<blocks, LW_WARPS * 32, 0, st>>>(L.rowptr, L.col, val, L.nrows, h->hmin, \
                                                                       X, ldx, Y, ldy, counter);           \
         break;
     switch (nv) {
@@ -325,8 +327,8 @@ int sp_spmm(pci_gpu *h, const double *X, int ldx, double *Y, int ldy, int nv, cu
 {
     if (use_lower(h)) {
         h->spmm_lower_used = 1;
-        return h->H.val_f32 ? spmm_lower_dispatch<float>(h, X, ldx, Y, ldy, nv, st)
-                            : spmm_lower_dispatch<double>(h, X, ldx, Y, ldy, nv, st);
+        return h->H.val_f32 ? spmm_lower_dispatch<float, double>(h, X, ldx, Y, ldy, nv, st)
+                            : spmm_lower_dispatch<double, double>(h, X, ldx, Y, ldy, nv, st);
     }
     h->spmm_lower_used = 0;
     int rc = sp_build_full(h);
@@ -337,6 +339,12 @@ int sp_spmm(pci_gpu *h, const double *X, int ldx, double *Y, int ldy, int nv, cu
 
 int sp_spmm_f32(pci_gpu *h, const float *X, int ldx, float *Y, int ldy, int nv, cudaStream_t st)
 {
+    if (use_lower(h)) {
+        h->spmm_lower_used = 1;
+        return h->H.val_f32 ? spmm_lower_dispatch<float, float>(h, X, ldx, Y, ldy, nv, st)
+                            : spmm_lower_dispatch<double, float>(h, X, ldx, Y, ldy, nv, st);
+    }
+    h->spmm_lower_used = 0;
     int rc = sp_build_full(h);
     if (rc) return rc;
     if (h->Hfull.val_f32) return spmm_dispatch<float, float>(h, X, ldx, Y, ldy, nv, st);

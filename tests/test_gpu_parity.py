@@ -181,6 +181,40 @@ def test_davidson_kv3_zero_term_is_rejected(engine):
     assert ei.value.code == 1 and "divides by zero" in str(ei.value)
 
 
+@pytest.mark.parametrize("name,spmm", [("tiny", "full"), ("cfg1", "full"), ("cfg1", "lower")])
+def test_davidson_fp32_form(name, spmm, monkeypatch):
+    """Precision form: H stored in FP32 and FP32 SpMM (FP32 accumulate), FP64
+    elsewhere.  Its levels match the FP64 oracle's to FP32 accuracy: within
+    2e-6 Ha per level (stated per level in the assertion message)."""
+    from pci_b200.capi import Engine
+    monkeypatch.setenv("PCI_SPMM", spmm)
+    s = get_system(name)
+    (rp, col, val, nz, hmin, pairs), (jr, jc, jv) = oracle_h(name)
+    p = dict(s.params)
+    ref = O.diag4(s.nd, (rp, col, val), hmin, (jr, jc, jv), p, s.ndc)
+    with Engine(0) as e:
+        e.load_system(s)
+        e.form_h(32)
+        e.form_j()
+        res = e.davidson(s.nd, Nlv=p["Nlv"], N_it=p["N_it"], Crt4=1e-6, mode=1, MaxNd0=p["MaxNd0"],
+                         admix_crit=0.0)
+        assert e.stats()["spmm_calls"] > 0
+    err = np.abs(res["Tk"] - ref["Tk"])
+    assert np.all(err <= 2e-6), f"per-level |dE| vs FP64: {err}"
+    assert np.allclose(res["Tj"], ref["Tj"], atol=1e-4)
+
+
+def test_fp32_form_needs_fp32_h(engine):
+    from pci_b200.capi import PciError
+    s = get_system("tiny")
+    _load(engine, s)
+    engine.form_h(64)
+    engine.form_j()
+    with pytest.raises(PciError) as ei:
+        engine.davidson(s.nd, Nlv=3, mode=1)
+    assert ei.value.code == 1
+
+
 def test_missing_integral_is_reported(engine):
     from pci_b200.capi import PciError
     kw = S.CONFIGS["tiny"]()
