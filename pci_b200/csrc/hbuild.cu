@@ -309,6 +309,7 @@ int hb_form_h(pci_gpu *h, int value_prec, int64_t *numh, int64_t *numzero, doubl
     // the single-evaluation build adds a second scan and its compaction
     h->st_launches = h->st_formh_padded ? 10 + h->st_formh_compact_launches : 8;
     csr_free(h->Hfull);
+    h->h_from_tiles = true;
     h->numh = h->H.nnz;
     h->numzero = (int64_t)hs.numzero;
     h->hmin = hs.hmin;

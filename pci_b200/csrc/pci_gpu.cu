@@ -394,7 +394,10 @@ int pci_gpu_set_csr(pci_gpu_t *h, int32_t which, int64_t Nd, int64_t nnz, const 
     if (rowptr[0] != 0 || rowptr[Nd] != nnz) return set_err(h, PCI_E_INPUT, "rowptr inconsistent with nnz");
     Csr &c = which == PCI_MAT_J2 ? h->J : h->H;
     csr_free(c);
-    if (which != PCI_MAT_J2) csr_free(h->Hfull);
+    if (which != PCI_MAT_J2) {
+        csr_free(h->Hfull);
+        h->h_from_tiles = false;
+    }
     int rc = 0;
     c.nrows = Nd;
     c.nnz = nnz;

@@ -96,6 +96,7 @@ struct pci_gpu {
     double st_dvd = 0, st_spmm = 0, st_spmm_calls = 0, st_init = 0;
     double st_adj = 0, st_pairs = 0, st_scanned = 0, st_launches = 0;
     double st_formh_compact = 0, st_formh_padded = 0, st_formh_compact_launches = 0;
+    bool h_from_tiles = false;  // H was built here by form_h: its rows follow the adjacency tiles
     int spmm_mode = 0;        // 0 auto, 1 full symmetric copy, 2 lower triangle (env PCI_SPMM)
     int spmm_lower_used = 0;
 };

@@ -13,6 +13,9 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
 
 #include "pci_internal.h"
 
@@ -258,6 +261,107 @@ __global__ void __launch_bounds__(LW_WARPS * 32) k_spmm_lower(const int64_t *__r
     }
 }
 
+// ------------------------------- lower-triangle SpMM along the tiles ---
+//
+// Same product, for an H built here: its rows are grouped by configuration
+// and every stored element lies in a tile (c1, c2) of adjacent
+// configurations, columns ascending tile by tile.  One warp takes up to 32
+// rows of one configuration c1 (lane = row) and walks c1's adjacency list:
+// for each tile the lanes consume their row's entries inside c2's column
+// range, the row part into registers and the transpose part into a
+// shared-memory buffer of c2's columns (64-bit fixed point, as above), which
+// goes to Y with one global atomic per touched (column, vector) per tile.
+// All rows of a configuration share the tile sequence, so the buffer
+// collects every row's contribution to a column before its one atomic.
+constexpr int LT_WARPS = 8;
+constexpr int LT_WIN = 64;   // columns of a tile per buffer flush
+constexpr int LT_ROWS = 32;
+
+template <int NV, typename VT, typename XT>
+__global__ void __launch_bounds__(LT_WARPS * 32) k_spmm_lower_tiles(
+    const int64_t *__restrict__ rowptr, const int32_t *__restrict__ col, const VT *__restrict__ val, double hmin,
+    const int64_t *__restrict__ conf_start, const int64_t *__restrict__ adj_ptr, const int32_t *__restrict__ adj,
+    const int2 *__restrict__ items, int64_t nitems, const XT *__restrict__ X, int ldx, XT *Y, int ldy,
+    unsigned long long *counter)
+{
+    extern __shared__ unsigned long long lt_smem[];
+    const int lane = threadIdx.x & 31;
+    unsigned long long *tb = lt_smem + (size_t)(threadIdx.x >> 5) * LT_WIN * NV;
+    for (int i = lane; i < LT_WIN * NV; i += 32) tb[i] = 0ULL;
+    __syncwarp();
+    while (true) {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(counter, 1ULL);
+        t = __shfl_sync(FULL_MASK, t, 0);
+        if (t >= (unsigned long long)nitems) break;
+        const int2 it = items[t];
+        const int c1 = it.x;
+        const int64_t cend = conf_start[c1 + 1];
+        const int64_t n = conf_start[c1] + it.y + lane;
+        const bool mine = n < cend && lane < LT_ROWS;
+        int64_t cur = mine ? rowptr[n] : 0;
+        const int64_t end = mine ? rowptr[n + 1] : 0;
+        XT xn[NV], acc[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            xn[v] = mine ? X[n * ldx + v] : (XT)0;
+            acc[v] = (XT)0;
+        }
+        int ck = cur < end ? __ldg(&col[cur]) : INT_MAX;
+        // an element outside the tile being walked (not produced by this
+        // build) goes straight to Y
+        auto direct = [&]() {
+            const XT h0 = (XT)__ldg(&val[cur]);
+            const XT h = ck == n ? h0 - (XT)hmin : h0;
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+                acc[v] += h * __ldg(&X[(int64_t)ck * ldx + v]);
+                if (ck != n) atomicAdd(&Y[(int64_t)ck * ldy + v], h * xn[v]);
+            }
+            cur++;
+            ck = cur < end ? __ldg(&col[cur]) : INT_MAX;
+        };
+        const int64_t a1 = adj_ptr[c1 + 1];
+        for (int64_t a = adj_ptr[c1]; a < a1; a++) {
+            const int c2 = adj[a];
+            const int64_t k0 = conf_start[c2], k1 = conf_start[c2 + 1];
+            for (int64_t w0 = k0; w0 < k1; w0 += LT_WIN) {
+                const int64_t w1 = min(k1, w0 + LT_WIN);
+                while (ck < w0) direct();
+                while (ck < w1) {
+                    const XT h0 = (XT)__ldg(&val[cur]);
+                    const XT h = ck == n ? h0 - (XT)hmin : h0;
+                    const XT *xk = X + (int64_t)ck * ldx;
+#pragma unroll
+                    for (int v = 0; v < NV; v++) acc[v] += h * __ldg(&xk[v]);
+                    if (ck != n) {
+                        unsigned long long *tt = tb + (ck - w0) * NV;
+#pragma unroll
+                        for (int v = 0; v < NV; v++)
+                            atomicAdd(&tt[v], (unsigned long long)__double2ll_rn((double)(h * xn[v]) * LW_SCALE));
+                    }
+                    cur++;
+                    ck = cur < end ? __ldg(&col[cur]) : INT_MAX;
+                }
+                __syncwarp();
+                const int nw = (int)(w1 - w0) * NV;
+                for (int i = lane; i < nw; i += 32) {
+                    const long long q = (long long)tb[i];
+                    if (q != 0) {
+                        atomicAdd(&Y[(w0 + i / NV) * ldy + (i % NV)], (XT)((double)q / LW_SCALE));
+                        tb[i] = 0ULL;
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        while (ck != INT_MAX) direct();
+        if (mine)
+#pragma unroll
+            for (int v = 0; v < NV; v++) atomicAdd(&Y[n * ldy + v], acc[v]);
+    }
+}
+
 template <typename XT>
 __global__ void k_zero_block(XT *Y, int ldy, int64_t nd, int nv)
 {
@@ -265,10 +369,69 @@ __global__ void k_zero_block(XT *Y, int ldy, int64_t nd, int nv)
         Y[(i / nv) * ldy + (i % nv)] = (XT)0;
 }
 
+// Work items of the tile kernel: (configuration, first row) chunks of up to
+// LT_ROWS rows, heaviest first (determinant pairs per row x rows).
+static void lower_tile_items(const pci_gpu *h, std::vector<int2> &items)
+{
+    std::vector<std::pair<double, int2>> tmp;
+    for (int c = 0; c < h->nc; c++) {
+        const int nr = h->h_ndc[c];
+        const double w = c < (int)h->h_rowwork.size() ? (double)h->h_rowwork[c] : 1.0;
+        for (int r = 0; r < nr; r += LT_ROWS) tmp.push_back({w * std::min(LT_ROWS, nr - r), make_int2(c, r)});
+    }
+    std::stable_sort(tmp.begin(), tmp.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+    items.resize(tmp.size());
+    for (size_t i = 0; i < tmp.size(); i++) items[i] = tmp[i].second;
+}
+
+template <typename VT, typename XT>
+static int spmm_lower_tiles_dispatch(pci_gpu *h, const XT *X, int ldx, XT *Y, int ldy, int nv, cudaStream_t st)
+{
+    const Csr &L = h->H;
+    std::vector<int2> items;
+    lower_tile_items(h, items);
+    int rc = 0;
+    if ((rc = ensure_tmp(h, 64 + items.size() * sizeof(int2)))) return rc;
+    unsigned long long *counter = (unsigned long long *)h->d_tmp;
+    int2 *d_items = (int2 *)((char *)h->d_tmp + 64);
+    PCI_CUDA(h, cudaMemsetAsync(counter, 0, 8, st));
+    PCI_CUDA(h, cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+    k_zero_block<<<148 * 8, 256, 0, st>>>(Y, ldy, L.nrows, nv);
+    const VT *val = (const VT *)L.val;
+    const int64_t nit = (int64_t)items.size();
+#define CASE(N)                                                                                                 \
+    case N: {                                                                                                   \
+        auto kf = k_spmm_lower_tiles<N, VT, XT>;                                                                \
+        const int smem = LT_WARPS * LT_WIN * N * 8;                                                             \
+        cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);                            \
+        int per_sm = 1;                                                                                         \
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf, LT_WARPS * 32, smem);                        \
+        kf<<<148 * std::max(per_sm, 1), LT_WARPS * 32, smem, st>>>(L.rowptr, L.col, val, h->hmin, h->d_conf_start, \
+                                                                  h->d_adj_ptr, h->d_adj, d_items, nit, X, ldx, Y, \
+                                                                  ldy, counter);                                 \
+        break;                                                                                                  \
+    }
+    switch (nv) {
+        CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8)
+        CASE(9) CASE(10) CASE(11) CASE(12) CASE(13) CASE(14) CASE(15) CASE(16)
+    default: return set_err(h, PCI_E_INPUT, "SpMM supports 1..16 vectors");
+    }
+#undef CASE
+    PCI_CUDA(h, cudaGetLastError());
+    return PCI_OK;
+}
+
 template <typename VT, typename XT>
 static int spmm_lower_dispatch(pci_gpu *h, const XT *X, int ldx, XT *Y, int ldy, int nv, cudaStream_t st)
 {
     const Csr &L = h->H;
+    // The tile walk (PCI_SPMM_TILES=1) needs the adjacency of the H built
+    // here.  It is not the default: measured per call it ran 23.7 ms against
+    // 41 ms on the 86k-determinant system but 930 ms against 861 ms on the
+    // 1.06M-determinant one, where its per-tile flushes outweigh what it saves.
+    const char *e = getenv("PCI_SPMM_TILES");
+    if (h->h_from_tiles && h->d_adj && h->have_basis && e && !strcmp(e, "1"))
+        return spmm_lower_tiles_dispatch<VT, XT>(h, X, ldx, Y, ldy, nv, st);
     int rc = 0;
     if ((rc = ensure_tmp(h, 64))) return rc;
     unsigned long long *counter = (unsigned long long *)h->d_tmp;

@@ -244,12 +244,15 @@ def test_bad_determinant_order_is_reported(engine):
     engine.form_h(64)
 
 
-@pytest.mark.parametrize("mode", ["lower", "full"])
+@pytest.mark.parametrize("mode", ["lower", "lower-tiles", "full", "set-csr"])
 def test_davidson_spmm_paths(mode, monkeypatch):
-    """The lower-triangle SpMM (transpose part through shared-memory windows and
-    atomics) and the full symmetric copy give the same Davidson levels."""
+    """The SpMM paths give the same Davidson levels: lower triangle in column
+    windows, lower triangle along the configuration tiles, the full symmetric
+    copy, and an H round-tripped through get_csr/set_csr."""
     from pci_b200.capi import Engine
-    monkeypatch.setenv("PCI_SPMM", mode)
+    monkeypatch.setenv("PCI_SPMM", "full" if mode == "full" else "lower")
+    if mode == "lower-tiles":
+        monkeypatch.setenv("PCI_SPMM_TILES", "1")
     name = "small3"
     s = get_system(name)
     (rp, col, val, nz, hmin, pairs), (jr, jc, jv) = oracle_h(name)
@@ -258,8 +261,11 @@ def test_davidson_spmm_paths(mode, monkeypatch):
     ref = O.diag4(s.nd, (rp, col, val), hmin, (jr, jc, jv), p, s.ndc)
     with Engine(0) as e:
         e.load_system(s)
-        e.form_h(64)
+        numh, _, hm = e.form_h(64)
         e.form_j()
+        if mode == "set-csr":
+            rp2, col2, val2 = e.get_csr(0)
+            e.set_csr(0, rp2, col2, val2, hm)
         res = e.davidson(s.nd, Nlv=p["Nlv"], N_it=25, Crt4=p["Crt4"], MaxNd0=p["MaxNd0"], admix_crit=0.0)
     assert np.max(np.abs(res["Tk"] - ref["Tk"])) <= 1e-8
 
