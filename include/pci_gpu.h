@@ -167,7 +167,8 @@ int32_t pci_gpu_jterms(pci_gpu_t *h, int32_t *out, int32_t cap);
  * adjacency build, [9] determinant pairs with difference <= 2, [10]
  * determinant pairs compared, [11] kernel launches of the last FormH,
  * [12] FormH compaction, [13] 1 when the last FormH took the single-
- * evaluation build, 0 for the two-pass build.  n is the capacity of `out`;
+ * evaluation build, 0 for the two-pass build, [14] element slots of the
+ * padded rows in the single-evaluation build.  n is the capacity of `out`;
  * returns the number written. */
 int32_t pci_gpu_stats(pci_gpu_t *h, double *out, int32_t n);
 

@@ -199,9 +199,9 @@ class Engine:
         return out[:n].tolist()
 
     def stats(self):
-        out = np.zeros(14)
-        n = self.L.pci_gpu_stats(self.h, _p(out), 14)
+        out = np.zeros(15)
+        n = self.L.pci_gpu_stats(self.h, _p(out), 15)
         keys = ["formh_ms", "formh_count_ms", "formh_fill_ms", "formj_ms", "davidson_ms", "spmm_ms",
                 "spmm_calls", "init_ms", "adjacency_ms", "pairs", "scanned", "formh_launches",
-                "formh_compact_ms", "formh_single_eval"]
+                "formh_compact_ms", "formh_single_eval", "formh_slots"]
         return dict(zip(keys[:n], out[:n].tolist()))

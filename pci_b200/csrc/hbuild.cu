@@ -16,11 +16,12 @@
 // the warp looks them up once per tile into a shared-memory cache.  Pairs are
 // compared on occupation lists (Ne <= 8 m-states as uint16); non-zeros are
 // compacted per row with __match_any_sync/__ballot_sync/__popc so each row's
-// columns stay ascending.  Two builds: single evaluation (count the
-// candidate pairs per row without evaluating them, evaluate once into
-// rows padded to that bound, squeeze the rows into CSR), taken when the
+// columns stay ascending.  Two builds: single evaluation (bound the
+// candidate pairs of each row from the configurations alone, evaluate once
+// into rows padded to that bound, squeeze the rows into CSR), taken when the
 // padded rows fit in device memory; otherwise two passes (count with values
 // evaluated and zeros dropped, then, after a scan, fill straight into CSR).
+// The fill checks every write against its row's slots.
 #include <algorithm>
 #include <cmath>
 #include <cstring>

@@ -678,6 +678,7 @@ struct WarpSmem {
         TilePlan plan;   // one- and two-orbital tiles
     } c;
     int64_t rowbase[TR];
+    int64_t rowend[TR];      // end of each row's slots (fill pass)
     int32_t rowcnt[TR];
     uint16_t drow[TR * NE];
     uint16_t orow[TR * NE];  // orbital of each row m-state
@@ -776,8 +777,12 @@ __device__ __forceinline__ void eval_queue(const DevSys &S, WarpSmem<NE> *ws, in
             if (vd < ty.hmin) ty.hmin = vd;
             if (FILL) {
                 int64_t pos = ws->rowbase[r] + cur + __popc(same & lt);
-                col[pos] = (int32_t)k;
-                val[pos] = vs;
+                if (pos < ws->rowend[r]) {
+                    col[pos] = (int32_t)k;
+                    val[pos] = vs;
+                } else {
+                    atomicOr(S.err, DERR_ROW_SLOTS);
+                }
             }
             if ((same & lt) == 0) ws->rowcnt[r] = cur + __popc(same);
         }
@@ -798,8 +803,6 @@ __device__ __forceinline__ void eval_queue(const DevSys &S, WarpSmem<NE> *ws, in
 // FILL 0: per-row non-zero counts into rowinfo (values evaluated).
 // FILL 1: rowinfo holds each row's first slot; non-zeros are written there
 //         and, when rowcnt_out is given, each row's count goes to rowcnt_out.
-// FILL 2: per-row candidate counts (difference <= 2) into rowinfo, nothing
-//         evaluated: the slot bound of the single-evaluation build.
 template <int NE, int KIND, int FILL, typename VT>
 __global__ void __launch_bounds__(WARPS * 32, PCI_TILES_MIN_BLOCKS) k_tiles(DevSys S, const int4 *items, int64_t nitems,
                                                       unsigned long long *counter, int64_t *rowinfo, int32_t *col,
@@ -833,15 +836,14 @@ __global__ void __launch_bounds__(WARPS * 32, PCI_TILES_MIN_BLOCKS) k_tiles(DevS
             for (int i = lane; i < nrc * NE; i += 32) {
                 const uint16_t m = S.occ[rb * NE + i];
                 ws->drow[i] = m;
-                if (FILL != 2) {
-                    const uint32_t w = __ldg(&S.msd[m]);
-                    ws->trow[i] = (uint8_t)((w >> 10) & 63u);
-                    ws->orow[i] = (uint16_t)(w & 1023u);
-                }
+                const uint32_t w = __ldg(&S.msd[m]);
+                ws->trow[i] = (uint8_t)((w >> 10) & 63u);
+                ws->orow[i] = (uint16_t)(w & 1023u);
             }
             for (int i = lane; i < nrc; i += 32) {
                 ws->rowcnt[i] = 0;
                 ws->rowbase[i] = FILL == 1 ? rowinfo[rb + i] : 0;
+                ws->rowend[i] = FILL == 1 ? rowinfo[rb + i + 1] : 0;
             }
             __syncwarp();
             for (int64_t a = a0; a < a1; a++) {
@@ -850,7 +852,7 @@ __global__ void __launch_bounds__(WARPS * 32, PCI_TILES_MIN_BLOCKS) k_tiles(DevS
                 const int nk = (int)(S.conf_start[c2 + 1] - k0);
                 const bool diag = c2 == c1;
                 int tkind = TILE_GENERIC;
-                if (KIND == 0 && FILL != 2) {
+                if (KIND == 0) {
                     uint16_t o2[NE];
 #pragma unroll
                     for (int e = 0; e < NE; e++) o2[e] = S.conf_orb[(int64_t)c2 * NE + e];
@@ -863,7 +865,7 @@ __global__ void __launch_bounds__(WARPS * 32, PCI_TILES_MIN_BLOCKS) k_tiles(DevS
                     for (int i = lane; i < nkc * NE; i += 32) {
                         const uint16_t m = S.occ[(k0 + kc) * NE + i];
                         ws->u.t.dcol[i] = m;
-                        if (FILL != 2) ws->u.t.tcol[i] = (uint8_t)((__ldg(&S.msd[m]) >> 10) & 63u);
+                        ws->u.t.tcol[i] = (uint8_t)((__ldg(&S.msd[m]) >> 10) & 63u);
                     }
                     __syncwarp();
                     const int np = nrc * nkc;
@@ -888,18 +890,6 @@ __global__ void __launch_bounds__(WARPS * 32, PCI_TILES_MIN_BLOCKS) k_tiles(DevS
                             cand = KIND == 0 ? nf <= 2 : (nf == 0 || nf == 2);
                         }
                         const unsigned cm = __ballot_sync(FULL_MASK, cand);
-                        if (FILL == 2) {
-                            // the lanes of one row are a contiguous run; its first lane adds the run's count
-                            if (idx < np) {
-                                const int lo = max(r * nkc - base, 0), hi = min((r + 1) * nkc - base, 32);
-                                if (lane == lo) {
-                                    const unsigned run = (hi == 32 ? FULL_MASK : ((1u << hi) - 1u)) & ~((1u << lo) - 1u);
-                                    ws->rowcnt[r] += __popc(cm & run);
-                                }
-                            }
-                            __syncwarp();
-                            continue;
-                        }
                         if (cand) ws->u.t.queue[qn + __popc(cm & lt)] = ((uint32_t)r << 16) | (uint32_t)kk;
                         qn += __popc(cm);
                         __syncwarp();
@@ -935,6 +925,122 @@ __global__ void __launch_bounds__(WARPS * 32, PCI_TILES_MIN_BLOCKS) k_tiles(DevS
     }
 }
 
+// ------------------------------------------------------ candidate bound ---
+
+// Pairs of m values (2m units) of two electrons placed in orbitals with 2j =
+// j0 and j1 (the same orbital when same: distinct, unordered) whose sum is
+// m2.  All 2m values are odd and m2 is even, so the odd members of an
+// interval are counted in closed form.
+__device__ __forceinline__ int pair_fillings(int j0, int j1, bool same, int m2)
+{
+    int lo, hi;
+    if (!same) {
+        lo = max(-j0, m2 - j1);
+        hi = min(j0, m2 + j1);
+    } else {
+        // m0 < m1 = m2 - m0 <= j0
+        lo = max(-j0, m2 - j0);
+        const int h = m2 / 2;
+        hi = (h & 1) ? h - 2 : h - 1;
+    }
+    return hi >= lo ? (hi - lo) / 2 + 1 : 0;
+}
+
+// Upper bound on the candidate pairs (difference <= 2) of every row, from
+// the configurations alone.  For a tile whose configurations differ by two
+// orbitals, C+{A0,A1} against C+{B0,B1}, with no A or B orbital in C, a
+// column determinant is a candidate exactly when it holds the row's
+// m-states in C, and then its two electrons in B0, B1 must carry the m of
+// the row's two electrons in A0, A1: the count is pair_fillings.  Other
+// tiles count every column determinant (the diagonal tile: those up to the
+// row).  One lane per row; the next 32 tiles' descriptions are loaded one
+// per lane.
+template <int NE>
+__global__ void __launch_bounds__(256) k_bound(DevSys S, const int4 *items, int64_t nitems, unsigned long long *counter,
+                                               int64_t *bound)
+{
+    const int lane = threadIdx.x & 31;
+    while (true) {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(counter, 1ULL);
+        t = __shfl_sync(FULL_MASK, t, 0);
+        if (t >= (unsigned long long)nitems) break;
+        const int4 it = items[t];
+        const int c1 = it.x;
+        const int64_t cs1 = S.conf_start[c1];
+        uint16_t o1[NE];
+#pragma unroll
+        for (int e = 0; e < NE; e++) o1[e] = S.conf_orb[(int64_t)c1 * NE + e];
+        const int64_t a0 = S.adj_ptr[c1], a1 = S.adj_ptr[c1 + 1];
+        for (int rp = 0; rp < it.z; rp += 32) {
+            const int64_t n = cs1 + it.y + rp + lane;
+            const bool mine = rp + lane < it.z;
+            int ro[NE], rjz[NE];
+#pragma unroll
+            for (int e = 0; e < NE; e++) {
+                const uint32_t w = mine ? __ldg(&S.msd[S.occ[n * NE + e]]) : 0u;
+                ro[e] = (int)(w & 1023u);
+                rjz[e] = (int)((w >> 16) & 255u) - 128;
+            }
+            int64_t cnt = 0;
+            for (int64_t ab = a0; ab < a1; ab += 32) {
+                const int64_t al = ab + lane;
+                int c2l = c1;
+                int64_t k0l = 0, k1l = 0;
+                uint32_t o2l[(NE + 1) / 2];
+#pragma unroll
+                for (int e = 0; e < (NE + 1) / 2; e++) o2l[e] = 0u;
+                if (al < a1) {
+                    c2l = S.adj[al];
+                    k0l = S.conf_start[c2l];
+                    k1l = S.conf_start[c2l + 1];
+#pragma unroll
+                    for (int e = 0; e < NE; e++)
+                        o2l[e >> 1] |= (uint32_t)S.conf_orb[(int64_t)c2l * NE + e] << (16 * (e & 1));
+                }
+                const int na = (int)(a1 - ab < 32 ? a1 - ab : 32);
+                for (int j = 0; j < na; j++) {
+                    const int c2 = __shfl_sync(FULL_MASK, c2l, j);
+                    const int64_t k0 = __shfl_sync(FULL_MASK, k0l, j);
+                    const int64_t nk = __shfl_sync(FULL_MASK, k1l, j) - k0;
+                    if (c2 == c1) {
+                        cnt += n - cs1 + 1;
+                        continue;
+                    }
+                    int o2[NE];
+#pragma unroll
+                    for (int e = 0; e < NE; e++) o2[e] = (int)((__shfl_sync(FULL_MASK, o2l[e >> 1], j) >> (16 * (e & 1))) & 0xffffu);
+                    // multiset differences A = c1 - c2, B = c2 - c1 and the common part
+                    int A[NE], B[NE], Cm[NE], nA = 0, nB = 0, nC = 0;
+                    {
+                        int i = 0, k = 0;
+                        while (i < NE && k < NE) {
+                            if (o1[i] == o2[k]) { Cm[nC++] = o1[i]; i++; k++; }
+                            else if (o1[i] < o2[k]) A[nA++] = o1[i++];
+                            else B[nB++] = o2[k++];
+                        }
+                        while (i < NE) A[nA++] = o1[i++];
+                        while (k < NE) B[nB++] = o2[k++];
+                    }
+                    bool typical = nA == 2;
+                    for (int x = 0; x < nC && typical; x++)
+                        if (Cm[x] == A[0] || Cm[x] == A[1] || Cm[x] == B[0] || Cm[x] == B[1]) typical = false;
+                    if (!typical) {
+                        cnt += nk;
+                        continue;
+                    }
+                    int m2 = 0;
+#pragma unroll
+                    for (int e = 0; e < NE; e++)
+                        if (ro[e] == A[0] || ro[e] == A[1]) m2 += rjz[e];
+                    cnt += pair_fillings(S.orb_j[B[0]], S.orb_j[B[1]], B[0] == B[1], m2);
+                }
+            }
+            if (mine) bound[n] = cnt;
+        }
+    }
+}
+
 // Work items (configuration, first row, row count), heaviest first.  A
 // configuration's rows are split so that no item holds much more than
 // `target` determinant pairs; for J^2 every configuration is one item.
@@ -967,9 +1073,9 @@ static inline void make_items(const pci_gpu *h, const std::vector<unsigned long 
     for (auto &p : tmp) items.push_back(p.second);
 }
 
-// Which FormH layout to build: the single-evaluation build (candidate
-// bound per row, values evaluated once into padded rows, then compacted)
-// needs slots for every candidate pair; the two-pass build (count, then
+// Which FormH layout to build: the single-evaluation build (a bound on the
+// candidate pairs of each row from the configurations, values evaluated
+// once into rows padded to it, then compacted) needs slots for every bound; the two-pass build (count, then
 // fill) needs exactly NumH slots but evaluates every value twice.
 // PCI_FORMH=exact|padded forces one; by default padded is taken when its
 // slots and the compaction buffer fit in free device memory.
@@ -1022,12 +1128,10 @@ static int rows_impl(pci_gpu *h, int value_prec, Csr &out, RowStats *hs)
     auto kc32 = k_tiles<NE, KIND, 0, float>;
     auto kf64 = k_tiles<NE, KIND, 1, double>;
     auto kf32 = k_tiles<NE, KIND, 1, float>;
-    auto ksc = k_tiles<NE, KIND, 2, double>;
     cudaFuncSetAttribute(kc64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(kc32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(kf64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(kf32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(ksc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kc64, WARPS * 32, smem);
     int dev_sms = 148;
@@ -1049,6 +1153,7 @@ static int rows_impl(pci_gpu *h, int value_prec, Csr &out, RowStats *hs)
         if (!derr) return PCI_OK;
         PCI_CUDA(h, cudaMemset(h->d_err, 0, 4));
         if (derr & DERR_MISSING_INTEGRAL) return set_err(h, PCI_E_MISSING_INTEGRAL, "Gint: integral is absent");
+        if (derr & DERR_ROW_SLOTS) return set_err(h, PCI_E_CUDA, "FormH: a row produced more elements than its slots");
         return set_err(h, PCI_E_INPUT, "Gint error: ma+mb /= mc+md (determinant list inconsistent)");
     };
     auto launch_fill = [&](int64_t *rowinfo, int64_t *rowcnt_out, RowStats *st) {
@@ -1073,7 +1178,7 @@ static int rows_impl(pci_gpu *h, int value_prec, Csr &out, RowStats *hs)
     cudaEventRecord(e0, h->st);
     if (KIND == 0 && forced != 0) {
         // Single evaluation: candidate bound per row, padded fill, compaction.
-        ksc<<<blocks, WARPS * 32, smem, h->st>>>(S, d_items, nit, d_counter, cnt, nullptr, nullptr, nullptr, nullptr);
+        k_bound<NE><<<dev_sms * 8, 256, 0, h->st>>>(S, d_items, nit, d_counter, cnt);
         PCI_CUDA(h, cudaGetLastError());
         pptr = (int64_t *)dev_alloc(h, (nd + 1) * 8, &rc);
         if (rc) return cleanup(rc);
@@ -1108,6 +1213,7 @@ static int rows_impl(pci_gpu *h, int value_prec, Csr &out, RowStats *hs)
             cudaEventElapsedTime(&t12, e1, e2);
             cudaEventElapsedTime(&t23, e2, e3);
             h->st_formh_padded = 1;
+            h->st_formh_slots = (double)ncand;
             h->st_formh_compact = t23;
             done = true;
         } else {

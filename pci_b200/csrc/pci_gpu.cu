@@ -454,11 +454,11 @@ int pci_gpu_j_av(pci_gpu_t *h, const double *X, int32_t nv, int64_t nlim, double
 int32_t pci_gpu_stats(pci_gpu_t *h, double *out, int32_t n)
 {
     if (!h || !out) return 0;
-    double v[14] = {h->st_formh, h->st_formh_count, h->st_formh_fill, h->st_formj,
+    double v[15] = {h->st_formh, h->st_formh_count, h->st_formh_fill, h->st_formj,
                     h->st_dvd, h->st_spmm, h->st_spmm_calls, h->st_init,
                     h->st_adj, h->st_pairs, h->st_scanned, h->st_launches,
-                    h->st_formh_compact, h->st_formh_padded};
-    int32_t m = std::min<int32_t>(n, 14);
+                    h->st_formh_compact, h->st_formh_padded, h->st_formh_slots};
+    int32_t m = std::min<int32_t>(n, 15);
     for (int i = 0; i < m; i++) out[i] = v[i];
     return m;
 }

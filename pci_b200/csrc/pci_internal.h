@@ -15,6 +15,7 @@
 #define DERR_MISSING_INTEGRAL 1u
 #define DERR_M_NOT_CONSERVED  2u
 #define DERR_BAD_INDEX        4u
+#define DERR_ROW_SLOTS        8u   // a row produced more elements than its slots
 
 struct Csr {
     int64_t nrows = 0, nnz = 0;
@@ -95,7 +96,7 @@ struct pci_gpu {
     double st_formh = 0, st_formh_count = 0, st_formh_fill = 0, st_formj = 0;
     double st_dvd = 0, st_spmm = 0, st_spmm_calls = 0, st_init = 0;
     double st_adj = 0, st_pairs = 0, st_scanned = 0, st_launches = 0;
-    double st_formh_compact = 0, st_formh_padded = 0, st_formh_compact_launches = 0;
+    double st_formh_compact = 0, st_formh_padded = 0, st_formh_compact_launches = 0, st_formh_slots = 0;
     bool h_from_tiles = false;  // H was built here by form_h: its rows follow the adjacency tiles
     int spmm_mode = 0;        // 0 auto, 1 full symmetric copy, 2 lower triangle (env PCI_SPMM)
     int spmm_lower_used = 0;
