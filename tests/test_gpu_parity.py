@@ -219,6 +219,35 @@ def test_fp32_form_needs_fp32_h(engine):
     assert ei.value.code == 1
 
 
+@pytest.mark.parametrize("build", ["padded", "exact"])
+@pytest.mark.parametrize("name", ["tiny", "cfg1", "small3"])
+def test_form_h_matches_golden(engine, name, build, monkeypatch):
+    """The CUDA FormH against the committed fixtures (independent of the
+    oracle code): CSR SHA-256, NumH, numzero and Hmin; then the Davidson
+    levels over the fixture's iterations."""
+    import hashlib
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", f"{name}.npz"))
+    s = get_system(name)
+    _load(engine, s)
+    monkeypatch.setenv("PCI_FORMH", build)
+    numh, numzero, hmin = engine.form_h(64)
+    rp, col, val = engine.get_csr(0)
+    h = hashlib.sha256()
+    for a, t in ((rp, np.int64), (col, np.int32), (val, np.float64)):
+        h.update(np.ascontiguousarray(a, t).tobytes())
+    assert (numh, numzero, hmin) == (int(g["numh"]), int(g["numzero"]), float(g["hmin"]))
+    assert h.hexdigest() == str(g["h_sha"])
+    assert engine.jterms() == g["jterms"].tolist()
+    engine.form_j()
+    p = dict(s.params)
+    n_it = int(g["n_it"]) if int(g["n_it"]) > 0 else p["N_it"]
+    crit = 0.0 if int(g["n_it"]) > 0 else p["admix_crit"]
+    res = engine.davidson(s.nd, Nlv=p["Nlv"], N_it=n_it, Crt4=p["Crt4"], MaxNd0=p["MaxNd0"], admix_crit=crit)
+    assert res["iterations"] == int(g["iterations"])
+    assert np.max(np.abs(res["Tk"] - g["tk"])) <= 1e-8
+
+
 def test_missing_integral_is_reported(engine):
     from pci_b200.capi import PciError
     kw = S.CONFIGS["tiny"]()
