@@ -63,7 +63,7 @@ double host_gaunt(int nlx, const double *lut, int64_t nlut, int k, double xj1, d
 
 #include "hbuild_impl.cuh"
 
-__global__ void k_hash_insert(unsigned long long *keys, unsigned int *pos, unsigned long long mask,
+__global__ void k_hash_insert(unsigned long long *htab, int hw, unsigned int *pos, unsigned long long mask,
                               const int32_t *iint2, const int32_t *iint3, int64_t n, unsigned int *err)
 {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -73,7 +73,7 @@ __global__ void k_hash_insert(unsigned long long *keys, unsigned int *pos, unsig
         unsigned long long s = hmix(key) & mask;
         int p = 0;
         for (; p < PCI_MAX_PROBE; p++) {
-            unsigned long long prev = atomicCAS(&keys[s], 0ULL, key);
+            unsigned long long prev = atomicCAS(&htab[s * hw], 0ULL, key);
             if (prev == 0ULL || prev == key) {
                 atomicMin(&pos[s], (unsigned int)i);  // first occurrence wins, as in FindGint
                 break;
@@ -85,14 +85,15 @@ __global__ void k_hash_insert(unsigned long long *keys, unsigned int *pos, unsig
 }
 
 template <typename RT>
-__global__ void k_hash_fill(const unsigned long long *keys, const unsigned int *pos, double *vals,
-                            unsigned long long cap, const RT *r2, int stride)
+__global__ void k_hash_fill(unsigned long long *htab, int hw, const unsigned int *pos, unsigned long long cap,
+                            const RT *r2, int stride)
 {
     for (unsigned long long s = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; s < cap;
          s += (unsigned long long)gridDim.x * blockDim.x) {
-        if (keys[s] != 0ULL) {
+        if (htab[s * hw] != 0ULL) {
             unsigned long long p = pos[s];
-            for (int c = 0; c < stride; c++) vals[s * stride + c] = (double)r2[p * stride + c];
+            for (int c = 0; c < stride; c++)
+                htab[s * hw + 1 + c] = (unsigned long long)__double_as_longlong((double)r2[p * stride + c]);
         }
     }
 }
@@ -105,12 +106,13 @@ int hb_build_hash(pci_gpu *h, int64_t ngint, int kbrt, int r2_is_f64, const void
     while (cap < 2ULL * (unsigned long long)ngint) cap <<= 1;
     int stride = kbrt ? 2 : 1;
     int rc = 0;
-    dev_free(h->d_hkey);
-    dev_free(h->d_hval);
-    h->d_hkey = (unsigned long long *)dev_alloc(h, cap * 8, &rc);
+    // key and value(s) of a slot share one 16-byte (32 with Breit) line, so
+    // a probe reads both with one load
+    const int hw = stride == 2 ? 4 : 2;
+    dev_free(h->d_htab);
+    h->d_htab = (unsigned long long *)dev_alloc(h, cap * 8 * hw, &rc);
     if (rc) return rc;
-    h->d_hval = (double *)dev_alloc(h, cap * 8 * stride, &rc);
-    if (rc) return rc;
+    h->hw = hw;
     h->hcap = cap;
     size_t esz = r2_is_f64 ? 8 : 4;
     size_t need = cap * 4 + (size_t)ngint * (8 + esz * stride);
@@ -119,17 +121,16 @@ int hb_build_hash(pci_gpu *h, int64_t ngint, int kbrt, int r2_is_f64, const void
     int32_t *d_i2 = (int32_t *)((char *)h->d_tmp + cap * 4);
     int32_t *d_i3 = d_i2 + ngint;
     void *d_r2 = (void *)(d_i3 + ngint);
-    PCI_CUDA(h, cudaMemsetAsync(h->d_hkey, 0, cap * 8, h->st));
-    PCI_CUDA(h, cudaMemsetAsync(h->d_hval, 0, cap * 8 * stride, h->st));
+    PCI_CUDA(h, cudaMemsetAsync(h->d_htab, 0, cap * 8 * hw, h->st));
     PCI_CUDA(h, cudaMemsetAsync(d_pos, 0xff, cap * 4, h->st));
     PCI_CUDA(h, cudaMemcpyAsync(d_i2, iint2, ngint * 4, cudaMemcpyHostToDevice, h->st));
     PCI_CUDA(h, cudaMemcpyAsync(d_i3, iint3, ngint * 4, cudaMemcpyHostToDevice, h->st));
     PCI_CUDA(h, cudaMemcpyAsync(d_r2, rint2, (size_t)ngint * esz * stride, cudaMemcpyHostToDevice, h->st));
-    k_hash_insert<<<148 * 8, 256, 0, h->st>>>(h->d_hkey, d_pos, cap - 1, d_i2, d_i3, ngint, h->d_err);
+    k_hash_insert<<<148 * 8, 256, 0, h->st>>>(h->d_htab, hw, d_pos, cap - 1, d_i2, d_i3, ngint, h->d_err);
     if (r2_is_f64)
-        k_hash_fill<double><<<148 * 8, 256, 0, h->st>>>(h->d_hkey, d_pos, h->d_hval, cap, (const double *)d_r2, stride);
+        k_hash_fill<double><<<148 * 8, 256, 0, h->st>>>(h->d_htab, hw, d_pos, cap, (const double *)d_r2, stride);
     else
-        k_hash_fill<float><<<148 * 8, 256, 0, h->st>>>(h->d_hkey, d_pos, h->d_hval, cap, (const float *)d_r2, stride);
+        k_hash_fill<float><<<148 * 8, 256, 0, h->st>>>(h->d_htab, hw, d_pos, cap, (const float *)d_r2, stride);
     PCI_CUDA(h, cudaGetLastError());
     unsigned int e = 0;
     PCI_CUDA(h, cudaMemcpyAsync(&e, h->d_err, 4, cudaMemcpyDeviceToHost, h->st));

@@ -32,14 +32,24 @@ __host__ __device__ __forceinline__ unsigned long long hkey(int iac, int ibd)
 
 // ------------------------------------------------------- device physics ---
 
+// One hash slot: key and value(s) with one 16-byte load (two with Breit).
+__device__ __forceinline__ unsigned long long hslot(const DevSys &S, unsigned long long s, double &v0, double &v1)
+{
+    const ulonglong2 *p = reinterpret_cast<const ulonglong2 *>(S.htab) + s * (S.hw >> 1);
+    const ulonglong2 a = __ldg(p);
+    v0 = __longlong_as_double((long long)a.y);
+    v1 = S.hw == 4 ? __longlong_as_double((long long)__ldg(p + 1).x) : 0.0;
+    return a.x;
+}
+
 __device__ __forceinline__ double d_lookup(const DevSys &S, int iac, int ibd, int comp)
 {
     unsigned long long key = hkey(iac, ibd);
     unsigned long long s = hmix(key) & S.hmask;
-    int stride = S.kbrt ? 2 : 1;
     for (int p = 0; p < PCI_MAX_PROBE; p++) {
-        unsigned long long k = __ldg(&S.hkey[s]);
-        if (k == key) return __ldg(&S.hval[s * stride + comp]);
+        double v0, v1;
+        const unsigned long long k = hslot(S, s, v0, v1);
+        if (k == key) return comp ? v1 : v0;
         if (k == 0ULL) break;
         s = (s + 1) & S.hmask;
     }
@@ -467,8 +477,9 @@ static __device__ bool plan_quad(const DevSys &S, QuadTerms *P, int qa, int qb, 
         unsigned long long s = hmix(key) & S.hmask;
         found = false;
         for (int p = 0; p < PCI_MAX_PROBE; p++) {
-            const unsigned long long kq = __ldg(&S.hkey[s]);
-            if (kq == key) { r = __ldg(&S.hval[s]); found = true; break; }
+            double v0, v1;
+            const unsigned long long kq = hslot(S, s, v0, v1);
+            if (kq == key) { r = v0; found = true; break; }
             if (kq == 0ULL) break;
             s = (s + 1) & S.hmask;
         }
@@ -611,7 +622,6 @@ __device__ int prepare_tile(const DevSys &S, TileCache *tc, TilePlan *plan, unsi
     }
     nkeys = __shfl_sync(FULL_MASK, nkeys, 0);
     __syncwarp();
-    const int stride = S.kbrt ? 2 : 1;
     for (int base = 0; base < nkeys; base += 32) {
         int idx = base + lane;
         unsigned long long key = idx < nkeys ? keys[idx] : 0ULL;
@@ -623,11 +633,12 @@ __device__ int prepare_tile(const DevSys &S, TileCache *tc, TilePlan *plan, unsi
             // cache, so the element that needs it reports the missing integral
             unsigned long long s = hmix(key) & S.hmask;
             for (int p = 0; p < PCI_MAX_PROBE; p++) {
-                unsigned long long kk = __ldg(&S.hkey[s]);
+                double v0, v1;
+                const unsigned long long kk = hslot(S, s, v0, v1);
                 if (kk == key) {
                     tc->key[slot] = key;
-                    tc->val[2 * slot] = __ldg(&S.hval[s * stride]);
-                    tc->val[2 * slot + 1] = stride == 2 ? __ldg(&S.hval[s * stride + 1]) : 0.0;
+                    tc->val[2 * slot] = v0;
+                    tc->val[2 * slot + 1] = v1;
                     break;
                 }
                 if (kk == 0ULL) break;

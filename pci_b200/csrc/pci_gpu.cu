@@ -69,7 +69,7 @@ DevSys make_devsys(const pci_gpu *h)
     S.adj_ptr = h->d_adj_ptr; S.adj = h->d_adj;
     S.ms_orb = h->d_ms_orb; S.ms_jz = h->d_ms_jz; S.ms_type = h->d_ms_type; S.msd = h->d_msd;
     S.orb_l = h->d_orb_l; S.orb_j = h->d_orb_j;
-    S.h1 = h->d_h1; S.gaunt = h->d_gaunt; S.hkey = h->d_hkey; S.hval = h->d_hval;
+    S.h1 = h->d_h1; S.gaunt = h->d_gaunt; S.htab = h->d_htab; S.hw = h->hw;
     S.hmask = h->hcap ? h->hcap - 1 : 0;
     S.err = h->d_err;
     return S;
@@ -475,7 +475,7 @@ void pci_gpu_destroy(pci_gpu_t *h)
     if (h->st) cudaStreamSynchronize(h->st);
     free_basis(h);
     csr_free(h->H); csr_free(h->J); csr_free(h->Hfull);
-    dev_free(h->d_h1); dev_free(h->d_gaunt); dev_free(h->d_hkey); dev_free(h->d_hval);
+    dev_free(h->d_h1); dev_free(h->d_gaunt); dev_free(h->d_htab);
     dev_free(h->d_err); dev_free(h->d_tmp);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;

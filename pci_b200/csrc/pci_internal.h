@@ -45,8 +45,10 @@ struct DevSys {
     const int8_t *orb_j;        // [nsu] 2j
     const double *h1;           // [nsu*nsu] one-electron integrals, 0 unless kappa equal
     const double *gaunt;        // [kdim][ntype][ntype]
-    const unsigned long long *hkey;  // [hcap] 0 = empty
-    const double *hval;         // [hcap*(kbrt?2:1)]
+    // radial-integral hash: slot s = 2 (or 4 with the Breit term) 64-bit
+    // words at htab + s * hw: key, value(s); key 0 = empty
+    const unsigned long long *htab;
+    int hw;
     unsigned long long hmask;
     unsigned int *err;
 };
@@ -81,8 +83,8 @@ struct pci_gpu {
     double *d_h1 = nullptr;
     double *d_gaunt = nullptr;
     int kdim = 0, ntype = 0, nlx = 0, kbrt = 0;
-    unsigned long long *d_hkey = nullptr;
-    double *d_hval = nullptr;
+    unsigned long long *d_htab = nullptr;   // interleaved key/value slots
+    int hw = 2;
     unsigned long long hcap = 0;
     // matrices
     Csr H, J, Hfull;
