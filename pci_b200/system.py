@@ -409,6 +409,40 @@ def cfg1(seed=1):
                 params=dict(Nlv=6, MaxNd0=3000))
 
 
+# Small systems at the other electron counts the H-build is compiled for
+# (one translation unit per Ne), used by the parity tests.
+@_register
+def ne1(seed=21):
+    """One electron: every element is a one-electron (Hint) element."""
+    shells = _shells({0: (3, 8), 1: (3, 6), 2: (3, 5)})
+    return dict(name="ne1", shells=shells, ne=1, mj=1, parity=0, refs=[[1]], seed=seed,
+                params=dict(Nlv=3, MaxNd0=6))
+
+
+@_register
+def ne5(seed=22):
+    """Five electrons over eleven orbitals."""
+    shells = _shells({0: (3, 5), 1: (3, 4), 2: (3, 4)})
+    return dict(name="ne5", shells=shells, ne=5, mj=1, parity=1, refs=[[1, 1, 2, 3, 3]], seed=seed,
+                params=dict(Nlv=3, MaxNd0=200))
+
+
+@_register
+def ne6(seed=23):
+    """Six electrons over eight orbitals."""
+    shells = _shells({0: (3, 4), 1: (3, 4), 2: (3, 3)})
+    return dict(name="ne6", shells=shells, ne=6, mj=0, parity=0, refs=[[1, 1, 2, 2, 3, 3]], seed=seed,
+                params=dict(Nlv=3, MaxNd0=200))
+
+
+@_register
+def ne8(seed=24):
+    """Eight electrons over eight orbitals (the largest Ne compiled)."""
+    shells = _shells({0: (3, 4), 1: (3, 4), 2: (3, 3)})
+    return dict(name="ne8", shells=shells, ne=8, mj=0, parity=0, refs=[[1, 1, 2, 2, 3, 3, 4, 4]], seed=seed,
+                params=dict(Nlv=3, MaxNd0=200))
+
+
 def _random_refs(shells, ne, parity, n, nlow, seed):
     b = make_basis(shells)
     rng = np.random.default_rng(seed)

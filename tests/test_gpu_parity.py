@@ -248,6 +248,40 @@ def test_form_h_matches_golden(engine, name, build, monkeypatch):
     assert np.max(np.abs(res["Tk"] - g["tk"])) <= 1e-8
 
 
+@pytest.mark.parametrize("build", ["padded", "exact"])
+@pytest.mark.parametrize("name", ["ne1", "ne5", "ne6", "ne8"])
+def test_form_h_other_electron_counts(engine, name, build, monkeypatch):
+    """The H-build units for Ne = 1, 5, 6 and 8 (one per electron count):
+    pattern, values (bit for bit), numzero, Hmin and J^2 as the oracle."""
+    s = get_system(name)
+    (rp, col, val, nz, hmin, pairs), (jr, jc, jv) = oracle_h(name)
+    _load(engine, s)
+    monkeypatch.setenv("PCI_FORMH", build)
+    numh, numzero, ghmin = engine.form_h(64)
+    grp, gcol, gval = engine.get_csr(0)
+    assert numzero == nz and ghmin == hmin
+    assert np.array_equal(grp, rp) and np.array_equal(gcol, col)
+    assert np.array_equal(gval.view(np.int64), val.view(np.int64))
+    engine.form_j()
+    jrp, jcol, jval = engine.get_csr(1)
+    assert np.array_equal(jrp, jr) and np.array_equal(jcol, jc) and np.array_equal(jval, jv)
+
+
+@pytest.mark.parametrize("name", ["ne1", "ne5", "ne8"])
+def test_davidson_other_electron_counts(engine, name):
+    """Ten Davidson iterations (or convergence) give the oracle's levels."""
+    s = get_system(name)
+    (rp, col, val, nz, hmin, pairs), (jr, jc, jv) = oracle_h(name)
+    p = dict(s.params, N_it=10, admix_crit=0.0)
+    ref = O.diag4(s.nd, (rp, col, val), hmin, (jr, jc, jv), p, s.ndc)
+    _load(engine, s)
+    engine.form_h(64)
+    engine.form_j()
+    res = engine.davidson(s.nd, Nlv=p["Nlv"], N_it=10, Crt4=p["Crt4"], MaxNd0=p["MaxNd0"], admix_crit=0.0)
+    assert res["iterations"] == ref["iterations"]
+    assert np.max(np.abs(res["Tk"] - ref["Tk"])) <= 1e-8
+
+
 def test_missing_integral_is_reported(engine):
     from pci_b200.capi import PciError
     kw = S.CONFIGS["tiny"]()
