@@ -295,7 +295,7 @@ def run_ours(args):
             "max_residual": float(np.max(res["resid"])),
             "spmm_roofline": {"bound": "hbm", "achieved": sp_ach, "peak": peak, "unit": "GB/s",
                               "frac": sp_ach / peak, "algorithmic_bytes": int(spmm_bytes),
-                              "storage": "lower triangle, transpose via windows + atomics"
+                              "storage": "lower triangle, transpose by global reductions"
                               if os.environ.get("PCI_SPMM") == "lower" or numh * 24 > 100e9
                               else "full symmetric copy"},
         }

@@ -362,6 +362,54 @@ __global__ void __launch_bounds__(LT_WARPS * 32) k_spmm_lower_tiles(
     }
 }
 
+// ------------------------- lower-triangle SpMM with transpose reductions ---
+//
+// Same product, one warp per row with NV lanes per stored element (as the
+// full-copy kernel): the row part accumulates in registers and is reduced
+// across the element groups at the row's end; the transpose part of every
+// element goes to Y with a global reduction (no return value) per vector.
+// The columns of one row are distinct, so a warp never reduces twice into
+// one address in a step; rows of other warps meet in L2.
+template <int NV, typename VT, typename XT>
+__global__ void __launch_bounds__(256) k_spmm_lower_red(const int64_t *__restrict__ rowptr,
+                                                         const int32_t *__restrict__ col,
+                                                         const VT *__restrict__ val, int64_t nd, double hmin,
+                                                         const XT *__restrict__ X, int ldx, XT *Y, int ldy)
+{
+    constexpr int G = 32 / NV;
+    const int lane = threadIdx.x & 31;
+    const int g = lane / NV, v = lane - g * NV;
+    const bool active = g < G;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t n = warp; n < nd; n += nwarps) {
+        const int64_t r0 = rowptr[n], r1 = rowptr[n + 1];
+        const XT xn = active ? __ldg(&X[n * (int64_t)ldx + v]) : (XT)0;
+        XT acc = 0;
+        if (active) {
+            for (int64_t l = r0 + g; l < r1; l += G) {
+                const int k = __ldg(&col[l]);
+                XT t = (XT)__ldg(&val[l]);
+                if (k == n) {
+                    t -= (XT)hmin;
+                } else {
+                    atomicAdd(&Y[(int64_t)k * ldy + v], t * xn);
+                }
+                acc += t * __ldg(&X[(int64_t)k * ldx + v]);
+            }
+        }
+#pragma unroll
+        for (int gg = 1; gg < G; gg++) {
+            XT o = __shfl_sync(FULL_MASK, acc, (lane + gg * NV) & 31);
+            if (g == 0) acc += o;
+        }
+        if (g == 0) atomicAdd(&Y[n * (int64_t)ldy + v], acc);
+    }
+}
+
+template <typename VT, typename XT>
+static int spmm_lower_red_dispatch(pci_gpu *h, const XT *X, int ldx, XT *Y, int ldy, int nv, cudaStream_t st);
+
 template <typename XT>
 __global__ void k_zero_block(XT *Y, int ldy, int64_t nd, int nv)
 {
@@ -425,13 +473,16 @@ template <typename VT, typename XT>
 static int spmm_lower_dispatch(pci_gpu *h, const XT *X, int ldx, XT *Y, int ldy, int nv, cudaStream_t st)
 {
     const Csr &L = h->H;
-    // The tile walk (PCI_SPMM_TILES=1) needs the adjacency of the H built
-    // here.  It is not the default: measured per call it ran 23.7 ms against
-    // 41 ms on the 86k-determinant system but 930 ms against 861 ms on the
-    // 1.06M-determinant one, where its per-tile flushes outweigh what it saves.
-    const char *e = getenv("PCI_SPMM_TILES");
-    if (h->h_from_tiles && h->d_adj && h->have_basis && e && !strcmp(e, "1"))
+    // Default: warp per row with global reductions for the transpose part.
+    // Measured per call (10 vectors): 279 ms FP64 / 178 ms FP32 on config 2
+    // against 795 / 736 ms for the window kernel and 930 ms for the tile
+    // walk; 8.2 / 3.2 ms on the 86k-determinant system against 43 / 41 ms.
+    // PCI_SPMM_LOWER=windows|tiles selects the others (the tile walk needs
+    // the adjacency of an H built here).
+    const char *e = getenv("PCI_SPMM_LOWER");
+    if (e && !strcmp(e, "tiles") && h->h_from_tiles && h->d_adj && h->have_basis)
         return spmm_lower_tiles_dispatch<VT, XT>(h, X, ldx, Y, ldy, nv, st);
+    if (!(e && !strcmp(e, "windows"))) return spmm_lower_red_dispatch<VT, XT>(h, X, ldx, Y, ldy, nv, st);
     int rc = 0;
     if ((rc = ensure_tmp(h, 64))) return rc;
     unsigned long long *counter = (unsigned long long *)h->d_tmp;
@@ -443,6 +494,26 @@ static int spmm_lower_dispatch(pci_gpu *h, const XT *X, int ldx, XT *Y, int ldy,
     case N:                                                                                               \
         k_spmm_lower<N, VT, XT><<<blocks, LW_WARPS * 32, 0, st>>>(L.rowptr, L.col, val, L.nrows, h->hmin, \
                                                                       X, ldx, Y, ldy, counter);           \
+        break;
+    switch (nv) {
+        CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8)
+        CASE(9) CASE(10) CASE(11) CASE(12) CASE(13) CASE(14) CASE(15) CASE(16)
+    default: return set_err(h, PCI_E_INPUT, "SpMM supports 1..16 vectors");
+    }
+#undef CASE
+    PCI_CUDA(h, cudaGetLastError());
+    return PCI_OK;
+}
+
+template <typename VT, typename XT>
+static int spmm_lower_red_dispatch(pci_gpu *h, const XT *X, int ldx, XT *Y, int ldy, int nv, cudaStream_t st)
+{
+    const Csr &L = h->H;
+    k_zero_block<<<148 * 8, 256, 0, st>>>(Y, ldy, L.nrows, nv);
+    const VT *val = (const VT *)L.val;
+#define CASE(N)                                                                                               \
+    case N:                                                                                                   \
+        k_spmm_lower_red<N, VT, XT><<<148 * 16, 256, 0, st>>>(L.rowptr, L.col, val, L.nrows, h->hmin, X, ldx, Y, ldy); \
         break;
     switch (nv) {
         CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8)

@@ -311,15 +311,16 @@ def test_bad_determinant_order_is_reported(engine):
     engine.form_h(64)
 
 
-@pytest.mark.parametrize("mode", ["lower", "lower-tiles", "full", "set-csr"])
+@pytest.mark.parametrize("mode", ["lower", "lower-tiles", "lower-windows", "full", "set-csr"])
 def test_davidson_spmm_paths(mode, monkeypatch):
-    """The SpMM paths give the same Davidson levels: lower triangle in column
-    windows, lower triangle along the configuration tiles, the full symmetric
-    copy, and an H round-tripped through get_csr/set_csr."""
+    """The SpMM paths give the same Davidson levels: lower triangle with
+    transpose reductions (default), along the configuration tiles and in
+    column windows, the full symmetric copy, and an H round-tripped through
+    get_csr/set_csr."""
     from pci_b200.capi import Engine
     monkeypatch.setenv("PCI_SPMM", "full" if mode == "full" else "lower")
-    if mode == "lower-tiles":
-        monkeypatch.setenv("PCI_SPMM_TILES", "1")
+    if mode in ("lower-tiles", "lower-windows"):
+        monkeypatch.setenv("PCI_SPMM_LOWER", mode.split("-")[1])
     name = "small3"
     s = get_system(name)
     (rp, col, val, nz, hmin, pairs), (jr, jc, jv) = oracle_h(name)
