@@ -60,6 +60,9 @@ typedef struct {
 
 #define PCI_DVD_FP64 0
 #define PCI_DVD_FP32 1
+#define PCI_DVD_LEARNED 2   /* FP64; on rows >= Nd0 the correction takes the attached model's
+                               direction and the diagonal correction's length; a level whose
+                               residual stops decreasing falls back to the diagonal correction */
 
 /* Replaces: the device has no counterpart in pconf; this opens a handle on
  * CUDA device `device` (the MPI rank's process is the reference's unit). */
@@ -158,6 +161,45 @@ int pci_gpu_j_av_noalloc(const int64_t *rowptr, const int32_t *col, const double
  * them.  Copies up to cap values into out (may be NULL) and returns Njd, or
  * -1 before set_basis. */
 int32_t pci_gpu_jterms(pci_gpu_t *h, int32_t *out, int32_t cap);
+
+/* ---- Learned Davidson correction ------------------------------------------
+ * A small MLP (nin -> 128 -> 128 -> 128 -> 1, ReLU) whose forward and
+ * backward kernels read BF16 weights and accumulate in FP32, with FP32
+ * master weights and Adam moments; trained on the GPU.  No counterpart in
+ * the reference, which has only the diagonal correction of Dvdsn
+ * (davidson.f90:436-570).  Parameters are laid out layer by layer as
+ * W (din x dout, row-major) then b (dout). */
+typedef struct pci_mlp pci_mlp_t;
+int pci_mlp_create(int32_t device, int32_t nin, int32_t seed, pci_mlp_t **m);
+int64_t pci_mlp_num_params(pci_mlp_t *m);
+int pci_mlp_set_params(pci_mlp_t *m, const float *p, int64_t n);
+int pci_mlp_get_params(pci_mlp_t *m, float *p, int64_t n);
+/* y[n] from X[n x nin] (host arrays). */
+int pci_mlp_forward(pci_mlp_t *m, const float *X, int64_t n, float *y);
+/* Mean squared error against T[n] and its gradient (length num_params,
+ * may be NULL) for X[n x nin] (host arrays). */
+int pci_mlp_loss_grad(pci_mlp_t *m, const float *X, const float *T, int64_t n, float *loss, float *grad);
+/* Adam (lr, betas 0.9/0.999) over shuffled batches for `epochs` passes of
+ * (X, T); *loss_out receives the last epoch's mean batch loss. */
+int pci_mlp_train(pci_mlp_t *m, const float *X, const float *T, int64_t n, int32_t epochs, int32_t batch, float lr,
+                  int32_t seed, float *loss_out);
+const char *pci_mlp_last_error(pci_mlp_t *m);
+void pci_mlp_destroy(pci_mlp_t *m);
+/* The FP64 Davidson with every unconverged level's correction rows >= Nd0
+ * recorded as samples for the model: features (Nsu occupation counts,
+ * D_n - theta, residual entry times sqrt(Nd)/|r|; Nsu + 2 floats per
+ * sample) into feat, and after the solve the targets (converged vector
+ * minus that iteration's vector, signs aligned, scaled to unit RMS over the
+ * rows >= Nd0 of that level and iteration) into target.  The converged vectors are Xref (Nd x Nlv, column-major, e.g.
+ * from a solve whose initial block covers every determinant) or, when Xref
+ * is NULL, the solve's own final vectors.  Up to cap samples are written;
+ * *count receives the number recorded.  Tk, Iconverge (Nlv each) and iters
+ * as pci_gpu_davidson. */
+int pci_gpu_davidson_harvest(pci_gpu_t *h, const pci_dvd_params *p, const double *Xref, float *feat, float *target,
+                             int64_t cap, int64_t *count, double *Tk, int32_t *Iconverge, int32_t *iters);
+/* Attach a trained model to the handle for the learned Davidson form
+ * (mode PCI_DVD_LEARNED); NULL detaches.  The model must outlive its use. */
+int pci_gpu_set_correction_model(pci_gpu_t *h, pci_mlp_t *m);
 
 /* Per-stage device times (milliseconds) and counters of the last calls:
  * [0] FormH total (adjacency + count + fill + compaction), [1] FormH count

@@ -17,12 +17,14 @@ PCI_OK = 0
 ERRORS = {1: "PCI_E_INPUT", 2: "PCI_E_OOM", 3: "PCI_E_MISSING_INTEGRAL", 4: "PCI_E_ORTHO_FAIL",
           5: "PCI_E_TIMEOUT", 6: "PCI_E_CUDA", 7: "PCI_E_STATE", 8: "PCI_E_NOT_CONVERGED"}
 PCI_MAT_H, PCI_MAT_J2 = 0, 1
-PCI_DVD_FP64, PCI_DVD_FP32 = 0, 1
+PCI_DVD_FP64, PCI_DVD_FP32, PCI_DVD_LEARNED = 0, 1, 2
 
 EXPORTS = ["pci_gpu_create", "pci_gpu_set_basis", "pci_gpu_set_integrals", "pci_gpu_form_h",
            "pci_gpu_form_j", "pci_gpu_csr_info", "pci_gpu_get_csr", "pci_gpu_set_csr",
            "pci_gpu_davidson", "pci_gpu_j_av", "pci_gpu_j_av_noalloc", "pci_gpu_jterms", "pci_gpu_stats",
-           "pci_gpu_last_error", "pci_gpu_destroy"]
+           "pci_gpu_last_error", "pci_gpu_destroy", "pci_mlp_create", "pci_mlp_num_params", "pci_mlp_set_params",
+           "pci_mlp_get_params", "pci_mlp_forward", "pci_mlp_loss_grad", "pci_mlp_train", "pci_mlp_last_error",
+           "pci_mlp_destroy", "pci_gpu_set_correction_model", "pci_gpu_davidson_harvest"]
 
 
 class PciError(RuntimeError):
@@ -61,6 +63,21 @@ def load(path: str = LIB):
     L.pci_gpu_davidson.argtypes = [P, C.POINTER(DvdParams), P, P, P, P, P, C.POINTER(i32), P]
     L.pci_gpu_j_av.argtypes = [P, P, i32, i64, P]
     L.pci_gpu_j_av_noalloc.argtypes = [P, P, P, i64, P, i64, i32, i64, P, P, C.c_char_p, i32]
+    L.pci_mlp_create.argtypes = [i32, i32, i32, C.POINTER(P)]
+    L.pci_mlp_num_params.argtypes = [P]
+    L.pci_mlp_num_params.restype = i64
+    L.pci_mlp_set_params.argtypes = [P, P, i64]
+    L.pci_mlp_get_params.argtypes = [P, P, i64]
+    L.pci_mlp_forward.argtypes = [P, P, i64, P]
+    L.pci_mlp_loss_grad.argtypes = [P, P, P, i64, P, P]
+    L.pci_mlp_train.argtypes = [P, P, P, i64, i32, i32, C.c_float, i32, P]
+    L.pci_mlp_last_error.argtypes = [P]
+    L.pci_mlp_last_error.restype = C.c_char_p
+    L.pci_mlp_destroy.argtypes = [P]
+    L.pci_mlp_destroy.restype = None
+    L.pci_gpu_set_correction_model.argtypes = [P, P]
+    L.pci_gpu_davidson_harvest.argtypes = [P, C.POINTER(DvdParams), P, P, P, i64, C.POINTER(i64), P, P,
+                                           C.POINTER(i32)]
     L.pci_gpu_jterms.argtypes = [P, P, i32]
     L.pci_gpu_jterms.restype = i32
     L.pci_gpu_stats.argtypes = [P, P, i32]
@@ -189,6 +206,29 @@ class Engine:
         self._check(self.L.pci_gpu_j_av(self.h, _p(xc), nv, nd if nlim is None else nlim, _p(out)))
         return out
 
+    def set_correction_model(self, mlp):
+        """Attach a trained Mlp for mode=PCI_DVD_LEARNED (None detaches)."""
+        self._check(self.L.pci_gpu_set_correction_model(self.h, None if mlp is None else mlp.m))
+        self._model = mlp
+
+    def davidson_harvest(self, nd, nsu, Nlv, N_it=30, MaxNd0=3000, Xref=None, cap=None, Crt4=1e-8):
+        """FP64 Davidson recording samples for the correction model: returns
+        (features [n, Nsu+2], targets [n], result dict)."""
+        p = DvdParams(Nlv, N_it, 1, 4, 0, MaxNd0, PCI_DVD_FP64, 0, Crt4, 0.0, 0.0)
+        cap = cap if cap is not None else N_it * Nlv * nd
+        nin = nsu + 2
+        feat = np.zeros((cap, nin), np.float32)
+        targ = np.zeros(cap, np.float32)
+        xr = None if Xref is None else np.ascontiguousarray(np.asarray(Xref, np.float64).T)
+        cnt = C.c_int64()
+        Tk = np.zeros(Nlv)
+        ic = np.zeros(Nlv, np.int32)
+        iters = C.c_int32()
+        self._check(self.L.pci_gpu_davidson_harvest(self.h, C.byref(p), _p(xr), _p(feat), _p(targ), cap,
+                                                    C.byref(cnt), _p(Tk), _p(ic), C.byref(iters)))
+        n = min(cnt.value, cap)
+        return feat[:n], targ[:n], dict(Tk=Tk, Iconverge=ic, iterations=iters.value, count=cnt.value)
+
     def jterms(self):
         """Jt(1:Njd) of the current basis (sorted 2J of the terms present)."""
         n = self.L.pci_gpu_jterms(self.h, None, 0)
@@ -205,3 +245,62 @@ class Engine:
                 "spmm_calls", "init_ms", "adjacency_ms", "pairs", "scanned", "formh_launches",
                 "formh_compact_ms", "formh_single_eval", "formh_slots"]
         return dict(zip(keys[:n], out[:n].tolist()))
+
+
+class Mlp:
+    """The learned-correction network on one device (pci_mlp_* of the C ABI)."""
+
+    def __init__(self, nin: int, device: int = 0, seed: int = 0):
+        self.L = load()
+        self.m = C.c_void_p()
+        rc = self.L.pci_mlp_create(device, nin, seed, C.byref(self.m))
+        if rc != PCI_OK:
+            raise PciError(rc, "pci_mlp_create failed")
+        self.nin = nin
+        self.nparam = int(self.L.pci_mlp_num_params(self.m))
+
+    def _check(self, rc):
+        if rc != PCI_OK:
+            raise PciError(rc, self.L.pci_mlp_last_error(self.m).decode())
+
+    def params(self):
+        p = np.zeros(self.nparam, np.float32)
+        self._check(self.L.pci_mlp_get_params(self.m, _p(p), self.nparam))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        self._check(self.L.pci_mlp_set_params(self.m, _p(p), p.size))
+
+    def forward(self, X):
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.zeros(X.shape[0], np.float32)
+        self._check(self.L.pci_mlp_forward(self.m, _p(X), X.shape[0], _p(y)))
+        return y
+
+    def loss_grad(self, X, T):
+        X = np.ascontiguousarray(X, np.float32)
+        T = np.ascontiguousarray(T, np.float32)
+        loss = C.c_float()
+        g = np.zeros(self.nparam, np.float32)
+        self._check(self.L.pci_mlp_loss_grad(self.m, _p(X), _p(T), X.shape[0], C.byref(loss), _p(g)))
+        return float(loss.value), g
+
+    def train(self, X, T, epochs=10, batch=4096, lr=1e-3, seed=0):
+        X = np.ascontiguousarray(X, np.float32)
+        T = np.ascontiguousarray(T, np.float32)
+        loss = C.c_float()
+        self._check(self.L.pci_mlp_train(self.m, _p(X), _p(T), X.shape[0], epochs, batch, lr, seed,
+                                         C.byref(loss)))
+        return float(loss.value)
+
+    def close(self):
+        if self.m:
+            self.L.pci_mlp_destroy(self.m)
+            self.m = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -223,7 +223,7 @@ __global__ void k_diag(const int64_t *rowptr, const int32_t *col, const VT *val,
 // diagonal preconditioner t/(theta - Diag) written in place into column Nlv+j;
 // per-block partial sums of t^2 go to part[b*nlv + j].
 __global__ void __launch_bounds__(256) k_resid(double *A, int ld, int64_t nd, int nlv, int nd0, const double *theta,
-                                               const double *D, double *C, double *part)
+                                               const double *D, double *C, double *part, int raw)
 {
     __shared__ double red[8][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(256) k_resid(double *A, int ld, int64_t nd, in
             double t = row[nlv + j] - theta[j] * row[j];
             acc[j] += t * t;
             if (n < nd0) C[(int64_t)j * nd0 + n] = t;
-            else row[nlv + j] = t / (theta[j] - D[n]);
+            else row[nlv + j] = raw ? t : t / (theta[j] - D[n]);
         }
     }
     for (int j = 0; j < nlv; j++) {
@@ -388,6 +388,69 @@ __global__ void k_prj_scale(double *A, int ld, int64_t nd, int cin, int nv, cons
             if (!iconv[v]) A[n * ld + cin + v] *= inv[v];
 }
 
+// ------------------------------------------------ learned correction ---
+
+// Features of rows n0 .. n0+cnt of level j for the correction model:
+// occupation count of each orbital (Nsu values), D_n - theta_j, and the
+// residual entry (raw, column col) times fscale = sqrt(Nd) / |r_j|.
+__global__ void k_features(DevSys S, const double *A, int ld, const double *D, int64_t n0, int64_t cnt, int col,
+                           double theta, float fscale, int nin, float *F)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t n = n0 + i;
+        float *f = F + i * nin;
+        for (int q = 0; q < nin - 2; q++) f[q] = 0.0f;
+        for (int e = 0; e < S.ne; e++) {
+            const int o = S.ms_orb[S.occ[n * S.ne + e]];
+            if (o < nin - 2) f[o] += 1.0f;
+        }
+        f[nin - 2] = (float)(D[n] - theta);
+        f[nin - 1] = (float)A[n * ld + col] * fscale;
+    }
+}
+
+// rows n0 .. n0+cnt of column col <- y * scale (the model's correction)
+__global__ void k_apply_net(double *A, int ld, int64_t n0, int64_t cnt, int col, const float *y, double scale)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x)
+        A[(n0 + i) * ld + col] = (double)y[i] * scale;
+}
+
+// rows n0 .. n0+cnt of column col: raw residual -> r / (theta - D) (Dvdsn's correction)
+__global__ void k_apply_diag(double *A, int ld, const double *D, int64_t n0, int64_t cnt, int col, double theta)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t n = n0 + i;
+        A[n * ld + col] = A[n * ld + col] / (theta - D[n]);
+    }
+}
+
+__global__ void k_get_col(const double *A, int ld, int64_t n0, int64_t cnt, int col, double *out)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = A[(n0 + i) * ld + col];
+}
+
+// sum of squares of x[0..n) into out (atomic)
+template <typename T>
+__global__ void k_sumsq(const T *x, int64_t n, int64_t stride, double *out)
+{
+    double s = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = (double)x[i * stride];
+        s += v * v;
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(FULL_MASK, s, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
+struct HarvestRec {
+    int it = 0, j = 0;
+    int64_t n0 = 0, cnt = 0;
+    std::vector<float> feat;
+    std::vector<double> xk;
+};
+
 // -------------------------------------------------- SpMM block packing ---
 
 // The probe block goes to the SpMM as a contiguous Nd x nv array (the basis
@@ -418,6 +481,11 @@ struct Dvd {
     double *A = nullptr, *D = nullptr, *Z1 = nullptr, *E1 = nullptr, *C = nullptr, *Bz = nullptr, *Sz = nullptr;
     double *part = nullptr, *small = nullptr;  // small: scratch scalars
     void *xp = nullptr, *yp = nullptr;         // packed SpMM input / output blocks
+    bool learned = false;                      // learned correction on rows >= Nd0
+    int nin = 0;
+    int64_t chunk = 0;
+    float *feat = nullptr, *yout = nullptr;    // features / model output of one chunk of rows
+    double *ycol = nullptr;
     bool fp32 = false;                         // FP32 form: float blocks, FP32 SpMM
     OrtnState *ost = nullptr;
     int *iconv_d = nullptr, *jsel_d = nullptr;
@@ -495,7 +563,7 @@ void free_dvd(Dvd &d)
 {
     dev_free(d.A); dev_free(d.D); dev_free(d.Z1); dev_free(d.E1); dev_free(d.C); dev_free(d.Bz); dev_free(d.Sz);
     dev_free(d.part); dev_free(d.small); dev_free(d.ost); dev_free(d.iconv_d); dev_free(d.jsel_d);
-    dev_free(d.xp); dev_free(d.yp);
+    dev_free(d.xp); dev_free(d.yp); dev_free(d.feat); dev_free(d.yout); dev_free(d.ycol);
     if (d.cub) cublasDestroy(d.cub);
     if (d.sol) cusolverDnDestroy(d.sol);
     if (d.ea) cudaEventDestroy(d.ea);
@@ -505,12 +573,15 @@ void free_dvd(Dvd &d)
 }  // namespace
 
 int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out, double *Tj_out,
-           int32_t *Iconverge_out, double *X_out, int32_t *iters_out, double *resid_out)
+           int32_t *Iconverge_out, double *X_out, int32_t *iters_out, double *resid_out, DvdHarvest *hv)
 {
     if (!h->H.rowptr) return set_err(h, PCI_E_STATE, "davidson before form_h");
     if (!h->J.rowptr) return set_err(h, PCI_E_STATE, "davidson before form_j");
     if (p->Nlv < 1 || p->Nlv > 16) return set_err(h, PCI_E_INPUT, "Nlv must be 1..16");
-    if (p->mode != PCI_DVD_FP64 && p->mode != PCI_DVD_FP32) return set_err(h, PCI_E_INPUT, "mode must be FP64 or FP32");
+    if (p->mode != PCI_DVD_FP64 && p->mode != PCI_DVD_FP32 && p->mode != PCI_DVD_LEARNED)
+        return set_err(h, PCI_E_INPUT, "mode must be FP64, FP32 or LEARNED");
+    if (p->mode == PCI_DVD_LEARNED && (!h->corr_model || mlp_num_inputs(h->corr_model) != h->nsu + 2))
+        return set_err(h, PCI_E_INPUT, "the learned form needs a correction model with Nsu + 2 inputs");
     if (p->mode == PCI_DVD_FP32 && !h->H.val_f32)
         return set_err(h, PCI_E_INPUT, "the FP32 form needs H stored in FP32 (form_h with value_prec 32)");
     if (p->Kv != 3 && p->Kv != 4) return set_err(h, PCI_E_INPUT, "Kv must be 4 or 3");
@@ -561,6 +632,14 @@ int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out
     ALLOC(d.iconv_d, int, 16);
     ALLOC(d.jsel_d, int, 16);
     d.fp32 = p->mode == PCI_DVD_FP32;
+    d.learned = p->mode == PCI_DVD_LEARNED;
+    if (d.learned || hv) {
+        d.nin = h->nsu + 2;
+        d.chunk = std::max<int64_t>(1, std::min<int64_t>(nd - nd0, (int64_t)1 << 18));
+        ALLOC(d.feat, float, d.chunk * d.nin);
+        ALLOC(d.yout, float, std::max<int64_t>(1, nd - nd0));
+        ALLOC(d.ycol, double, d.chunk);
+    }
     ALLOC(d.xp, double, nd * Nlv);
     ALLOC(d.yp, double, nd * Nlv);
 #undef ALLOC
@@ -634,6 +713,10 @@ int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out
         }
     }
     // Davidson loop
+    const DevSys S = make_devsys(h);
+    std::vector<int> learned_on(Nlv, 1);
+    std::vector<double> prev_cn(Nlv, 0.0);
+    std::vector<HarvestRec> harvest;
     std::vector<double> P((size_t)4 * Nlv * Nlv, 0.0), Pt((size_t)2 * Nlv * Nlv), cn(Nlv, 0.0);
     std::vector<double> part_h((size_t)d.blocks * Nlv);
     d.iconv.assign(Nlv, 0);
@@ -667,7 +750,8 @@ int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out
         std::vector<double> theta(Nlv);
         for (int j = 0; j < Nlv; j++) theta[j] = P[j + (size_t)j * n1];
         PCI_CUDA(h, cudaMemcpyAsync(d.small + SM_THETA, theta.data(), Nlv * 8, cudaMemcpyHostToDevice, d.st));
-        k_resid<<<d.blocks, 256, 0, d.st>>>(d.A, d.ld, nd, Nlv, nd0, d.small + SM_THETA, d.D, d.C, d.part);
+        const bool raw_rows = d.learned || hv;   // rows >= Nd0 keep the raw residual for the features
+        k_resid<<<d.blocks, 256, 0, d.st>>>(d.A, d.ld, nd, Nlv, nd0, d.small + SM_THETA, d.D, d.C, d.part, raw_rows);
         PCI_CUDA(h, cudaGetLastError());
         PCI_CUDA(h, cudaMemcpyAsync(part_h.data(), d.part, (size_t)d.blocks * Nlv * 8, cudaMemcpyDeviceToHost, d.st));
         PCI_CUDA(h, cudaStreamSynchronize(d.st));
@@ -684,6 +768,59 @@ int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out
         PCI_CUDA(h, cudaMemcpyAsync(d.iconv_d, d.iconv.data(), Nlv * 4, cudaMemcpyHostToDevice, d.st));
         for (int j = 0; j < Nlv; j++)
             if (d.iconv[j]) k_zero_col<<<d.blocks, 256, 0, d.st>>>(d.A, d.ld, nd, Nlv + j);
+        if (raw_rows && nd > nd0) {
+            // rows >= Nd0: the learned correction (with the diagonal one as the fallback of
+            // each level whose residual stopped decreasing), or the diagonal one while harvesting
+            const int64_t nrest = nd - nd0;
+            const double rs = sqrt((double)nd);
+            for (int j : jsel) {
+                if (d.learned && it > 1 && learned_on[j] && cn[j] >= prev_cn[j]) learned_on[j] = 0;
+                const bool use_net = d.learned && learned_on[j];
+                const float fscale = (float)(rs / cn[j]);
+                for (int64_t c0 = 0; c0 < nrest; c0 += d.chunk) {
+                    const int64_t cnt = std::min<int64_t>(d.chunk, nrest - c0);
+                    if (!use_net && !hv) break;
+                    k_features<<<d.blocks, 256, 0, d.st>>>(S, d.A, d.ld, d.D, nd0 + c0, cnt, Nlv + j, theta[j], fscale,
+                                                           d.nin, d.feat);
+                    PCI_CUDA(h, cudaGetLastError());
+                    if (hv) {
+                        // features now; the current vector's rows to form the target after the solve
+                        HarvestRec rec;
+                        rec.it = it;
+                        rec.j = j;
+                        rec.n0 = nd0 + c0;
+                        rec.cnt = cnt;
+                        rec.feat.resize((size_t)cnt * d.nin);
+                        rec.xk.resize((size_t)cnt);
+                        PCI_CUDA(h, cudaMemcpyAsync(rec.feat.data(), d.feat, rec.feat.size() * 4, cudaMemcpyDeviceToHost, d.st));
+                        k_get_col<<<d.blocks, 256, 0, d.st>>>(d.A, d.ld, nd0 + c0, cnt, j, d.ycol);
+                        PCI_CUDA(h, cudaMemcpyAsync(rec.xk.data(), d.ycol, (size_t)cnt * 8, cudaMemcpyDeviceToHost, d.st));
+                        PCI_CUDA(h, cudaStreamSynchronize(d.st));
+                        harvest.push_back(std::move(rec));
+                    }
+                    if (use_net && (rc = mlp_forward_device(h->corr_model, d.feat, cnt, d.yout + c0, d.st))) {
+                        free_dvd(d);
+                        return set_err(h, rc, "learned correction: model forward failed");
+                    }
+                }
+                // Dvdsn's correction r / (theta - D) on rows >= Nd0
+                k_apply_diag<<<d.blocks, 256, 0, d.st>>>(d.A, d.ld, d.D, nd0, nrest, Nlv + j, theta[j]);
+                if (use_net) {
+                    // the model gives the direction on rows >= Nd0, the diagonal correction its length
+                    PCI_CUDA(h, cudaMemsetAsync(d.small + SM_N2, 0, 16, d.st));
+                    k_sumsq<double><<<d.blocks, 256, 0, d.st>>>(d.A + (size_t)nd0 * d.ld + Nlv + j, nrest, d.ld,
+                                                                d.small + SM_N2);
+                    k_sumsq<float><<<d.blocks, 256, 0, d.st>>>(d.yout, nrest, 1, d.small + SM_N2 + 1);
+                    double n2[2];
+                    PCI_CUDA(h, cudaMemcpyAsync(n2, d.small + SM_N2, 16, cudaMemcpyDeviceToHost, d.st));
+                    PCI_CUDA(h, cudaStreamSynchronize(d.st));
+                    if (n2[1] > 0.0 && std::isfinite(n2[1]))
+                        k_apply_net<<<d.blocks, 256, 0, d.st>>>(d.A, d.ld, nd0, nrest, Nlv + j, d.yout, sqrt(n2[0] / n2[1]));
+                }
+                PCI_CUDA(h, cudaGetLastError());
+            }
+        }
+        for (int j = 0; j < Nlv; j++) prev_cn[j] = cn[j];
         const int nj = (int)jsel.size();
         if (nj > 0) {
             // Z1 projection preconditioner on rows < nd0, batched over levels
@@ -808,6 +945,51 @@ int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out
         }
     }
     (void)converged;
+    if (hv) {
+        // targets of the recorded samples: the converged vector minus the vector of
+        // that iteration (signs aligned), in units of the residual scale
+        hv->count = 0;
+        // targets per (iteration, level): the difference scaled to unit RMS over rows >= Nd0
+        std::vector<std::vector<double>> dif(harvest.size());
+        for (size_t r = 0; r < harvest.size(); r++) {
+            const HarvestRec &rec = harvest[r];
+            std::vector<double> xs((size_t)rec.cnt);
+            if (hv->xref) {
+                memcpy(xs.data(), hv->xref + (size_t)rec.j * nd + rec.n0, (size_t)rec.cnt * 8);
+            } else {
+                k_get_col<<<d.blocks, 256, 0, d.st>>>(d.A, d.ld, rec.n0, rec.cnt, rec.j, d.ycol);
+                PCI_CUDA(h, cudaMemcpyAsync(xs.data(), d.ycol, (size_t)rec.cnt * 8, cudaMemcpyDeviceToHost, d.st));
+                PCI_CUDA(h, cudaStreamSynchronize(d.st));
+            }
+            dif[r] = xs;
+        }
+        for (size_t g0 = 0; g0 < harvest.size();) {
+            size_t g1 = g0;
+            double dot = 0.0;
+            int64_t rows = 0;
+            while (g1 < harvest.size() && harvest[g1].it == harvest[g0].it && harvest[g1].j == harvest[g0].j) {
+                for (int64_t i = 0; i < harvest[g1].cnt; i++) dot += dif[g1][i] * harvest[g1].xk[i];
+                rows += harvest[g1].cnt;
+                g1++;
+            }
+            const double sg = dot < 0.0 ? -1.0 : 1.0;
+            double ss = 0.0;
+            for (size_t r = g0; r < g1; r++)
+                for (int64_t i = 0; i < harvest[r].cnt; i++) {
+                    dif[r][i] = sg * dif[r][i] - harvest[r].xk[i];
+                    ss += dif[r][i] * dif[r][i];
+                }
+            const double inv = ss > 0.0 ? sqrt((double)rows / ss) : 0.0;
+            for (size_t r = g0; r < g1; r++)
+                for (int64_t i = 0; i < harvest[r].cnt; i++, hv->count++) {
+                    if (hv->count >= hv->cap) continue;
+                    if (hv->feat)
+                        memcpy(hv->feat + hv->count * d.nin, harvest[r].feat.data() + i * d.nin, (size_t)d.nin * 4);
+                    if (hv->target) hv->target[hv->count] = (float)(dif[r][i] * inv);
+                }
+            g0 = g1;
+        }
+    }
     // WriteFinalXIJ: J of each level
     if ((rc = sp_jav(h, d.A, d.ld, Nlv, nd, Tj.data()))) { free_dvd(d); return rc; }
     if (X_out) {

@@ -432,6 +432,30 @@ int pci_gpu_davidson(pci_gpu_t *h, const pci_dvd_params *p, const double *X0, do
     return dv_run(h, p, X0, Tk, Tj, Iconverge, X, iters, resid);
 }
 
+int pci_gpu_davidson_harvest(pci_gpu_t *h, const pci_dvd_params *p, const double *Xref, float *feat, float *target,
+                             int64_t cap, int64_t *count, double *Tk, int32_t *Iconverge, int32_t *iters)
+{
+    if (!h || !p || !count) return PCI_E_INPUT;
+    cudaSetDevice(h->device);
+    if (p->mode != PCI_DVD_FP64) return set_err(h, PCI_E_INPUT, "harvest runs the FP64 form");
+    DvdHarvest hv;
+    hv.feat = feat;
+    hv.target = target;
+    hv.cap = cap;
+    hv.xref = Xref;
+    std::vector<double> tj(p->Nlv);
+    int rc = dv_run(h, p, nullptr, Tk, tj.data(), Iconverge, nullptr, iters, nullptr, &hv);
+    *count = hv.count;
+    return rc;
+}
+
+int pci_gpu_set_correction_model(pci_gpu_t *h, pci_mlp_t *m)
+{
+    if (!h) return PCI_E_INPUT;
+    h->corr_model = m;
+    return PCI_OK;
+}
+
 int pci_gpu_j_av(pci_gpu_t *h, const double *X, int32_t nv, int64_t nlim, double *Tj)
 {
     if (!h) return PCI_E_INPUT;

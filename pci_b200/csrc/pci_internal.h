@@ -100,9 +100,14 @@ struct pci_gpu {
     double st_adj = 0, st_pairs = 0, st_scanned = 0, st_launches = 0;
     double st_formh_compact = 0, st_formh_padded = 0, st_formh_compact_launches = 0, st_formh_slots = 0;
     bool h_from_tiles = false;  // H was built here by form_h: its rows follow the adjacency tiles
+    pci_mlp *corr_model = nullptr;   // learned Davidson correction (not owned)
     int spmm_mode = 0;        // 0 auto, 1 full symmetric copy, 2 lower triangle (env PCI_SPMM)
     int spmm_lower_used = 0;
 };
+
+// learned correction model (mlp.cu)
+int mlp_forward_device(pci_mlp *m, const float *dX, int64_t n, float *dy, cudaStream_t st);
+int mlp_num_inputs(const pci_mlp *m);
 
 // error helpers
 int set_err(pci_gpu *h, int code, const std::string &msg);
@@ -147,5 +152,13 @@ int sp_jav_strided(pci_gpu *h, const double *X, int64_t sn, int64_t sv, int nv, 
 void csr_free(Csr &c);
 
 // davidson.cu
+// Samples of the learned correction recorded during a solve (features of
+// rows >= Nd0 for each unconverged level and iteration, and after the solve
+// their targets); see pci_gpu_davidson_harvest.
+struct DvdHarvest {
+    float *feat = nullptr, *target = nullptr;
+    const double *xref = nullptr;   // reference vectors (Nd x Nlv, column-major) or null: the solve's own
+    int64_t cap = 0, count = 0;
+};
 int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk, double *Tj,
-           int32_t *Iconverge, double *X, int32_t *iters, double *resid);
+           int32_t *Iconverge, double *X, int32_t *iters, double *resid, DvdHarvest *hv = nullptr);

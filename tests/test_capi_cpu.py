@@ -10,7 +10,7 @@ from conftest import ROOT
 def declared_symbols():
     hdr = open(os.path.join(ROOT, "include", "pci_gpu.h")).read()
     hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
-    return sorted(set(re.findall(r"\b(pci_gpu_\w+)\s*\(", hdr)))
+    return sorted(set(re.findall(r"\b(pci_(?:gpu|mlp)_\w+)\s*\(", hdr)))
 
 
 def test_library_exports_header_symbols():
