@@ -1,0 +1,92 @@
+/*
+ * pci_batch.h -- C ABI of the batched form: many independent CI blocks
+ * (different ions, M_J and parity), each with its own lower-triangle
+ * Hamiltonian, solved for their lowest roots together on one GPU.
+ *
+ * The reference solves one block per pconf run: Diag4 (pconf.F90:238, with
+ * the Davidson module davidson.f90) takes Nlv, N_it and the residual criterion
+ * Crt4 and returns the energies Tk(1:Nlv) and vectors ArrB.  This interface
+ * keeps those meanings per block (nlv, max_it, tol; energies and vectors in
+ * the same order), with H stored in FP32.
+ *
+ * Every iteration step of the solve is one kernel launch over all blocks,
+ * the SpMM one persistent kernel over the rows of every block, and the
+ * iterations are replayed from a CUDA graph.  Blocks are added from
+ * pci_gpu_t handles whose Hamiltonian is resident (pci_gpu_form_h or
+ * pci_gpu_set_csr); the batch takes over that matrix.
+ *
+ * Every int-returning entry point returns PCI_OK (0) or a PCI_E_* code of
+ * pci_gpu.h; pci_batch_last_error() then holds a message.
+ */
+#ifndef PCI_BATCH_H
+#define PCI_BATCH_H
+
+#include <stdint.h>
+
+#include "pci_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pci_batch pci_batch_t;
+
+#define PCI_BATCH_MAX_LV   8    /* roots per block */
+#define PCI_BATCH_MAX_SUB  64   /* subspace vectors per block */
+
+typedef struct {
+    int32_t nlv;            /* roots per block, 1..PCI_BATCH_MAX_LV (Nlv) */
+    int32_t max_sub;        /* subspace size at which a block restarts, 2*nlv..PCI_BATCH_MAX_SUB */
+    int32_t keep;           /* Ritz vectors kept at a restart, nlv..max_sub-nlv */
+    int32_t max_it;         /* iteration limit per block (N_it) */
+    double tol;             /* residual 2-norm per root (Crt4) */
+    int32_t it_per_graph;   /* iterations captured in one CUDA graph, >= 1 */
+    int32_t spmm_variant;   /* SpMM variant (pci_batch_tune), -1 = tuned or default */
+} pci_batch_params;
+
+int pci_batch_create(int32_t device, pci_batch_t **out);
+
+/* Append the Hamiltonian resident in `h` as the next block and take it over
+ * (h keeps its basis and integrals but no longer holds H).  FP64 values are
+ * rounded to FP32.  *index receives the block's index. */
+int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index);
+
+/* Blocks, total rows and total stored (lower-triangle) elements. */
+int pci_batch_info(pci_batch_t *b, int32_t *nblocks, int64_t *rows, int64_t *nnz);
+
+/* Pick the SpMM variant for nv vectors by timing each candidate on the
+ * batch's matrix (ms = the chosen variant's time per SpMM), or take it from
+ * the cache file `cache_path` (NULL = no cache) when it holds a line for the
+ * same device and matrix; new results are appended there.  The pick is used
+ * by later pci_batch_davidson calls with spmm_variant = -1. */
+int pci_batch_tune(pci_batch_t *b, int32_t nv, const char *cache_path, int32_t *variant, double *ms,
+                   int32_t *from_cache);
+
+/* Number of SpMM variants and the parameters of one: lanes per row and
+ * thread blocks per SM. */
+int pci_batch_variant(int32_t variant, int32_t *lanes_per_row, int32_t *blocks_per_sm);
+
+/* Solve every block.  E[blk*nlv + j] = energy of root j, rnorm likewise its
+ * final residual 2-norm, iters[blk] = iterations the block took, status[blk]
+ * = 1 converged, 2 iteration limit, 3 no new direction left.  graph_launches
+ * (may be NULL) receives the number of graph replays. */
+int pci_batch_davidson(pci_batch_t *b, const pci_batch_params *p, double *E, double *rnorm, int32_t *iters,
+                       int32_t *status, int32_t *graph_launches);
+
+/* Ritz vectors of block blk after pci_batch_davidson: X[nd_blk x nlv],
+ * column-major, unit 2-norm. */
+int pci_batch_vectors(pci_batch_t *b, int32_t blk, double *X);
+
+/* Timings of the last solve: out[0] total ms, [1] iterations (largest over
+ * blocks), [2] SpMM ms per call (measured outside the graph), [3] SpMM
+ * variant used, [4] setup ms, [5] kernel launches per iteration; n <= 6. */
+int pci_batch_stats(pci_batch_t *b, double *out, int32_t n);
+
+const char *pci_batch_last_error(pci_batch_t *b);
+void pci_batch_destroy(pci_batch_t *b);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

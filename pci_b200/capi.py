@@ -25,6 +25,15 @@ EXPORTS = ["pci_gpu_create", "pci_gpu_set_basis", "pci_gpu_set_integrals", "pci_
            "pci_gpu_last_error", "pci_gpu_destroy", "pci_mlp_create", "pci_mlp_num_params", "pci_mlp_set_params",
            "pci_mlp_get_params", "pci_mlp_forward", "pci_mlp_loss_grad", "pci_mlp_train", "pci_mlp_last_error",
            "pci_mlp_destroy", "pci_gpu_set_correction_model", "pci_gpu_davidson_harvest"]
+BATCH_EXPORTS = ["pci_batch_create", "pci_batch_add_block", "pci_batch_info", "pci_batch_tune",
+                 "pci_batch_variant", "pci_batch_davidson", "pci_batch_vectors", "pci_batch_stats",
+                 "pci_batch_last_error", "pci_batch_destroy"]
+BATCH_STATUS = {1: "converged", 2: "iteration limit", 3: "no new direction"}
+
+
+class BatchParams(C.Structure):
+    _fields_ = [("nlv", C.c_int32), ("max_sub", C.c_int32), ("keep", C.c_int32), ("max_it", C.c_int32),
+                ("tol", C.c_double), ("it_per_graph", C.c_int32), ("spmm_variant", C.c_int32)]
 
 
 class PciError(RuntimeError):
@@ -86,6 +95,18 @@ def load(path: str = LIB):
     L.pci_gpu_last_error.restype = C.c_char_p
     L.pci_gpu_destroy.argtypes = [P]
     L.pci_gpu_destroy.restype = None
+    L.pci_batch_create.argtypes = [i32, C.POINTER(P)]
+    L.pci_batch_add_block.argtypes = [P, P, C.POINTER(i32)]
+    L.pci_batch_info.argtypes = [P, C.POINTER(i32), C.POINTER(i64), C.POINTER(i64)]
+    L.pci_batch_tune.argtypes = [P, i32, C.c_char_p, C.POINTER(i32), C.POINTER(f64), C.POINTER(i32)]
+    L.pci_batch_variant.argtypes = [i32, C.POINTER(i32), C.POINTER(i32)]
+    L.pci_batch_davidson.argtypes = [P, C.POINTER(BatchParams), P, P, P, P, C.POINTER(i32)]
+    L.pci_batch_vectors.argtypes = [P, i32, P]
+    L.pci_batch_stats.argtypes = [P, P, i32]
+    L.pci_batch_last_error.argtypes = [P]
+    L.pci_batch_last_error.restype = C.c_char_p
+    L.pci_batch_destroy.argtypes = [P]
+    L.pci_batch_destroy.restype = None
     _lib = L
     return L
 
@@ -298,6 +319,110 @@ class Mlp:
         if self.m:
             self.L.pci_mlp_destroy(self.m)
             self.m = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_variants():
+    """(lanes per row, thread blocks per SM) of every SpMM variant of the batched form."""
+    L = load()
+    out, v = [], 0
+    a, b = C.c_int32(), C.c_int32()
+    while L.pci_batch_variant(v, C.byref(a), C.byref(b)) == PCI_OK:
+        out.append((a.value, b.value))
+        v += 1
+    return out
+
+
+class Batch:
+    """Many independent CI blocks solved together (pci_batch_* of include/pci_batch.h)."""
+
+    def __init__(self, device: int = 0):
+        self.L = load()
+        self.b = C.c_void_p()
+        self.device = device
+        rc = self.L.pci_batch_create(device, C.byref(self.b))
+        if rc != PCI_OK:
+            msg = self.L.pci_batch_last_error(self.b).decode() if self.b else "pci_batch_create failed"
+            raise PciError(rc, msg)
+        self.sizes = []
+
+    def _check(self, rc):
+        if rc != PCI_OK:
+            raise PciError(rc, self.L.pci_batch_last_error(self.b).decode())
+
+    def add_engine(self, eng):
+        """Take over the Hamiltonian resident in an Engine as the next block."""
+        nd = C.c_int64()
+        nnz = C.c_int64()
+        self.L.pci_gpu_csr_info(eng.h, PCI_MAT_H, C.byref(nd), C.byref(nnz))
+        idx = C.c_int32()
+        self._check(self.L.pci_batch_add_block(self.b, eng.h, C.byref(idx)))
+        self.sizes.append(int(nd.value))
+        return idx.value
+
+    def add_system(self, sysm, value_prec: int = 32):
+        """Build a system's H on the device (FormH) and add it as the next block."""
+        with Engine(self.device) as e:
+            e.load_system(sysm)
+            e.form_h(value_prec)
+            return self.add_engine(e)
+
+    def add_csr(self, rowptr, col, val):
+        """Add a lower-triangle CSR held on the host (0-based rowptr, 1-based col)."""
+        with Engine(self.device) as e:
+            e.set_csr(PCI_MAT_H, rowptr, col, val)
+            return self.add_engine(e)
+
+    def info(self):
+        n, r, z = C.c_int32(), C.c_int64(), C.c_int64()
+        self._check(self.L.pci_batch_info(self.b, C.byref(n), C.byref(r), C.byref(z)))
+        return n.value, r.value, z.value
+
+    def tune(self, nv: int, cache=None):
+        v, ms, fc = C.c_int32(), C.c_double(), C.c_int32()
+        self._check(self.L.pci_batch_tune(self.b, nv, cache.encode() if cache else None, C.byref(v),
+                                          C.byref(ms), C.byref(fc)))
+        return v.value, ms.value, bool(fc.value)
+
+    def davidson(self, nlv=6, max_sub=48, keep=None, max_it=300, tol=1e-8, it_per_graph=4, spmm_variant=-1):
+        nblk = len(self.sizes)
+        p = BatchParams(nlv, max_sub, keep if keep is not None else 2 * nlv, max_it, tol, it_per_graph,
+                        spmm_variant)
+        E = np.zeros((nblk, nlv))
+        rn = np.zeros((nblk, nlv))
+        it = np.zeros(nblk, np.int32)
+        st = np.zeros(nblk, np.int32)
+        gl = C.c_int32()
+        self._check(self.L.pci_batch_davidson(self.b, C.byref(p), _p(E), _p(rn), _p(it), _p(st), C.byref(gl)))
+        self.nlv = nlv
+        return dict(E=E, rnorm=rn, iters=it, status=st, graph_launches=gl.value)
+
+    def vectors(self, blk):
+        X = np.zeros((self.nlv, self.sizes[blk]))
+        self._check(self.L.pci_batch_vectors(self.b, blk, _p(X)))
+        return X.T
+
+    def stats(self):
+        out = np.zeros(6)
+        self._check(self.L.pci_batch_stats(self.b, _p(out), 6))
+        keys = ["total_ms", "iterations", "spmm_ms", "spmm_variant", "setup_ms", "launches_per_iteration"]
+        return dict(zip(keys, out.tolist()))
+
+    def close(self):
+        if self.b:
+            self.L.pci_batch_destroy(self.b)
+            self.b = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
     def __del__(self):
         try:

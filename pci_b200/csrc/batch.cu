@@ -1,0 +1,1260 @@
+// Batched form: many independent CI blocks solved together on one GPU.
+//
+// The reference runs one block per pconf job (Diag4, pconf.F90:238, and the
+// Davidson module davidson.f90: Nlv roots, N_it iterations, residual
+// criterion Crt4).  Here every block keeps its own lower-triangle FP32 CSR
+// where its H-build left it (no concatenation copy); a table of per-block
+// pointers lets one persistent SpMM kernel walk the rows of all blocks, and
+// all vectors live in shared tall arrays (rows of every block stacked,
+// column-major, leading dimension = total rows).
+//
+// The solver is a block Davidson with the diagonal correction and a thick
+// restart, run in lock step over the blocks: each step of an iteration (SpMM,
+// Gram update, projected eigensolve, residuals, correction,
+// orthonormalisation) is ONE launch over all blocks, per-block reductions go
+// through per-chunk partial sums added in a fixed order (deterministic), and
+// the per-block decisions (convergence, restart, dropped directions) are
+// taken on the device, so the iterations replay from a CUDA graph with one
+// 4-byte read-back per replay.  A converged block drops out of every kernel.
+//
+// Iteration for block b with orthonormal basis V (m columns), W = H V:
+//   G = V^T W (only the new columns are formed), G = E diag(w) E^T (Jacobi),
+//   x_j = V e_j, r_j = W e_j - w_j x_j for the nlv lowest w_j,
+//   t_j = r_j / (w_j - H_nn) for unconverged roots,
+//   restart V <- V E[:, :keep] when the basis would exceed max_sub,
+//   t <- normalised, two classical Gram-Schmidt passes against V, two
+//   Cholesky-QR passes (dependent directions dropped), appended to V.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "pci_internal.h"
+#include "../../include/pci_batch.h"
+
+#define FULL_MASK 0xffffffffu
+
+namespace {
+
+constexpr int BT_CH = 1024;                                  // rows per chunk
+constexpr int BT_TR = 32;                                    // rows per tile of the TN products
+constexpr int BT_MS = PCI_BATCH_MAX_SUB;
+constexpr int BT_LV = PCI_BATCH_MAX_LV;
+constexpr int BT_PW = BT_MS * BT_LV;                         // partial words per chunk
+constexpr int BT_ROT_THREADS = 128;
+
+struct BlkCsr {
+    const int64_t *rowptr;
+    const int32_t *col;
+    const float *val;
+    int64_t r0, nd;
+};
+
+struct Chunk {
+    int32_t blk, pad;
+    int64_t row0, row1;
+};
+
+// Per-block solver state, on the device.
+struct BState {
+    int m;        // basis vectors (the last knew of them still need H V)
+    int knew;
+    int done;     // 0 running, 1 converged, 2 iteration limit, 3 no new direction
+    int iters;
+    int restart;  // rotate V, W to `base` Ritz vectors this iteration
+    int base;     // basis vectors the corrections are orthogonalised against
+    int kk;       // corrections formed this iteration
+    int k1, k2;   // corrections left after the first and second Cholesky-QR
+    int pad;
+    int jsel[BT_LV];
+    double theta[BT_LV];
+    double rnorm[BT_LV];
+    double scale[BT_LV];
+};
+
+struct Bufs {
+    double *V, *W, *R, *T, *T2, *P, *Q, *G, *EV, *EW, *part, *coef, *D;
+    int64_t ld;
+    int msub, nlv, keep, max_it;
+    double tol;
+};
+
+enum { TN_GRAM = 0, TN_TT = 1, TN_VT = 2, TN_T2 = 3 };
+enum { FIN_GRAM = 0, FIN_NORM = 1, FIN_VT1 = 2, FIN_VT2 = 3, FIN_CHOL1 = 4, FIN_CHOL2 = 5, FIN_RESID = 6 };
+
+// ------------------------------------------------------------ setup ---
+
+__global__ void k_to_f32(const double *a, float *b, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+__global__ void kb_diag(const BlkCsr *blks, const int32_t *row_blk, int64_t rows, double *D)
+{
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < rows; n += (int64_t)gridDim.x * blockDim.x) {
+        const BlkCsr B = blks[row_blk[n]];
+        const int64_t ln = n - B.r0;
+        double d = 0.0;
+        for (int64_t l = B.rowptr[ln + 1] - 1; l >= B.rowptr[ln]; l--)
+            if (B.col[l] == ln) { d = (double)B.val[l]; break; }
+        D[n] = d;
+    }
+}
+
+__global__ void kb_set_units(double *V, int64_t ld, const int64_t *pos, int n)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) V[pos[i]] = 1.0;
+}
+
+// ------------------------------------------------------------- SpMM ---
+
+// Y = H X over the rows of every running block, X and Y row-major with NV
+// vectors.  A team of SUB lanes owns a row; within it NV lanes share one
+// stored element (lane v takes vector v) and SUB/NV elements go per step.
+// The transpose part of each element goes to Y as a global reduction, and
+// so does the row part (other rows add into it), so Y starts at zero.
+template <int NV, int SUB>
+__global__ void __launch_bounds__(256) kb_spmm(const BlkCsr *__restrict__ blks, const int32_t *__restrict__ row_blk,
+                                               const BState *__restrict__ bst, int64_t rows,
+                                               const double *__restrict__ X, double *Y)
+{
+    constexpr int G = SUB / NV;
+    constexpr int TPW = 32 / SUB;
+    const int lane = threadIdx.x & 31;
+    const int sl = lane % SUB;
+    const int g = sl / NV, v = sl - g * NV;
+    const bool act = g < G;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t n0 = warp * TPW; n0 < rows; n0 += nwarps * TPW) {
+        const int64_t n = n0 + lane / SUB;
+        bool ok = n < rows;
+        const int b = ok ? __ldg(&row_blk[n]) : 0;
+        ok = ok && bst[b].done == 0;
+        double acc = 0.0;
+        if (ok && act) {
+            const BlkCsr B = blks[b];
+            const int64_t ln = n - B.r0;
+            const int64_t l0 = __ldg(&B.rowptr[ln]), l1 = __ldg(&B.rowptr[ln + 1]);
+            const double xn = __ldg(&X[n * NV + v]);
+            for (int64_t l = l0 + g; l < l1; l += G) {
+                const int k = __ldg(&B.col[l]);
+                const double t = (double)__ldg(&B.val[l]);
+                const int64_t kg = B.r0 + k;
+                if (k != ln) atomicAdd(&Y[kg * NV + v], t * xn);
+                acc += t * __ldg(&X[kg * NV + v]);
+            }
+        }
+#pragma unroll
+        for (int gg = 1; gg < G; gg++) {
+            const double o = __shfl_sync(FULL_MASK, acc, g == 0 ? lane + gg * NV : lane);
+            if (g == 0) acc += o;
+        }
+        if (ok && act && g == 0) atomicAdd(&Y[n * NV + v], acc);
+    }
+}
+
+constexpr int N_SUB = 3, N_CTAS = 4;
+constexpr int SUBS[N_SUB] = {32, 16, 8};
+constexpr int CTAS[N_CTAS] = {4, 8, 16, 32};
+constexpr int N_VARIANTS = N_SUB * N_CTAS;
+constexpr int DEFAULT_VARIANT = 2;   // 32 lanes per row, 16 blocks per SM
+
+template <int NV>
+void launch_spmm_nv(int sub, int grid, cudaStream_t st, const BlkCsr *blks, const int32_t *row_blk, const BState *bst,
+                    int64_t rows, const double *X, double *Y)
+{
+    if (sub == 32) kb_spmm<NV, 32><<<grid, 256, 0, st>>>(blks, row_blk, bst, rows, X, Y);
+    else if (sub == 16) kb_spmm<NV, 16><<<grid, 256, 0, st>>>(blks, row_blk, bst, rows, X, Y);
+    else kb_spmm<NV, 8><<<grid, 256, 0, st>>>(blks, row_blk, bst, rows, X, Y);
+}
+
+void launch_spmm(int nv, int variant, int nsm, cudaStream_t st, const BlkCsr *blks, const int32_t *row_blk,
+                 const BState *bst, int64_t rows, const double *X, double *Y)
+{
+    const int sub = SUBS[variant / N_CTAS];
+    const int grid = nsm * CTAS[variant % N_CTAS];
+    switch (nv) {
+    case 1: launch_spmm_nv<1>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
+    case 2: launch_spmm_nv<2>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
+    case 3: launch_spmm_nv<3>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
+    case 4: launch_spmm_nv<4>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
+    case 5: launch_spmm_nv<5>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
+    case 6: launch_spmm_nv<6>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
+    case 7: launch_spmm_nv<7>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
+    default: launch_spmm_nv<8>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
+    }
+}
+
+// ------------------------------------------------------ per-row steps ---
+
+// P[n, s] = V[n, m-knew+s] (s < knew), 0 otherwise; Q = 0 for the SpMM.
+__global__ void kb_pack(const Chunk *__restrict__ chunks, const BState *__restrict__ bst, Bufs B)
+{
+    const Chunk ch = chunks[blockIdx.x];
+    const BState &s = bst[ch.blk];
+    if (s.done) return;
+    const int c0 = s.m - s.knew, kn = s.knew, nv = B.nlv;
+    for (int64_t n = ch.row0 + threadIdx.x; n < ch.row1; n += blockDim.x) {
+        for (int c = 0; c < nv; c++) {
+            B.P[n * nv + c] = c < kn ? B.V[(int64_t)(c0 + c) * B.ld + n] : 0.0;
+            B.Q[n * nv + c] = 0.0;
+        }
+    }
+}
+
+__device__ __forceinline__ void tn_dims(int mode, const BState &s, const Bufs &B, const double *&A, int &ma,
+                                        const double *&Bm, int &b0, int &kb)
+{
+    if (mode == TN_GRAM) { A = B.V; ma = s.m; Bm = B.Q; b0 = s.m - s.knew; kb = s.knew; }
+    else if (mode == TN_TT) { A = B.T; ma = s.kk; Bm = B.T; b0 = 0; kb = s.kk; }
+    else if (mode == TN_VT) { A = B.V; ma = s.base; Bm = B.T; b0 = 0; kb = s.kk; }
+    else { A = B.T2; ma = s.k1; Bm = B.T2; b0 = 0; kb = s.k1; }
+}
+
+// Per-chunk partial of A[:, :ma]^T B[:, b0:b0+kb] over the chunk's rows.  In
+// TN_GRAM mode B is the SpMM output Q (row-major) and the kernel also stores
+// it as W's new columns.
+template <int MODE>
+__global__ void __launch_bounds__(256) kb_tn(const Chunk *__restrict__ chunks, const BState *__restrict__ bst, Bufs B)
+{
+    const Chunk ch = chunks[blockIdx.x];
+    const BState &s = bst[ch.blk];
+    if (s.done) return;
+    const double *A, *Bm;
+    int ma, b0, kb;
+    tn_dims(MODE, s, B, A, ma, Bm, b0, kb);
+    __shared__ double As[BT_TR][BT_MS + 1];
+    __shared__ double Bs[BT_TR][BT_LV + 1];
+    const int ne = ma * kb, t = threadIdx.x;
+    const int i0 = kb ? t / kb : 0, c0 = kb ? t % kb : 0;
+    const int i1 = kb ? (t + 256) / kb : 0, c1 = kb ? (t + 256) % kb : 0;
+    double acc0 = 0.0, acc1 = 0.0;
+    const int64_t ld = B.ld;
+    for (int64_t r0 = ch.row0; r0 < ch.row1; r0 += BT_TR) {
+        const int nr = (int)min((int64_t)BT_TR, ch.row1 - r0);
+        for (int idx = t; idx < BT_TR * ma; idx += blockDim.x) {
+            const int r = idx % BT_TR, i = idx / BT_TR;
+            As[r][i] = r < nr ? A[(int64_t)i * ld + r0 + r] : 0.0;
+        }
+        for (int idx = t; idx < BT_TR * kb; idx += blockDim.x) {
+            const int r = idx % BT_TR, c = idx / BT_TR;
+            double v = 0.0;
+            if (r < nr) {
+                if (MODE == TN_GRAM) {
+                    v = Bm[(r0 + r) * B.nlv + c];
+                    B.W[(int64_t)(b0 + c) * ld + r0 + r] = v;
+                } else {
+                    v = Bm[(int64_t)(b0 + c) * ld + r0 + r];
+                }
+            }
+            Bs[r][c] = v;
+        }
+        __syncthreads();
+        if (t < ne) {
+#pragma unroll 8
+            for (int r = 0; r < BT_TR; r++) acc0 += As[r][i0] * Bs[r][c0];
+        }
+        if (t + 256 < ne) {
+#pragma unroll 8
+            for (int r = 0; r < BT_TR; r++) acc1 += As[r][i1] * Bs[r][c1];
+        }
+        __syncthreads();
+    }
+    double *out = B.part + (int64_t)blockIdx.x * BT_PW;
+    if (t < ne) out[t] = acc0;
+    if (t + 256 < ne) out[t + 256] = acc1;
+}
+
+// Sum of up to BT_LV per-thread values over the thread block into out[0..n).
+__device__ void block_sum(double (&v)[BT_LV], int n, double *out)
+{
+    __shared__ double red[8][BT_LV];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < BT_LV; j++) {
+        double x = v[j];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(FULL_MASK, x, o);
+        if (lane == 0) red[w][j] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < n) {
+        double x = 0.0;
+        for (int ww = 0; ww < (int)(blockDim.x >> 5); ww++) x += red[ww][threadIdx.x];
+        out[threadIdx.x] = x;
+    }
+}
+
+// R = W E[:, :nlv] - V E[:, :nlv] diag(theta); partial sums of |r_j|^2.
+__global__ void __launch_bounds__(256) kb_resid(const Chunk *__restrict__ chunks, const BState *__restrict__ bst, Bufs B)
+{
+    const Chunk ch = chunks[blockIdx.x];
+    const BState &s = bst[ch.blk];
+    if (s.done) return;
+    const int m = s.m, nlv = B.nlv;
+    __shared__ double Ys[BT_MS * BT_LV];
+    const double *EV = B.EV + (int64_t)ch.blk * BT_MS * BT_MS;
+    for (int e = threadIdx.x; e < m * nlv; e += blockDim.x) {
+        const int i = e / nlv, j = e % nlv;
+        Ys[e] = EV[j * BT_MS + i];
+    }
+    double th[BT_LV];
+#pragma unroll
+    for (int j = 0; j < BT_LV; j++) th[j] = j < nlv ? s.theta[j] : 0.0;
+    __syncthreads();
+    double ss[BT_LV];
+#pragma unroll
+    for (int j = 0; j < BT_LV; j++) ss[j] = 0.0;
+    for (int64_t n = ch.row0 + threadIdx.x; n < ch.row1; n += blockDim.x) {
+        double x[BT_LV], hx[BT_LV];
+#pragma unroll
+        for (int j = 0; j < BT_LV; j++) x[j] = hx[j] = 0.0;
+        for (int i = 0; i < m; i++) {
+            const double v = B.V[(int64_t)i * B.ld + n], w = B.W[(int64_t)i * B.ld + n];
+#pragma unroll
+            for (int j = 0; j < BT_LV; j++) {
+                if (j < nlv) {
+                    x[j] += v * Ys[i * nlv + j];
+                    hx[j] += w * Ys[i * nlv + j];
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < BT_LV; j++) {
+            if (j < nlv) {
+                const double r = hx[j] - th[j] * x[j];
+                B.R[(int64_t)j * B.ld + n] = r;
+                ss[j] += r * r;
+            }
+        }
+    }
+    block_sum(ss, nlv, B.part + (int64_t)blockIdx.x * BT_PW);
+}
+
+// Thick restart: V[:, :base] = V[:, :m] E[:, :base], W likewise, row by row
+// through shared memory.
+__global__ void __launch_bounds__(BT_ROT_THREADS) kb_rotate(const Chunk *__restrict__ chunks,
+                                                            const BState *__restrict__ bst, Bufs B)
+{
+    const Chunk ch = chunks[blockIdx.x];
+    const BState &s = bst[ch.blk];
+    if (s.done || !s.restart) return;
+    extern __shared__ double sm[];
+    const int m = s.m, kb = s.base;
+    double *Es = sm;                         // [m][kb]
+    double *rowv = sm + BT_MS * BT_MS;       // [m][BT_ROT_THREADS]
+    const double *EV = B.EV + (int64_t)ch.blk * BT_MS * BT_MS;
+    for (int e = threadIdx.x; e < m * kb; e += blockDim.x) {
+        const int i = e / kb, c = e % kb;
+        Es[e] = EV[c * BT_MS + i];
+    }
+    __syncthreads();
+    for (int64_t nb = ch.row0; nb < ch.row1; nb += BT_ROT_THREADS) {
+        const int64_t n = nb + threadIdx.x;
+        const bool ok = n < ch.row1;
+        for (int pass = 0; pass < 2; pass++) {
+            double *A = pass ? B.W : B.V;
+            if (ok)
+                for (int i = 0; i < m; i++) rowv[i * BT_ROT_THREADS + threadIdx.x] = A[(int64_t)i * B.ld + n];
+            if (ok)
+                for (int c = 0; c < kb; c++) {
+                    double acc = 0.0;
+                    for (int i = 0; i < m; i++) acc += rowv[i * BT_ROT_THREADS + threadIdx.x] * Es[i * kb + c];
+                    A[(int64_t)c * B.ld + n] = acc;
+                }
+        }
+    }
+}
+
+// T[:, s] = R[:, jsel[s]] / (theta_j - H_nn).
+__global__ void kb_correct(const Chunk *__restrict__ chunks, const BState *__restrict__ bst, Bufs B)
+{
+    const Chunk ch = chunks[blockIdx.x];
+    const BState &s = bst[ch.blk];
+    if (s.done) return;
+    const int kk = s.kk;
+    for (int64_t n = ch.row0 + threadIdx.x; n < ch.row1; n += blockDim.x) {
+        const double dn = B.D[n];
+        for (int c = 0; c < kk; c++) {
+            const int j = s.jsel[c];
+            double d = s.theta[j] - dn;
+            if (fabs(d) < 1e-8) d = d < 0.0 ? -1e-8 : 1e-8;
+            B.T[(int64_t)c * B.ld + n] = B.R[(int64_t)j * B.ld + n] / d;
+        }
+    }
+}
+
+// T[:, s] = scale_s T[:, s] - V[:, :base] C[:, s].
+__global__ void __launch_bounds__(256) kb_proj(const Chunk *__restrict__ chunks, const BState *__restrict__ bst, Bufs B)
+{
+    const Chunk ch = chunks[blockIdx.x];
+    const BState &s = bst[ch.blk];
+    if (s.done) return;
+    const int kk = s.kk, base = s.base;
+    __shared__ double Cs[BT_PW];
+    const double *C = B.coef + (int64_t)ch.blk * BT_PW;
+    for (int e = threadIdx.x; e < base * kk; e += blockDim.x) Cs[e] = C[e];
+    __syncthreads();
+    for (int64_t n = ch.row0 + threadIdx.x; n < ch.row1; n += blockDim.x) {
+        double acc[BT_LV];
+#pragma unroll
+        for (int c = 0; c < BT_LV; c++) acc[c] = c < kk ? s.scale[c] * B.T[(int64_t)c * B.ld + n] : 0.0;
+        for (int i = 0; i < base; i++) {
+            const double v = B.V[(int64_t)i * B.ld + n];
+#pragma unroll
+            for (int c = 0; c < BT_LV; c++)
+                if (c < kk) acc[c] -= v * Cs[i * kk + c];
+        }
+#pragma unroll
+        for (int c = 0; c < BT_LV; c++)
+            if (c < kk) B.T[(int64_t)c * B.ld + n] = acc[c];
+    }
+}
+
+// out[:, :kout] = in[:, :kin] M (M = coef, kin x kout); pass 1 T -> T2,
+// pass 2 T2 -> V[:, base:].
+template <int PASS>
+__global__ void __launch_bounds__(256) kb_tri(const Chunk *__restrict__ chunks, const BState *__restrict__ bst, Bufs B)
+{
+    const Chunk ch = chunks[blockIdx.x];
+    const BState &s = bst[ch.blk];
+    if (s.done) return;
+    const int kin = PASS == 1 ? s.kk : s.k1, kout = PASS == 1 ? s.k1 : s.k2;
+    const double *in = PASS == 1 ? B.T : B.T2;
+    double *out = PASS == 1 ? B.T2 : B.V + (int64_t)s.base * B.ld;
+    __shared__ double Ms[BT_LV * BT_LV];
+    const double *M = B.coef + (int64_t)ch.blk * BT_PW;
+    for (int e = threadIdx.x; e < kin * kout; e += blockDim.x) Ms[e] = M[e];
+    __syncthreads();
+    for (int64_t n = ch.row0 + threadIdx.x; n < ch.row1; n += blockDim.x) {
+        double x[BT_LV];
+#pragma unroll
+        for (int c = 0; c < BT_LV; c++) x[c] = c < kin ? in[(int64_t)c * B.ld + n] : 0.0;
+        for (int o = 0; o < kout; o++) {
+            double acc = 0.0;
+#pragma unroll
+            for (int c = 0; c < BT_LV; c++)
+                if (c < kin) acc += x[c] * Ms[c * kout + o];
+            out[(int64_t)o * B.ld + n] = acc;
+        }
+    }
+}
+
+// Final Ritz vectors X[:, j] = V[:, :m] E[:, j] into R.
+__global__ void __launch_bounds__(256) kb_ritz(const Chunk *__restrict__ chunks, const BState *__restrict__ bst, Bufs B)
+{
+    const Chunk ch = chunks[blockIdx.x];
+    const BState &s = bst[ch.blk];
+    const int m = s.m, nlv = B.nlv;
+    __shared__ double Ys[BT_MS * BT_LV];
+    const double *EV = B.EV + (int64_t)ch.blk * BT_MS * BT_MS;
+    for (int e = threadIdx.x; e < m * nlv; e += blockDim.x) Ys[e] = EV[(e % nlv) * BT_MS + e / nlv];
+    __syncthreads();
+    for (int64_t n = ch.row0 + threadIdx.x; n < ch.row1; n += blockDim.x) {
+        double x[BT_LV];
+#pragma unroll
+        for (int j = 0; j < BT_LV; j++) x[j] = 0.0;
+        for (int i = 0; i < m; i++) {
+            const double v = B.V[(int64_t)i * B.ld + n];
+#pragma unroll
+            for (int j = 0; j < BT_LV; j++)
+                if (j < nlv) x[j] += v * Ys[i * nlv + j];
+        }
+        for (int j = 0; j < nlv; j++) B.R[(int64_t)j * B.ld + n] = x[j];
+    }
+}
+
+// --------------------------------------------------- per-block steps ---
+
+// Cholesky of the k x k Gram matrix S (row-major) with dependent columns
+// (pivot <= thr) dropped; M (k x kept, row-major) maps the k columns to the
+// kept orthonormal ones: out = in M.  Returns the number kept.
+__device__ int chol_drop(const double *S, int k, double thr, double *M)
+{
+    double L[BT_LV][BT_LV];
+    int kept[BT_LV], nk = 0;
+    for (int i = 0; i < BT_LV; i++)
+        for (int j = 0; j < BT_LV; j++) L[i][j] = 0.0;
+    for (int j = 0; j < k; j++) {
+        double d = S[j * k + j];
+        for (int a = 0; a < nk; a++) d -= L[j][kept[a]] * L[j][kept[a]];
+        if (!(d > thr)) continue;
+        const double ljj = sqrt(d);
+        L[j][j] = ljj;
+        for (int i = j + 1; i < k; i++) {
+            double x = S[i * k + j];
+            for (int a = 0; a < nk; a++) x -= L[i][kept[a]] * L[j][kept[a]];
+            L[i][j] = x / ljj;
+        }
+        kept[nk++] = j;
+    }
+    // Li = inverse of L restricted to the kept rows and columns (lower triangular)
+    double Li[BT_LV][BT_LV];
+    for (int a = 0; a < nk; a++) {
+        for (int c = 0; c < nk; c++) Li[a][c] = 0.0;
+        Li[a][a] = 1.0 / L[kept[a]][kept[a]];
+        for (int c = 0; c < a; c++) {
+            double x = 0.0;
+            for (int p = c; p < a; p++) x += L[kept[a]][kept[p]] * Li[p][c];
+            Li[a][c] = -x * Li[a][a];
+        }
+    }
+    for (int r = 0; r < k; r++)
+        for (int c = 0; c < nk; c++) M[r * nk + c] = 0.0;
+    for (int a = 0; a < nk; a++)
+        for (int c = 0; c < nk; c++) M[kept[a] * nk + c] = Li[c][a];
+    return nk;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) kb_fin(const int64_t *__restrict__ cb, BState *bst, Bufs B)
+{
+    const int b = blockIdx.x, t = threadIdx.x;
+    BState &s = bst[b];
+    if (s.done) return;
+    int ma, kb;
+    if (MODE == FIN_GRAM) { ma = s.m; kb = s.knew; }
+    else if (MODE == FIN_NORM || MODE == FIN_CHOL1) { ma = s.kk; kb = s.kk; }
+    else if (MODE == FIN_VT1 || MODE == FIN_VT2) { ma = s.base; kb = s.kk; }
+    else if (MODE == FIN_CHOL2) { ma = s.k1; kb = s.k1; }
+    else { ma = 1; kb = B.nlv; }
+    __shared__ double res[BT_PW];
+    const int ne = ma * kb;
+    const int64_t c0 = cb[b], c1 = cb[b + 1];
+    for (int e = t; e < ne; e += blockDim.x) {
+        double acc = 0.0;
+        for (int64_t c = c0; c < c1; c++) acc += B.part[c * BT_PW + e];
+        res[e] = acc;
+    }
+    __syncthreads();
+    double *coef = B.coef + (int64_t)b * BT_PW;
+    if (MODE == FIN_GRAM) {
+        double *G = B.G + (int64_t)b * BT_MS * BT_MS;
+        const int n0 = s.m - s.knew;
+        for (int e = t; e < ne; e += blockDim.x) {
+            const int i = e / kb, c = e % kb, col = n0 + c;
+            double v = res[e];
+            if (i >= n0) v = 0.5 * (v + res[col * kb + (i - n0)]);
+            G[i * BT_MS + col] = v;
+            G[col * BT_MS + i] = v;
+        }
+    } else if (MODE == FIN_NORM) {
+        if (t < kb) {
+            const double q = res[t * kb + t];
+            s.scale[t] = q > 0.0 ? 1.0 / sqrt(q) : 0.0;
+        }
+    } else if (MODE == FIN_VT1) {
+        for (int e = t; e < ne; e += blockDim.x) coef[e] = res[e] * s.scale[e % kb];
+    } else if (MODE == FIN_VT2) {
+        for (int e = t; e < ne; e += blockDim.x) coef[e] = res[e];
+        __syncthreads();
+        if (t < kb) s.scale[t] = 1.0;
+    } else if (MODE == FIN_CHOL1) {
+        if (t == 0) s.k1 = chol_drop(res, kb, 1e-16, coef);
+    } else if (MODE == FIN_CHOL2) {
+        if (t == 0) s.k2 = chol_drop(res, kb, 1e-3, coef);
+    } else {   // FIN_RESID: convergence, corrections to form, restart
+        __shared__ int sh_base, sh_restart;
+        if (t == 0) {
+            int nconv = 0;
+            for (int j = 0; j < B.nlv; j++) {
+                const double rn = sqrt(fmax(res[j], 0.0));
+                s.rnorm[j] = rn;
+                nconv += rn <= B.tol;
+            }
+            s.iters += 1;
+            sh_restart = 0;
+            sh_base = 0;
+            if (nconv == B.nlv) {
+                s.done = 1;
+            } else if (s.iters >= B.max_it) {
+                s.done = 2;
+            } else {
+                int kk = 0;
+                for (int j = 0; j < B.nlv; j++)
+                    if (!(s.rnorm[j] <= B.tol)) s.jsel[kk++] = j;
+                s.kk = kk;
+                if (s.m + kk > B.msub) {
+                    sh_base = min(B.keep, s.m);
+                    sh_restart = 1;
+                } else {
+                    sh_base = s.m;
+                }
+                s.base = sh_base;
+                s.restart = sh_restart;
+            }
+        }
+        __syncthreads();
+        if (sh_restart) {
+            double *G = B.G + (int64_t)b * BT_MS * BT_MS;
+            const double *EW = B.EW + (int64_t)b * BT_MS;
+            for (int e = t; e < sh_base * sh_base; e += blockDim.x) {
+                const int i = e / sh_base, j = e % sh_base;
+                G[i * BT_MS + j] = i == j ? EW[i] : 0.0;
+            }
+        }
+    }
+}
+
+// Eigenpairs of the m x m projected matrix of every running block by cyclic
+// Jacobi rotations in round-robin order (m/2 disjoint rotations per step; the
+// rotation angle as in Golub & Van Loan, Matrix Computations, sec. 8.5),
+// eigenvalues ascending.
+__global__ void __launch_bounds__(256) kb_eig(BState *bst, Bufs B)
+{
+    const int b = blockIdx.x, t = threadIdx.x;
+    BState &s = bst[b];
+    if (s.done) return;
+    const int m = s.m, mp = m + (m & 1), h = mp / 2;
+    extern __shared__ double sm[];
+    double *A = sm, *Vm = sm + mp * mp;
+    __shared__ int pp[BT_MS / 2], qq[BT_MS / 2];
+    __shared__ double cc[BT_MS / 2], sn[BT_MS / 2];
+    __shared__ double red[2][8];
+    __shared__ int stop;
+    __shared__ int order[BT_MS];
+    const double *G = B.G + (int64_t)b * BT_MS * BT_MS;
+    for (int e = t; e < mp * mp; e += blockDim.x) {
+        const int i = e / mp, j = e % mp;
+        A[e] = (i < m && j < m) ? G[i * BT_MS + j] : 0.0;
+        Vm[e] = i == j ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    for (int sweep = 0; sweep < 40; sweep++) {
+        double off = 0.0, tot = 0.0;
+        for (int e = t; e < mp * mp; e += blockDim.x) {
+            const double a = A[e];
+            tot += a * a;
+            if (e / mp != e % mp) off += a * a;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            off += __shfl_down_sync(FULL_MASK, off, o);
+            tot += __shfl_down_sync(FULL_MASK, tot, o);
+        }
+        if ((t & 31) == 0) { red[0][t >> 5] = off; red[1][t >> 5] = tot; }
+        __syncthreads();
+        if (t == 0) {
+            double o2 = 0.0, t2 = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) { o2 += red[0][w]; t2 += red[1][w]; }
+            stop = !(o2 > 1e-30 * t2);
+        }
+        __syncthreads();
+        if (stop) break;
+        for (int r = 0; r < mp - 1; r++) {
+            if (t < h) {
+                int p, q;
+                if (t == 0) { p = mp - 1; q = r; }
+                else { p = (r + t) % (mp - 1); q = (r - t + mp - 1) % (mp - 1); }
+                if (p > q) { const int x = p; p = q; q = x; }
+                const double apq = A[p * mp + q];
+                double c = 1.0, sv = 0.0;
+                if (apq != 0.0) {
+                    const double th = (A[q * mp + q] - A[p * mp + p]) / (2.0 * apq);
+                    const double at = fabs(th);
+                    const double tt = at > 1e150 ? 0.5 / th : (th >= 0.0 ? 1.0 : -1.0) / (at + sqrt(th * th + 1.0));
+                    c = 1.0 / sqrt(tt * tt + 1.0);
+                    sv = tt * c;
+                }
+                pp[t] = p; qq[t] = q; cc[t] = c; sn[t] = sv;
+            }
+            __syncthreads();
+            for (int w = t; w < mp * h; w += blockDim.x) {   // columns: A <- A J, V <- V J
+                const int k = w % mp, i = w / mp;
+                const int p = pp[i], q = qq[i];
+                const double c = cc[i], sv = sn[i];
+                const double ap = A[k * mp + p], aq = A[k * mp + q];
+                A[k * mp + p] = c * ap - sv * aq;
+                A[k * mp + q] = sv * ap + c * aq;
+                const double vp = Vm[k * mp + p], vq = Vm[k * mp + q];
+                Vm[k * mp + p] = c * vp - sv * vq;
+                Vm[k * mp + q] = sv * vp + c * vq;
+            }
+            __syncthreads();
+            for (int w = t; w < mp * h; w += blockDim.x) {   // rows: A <- J^T A
+                const int k = w % mp, i = w / mp;
+                const int p = pp[i], q = qq[i];
+                const double c = cc[i], sv = sn[i];
+                const double ap = A[p * mp + k], aq = A[q * mp + k];
+                A[p * mp + k] = c * ap - sv * aq;
+                A[q * mp + k] = sv * ap + c * aq;
+            }
+            __syncthreads();
+        }
+    }
+    if (t == 0) {
+        for (int i = 0; i < m; i++) order[i] = i;
+        for (int i = 0; i < m; i++) {   // stable selection of the ascending order
+            int best = i;
+            for (int j = i + 1; j < m; j++) {
+                const double dj = A[order[j] * mp + order[j]], db = A[order[best] * mp + order[best]];
+                if (dj < db) best = j;
+            }
+            const int x = order[best];
+            for (int j = best; j > i; j--) order[j] = order[j - 1];
+            order[i] = x;
+        }
+        for (int j = 0; j < B.nlv; j++) s.theta[j] = A[order[j] * mp + order[j]];
+    }
+    __syncthreads();
+    double *EW = B.EW + (int64_t)b * BT_MS, *EV = B.EV + (int64_t)b * BT_MS * BT_MS;
+    for (int e = t; e < m * m; e += blockDim.x) {
+        const int j = e / m, i = e % m;
+        EV[j * BT_MS + i] = Vm[i * mp + order[j]];
+        if (i == 0) EW[j] = A[order[j] * mp + order[j]];
+    }
+}
+
+__global__ void kb_commit(BState *bst, int nblk)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nblk) return;
+    BState &s = bst[b];
+    if (s.done) return;
+    s.m = s.base + s.k2;
+    s.knew = s.k2;
+    s.restart = 0;
+    if (s.k2 == 0) s.done = 3;
+}
+
+__global__ void kb_count(const BState *bst, int nblk, int *ndone)
+{
+    __shared__ int c;
+    if (threadIdx.x == 0) c = 0;
+    __syncthreads();
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+        if (bst[b].done) atomicAdd(&c, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) *ndone = c;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- host ---
+
+struct BlockRec {
+    Csr H;
+    int64_t r0 = 0;
+};
+
+struct pci_batch {
+    pci_gpu core;   // device, stream, error text and scratch
+    int nsm = 148;
+    std::string devname;
+    std::vector<BlockRec> blocks;
+    int64_t rows = 0, nnz = 0;
+    bool dirty = true;
+    BlkCsr *d_blk = nullptr;
+    int32_t *d_row_blk = nullptr;
+    double *d_D = nullptr;
+    Chunk *d_chunks = nullptr;
+    int64_t *d_cb = nullptr;
+    int nch = 0;
+    // solve buffers
+    int64_t cap_rows = 0;
+    int cap_nlv = 0;
+    double *d_V = nullptr, *d_W = nullptr, *d_R = nullptr, *d_T = nullptr, *d_T2 = nullptr, *d_P = nullptr,
+           *d_Q = nullptr, *d_G = nullptr, *d_EV = nullptr, *d_EW = nullptr, *d_part = nullptr, *d_coef = nullptr;
+    BState *d_st = nullptr;
+    int *d_ndone = nullptr;
+    int last_nlv = 0;
+    int tuned_variant = -1, tuned_nv = 0;
+    double tuned_ms = 0.0;
+    double st_total = 0, st_iters = 0, st_spmm = 0, st_variant = 0, st_setup = 0, st_launches = 0;
+};
+
+static void free_solve(pci_batch *b)
+{
+    double **bufs[] = {&b->d_V, &b->d_W, &b->d_R, &b->d_T, &b->d_T2, &b->d_P, &b->d_Q,
+                       &b->d_G, &b->d_EV, &b->d_EW, &b->d_part, &b->d_coef};
+    for (double **p : bufs) { dev_free(*p); *p = nullptr; }
+    dev_free(b->d_st);
+    b->d_st = nullptr;
+    dev_free(b->d_ndone);
+    b->d_ndone = nullptr;
+    b->cap_rows = 0;
+    b->cap_nlv = 0;
+}
+
+static void free_tables(pci_batch *b)
+{
+    dev_free(b->d_blk);
+    dev_free(b->d_row_blk);
+    dev_free(b->d_D);
+    dev_free(b->d_chunks);
+    dev_free(b->d_cb);
+    b->d_blk = nullptr;
+    b->d_row_blk = nullptr;
+    b->d_D = nullptr;
+    b->d_chunks = nullptr;
+    b->d_cb = nullptr;
+    b->nch = 0;
+}
+
+// Block table, row -> block map, diagonal and the chunk table.
+static int build_tables(pci_batch *b)
+{
+    if (!b->dirty) return PCI_OK;
+    pci_gpu *h = &b->core;
+    free_tables(b);
+    const int nblk = (int)b->blocks.size();
+    std::vector<BlkCsr> tab(nblk);
+    std::vector<int32_t> rb(b->rows);
+    std::vector<Chunk> ch;
+    std::vector<int64_t> cb(nblk + 1, 0);
+    for (int i = 0; i < nblk; i++) {
+        const BlockRec &r = b->blocks[i];
+        tab[i] = BlkCsr{r.H.rowptr, r.H.col, (const float *)r.H.val, r.r0, r.H.nrows};
+        std::fill(rb.begin() + r.r0, rb.begin() + r.r0 + r.H.nrows, i);
+        cb[i] = (int64_t)ch.size();
+        for (int64_t s = 0; s < r.H.nrows; s += BT_CH)
+            ch.push_back(Chunk{i, 0, r.r0 + s, r.r0 + std::min<int64_t>(s + BT_CH, r.H.nrows)});
+    }
+    cb[nblk] = (int64_t)ch.size();
+    int rc = 0;
+    b->d_blk = (BlkCsr *)dev_alloc(h, sizeof(BlkCsr) * nblk, &rc);
+    if (rc) return rc;
+    b->d_row_blk = (int32_t *)dev_alloc(h, 4 * b->rows, &rc);
+    if (rc) return rc;
+    b->d_D = (double *)dev_alloc(h, 8 * b->rows, &rc);
+    if (rc) return rc;
+    b->d_chunks = (Chunk *)dev_alloc(h, sizeof(Chunk) * ch.size(), &rc);
+    if (rc) return rc;
+    b->d_cb = (int64_t *)dev_alloc(h, 8 * cb.size(), &rc);
+    if (rc) return rc;
+    PCI_CUDA(h, cudaMemcpy(b->d_blk, tab.data(), sizeof(BlkCsr) * nblk, cudaMemcpyHostToDevice));
+    PCI_CUDA(h, cudaMemcpy(b->d_row_blk, rb.data(), 4 * b->rows, cudaMemcpyHostToDevice));
+    PCI_CUDA(h, cudaMemcpy(b->d_chunks, ch.data(), sizeof(Chunk) * ch.size(), cudaMemcpyHostToDevice));
+    PCI_CUDA(h, cudaMemcpy(b->d_cb, cb.data(), 8 * cb.size(), cudaMemcpyHostToDevice));
+    b->nch = (int)ch.size();
+    kb_diag<<<b->nsm * 8, 256, 0, h->st>>>(b->d_blk, b->d_row_blk, b->rows, b->d_D);
+    PCI_CUDA(h, cudaGetLastError());
+    PCI_CUDA(h, cudaStreamSynchronize(h->st));
+    b->dirty = false;
+    return PCI_OK;
+}
+
+static int ensure_solve(pci_batch *b, int nlv)
+{
+    if (b->cap_rows == b->rows && b->cap_nlv == nlv) return PCI_OK;
+    free_solve(b);
+    pci_gpu *h = &b->core;
+    const int64_t R = b->rows, nblk = (int64_t)b->blocks.size();
+    int rc = 0;
+    auto al = [&](double **p, int64_t words) {
+        if (!rc) *p = (double *)dev_alloc(h, 8 * std::max<int64_t>(words, 1), &rc);
+    };
+    al(&b->d_V, R * BT_MS);
+    al(&b->d_W, R * BT_MS);
+    al(&b->d_R, R * nlv);
+    al(&b->d_T, R * nlv);
+    al(&b->d_T2, R * nlv);
+    al(&b->d_P, R * nlv);
+    al(&b->d_Q, R * nlv);
+    al(&b->d_G, nblk * BT_MS * BT_MS);
+    al(&b->d_EV, nblk * BT_MS * BT_MS);
+    al(&b->d_EW, nblk * BT_MS);
+    al(&b->d_part, (int64_t)b->nch * BT_PW);
+    al(&b->d_coef, nblk * BT_PW);
+    if (rc) return rc;
+    b->d_st = (BState *)dev_alloc(h, sizeof(BState) * nblk, &rc);
+    if (rc) return rc;
+    b->d_ndone = (int *)dev_alloc(h, 16, &rc);
+    if (rc) return rc;
+    b->cap_rows = R;
+    b->cap_nlv = nlv;
+    return PCI_OK;
+}
+
+static Bufs make_bufs(pci_batch *b, const pci_batch_params *p)
+{
+    Bufs B;
+    B.V = b->d_V; B.W = b->d_W; B.R = b->d_R; B.T = b->d_T; B.T2 = b->d_T2; B.P = b->d_P; B.Q = b->d_Q;
+    B.G = b->d_G; B.EV = b->d_EV; B.EW = b->d_EW; B.part = b->d_part; B.coef = b->d_coef; B.D = b->d_D;
+    B.ld = b->rows;
+    B.msub = p ? p->max_sub : BT_MS;
+    B.nlv = p ? p->nlv : b->cap_nlv;
+    B.keep = p ? p->keep : 0;
+    B.max_it = p ? p->max_it : 0;
+    B.tol = p ? p->tol : 0.0;
+    return B;
+}
+
+static int set_attrs(pci_batch *b)
+{
+    pci_gpu *h = &b->core;
+    PCI_CUDA(h, cudaFuncSetAttribute(kb_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * BT_MS * BT_MS * 8));
+    PCI_CUDA(h, cudaFuncSetAttribute(kb_rotate, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (BT_MS * BT_MS + BT_MS * BT_ROT_THREADS) * 8));
+    return PCI_OK;
+}
+
+// One iteration of every running block (26 launches, no host synchronisation).
+static int enqueue_iteration(pci_batch *b, const Bufs &B, int variant, int nv)
+{
+    pci_gpu *h = &b->core;
+    cudaStream_t st = h->st;
+    const int nch = b->nch, nblk = (int)b->blocks.size();
+    kb_pack<<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
+    launch_spmm(nv, variant, b->nsm, st, b->d_blk, b->d_row_blk, b->d_st, b->rows, B.P, B.Q);
+    kb_tn<TN_GRAM><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
+    kb_fin<FIN_GRAM><<<nblk, 256, 0, st>>>(b->d_cb, b->d_st, B);
+    kb_eig<<<nblk, 256, 2 * BT_MS * BT_MS * 8, st>>>(b->d_st, B);
+    kb_resid<<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
+    kb_fin<FIN_RESID><<<nblk, 256, 0, st>>>(b->d_cb, b->d_st, B);
+    kb_rotate<<<nch, BT_ROT_THREADS, (BT_MS * BT_MS + BT_MS * BT_ROT_THREADS) * 8, st>>>(b->d_chunks, b->d_st, B);
+    kb_correct<<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
+    kb_tn<TN_TT><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
+    kb_fin<FIN_NORM><<<nblk, 256, 0, st>>>(b->d_cb, b->d_st, B);
+    kb_tn<TN_VT><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
+    kb_fin<FIN_VT1><<<nblk, 256, 0, st>>>(b->d_cb, b->d_st, B);
+    kb_proj<<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
+    kb_tn<TN_VT><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
+    kb_fin<FIN_VT2><<<nblk, 256, 0, st>>>(b->d_cb, b->d_st, B);
+    kb_proj<<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
+    kb_tn<TN_TT><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
+    kb_fin<FIN_CHOL1><<<nblk, 256, 0, st>>>(b->d_cb, b->d_st, B);
+    kb_tri<1><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
+    kb_tn<TN_T2><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
+    kb_fin<FIN_CHOL2><<<nblk, 256, 0, st>>>(b->d_cb, b->d_st, B);
+    kb_tri<2><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
+    kb_commit<<<(nblk + 127) / 128, 128, 0, st>>>(b->d_st, nblk);
+    kb_count<<<1, 256, 0, st>>>(b->d_st, nblk, b->d_ndone);
+    PCI_CUDA(h, cudaGetLastError());
+    return PCI_OK;
+}
+
+static const int ITER_LAUNCHES = 25;
+
+// One SpMM of every block with the given variant on P (all blocks running),
+// timed with events; average ms over `reps`.
+static int time_spmm(pci_batch *b, int nv, int variant, int reps, double *ms)
+{
+    pci_gpu *h = &b->core;
+    cudaEvent_t e0, e1;
+    PCI_CUDA(h, cudaEventCreate(&e0));
+    PCI_CUDA(h, cudaEventCreate(&e1));
+    launch_spmm(nv, variant, b->nsm, h->st, b->d_blk, b->d_row_blk, b->d_st, b->rows, b->d_P, b->d_Q);
+    PCI_CUDA(h, cudaEventRecord(e0, h->st));
+    for (int r = 0; r < reps; r++) {
+        PCI_CUDA(h, cudaMemsetAsync(b->d_Q, 0, 8 * b->rows * nv, h->st));
+        launch_spmm(nv, variant, b->nsm, h->st, b->d_blk, b->d_row_blk, b->d_st, b->rows, b->d_P, b->d_Q);
+    }
+    PCI_CUDA(h, cudaEventRecord(e1, h->st));
+    PCI_CUDA(h, cudaGetLastError());
+    PCI_CUDA(h, cudaEventSynchronize(e1));
+    float f = 0.f;
+    cudaEventElapsedTime(&f, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = f / reps;
+    return PCI_OK;
+}
+
+static int prepare(pci_batch *b, int nlv)
+{
+    pci_gpu *h = &b->core;
+    cudaSetDevice(h->device);
+    if (b->blocks.empty()) return set_err(h, PCI_E_STATE, "batch has no blocks");
+    int rc = build_tables(b);
+    if (rc) return rc;
+    if ((rc = ensure_solve(b, nlv))) return rc;
+    return set_attrs(b);
+}
+
+static std::string tune_key(pci_batch *b, int nv)
+{
+    std::ostringstream k;
+    std::string dn = b->devname;
+    for (char &c : dn)
+        if (c == ' ') c = '_';
+    k << dn << "|blocks=" << b->blocks.size() << "|rows=" << b->rows << "|nnz=" << b->nnz << "|nv=" << nv;
+    return k.str();
+}
+
+extern "C" {
+
+int pci_batch_create(int32_t device, pci_batch_t **out)
+{
+    if (!out) return PCI_E_INPUT;
+    pci_batch *b = new pci_batch();
+    *out = b;
+    b->core.device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_err(&b->core, e, "cudaSetDevice");
+    e = cudaStreamCreateWithFlags(&b->core.st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_err(&b->core, e, "cudaStreamCreate");
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) {
+        b->nsm = prop.multiProcessorCount;
+        b->devname = prop.name;
+    }
+    return PCI_OK;
+}
+
+int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index)
+{
+    if (!b || !h) return PCI_E_INPUT;
+    pci_gpu *c = &b->core;
+    if (h->device != c->device) return set_err(c, PCI_E_INPUT, "block handle is on another device");
+    if (!h->H.rowptr) return set_err(c, PCI_E_STATE, "the handle holds no Hamiltonian");
+    if (b->blocks.size() >= (size_t)INT32_MAX) return set_err(c, PCI_E_INPUT, "too many blocks");
+    if (b->rows + h->H.nrows >= (int64_t)1 << 40) return set_err(c, PCI_E_INPUT, "too many rows");
+    cudaSetDevice(c->device);
+    BlockRec r;
+    r.H = h->H;
+    r.r0 = b->rows;
+    if (!r.H.val_f32) {
+        int rc = 0;
+        float *v = (float *)dev_alloc(c, std::max<int64_t>(r.H.nnz, 1) * 4, &rc);
+        if (rc) return rc;
+        k_to_f32<<<b->nsm * 8, 256, 0, c->st>>>((const double *)r.H.val, v, r.H.nnz);
+        PCI_CUDA(c, cudaGetLastError());
+        PCI_CUDA(c, cudaStreamSynchronize(c->st));
+        dev_free(r.H.val);
+        r.H.val = v;
+        r.H.val_f32 = 1;
+    }
+    h->H = Csr();
+    csr_free(h->Hfull);
+    h->h_from_tiles = false;
+    b->blocks.push_back(r);
+    b->rows += r.H.nrows;
+    b->nnz += r.H.nnz;
+    b->dirty = true;
+    b->tuned_variant = -1;
+    free_solve(b);
+    if (index) *index = (int32_t)(b->blocks.size() - 1);
+    return PCI_OK;
+}
+
+int pci_batch_info(pci_batch_t *b, int32_t *nblocks, int64_t *rows, int64_t *nnz)
+{
+    if (!b) return PCI_E_INPUT;
+    if (nblocks) *nblocks = (int32_t)b->blocks.size();
+    if (rows) *rows = b->rows;
+    if (nnz) *nnz = b->nnz;
+    return PCI_OK;
+}
+
+int pci_batch_variant(int32_t variant, int32_t *lanes_per_row, int32_t *blocks_per_sm)
+{
+    if (variant < 0 || variant >= N_VARIANTS) return N_VARIANTS;
+    if (lanes_per_row) *lanes_per_row = SUBS[variant / N_CTAS];
+    if (blocks_per_sm) *blocks_per_sm = CTAS[variant % N_CTAS];
+    return PCI_OK;
+}
+
+int pci_batch_tune(pci_batch_t *b, int32_t nv, const char *cache_path, int32_t *variant, double *ms,
+                   int32_t *from_cache)
+{
+    if (!b) return PCI_E_INPUT;
+    pci_gpu *h = &b->core;
+    if (nv < 1 || nv > BT_LV) return set_err(h, PCI_E_INPUT, "nv must be 1..8");
+    int rc = prepare(b, nv);
+    if (rc) return rc;
+    const std::string key = tune_key(b, nv);
+    int best = -1;
+    double best_ms = 0.0;
+    int cached = 0;
+    if (cache_path) {
+        std::ifstream f(cache_path);
+        std::string tag, k;
+        int v;
+        double t;
+        while (f >> tag >> k >> v >> t)
+            if (tag == "pci_batch_spmm" && k == key && v >= 0 && v < N_VARIANTS) { best = v; best_ms = t; cached = 1; }
+    }
+    if (best < 0) {
+        // every block running, P = 1
+        PCI_CUDA(h, cudaMemsetAsync(b->d_st, 0, sizeof(BState) * b->blocks.size(), h->st));
+        std::vector<double> ones(std::min<int64_t>(b->rows * nv, (int64_t)1 << 20), 1.0);
+        for (int64_t o = 0; o < b->rows * nv; o += (int64_t)ones.size()) {
+            const int64_t n = std::min<int64_t>((int64_t)ones.size(), b->rows * nv - o);
+            PCI_CUDA(h, cudaMemcpyAsync(b->d_P + o, ones.data(), 8 * n, cudaMemcpyHostToDevice, h->st));
+            PCI_CUDA(h, cudaStreamSynchronize(h->st));
+        }
+        for (int v = 0; v < N_VARIANTS; v++) {
+            double t = 0.0;
+            if ((rc = time_spmm(b, nv, v, 3, &t))) return rc;
+            if (best < 0 || t < best_ms) { best = v; best_ms = t; }
+        }
+        if (cache_path) {
+            std::ofstream f(cache_path, std::ios::app);
+            if (f) f << "pci_batch_spmm " << key << " " << best << " " << best_ms << "\n";
+        }
+    }
+    b->tuned_variant = best;
+    b->tuned_nv = nv;
+    b->tuned_ms = best_ms;
+    if (variant) *variant = best;
+    if (ms) *ms = best_ms;
+    if (from_cache) *from_cache = cached;
+    return PCI_OK;
+}
+
+int pci_batch_davidson(pci_batch_t *b, const pci_batch_params *p, double *E, double *rnorm, int32_t *iters,
+                       int32_t *status, int32_t *graph_launches)
+{
+    if (!b || !p) return PCI_E_INPUT;
+    pci_gpu *h = &b->core;
+    const int nlv = p->nlv;
+    if (nlv < 1 || nlv > BT_LV) return set_err(h, PCI_E_INPUT, "nlv must be 1..8");
+    if (p->max_sub < 2 * nlv || p->max_sub > BT_MS) return set_err(h, PCI_E_INPUT, "max_sub must be 2*nlv..64");
+    if (p->keep < nlv || p->keep > p->max_sub - nlv) return set_err(h, PCI_E_INPUT, "keep must be nlv..max_sub-nlv");
+    if (p->max_it < 1 || p->it_per_graph < 1 || !(p->tol > 0.0)) return set_err(h, PCI_E_INPUT, "bad max_it/it_per_graph/tol");
+    if (p->spmm_variant >= N_VARIANTS) return set_err(h, PCI_E_INPUT, "unknown SpMM variant");
+    for (const BlockRec &r : b->blocks)
+        if (r.H.nrows < nlv) return set_err(h, PCI_E_INPUT, "a block has fewer rows than nlv");
+    auto t0 = std::chrono::steady_clock::now();
+    int rc = prepare(b, nlv);
+    if (rc) return rc;
+    const int nblk = (int)b->blocks.size();
+    const int variant = p->spmm_variant >= 0 ? p->spmm_variant
+                        : (b->tuned_variant >= 0 && b->tuned_nv == nlv ? b->tuned_variant : DEFAULT_VARIANT);
+    Bufs B = make_bufs(b, p);
+    b->last_nlv = nlv;
+
+    // SpMM time per call, outside the solve
+    PCI_CUDA(h, cudaMemsetAsync(b->d_st, 0, sizeof(BState) * nblk, h->st));
+    PCI_CUDA(h, cudaMemsetAsync(b->d_P, 0, 8 * b->rows * nlv, h->st));
+    double spmm_ms = 0.0;
+    if ((rc = time_spmm(b, nlv, variant, 2, &spmm_ms))) return rc;
+
+    cudaEvent_t e0, e1;
+    PCI_CUDA(h, cudaEventCreate(&e0));
+    PCI_CUDA(h, cudaEventCreate(&e1));
+    // initial basis: unit vectors at the nlv lowest diagonal elements of each block
+    std::vector<double> D(b->rows);
+    PCI_CUDA(h, cudaMemcpy(D.data(), b->d_D, 8 * b->rows, cudaMemcpyDeviceToHost));
+    std::vector<int64_t> pos;
+    std::vector<BState> st0(nblk);
+    for (int i = 0; i < nblk; i++) {
+        const BlockRec &r = b->blocks[i];
+        std::vector<int64_t> idx(r.H.nrows);
+        for (int64_t n = 0; n < r.H.nrows; n++) idx[n] = n;
+        std::partial_sort(idx.begin(), idx.begin() + nlv, idx.end(), [&](int64_t a, int64_t c) {
+            const double da = D[r.r0 + a], dc = D[r.r0 + c];
+            return da < dc || (da == dc && a < c);
+        });
+        for (int s = 0; s < nlv; s++) pos.push_back((int64_t)s * b->rows + r.r0 + idx[s]);
+        BState s{};
+        s.m = nlv;
+        s.knew = nlv;
+        st0[i] = s;
+    }
+    int64_t *d_pos = (int64_t *)dev_alloc(h, 8 * pos.size(), &rc);
+    if (rc) return rc;
+    PCI_CUDA(h, cudaEventRecord(e0, h->st));
+    PCI_CUDA(h, cudaMemcpyAsync(d_pos, pos.data(), 8 * pos.size(), cudaMemcpyHostToDevice, h->st));
+    PCI_CUDA(h, cudaMemcpyAsync(b->d_st, st0.data(), sizeof(BState) * nblk, cudaMemcpyHostToDevice, h->st));
+    PCI_CUDA(h, cudaMemsetAsync(b->d_V, 0, 8 * b->rows * BT_MS, h->st));
+    PCI_CUDA(h, cudaMemsetAsync(b->d_G, 0, 8 * (int64_t)nblk * BT_MS * BT_MS, h->st));
+    kb_set_units<<<((int)pos.size() + 255) / 256, 256, 0, h->st>>>(b->d_V, b->rows, d_pos, (int)pos.size());
+    PCI_CUDA(h, cudaGetLastError());
+    PCI_CUDA(h, cudaStreamSynchronize(h->st));
+    dev_free(d_pos);
+    auto t1 = std::chrono::steady_clock::now();
+
+    // capture it_per_graph iterations once, replay until every block is done
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    PCI_CUDA(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < p->it_per_graph && !rc; i++) rc = enqueue_iteration(b, B, variant, nlv);
+    cudaError_t ce = cudaStreamEndCapture(h->st, &graph);
+    if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+    if (ce != cudaSuccess) return cuda_err(h, ce, "cudaStreamEndCapture");
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    if (ce != cudaSuccess) { cudaGraphDestroy(graph); return cuda_err(h, ce, "cudaGraphInstantiate"); }
+    int replays = 0, ndone = 0;
+    const int max_replays = (p->max_it + p->it_per_graph - 1) / p->it_per_graph + 1;
+    while (replays < max_replays) {
+        ce = cudaGraphLaunch(exec, h->st);
+        if (ce != cudaSuccess) break;
+        replays++;
+        ce = cudaMemcpyAsync(&ndone, b->d_ndone, 4, cudaMemcpyDeviceToHost, h->st);
+        if (ce != cudaSuccess) break;
+        ce = cudaStreamSynchronize(h->st);
+        if (ce != cudaSuccess || ndone == nblk) break;
+    }
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return cuda_err(h, ce, "graph replay");
+    kb_ritz<<<b->nch, 256, 0, h->st>>>(b->d_chunks, b->d_st, B);
+    PCI_CUDA(h, cudaGetLastError());
+    PCI_CUDA(h, cudaEventRecord(e1, h->st));
+    std::vector<BState> sf(nblk);
+    PCI_CUDA(h, cudaMemcpyAsync(sf.data(), b->d_st, sizeof(BState) * nblk, cudaMemcpyDeviceToHost, h->st));
+    PCI_CUDA(h, cudaStreamSynchronize(h->st));
+    float total = 0.f;
+    cudaEventElapsedTime(&total, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int maxit = 0;
+    for (int i = 0; i < nblk; i++) {
+        for (int j = 0; j < nlv; j++) {
+            if (E) E[(int64_t)i * nlv + j] = sf[i].theta[j];
+            if (rnorm) rnorm[(int64_t)i * nlv + j] = sf[i].rnorm[j];
+        }
+        if (iters) iters[i] = sf[i].iters;
+        if (status) status[i] = sf[i].done;
+        maxit = std::max(maxit, sf[i].iters);
+    }
+    if (graph_launches) *graph_launches = replays;
+    b->st_total = total;
+    b->st_iters = maxit;
+    b->st_spmm = spmm_ms;
+    b->st_variant = variant;
+    b->st_setup = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    b->st_launches = ITER_LAUNCHES;
+    return ndone == nblk ? PCI_OK : set_err(h, PCI_E_NOT_CONVERGED, "graph replays ended before every block stopped");
+}
+
+int pci_batch_vectors(pci_batch_t *b, int32_t blk, double *X)
+{
+    if (!b || !X) return PCI_E_INPUT;
+    pci_gpu *h = &b->core;
+    if (blk < 0 || blk >= (int)b->blocks.size()) return set_err(h, PCI_E_INPUT, "block index out of range");
+    if (!b->d_R || !b->last_nlv) return set_err(h, PCI_E_STATE, "no solve yet");
+    const BlockRec &r = b->blocks[blk];
+    for (int j = 0; j < b->last_nlv; j++)
+        PCI_CUDA(h, cudaMemcpy(X + (int64_t)j * r.H.nrows, b->d_R + (int64_t)j * b->rows + r.r0, 8 * r.H.nrows,
+                               cudaMemcpyDeviceToHost));
+    return PCI_OK;
+}
+
+int pci_batch_stats(pci_batch_t *b, double *out, int32_t n)
+{
+    if (!b || !out || n < 0) return PCI_E_INPUT;
+    const double v[6] = {b->st_total, b->st_iters, b->st_spmm, b->st_variant, b->st_setup, b->st_launches};
+    for (int i = 0; i < n && i < 6; i++) out[i] = v[i];
+    return PCI_OK;
+}
+
+const char *pci_batch_last_error(pci_batch_t *b)
+{
+    return b ? b->core.err.c_str() : "null batch";
+}
+
+void pci_batch_destroy(pci_batch_t *b)
+{
+    if (!b) return;
+    cudaSetDevice(b->core.device);
+    if (b->core.st) cudaStreamSynchronize(b->core.st);
+    for (BlockRec &r : b->blocks) csr_free(r.H);
+    free_solve(b);
+    free_tables(b);
+    dev_free(b->core.d_tmp);
+    if (b->core.st) cudaStreamDestroy(b->core.st);
+    delete b;
+}
+
+}  // extern "C"

@@ -321,15 +321,19 @@ def make_integrals(basis: Basis, nsu: int, seed: int, nx: int = NX_DEFAULT,
 def make_system(name: str, shells, ne: int, mj: int, parity: int, refs,
                 seed: int, level: int = 2, r2_dtype=np.float64, kbrt: int = 0,
                 orbitals=None, params=None, gj: float = 0.0, xj_av: float = 0.0,
-                drop_empty: bool = True) -> CISystem:
+                drop_empty: bool = True, max_nd=None) -> CISystem:
     """Build a seeded synthetic system.
 
     ``refs`` holds reference configurations as lists of orbital indices, one per
     electron (1-based).  Configurations are all excitations up to ``level`` of
-    the references with the given parity; determinants have 2M = mj.
+    the references with the given parity; determinants have 2M = mj.  With
+    ``max_nd`` the configuration list is cut after the first configuration at
+    which the determinant count reaches ``max_nd``.
     """
     basis = make_basis(shells)
     configs = sd_excitations(basis, refs, parity, mj, level, orbitals)
+    if max_nd is not None:
+        configs = _truncate_configs(basis, configs, ne, mj, int(max_nd))
     iarr, ndc = enumerate_determinants(basis, configs, ne, mj)
     if drop_empty:
         keep = ndc > 0
@@ -350,6 +354,20 @@ def make_system(name: str, shells, ne: int, mj: int, parity: int, refs,
                     rint2=rint2, iint2=iint2, iint3=iint3, kbrt=kbrt, nlx=nlx,
                     gaunt_in=gin, gaunt_gnt=ggnt, gaunt_per_wave=gper, gaunt_lut=glut,
                     gj=gj, xj_av=xj_av, params=p)
+
+
+def _truncate_configs(basis, configs, ne, mj, max_nd, chunk=256):
+    """Leading configurations of ``configs`` whose determinant count first reaches max_nd."""
+    total = 0
+    for c0 in range(0, len(configs), chunk):
+        part = configs[c0:c0 + chunk]
+        _, ndc = enumerate_determinants(basis, part, ne, mj)
+        csum = total + np.cumsum(ndc)
+        hit = np.nonzero(csum >= max_nd)[0]
+        if hit.size:
+            return configs[:c0 + int(hit[0]) + 1]
+        total = int(csum[-1]) if csum.size else total
+    return configs
 
 
 def _shells(lmax_n):
@@ -470,3 +488,67 @@ def mid(seed=2):
     refs = _random_refs(shells, 3, 1, 6, 12, seed)
     return dict(name="mid", shells=shells, ne=3, mj=1, parity=1, refs=refs, seed=seed,
                 params=dict(Nlv=10, MaxNd0=3000))
+
+
+def _shells_count(norb, lmax):
+    """Shells (n, l), n from l+1, ordered by n then l, cut where the number of
+    relativistic orbitals (one for s, two otherwise) first reaches norb."""
+    out, cnt = [], 0
+    for n in range(1, 60):
+        for l in range(0, min(lmax, n - 1) + 1):
+            out.append((n, l))
+            cnt += 1 if l == 0 else 2
+            if cnt >= norb:
+                return out
+    return out
+
+
+def batch_block(index, seed0=1000, nd_lo=2000, nd_hi=400000):
+    """Block ``index`` of the batched workload: a synthetic ion with its own
+    seed (seed0 + index) drawing a determinant count log-uniform in
+    [nd_lo, nd_hi], 2-4 valence electrons (3-4 above 6000 determinants, 4
+    above 60000, where fewer electrons cannot reach the count), 30-120
+    orbitals (at least 60 for two electrons and 80 for four electrons above
+    150000), l <= 2..4, parity and 2M (0/2 for even, 1/3 for odd electron
+    counts); the configurations are the singles and doubles of two low-lying
+    references, cut at that count."""
+    seed = seed0 + index
+    rng = np.random.default_rng(seed)
+    nd_target = int(round(float(np.exp(rng.uniform(np.log(nd_lo), np.log(nd_hi))))))
+    if nd_target <= 6000:
+        ne = int(rng.integers(2, 5))
+    elif nd_target <= 60000:
+        ne = int(rng.integers(3, 5))
+    else:
+        ne = 4
+    parity = int(rng.integers(0, 2))
+    mj = int(rng.choice([0, 2])) if ne % 2 == 0 else int(rng.choice([1, 3]))
+    nmin = 60 if ne == 2 else (80 if nd_target > 150000 else 30)
+    norb = int(rng.integers(nmin, 121))
+    lmax = int(rng.integers(2, 5))
+    shells = _shells_count(norb, lmax)
+    refs = _random_refs(shells, ne, parity, 2, ne + 6, seed)
+    return dict(name=f"block{index}", shells=shells, ne=ne, mj=mj, parity=parity, refs=refs,
+                seed=seed, max_nd=nd_target, params=dict(Nlv=6))
+
+
+def batch_blocks(nblocks=64, seed0=1000, nd_lo=2000, nd_hi=400000):
+    """make_system keyword arguments of every block of the batched workload."""
+    return [batch_block(i, seed0, nd_lo, nd_hi) for i in range(nblocks)]
+
+
+def _make_block(kw):
+    return make_system(**kw)
+
+
+def make_batch(nblocks=64, seed0=1000, nd_lo=2000, nd_hi=400000, workers=None):
+    """Every block of the batched workload as a CISystem, generated in a pool
+    of spawned worker processes (safe to start after CUDA is initialised)."""
+    import multiprocessing as mp
+    import os
+    kws = batch_blocks(nblocks, seed0, nd_lo, nd_hi)
+    workers = workers or min(len(kws), os.cpu_count() or 1)
+    if workers <= 1:
+        return [make_system(**kw) for kw in kws]
+    with mp.get_context("spawn").Pool(workers) as pool:
+        return pool.map(_make_block, kws, chunksize=1)

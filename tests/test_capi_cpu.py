@@ -50,3 +50,43 @@ def test_no_device_is_reported_not_crashing():
     assert rc == 6
     assert b"CUDA" in L.pci_gpu_last_error(h)
     L.pci_gpu_destroy(h)
+
+
+def batch_declared_symbols():
+    hdr = open(os.path.join(ROOT, "include", "pci_batch.h")).read()
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    return sorted(set(re.findall(r"\b(pci_batch_\w+)\s*\(", hdr)))
+
+
+def test_batch_header_exported_and_bound():
+    from pci_b200 import build, capi
+    L = C.CDLL(build.build())
+    syms = batch_declared_symbols()
+    assert sorted(capi.BATCH_EXPORTS) == syms
+    for name in syms:
+        assert hasattr(L, name), name
+
+
+def test_batch_params_layout():
+    """pci_batch_params: 4 int32, a double, 2 int32 (32 bytes, no padding)."""
+    from pci_b200.capi import BatchParams
+    assert C.sizeof(BatchParams) == 32
+    hdr = open(os.path.join(ROOT, "include", "pci_batch.h")).read()
+    body = hdr[hdr.index("typedef struct {"):hdr.index("} pci_batch_params;")]
+    fields = re.findall(r"(int32_t|double)\s+(\w+);", body)
+    assert [f for _, f in fields] == [f for f, _ in BatchParams._fields_]
+
+
+def test_batch_variants_and_no_device():
+    """The SpMM variant table answers without a device; creating a batch
+    without a GPU fails with PCI_E_CUDA and a message."""
+    import torch
+    from pci_b200 import capi
+    assert capi.batch_variants() == [(s, c) for s in (32, 16, 8) for c in (4, 8, 16, 32)]
+    if torch.cuda.is_available():
+        return
+    L = capi.load()
+    b = C.c_void_p()
+    rc = L.pci_batch_create(0, C.byref(b))
+    assert rc == 6 and b"CUDA" in L.pci_batch_last_error(b)
+    L.pci_batch_destroy(b)
