@@ -146,7 +146,25 @@ __global__ void __launch_bounds__(256) kb_spmm(const BlkCsr *__restrict__ blks, 
             const int64_t ln = n - B.r0;
             const int64_t l0 = __ldg(&B.rowptr[ln]), l1 = __ldg(&B.rowptr[ln + 1]);
             const double xn = __ldg(&X[n * NV + v]);
-            for (int64_t l = l0 + g; l < l1; l += G) {
+            int64_t l = l0 + g;
+            // four elements per step: their loads are issued before any use
+            for (; l + 3 * G < l1; l += 4 * G) {
+                int k[4];
+                double t[4], xk[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    k[u] = __ldg(&B.col[l + u * G]);
+                    t[u] = (double)__ldg(&B.val[l + u * G]);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) xk[u] = __ldg(&X[(B.r0 + k[u]) * NV + v]);
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    if (k[u] != ln) atomicAdd(&Y[(B.r0 + k[u]) * NV + v], t[u] * xn);
+                    acc += t[u] * xk[u];
+                }
+            }
+            for (; l < l1; l += G) {
                 const int k = __ldg(&B.col[l]);
                 const double t = (double)__ldg(&B.val[l]);
                 const int64_t kg = B.r0 + k;
@@ -970,13 +988,17 @@ static int prepare(pci_batch *b, int nlv)
     return set_attrs(b);
 }
 
+// Revision of the SpMM kernels, part of the cache key: cached picks of an
+// older kernel are not reused.
+static const int SPMM_REV = 2;
+
 static std::string tune_key(pci_batch *b, int nv)
 {
     std::ostringstream k;
     std::string dn = b->devname;
     for (char &c : dn)
         if (c == ' ') c = '_';
-    k << dn << "|blocks=" << b->blocks.size() << "|rows=" << b->rows << "|nnz=" << b->nnz << "|nv=" << nv;
+    k << dn << "|rev=" << SPMM_REV << "|blocks=" << b->blocks.size() << "|rows=" << b->rows << "|nnz=" << b->nnz << "|nv=" << nv;
     return k.str();
 }
 

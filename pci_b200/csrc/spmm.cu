@@ -387,7 +387,29 @@ __global__ void __launch_bounds__(256) k_spmm_lower_red(const int64_t *__restric
         const XT xn = active ? __ldg(&X[n * (int64_t)ldx + v]) : (XT)0;
         XT acc = 0;
         if (active) {
-            for (int64_t l = r0 + g; l < r1; l += G) {
+            int64_t l = r0 + g;
+            // four elements per step: their loads are issued before any use
+            for (; l + 3 * G < r1; l += 4 * G) {
+                int k[4];
+                XT t[4], xk[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    k[u] = __ldg(&col[l + u * G]);
+                    t[u] = (XT)__ldg(&val[l + u * G]);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) xk[u] = __ldg(&X[(int64_t)k[u] * ldx + v]);
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    if (k[u] == n) {
+                        t[u] -= (XT)hmin;
+                    } else {
+                        atomicAdd(&Y[(int64_t)k[u] * ldy + v], t[u] * xn);
+                    }
+                    acc += t[u] * xk[u];
+                }
+            }
+            for (; l < r1; l += G) {
                 const int k = __ldg(&col[l]);
                 XT t = (XT)__ldg(&val[l]);
                 if (k == n) {
