@@ -51,6 +51,15 @@ int pci_batch_create(int32_t device, pci_batch_t **out);
  * rounded to FP32.  *index receives the block's index. */
 int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index);
 
+/* Storage of the blocks' matrices for the solve: 0 (default) = lower
+ * triangles only (the SpMM adds the transpose part by global reductions);
+ * 1 = blocks, largest first, get a symmetric copy of both triangles (the
+ * SpMM then gathers rows with no reductions, reading every element twice)
+ * while it fits in free device memory beside the solve buffers with a 4 GiB
+ * margin.  Takes effect at the next pci_batch_tune or pci_batch_davidson;
+ * cannot be switched back to 0 once copies exist. */
+int pci_batch_set_storage(pci_batch_t *b, int32_t mode);
+
 /* Blocks, total rows and total stored (lower-triangle) elements. */
 int pci_batch_info(pci_batch_t *b, int32_t *nblocks, int64_t *rows, int64_t *nnz);
 
@@ -79,7 +88,8 @@ int pci_batch_vectors(pci_batch_t *b, int32_t blk, double *X);
 
 /* Timings of the last solve: out[0] total ms, [1] iterations (largest over
  * blocks), [2] SpMM ms per call (measured outside the graph), [3] SpMM
- * variant used, [4] setup ms, [5] kernel launches per iteration; n <= 6. */
+ * variant used, [4] setup ms, [5] kernel launches per iteration, [6] share of
+ * the lower-triangle elements held as full copies; n <= 7. */
 int pci_batch_stats(pci_batch_t *b, double *out, int32_t n);
 
 const char *pci_batch_last_error(pci_batch_t *b);

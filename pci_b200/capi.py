@@ -25,7 +25,7 @@ EXPORTS = ["pci_gpu_create", "pci_gpu_set_basis", "pci_gpu_set_integrals", "pci_
            "pci_gpu_last_error", "pci_gpu_destroy", "pci_mlp_create", "pci_mlp_num_params", "pci_mlp_set_params",
            "pci_mlp_get_params", "pci_mlp_forward", "pci_mlp_loss_grad", "pci_mlp_train", "pci_mlp_last_error",
            "pci_mlp_destroy", "pci_gpu_set_correction_model", "pci_gpu_davidson_harvest"]
-BATCH_EXPORTS = ["pci_batch_create", "pci_batch_add_block", "pci_batch_info", "pci_batch_tune",
+BATCH_EXPORTS = ["pci_batch_create", "pci_batch_add_block", "pci_batch_set_storage", "pci_batch_info", "pci_batch_tune",
                  "pci_batch_variant", "pci_batch_davidson", "pci_batch_vectors", "pci_batch_stats",
                  "pci_batch_last_error", "pci_batch_destroy"]
 BATCH_STATUS = {1: "converged", 2: "iteration limit", 3: "no new direction"}
@@ -98,6 +98,7 @@ def load(path: str = LIB):
     L.pci_batch_create.argtypes = [i32, C.POINTER(P)]
     L.pci_batch_add_block.argtypes = [P, P, C.POINTER(i32)]
     L.pci_batch_info.argtypes = [P, C.POINTER(i32), C.POINTER(i64), C.POINTER(i64)]
+    L.pci_batch_set_storage.argtypes = [P, i32]
     L.pci_batch_tune.argtypes = [P, i32, C.c_char_p, C.POINTER(i32), C.POINTER(f64), C.POINTER(i32)]
     L.pci_batch_variant.argtypes = [i32, C.POINTER(i32), C.POINTER(i32)]
     L.pci_batch_davidson.argtypes = [P, C.POINTER(BatchParams), P, P, P, P, C.POINTER(i32)]
@@ -378,6 +379,10 @@ class Batch:
             e.set_csr(PCI_MAT_H, rowptr, col, val)
             return self.add_engine(e)
 
+    def set_storage(self, mode: int):
+        """0: lower triangles only (default), 1: full symmetric copies where memory allows."""
+        self._check(self.L.pci_batch_set_storage(self.b, mode))
+
     def info(self):
         n, r, z = C.c_int32(), C.c_int64(), C.c_int64()
         self._check(self.L.pci_batch_info(self.b, C.byref(n), C.byref(r), C.byref(z)))
@@ -408,9 +413,10 @@ class Batch:
         return X.T
 
     def stats(self):
-        out = np.zeros(6)
-        self._check(self.L.pci_batch_stats(self.b, _p(out), 6))
-        keys = ["total_ms", "iterations", "spmm_ms", "spmm_variant", "setup_ms", "launches_per_iteration"]
+        out = np.zeros(7)
+        self._check(self.L.pci_batch_stats(self.b, _p(out), 7))
+        keys = ["total_ms", "iterations", "spmm_ms", "spmm_variant", "setup_ms", "launches_per_iteration",
+                "full_share"]
         return dict(zip(keys, out.tolist()))
 
     def close(self):

@@ -32,6 +32,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <iomanip>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -55,6 +56,7 @@ struct BlkCsr {
     const int32_t *col;
     const float *val;
     int64_t r0, nd;
+    int64_t full;   // 1: both triangles stored (row-wise gather, no reductions)
 };
 
 struct Chunk {
@@ -120,8 +122,10 @@ __global__ void kb_set_units(double *V, int64_t ld, const int64_t *pos, int n)
 // Y = H X over the rows of every running block, X and Y row-major with NV
 // vectors.  A team of SUB lanes owns a row; within it NV lanes share one
 // stored element (lane v takes vector v) and SUB/NV elements go per step.
-// The transpose part of each element goes to Y as a global reduction, and
-// so does the row part (other rows add into it), so Y starts at zero.
+// Lower-triangle blocks: the transpose part of each element goes to Y as a
+// global reduction, and so does the row part (other rows add into it), so Y
+// starts at zero.  Blocks stored with both triangles: a plain row gather and
+// store, with no reductions.
 template <int NV, int SUB>
 __global__ void __launch_bounds__(256) kb_spmm(const BlkCsr *__restrict__ blks, const int32_t *__restrict__ row_blk,
                                                const BState *__restrict__ bst, int64_t rows,
@@ -141,12 +145,32 @@ __global__ void __launch_bounds__(256) kb_spmm(const BlkCsr *__restrict__ blks, 
         const int b = ok ? __ldg(&row_blk[n]) : 0;
         ok = ok && bst[b].done == 0;
         double acc = 0.0;
+        bool full = false;
         if (ok && act) {
             const BlkCsr B = blks[b];
             const int64_t ln = n - B.r0;
             const int64_t l0 = __ldg(&B.rowptr[ln]), l1 = __ldg(&B.rowptr[ln + 1]);
-            const double xn = __ldg(&X[n * NV + v]);
+            full = B.full != 0;
+            const double xn = full ? 0.0 : __ldg(&X[n * NV + v]);
             int64_t l = l0 + g;
+            if (full) {
+                for (; l + 3 * G < l1; l += 4 * G) {
+                    int k[4];
+                    double t[4], xk[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        k[u] = __ldg(&B.col[l + u * G]);
+                        t[u] = (double)__ldg(&B.val[l + u * G]);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; u++) xk[u] = __ldg(&X[(B.r0 + k[u]) * NV + v]);
+#pragma unroll
+                    for (int u = 0; u < 4; u++) acc += t[u] * xk[u];
+                }
+                for (; l < l1; l += G)
+                    acc += (double)__ldg(&B.val[l]) * __ldg(&X[(B.r0 + __ldg(&B.col[l])) * NV + v]);
+                l = l1;
+            }
             // four elements per step: their loads are issued before any use
             for (; l + 3 * G < l1; l += 4 * G) {
                 int k[4];
@@ -177,7 +201,10 @@ __global__ void __launch_bounds__(256) kb_spmm(const BlkCsr *__restrict__ blks, 
             const double o = __shfl_sync(FULL_MASK, acc, g == 0 ? lane + gg * NV : lane);
             if (g == 0) acc += o;
         }
-        if (ok && act && g == 0) atomicAdd(&Y[n * NV + v], acc);
+        if (ok && act && g == 0) {
+            if (full) Y[n * NV + v] = acc;
+            else atomicAdd(&Y[n * NV + v], acc);
+        }
     }
 }
 
@@ -759,8 +786,9 @@ __global__ void kb_count(const BState *bst, int nblk, int *ndone)
 // ------------------------------------------------------------- host ---
 
 struct BlockRec {
-    Csr H;
-    int64_t r0 = 0;
+    Csr H;            // lower triangle (freed once a full copy exists)
+    Csr F;            // both triangles, or empty
+    int64_t r0 = 0, nd = 0, nnz = 0;   // rows and stored lower-triangle elements
 };
 
 struct pci_batch {
@@ -784,6 +812,9 @@ struct pci_batch {
     BState *d_st = nullptr;
     int *d_ndone = nullptr;
     int last_nlv = 0;
+    int storage = 0;          // 1: full copies where memory allows, 0: lower triangles only
+    bool storage_done = false;
+    int64_t full_nnz = 0;     // lower-triangle elements of the blocks held as full copies
     int tuned_variant = -1, tuned_nv = 0;
     double tuned_ms = 0.0;
     double st_total = 0, st_iters = 0, st_spmm = 0, st_variant = 0, st_setup = 0, st_launches = 0;
@@ -830,11 +861,12 @@ static int build_tables(pci_batch *b)
     std::vector<int64_t> cb(nblk + 1, 0);
     for (int i = 0; i < nblk; i++) {
         const BlockRec &r = b->blocks[i];
-        tab[i] = BlkCsr{r.H.rowptr, r.H.col, (const float *)r.H.val, r.r0, r.H.nrows};
-        std::fill(rb.begin() + r.r0, rb.begin() + r.r0 + r.H.nrows, i);
+        const Csr &M = r.F.rowptr ? r.F : r.H;
+        tab[i] = BlkCsr{M.rowptr, M.col, (const float *)M.val, r.r0, r.nd, r.F.rowptr ? 1 : 0};
+        std::fill(rb.begin() + r.r0, rb.begin() + r.r0 + r.nd, i);
         cb[i] = (int64_t)ch.size();
-        for (int64_t s = 0; s < r.H.nrows; s += BT_CH)
-            ch.push_back(Chunk{i, 0, r.r0 + s, r.r0 + std::min<int64_t>(s + BT_CH, r.H.nrows)});
+        for (int64_t s = 0; s < r.nd; s += BT_CH)
+            ch.push_back(Chunk{i, 0, r.r0 + s, r.r0 + std::min<int64_t>(s + BT_CH, r.nd)});
     }
     cb[nblk] = (int64_t)ch.size();
     int rc = 0;
@@ -977,6 +1009,54 @@ static int time_spmm(pci_batch *b, int nv, int variant, int reps, double *ms)
     return PCI_OK;
 }
 
+// Full symmetric copy of one block (lower triangle freed afterwards).
+static int make_full(pci_batch *b, BlockRec &r)
+{
+    pci_gpu tmp;
+    tmp.device = b->core.device;
+    tmp.st = b->core.st;
+    tmp.H = r.H;
+    int rc = sp_build_full(&tmp);
+    dev_free(tmp.d_tmp);
+    tmp.d_tmp = nullptr;
+    if (rc) {
+        csr_free(tmp.Hfull);
+        b->core.err = tmp.err;
+        return rc;
+    }
+    r.F = tmp.Hfull;
+    csr_free(r.H);
+    return PCI_OK;
+}
+
+// With storage mode 1, blocks (largest first) get a full symmetric copy while
+// the copy fits in the free device memory beside the solve buffers with a
+// 4 GiB margin; the others stay lower triangles.
+static int choose_storage(pci_batch *b)
+{
+    if (b->storage_done) return PCI_OK;
+    b->storage_done = true;
+    if (b->storage != 1) return PCI_OK;
+    std::vector<int> order(b->blocks.size());
+    for (size_t i = 0; i < order.size(); i++) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return b->blocks[x].nnz > b->blocks[y].nnz; });
+    const size_t margin = (size_t)4 << 30;
+    for (int i : order) {
+        BlockRec &r = b->blocks[i];
+        if (r.F.rowptr) continue;
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        // the copy (both triangles, FP32 + int32) and its build scratch
+        const size_t need = (size_t)(2 * r.nnz) * 8 + (size_t)(r.nd + 1) * 24;
+        if (need + margin > fr) continue;
+        int rc = make_full(b, r);
+        if (rc) return rc;
+        b->full_nnz += r.nnz;
+        b->dirty = true;
+    }
+    return PCI_OK;
+}
+
 static int prepare(pci_batch *b, int nlv)
 {
     pci_gpu *h = &b->core;
@@ -985,12 +1065,14 @@ static int prepare(pci_batch *b, int nlv)
     int rc = build_tables(b);
     if (rc) return rc;
     if ((rc = ensure_solve(b, nlv))) return rc;
+    if ((rc = choose_storage(b))) return rc;
+    if ((rc = build_tables(b))) return rc;
     return set_attrs(b);
 }
 
 // Revision of the SpMM kernels, part of the cache key: cached picks of an
 // older kernel are not reused.
-static const int SPMM_REV = 2;
+static const int SPMM_REV = 3;
 
 static std::string tune_key(pci_batch *b, int nv)
 {
@@ -998,7 +1080,8 @@ static std::string tune_key(pci_batch *b, int nv)
     std::string dn = b->devname;
     for (char &c : dn)
         if (c == ' ') c = '_';
-    k << dn << "|rev=" << SPMM_REV << "|blocks=" << b->blocks.size() << "|rows=" << b->rows << "|nnz=" << b->nnz << "|nv=" << nv;
+    k << dn << "|rev=" << SPMM_REV << "|storage=" << b->storage << "|full=" << b->full_nnz
+      << "|blocks=" << b->blocks.size() << "|rows=" << b->rows << "|nnz=" << b->nnz << "|nv=" << nv;
     return k.str();
 }
 
@@ -1034,6 +1117,30 @@ int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index)
     BlockRec r;
     r.H = h->H;
     r.r0 = b->rows;
+    r.nd = r.H.nrows;
+    r.nnz = r.H.nnz;
+    if (r.H.cap > r.H.nnz) {
+        // a padded build leaves its candidate slots allocated: keep nnz of them
+        int rc = 0;
+        const int64_t n = std::max<int64_t>(r.H.nnz, 1);
+        int32_t *col = (int32_t *)dev_alloc(c, n * 4, &rc);
+        if (rc) return rc;
+        PCI_CUDA(c, cudaMemcpyAsync(col, r.H.col, r.H.nnz * 4, cudaMemcpyDeviceToDevice, c->st));
+        PCI_CUDA(c, cudaStreamSynchronize(c->st));
+        dev_free(r.H.col);
+        r.H.col = col;
+        h->H.col = col;
+        if (r.H.val_f32) {
+            float *val = (float *)dev_alloc(c, n * 4, &rc);
+            if (rc) return rc;
+            PCI_CUDA(c, cudaMemcpyAsync(val, r.H.val, r.H.nnz * 4, cudaMemcpyDeviceToDevice, c->st));
+            PCI_CUDA(c, cudaStreamSynchronize(c->st));
+            dev_free(r.H.val);
+            r.H.val = val;
+            h->H.val = val;
+        }
+        r.H.cap = 0;
+    }
     if (!r.H.val_f32) {
         int rc = 0;
         float *v = (float *)dev_alloc(c, std::max<int64_t>(r.H.nnz, 1) * 4, &rc);
@@ -1044,6 +1151,8 @@ int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index)
         dev_free(r.H.val);
         r.H.val = v;
         r.H.val_f32 = 1;
+        h->H.val = v;
+        h->H.val_f32 = 1;
     }
     h->H = Csr();
     csr_free(h->Hfull);
@@ -1052,9 +1161,22 @@ int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index)
     b->rows += r.H.nrows;
     b->nnz += r.H.nnz;
     b->dirty = true;
+    b->storage_done = false;
     b->tuned_variant = -1;
     free_solve(b);
     if (index) *index = (int32_t)(b->blocks.size() - 1);
+    return PCI_OK;
+}
+
+int pci_batch_set_storage(pci_batch_t *b, int32_t mode)
+{
+    if (!b) return PCI_E_INPUT;
+    if (mode != 0 && mode != 1) return set_err(&b->core, PCI_E_INPUT, "storage mode must be 0 or 1");
+    if (b->storage_done && mode != b->storage && b->full_nnz)
+        return set_err(&b->core, PCI_E_STATE, "full copies already made; set the storage before the first solve");
+    b->storage = mode;
+    b->storage_done = false;
+    b->tuned_variant = -1;
     return PCI_OK;
 }
 
@@ -1111,7 +1233,7 @@ int pci_batch_tune(pci_batch_t *b, int32_t nv, const char *cache_path, int32_t *
         }
         if (cache_path) {
             std::ofstream f(cache_path, std::ios::app);
-            if (f) f << "pci_batch_spmm " << key << " " << best << " " << best_ms << "\n";
+            if (f) f << std::setprecision(9) << "pci_batch_spmm " << key << " " << best << " " << best_ms << "\n";
         }
     }
     b->tuned_variant = best;
@@ -1135,7 +1257,7 @@ int pci_batch_davidson(pci_batch_t *b, const pci_batch_params *p, double *E, dou
     if (p->max_it < 1 || p->it_per_graph < 1 || !(p->tol > 0.0)) return set_err(h, PCI_E_INPUT, "bad max_it/it_per_graph/tol");
     if (p->spmm_variant >= N_VARIANTS) return set_err(h, PCI_E_INPUT, "unknown SpMM variant");
     for (const BlockRec &r : b->blocks)
-        if (r.H.nrows < nlv) return set_err(h, PCI_E_INPUT, "a block has fewer rows than nlv");
+        if (r.nd < nlv) return set_err(h, PCI_E_INPUT, "a block has fewer rows than nlv");
     auto t0 = std::chrono::steady_clock::now();
     int rc = prepare(b, nlv);
     if (rc) return rc;
@@ -1161,8 +1283,8 @@ int pci_batch_davidson(pci_batch_t *b, const pci_batch_params *p, double *E, dou
     std::vector<BState> st0(nblk);
     for (int i = 0; i < nblk; i++) {
         const BlockRec &r = b->blocks[i];
-        std::vector<int64_t> idx(r.H.nrows);
-        for (int64_t n = 0; n < r.H.nrows; n++) idx[n] = n;
+        std::vector<int64_t> idx(r.nd);
+        for (int64_t n = 0; n < r.nd; n++) idx[n] = n;
         std::partial_sort(idx.begin(), idx.begin() + nlv, idx.end(), [&](int64_t a, int64_t c) {
             const double da = D[r.r0 + a], dc = D[r.r0 + c];
             return da < dc || (da == dc && a < c);
@@ -1248,7 +1370,7 @@ int pci_batch_vectors(pci_batch_t *b, int32_t blk, double *X)
     if (!b->d_R || !b->last_nlv) return set_err(h, PCI_E_STATE, "no solve yet");
     const BlockRec &r = b->blocks[blk];
     for (int j = 0; j < b->last_nlv; j++)
-        PCI_CUDA(h, cudaMemcpy(X + (int64_t)j * r.H.nrows, b->d_R + (int64_t)j * b->rows + r.r0, 8 * r.H.nrows,
+        PCI_CUDA(h, cudaMemcpy(X + (int64_t)j * r.nd, b->d_R + (int64_t)j * b->rows + r.r0, 8 * r.nd,
                                cudaMemcpyDeviceToHost));
     return PCI_OK;
 }
@@ -1256,8 +1378,9 @@ int pci_batch_vectors(pci_batch_t *b, int32_t blk, double *X)
 int pci_batch_stats(pci_batch_t *b, double *out, int32_t n)
 {
     if (!b || !out || n < 0) return PCI_E_INPUT;
-    const double v[6] = {b->st_total, b->st_iters, b->st_spmm, b->st_variant, b->st_setup, b->st_launches};
-    for (int i = 0; i < n && i < 6; i++) out[i] = v[i];
+    const double v[7] = {b->st_total, b->st_iters, b->st_spmm, b->st_variant, b->st_setup, b->st_launches,
+                         b->nnz ? (double)b->full_nnz / (double)b->nnz : 0.0};
+    for (int i = 0; i < n && i < 7; i++) out[i] = v[i];
     return PCI_OK;
 }
 
@@ -1271,7 +1394,10 @@ void pci_batch_destroy(pci_batch_t *b)
     if (!b) return;
     cudaSetDevice(b->core.device);
     if (b->core.st) cudaStreamSynchronize(b->core.st);
-    for (BlockRec &r : b->blocks) csr_free(r.H);
+    for (BlockRec &r : b->blocks) {
+        csr_free(r.H);
+        csr_free(r.F);
+    }
     free_solve(b);
     free_tables(b);
     dev_free(b->core.d_tmp);

@@ -1209,6 +1209,7 @@ static int rows_impl(pci_gpu *h, int value_prec, Csr &out, RowStats *hs)
             if (rc) return cleanup(rc);
             out.val = dev_alloc(h, std::max<int64_t>(ncand, 1) * vb, &rc);
             if (rc) return cleanup(rc);
+            out.cap = ncand;
             cudaEventRecord(e1, h->st);
             if ((rc = launch_fill(pptr, cnt, d_stats))) return cleanup(rc);
             cudaEventRecord(e2, h->st);

@@ -23,6 +23,7 @@ struct Csr {
     int32_t *col = nullptr;      // 0-based column
     void *val = nullptr;         // double or float
     int val_f32 = 0;
+    int64_t cap = 0;             // col/val slots allocated when more than nnz (padded build), else 0
 };
 
 // Everything the H-build kernels read; plain pointers so it can be passed by value.
