@@ -7,7 +7,7 @@
  * the Davidson module davidson.f90) takes Nlv, N_it and the residual criterion
  * Crt4 and returns the energies Tk(1:Nlv) and vectors ArrB.  This interface
  * keeps those meanings per block (nlv, max_it, tol; energies and vectors in
- * the same order), with H stored in FP32.
+ * the same order), with H stored in FP32 (or FP64) and FP64 vectors.
  *
  * Every iteration step of the solve is one kernel launch over all blocks,
  * the SpMM one persistent kernel over the rows of every block, and the
@@ -31,7 +31,7 @@ extern "C" {
 
 typedef struct pci_batch pci_batch_t;
 
-#define PCI_BATCH_MAX_LV   8    /* roots per block */
+#define PCI_BATCH_MAX_LV   12   /* roots per block */
 #define PCI_BATCH_MAX_SUB  64   /* subspace vectors per block */
 
 typedef struct {
@@ -48,8 +48,15 @@ int pci_batch_create(int32_t device, pci_batch_t **out);
 
 /* Append the Hamiltonian resident in `h` as the next block and take it over
  * (h keeps its basis and integrals but no longer holds H).  FP64 values are
- * rounded to FP32.  *index receives the block's index. */
+ * rounded to FP32 unless pci_batch_set_value_prec(b, 64) was called.
+ * *index receives the block's index. */
 int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index);
+
+/* Value precision of blocks added from now on: 32 (default) rounds FP64
+ * values to FP32 when a block is added; 64 keeps each block's values as its
+ * handle built them (FP64 from pci_gpu_form_h with value_prec 64).  The
+ * vectors and all sums are FP64 either way. */
+int pci_batch_set_value_prec(pci_batch_t *b, int32_t value_prec);
 
 /* Storage of the blocks' matrices for the solve: 0 (default) = lower
  * triangles only (the SpMM adds the transpose part by global reductions);
@@ -71,8 +78,9 @@ int pci_batch_info(pci_batch_t *b, int32_t *nblocks, int64_t *rows, int64_t *nnz
 int pci_batch_tune(pci_batch_t *b, int32_t nv, const char *cache_path, int32_t *variant, double *ms,
                    int32_t *from_cache);
 
-/* Number of SpMM variants and the parameters of one: lanes per row and
- * thread blocks per SM. */
+/* Parameters of SpMM variant `variant` (lanes per row, thread blocks per SM);
+ * returns the number of variants when `variant` is out of range.  A variant
+ * whose lanes per row are fewer than the vectors is not used. */
 int pci_batch_variant(int32_t variant, int32_t *lanes_per_row, int32_t *blocks_per_sm);
 
 /* Solve every block.  E[blk*nlv + j] = energy of root j, rnorm likewise its

@@ -25,7 +25,8 @@ EXPORTS = ["pci_gpu_create", "pci_gpu_set_basis", "pci_gpu_set_integrals", "pci_
            "pci_gpu_last_error", "pci_gpu_destroy", "pci_mlp_create", "pci_mlp_num_params", "pci_mlp_set_params",
            "pci_mlp_get_params", "pci_mlp_forward", "pci_mlp_loss_grad", "pci_mlp_train", "pci_mlp_last_error",
            "pci_mlp_destroy", "pci_gpu_set_correction_model", "pci_gpu_davidson_harvest"]
-BATCH_EXPORTS = ["pci_batch_create", "pci_batch_add_block", "pci_batch_set_storage", "pci_batch_info", "pci_batch_tune",
+BATCH_EXPORTS = ["pci_batch_create", "pci_batch_add_block", "pci_batch_set_storage", "pci_batch_set_value_prec",
+                 "pci_batch_info", "pci_batch_tune",
                  "pci_batch_variant", "pci_batch_davidson", "pci_batch_vectors", "pci_batch_stats",
                  "pci_batch_last_error", "pci_batch_destroy"]
 BATCH_STATUS = {1: "converged", 2: "iteration limit", 3: "no new direction"}
@@ -99,6 +100,7 @@ def load(path: str = LIB):
     L.pci_batch_add_block.argtypes = [P, P, C.POINTER(i32)]
     L.pci_batch_info.argtypes = [P, C.POINTER(i32), C.POINTER(i64), C.POINTER(i64)]
     L.pci_batch_set_storage.argtypes = [P, i32]
+    L.pci_batch_set_value_prec.argtypes = [P, i32]
     L.pci_batch_tune.argtypes = [P, i32, C.c_char_p, C.POINTER(i32), C.POINTER(f64), C.POINTER(i32)]
     L.pci_batch_variant.argtypes = [i32, C.POINTER(i32), C.POINTER(i32)]
     L.pci_batch_davidson.argtypes = [P, C.POINTER(BatchParams), P, P, P, P, C.POINTER(i32)]
@@ -378,6 +380,10 @@ class Batch:
         with Engine(self.device) as e:
             e.set_csr(PCI_MAT_H, rowptr, col, val)
             return self.add_engine(e)
+
+    def set_value_prec(self, value_prec: int):
+        """32: blocks rounded to FP32 when added (default); 64: kept as built."""
+        self._check(self.L.pci_batch_set_value_prec(self.b, value_prec))
 
     def set_storage(self, mode: int):
         """0: lower triangles only (default), 1: full symmetric copies where memory allows."""

@@ -54,9 +54,10 @@ constexpr int BT_ROT_THREADS = 128;
 struct BlkCsr {
     const int64_t *rowptr;
     const int32_t *col;
-    const float *val;
+    const void *val;   // float, or double when f64
     int64_t r0, nd;
-    int64_t full;   // 1: both triangles stored (row-wise gather, no reductions)
+    int32_t full;      // 1: both triangles stored (row-wise gather, no reductions)
+    int32_t f64;
 };
 
 struct Chunk {
@@ -106,7 +107,10 @@ __global__ void kb_diag(const BlkCsr *blks, const int32_t *row_blk, int64_t rows
         const int64_t ln = n - B.r0;
         double d = 0.0;
         for (int64_t l = B.rowptr[ln + 1] - 1; l >= B.rowptr[ln]; l--)
-            if (B.col[l] == ln) { d = (double)B.val[l]; break; }
+            if (B.col[l] == ln) {
+                d = B.f64 ? ((const double *)B.val)[l] : (double)((const float *)B.val)[l];
+                break;
+            }
         D[n] = d;
     }
 }
@@ -126,6 +130,69 @@ __global__ void kb_set_units(double *V, int64_t ld, const int64_t *pos, int n)
 // global reduction, and so does the row part (other rows add into it), so Y
 // starts at zero.  Blocks stored with both triangles: a plain row gather and
 // store, with no reductions.
+// Row n (local row ln) of block B for vector v: the row part of the product
+// (returned; both triangles for a full copy) and, for a lower triangle, the
+// transpose part added to Y by global reductions.
+template <int NV, int G, typename VT>
+__device__ __forceinline__ double spmm_row(const BlkCsr &B, int64_t ln, int64_t n, int g, int v,
+                                           const double *__restrict__ X, double *Y)
+{
+    const VT *__restrict__ val = (const VT *)B.val;
+    const int64_t l0 = __ldg(&B.rowptr[ln]), l1 = __ldg(&B.rowptr[ln + 1]);
+    double acc = 0.0;
+    int64_t l = l0 + g;
+    if (B.full) {
+        for (; l + 3 * G < l1; l += 4 * G) {
+            int k[4];
+            double t[4], xk[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                k[u] = __ldg(&B.col[l + u * G]);
+                t[u] = (double)__ldg(&val[l + u * G]);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) xk[u] = __ldg(&X[(B.r0 + k[u]) * NV + v]);
+#pragma unroll
+            for (int u = 0; u < 4; u++) acc += t[u] * xk[u];
+        }
+        for (; l < l1; l += G) acc += (double)__ldg(&val[l]) * __ldg(&X[(B.r0 + __ldg(&B.col[l])) * NV + v]);
+        return acc;
+    }
+    const double xn = __ldg(&X[n * NV + v]);
+    // four elements per step: their loads are issued before any use
+    for (; l + 3 * G < l1; l += 4 * G) {
+        int k[4];
+        double t[4], xk[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            k[u] = __ldg(&B.col[l + u * G]);
+            t[u] = (double)__ldg(&val[l + u * G]);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) xk[u] = __ldg(&X[(B.r0 + k[u]) * NV + v]);
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            if (k[u] != ln) atomicAdd(&Y[(B.r0 + k[u]) * NV + v], t[u] * xn);
+            acc += t[u] * xk[u];
+        }
+    }
+    for (; l < l1; l += G) {
+        const int k = __ldg(&B.col[l]);
+        const double t = (double)__ldg(&val[l]);
+        const int64_t kg = B.r0 + k;
+        if (k != ln) atomicAdd(&Y[kg * NV + v], t * xn);
+        acc += t * __ldg(&X[kg * NV + v]);
+    }
+    return acc;
+}
+
+// Y = H X over the rows of every running block, X and Y row-major with NV
+// vectors.  A team of SUB lanes owns a row; within it NV lanes share one
+// stored element (lane v takes vector v) and SUB/NV elements go per step.
+// Lower-triangle blocks: the transpose part of each element goes to Y as a
+// global reduction, and so does the row part (other rows add into it), so Y
+// starts at zero.  Blocks stored with both triangles: a plain row gather and
+// store, with no reductions.
 template <int NV, int SUB>
 __global__ void __launch_bounds__(256) kb_spmm(const BlkCsr *__restrict__ blks, const int32_t *__restrict__ row_blk,
                                                const BState *__restrict__ bst, int64_t rows,
@@ -133,6 +200,7 @@ __global__ void __launch_bounds__(256) kb_spmm(const BlkCsr *__restrict__ blks, 
 {
     constexpr int G = SUB / NV;
     constexpr int TPW = 32 / SUB;
+    static_assert(G >= 1, "fewer lanes per row than vectors");
     const int lane = threadIdx.x & 31;
     const int sl = lane % SUB;
     const int g = sl / NV, v = sl - g * NV;
@@ -148,53 +216,9 @@ __global__ void __launch_bounds__(256) kb_spmm(const BlkCsr *__restrict__ blks, 
         bool full = false;
         if (ok && act) {
             const BlkCsr B = blks[b];
-            const int64_t ln = n - B.r0;
-            const int64_t l0 = __ldg(&B.rowptr[ln]), l1 = __ldg(&B.rowptr[ln + 1]);
             full = B.full != 0;
-            const double xn = full ? 0.0 : __ldg(&X[n * NV + v]);
-            int64_t l = l0 + g;
-            if (full) {
-                for (; l + 3 * G < l1; l += 4 * G) {
-                    int k[4];
-                    double t[4], xk[4];
-#pragma unroll
-                    for (int u = 0; u < 4; u++) {
-                        k[u] = __ldg(&B.col[l + u * G]);
-                        t[u] = (double)__ldg(&B.val[l + u * G]);
-                    }
-#pragma unroll
-                    for (int u = 0; u < 4; u++) xk[u] = __ldg(&X[(B.r0 + k[u]) * NV + v]);
-#pragma unroll
-                    for (int u = 0; u < 4; u++) acc += t[u] * xk[u];
-                }
-                for (; l < l1; l += G)
-                    acc += (double)__ldg(&B.val[l]) * __ldg(&X[(B.r0 + __ldg(&B.col[l])) * NV + v]);
-                l = l1;
-            }
-            // four elements per step: their loads are issued before any use
-            for (; l + 3 * G < l1; l += 4 * G) {
-                int k[4];
-                double t[4], xk[4];
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    k[u] = __ldg(&B.col[l + u * G]);
-                    t[u] = (double)__ldg(&B.val[l + u * G]);
-                }
-#pragma unroll
-                for (int u = 0; u < 4; u++) xk[u] = __ldg(&X[(B.r0 + k[u]) * NV + v]);
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    if (k[u] != ln) atomicAdd(&Y[(B.r0 + k[u]) * NV + v], t[u] * xn);
-                    acc += t[u] * xk[u];
-                }
-            }
-            for (; l < l1; l += G) {
-                const int k = __ldg(&B.col[l]);
-                const double t = (double)__ldg(&B.val[l]);
-                const int64_t kg = B.r0 + k;
-                if (k != ln) atomicAdd(&Y[kg * NV + v], t * xn);
-                acc += t * __ldg(&X[kg * NV + v]);
-            }
+            acc = B.f64 ? spmm_row<NV, G, double>(B, n - B.r0, n, g, v, X, Y)
+                        : spmm_row<NV, G, float>(B, n - B.r0, n, g, v, X, Y);
         }
 #pragma unroll
         for (int gg = 1; gg < G; gg++) {
@@ -219,8 +243,15 @@ void launch_spmm_nv(int sub, int grid, cudaStream_t st, const BlkCsr *blks, cons
                     int64_t rows, const double *X, double *Y)
 {
     if (sub == 32) kb_spmm<NV, 32><<<grid, 256, 0, st>>>(blks, row_blk, bst, rows, X, Y);
-    else if (sub == 16) kb_spmm<NV, 16><<<grid, 256, 0, st>>>(blks, row_blk, bst, rows, X, Y);
-    else kb_spmm<NV, 8><<<grid, 256, 0, st>>>(blks, row_blk, bst, rows, X, Y);
+    else if constexpr (NV <= 16) {
+        if (sub == 16) kb_spmm<NV, 16><<<grid, 256, 0, st>>>(blks, row_blk, bst, rows, X, Y);
+        else if constexpr (NV <= 8) kb_spmm<NV, 8><<<grid, 256, 0, st>>>(blks, row_blk, bst, rows, X, Y);
+    }
+}
+
+bool variant_ok(int nv, int variant)
+{
+    return variant >= 0 && variant < N_VARIANTS && SUBS[variant / N_CTAS] >= nv;
 }
 
 void launch_spmm(int nv, int variant, int nsm, cudaStream_t st, const BlkCsr *blks, const int32_t *row_blk,
@@ -236,7 +267,11 @@ void launch_spmm(int nv, int variant, int nsm, cudaStream_t st, const BlkCsr *bl
     case 5: launch_spmm_nv<5>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
     case 6: launch_spmm_nv<6>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
     case 7: launch_spmm_nv<7>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
-    default: launch_spmm_nv<8>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
+    case 8: launch_spmm_nv<8>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
+    case 9: launch_spmm_nv<9>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
+    case 10: launch_spmm_nv<10>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
+    case 11: launch_spmm_nv<11>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
+    default: launch_spmm_nv<12>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
     }
 }
 
@@ -280,10 +315,17 @@ __global__ void __launch_bounds__(256) kb_tn(const Chunk *__restrict__ chunks, c
     tn_dims(MODE, s, B, A, ma, Bm, b0, kb);
     __shared__ double As[BT_TR][BT_MS + 1];
     __shared__ double Bs[BT_TR][BT_LV + 1];
+    constexpr int OPT = (BT_PW + 255) / 256;   // outputs per thread
     const int ne = ma * kb, t = threadIdx.x;
-    const int i0 = kb ? t / kb : 0, c0 = kb ? t % kb : 0;
-    const int i1 = kb ? (t + 256) / kb : 0, c1 = kb ? (t + 256) % kb : 0;
-    double acc0 = 0.0, acc1 = 0.0;
+    int ii[OPT], cc[OPT];
+    double acc[OPT];
+#pragma unroll
+    for (int o = 0; o < OPT; o++) {
+        const int e = t + 256 * o;
+        ii[o] = kb ? e / kb : 0;
+        cc[o] = kb ? e % kb : 0;
+        acc[o] = 0.0;
+    }
     const int64_t ld = B.ld;
     for (int64_t r0 = ch.row0; r0 < ch.row1; r0 += BT_TR) {
         const int nr = (int)min((int64_t)BT_TR, ch.row1 - r0);
@@ -305,19 +347,19 @@ __global__ void __launch_bounds__(256) kb_tn(const Chunk *__restrict__ chunks, c
             Bs[r][c] = v;
         }
         __syncthreads();
-        if (t < ne) {
+#pragma unroll
+        for (int o = 0; o < OPT; o++) {
+            if (t + 256 * o < ne) {
 #pragma unroll 8
-            for (int r = 0; r < BT_TR; r++) acc0 += As[r][i0] * Bs[r][c0];
-        }
-        if (t + 256 < ne) {
-#pragma unroll 8
-            for (int r = 0; r < BT_TR; r++) acc1 += As[r][i1] * Bs[r][c1];
+                for (int r = 0; r < BT_TR; r++) acc[o] += As[r][ii[o]] * Bs[r][cc[o]];
+            }
         }
         __syncthreads();
     }
     double *out = B.part + (int64_t)blockIdx.x * BT_PW;
-    if (t < ne) out[t] = acc0;
-    if (t + 256 < ne) out[t + 256] = acc1;
+#pragma unroll
+    for (int o = 0; o < OPT; o++)
+        if (t + 256 * o < ne) out[t + 256 * o] = acc[o];
 }
 
 // Sum of up to BT_LV per-thread values over the thread block into out[0..n).
@@ -813,6 +855,7 @@ struct pci_batch {
     int *d_ndone = nullptr;
     int last_nlv = 0;
     int storage = 0;          // 1: full copies where memory allows, 0: lower triangles only
+    int value_prec = 32;      // 32: blocks rounded to FP32 when added; 64: kept as built
     bool storage_done = false;
     int64_t full_nnz = 0;     // lower-triangle elements of the blocks held as full copies
     int tuned_variant = -1, tuned_nv = 0;
@@ -862,7 +905,7 @@ static int build_tables(pci_batch *b)
     for (int i = 0; i < nblk; i++) {
         const BlockRec &r = b->blocks[i];
         const Csr &M = r.F.rowptr ? r.F : r.H;
-        tab[i] = BlkCsr{M.rowptr, M.col, (const float *)M.val, r.r0, r.nd, r.F.rowptr ? 1 : 0};
+        tab[i] = BlkCsr{M.rowptr, M.col, M.val, r.r0, r.nd, r.F.rowptr ? 1 : 0, M.val_f32 ? 0 : 1};
         std::fill(rb.begin() + r.r0, rb.begin() + r.r0 + r.nd, i);
         cb[i] = (int64_t)ch.size();
         for (int64_t s = 0; s < r.nd; s += BT_CH)
@@ -1072,7 +1115,7 @@ static int prepare(pci_batch *b, int nlv)
 
 // Revision of the SpMM kernels, part of the cache key: cached picks of an
 // older kernel are not reused.
-static const int SPMM_REV = 3;
+static const int SPMM_REV = 4;
 
 static std::string tune_key(pci_batch *b, int nv)
 {
@@ -1080,7 +1123,9 @@ static std::string tune_key(pci_batch *b, int nv)
     std::string dn = b->devname;
     for (char &c : dn)
         if (c == ' ') c = '_';
-    k << dn << "|rev=" << SPMM_REV << "|storage=" << b->storage << "|full=" << b->full_nnz
+    int f64 = 0;
+    for (const BlockRec &r : b->blocks) f64 += (r.F.rowptr ? !r.F.val_f32 : !r.H.val_f32);
+    k << dn << "|rev=" << SPMM_REV << "|storage=" << b->storage << "|full=" << b->full_nnz << "|f64=" << f64
       << "|blocks=" << b->blocks.size() << "|rows=" << b->rows << "|nnz=" << b->nnz << "|nv=" << nv;
     return k.str();
 }
@@ -1119,8 +1164,11 @@ int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index)
     r.r0 = b->rows;
     r.nd = r.H.nrows;
     r.nnz = r.H.nnz;
-    if (r.H.cap > r.H.nnz) {
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    if (r.H.cap > r.H.nnz && (size_t)r.H.nnz * 8 + ((size_t)1 << 30) < fr) {
         // a padded build leaves its candidate slots allocated: keep nnz of them
+        // (when a copy of the values fits beside them)
         int rc = 0;
         const int64_t n = std::max<int64_t>(r.H.nnz, 1);
         int32_t *col = (int32_t *)dev_alloc(c, n * 4, &rc);
@@ -1130,10 +1178,11 @@ int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index)
         dev_free(r.H.col);
         r.H.col = col;
         h->H.col = col;
-        if (r.H.val_f32) {
-            float *val = (float *)dev_alloc(c, n * 4, &rc);
+        if (r.H.val_f32 || b->value_prec == 64) {
+            const size_t vb = r.H.val_f32 ? 4 : 8;
+            void *val = dev_alloc(c, n * vb, &rc);
             if (rc) return rc;
-            PCI_CUDA(c, cudaMemcpyAsync(val, r.H.val, r.H.nnz * 4, cudaMemcpyDeviceToDevice, c->st));
+            PCI_CUDA(c, cudaMemcpyAsync(val, r.H.val, r.H.nnz * vb, cudaMemcpyDeviceToDevice, c->st));
             PCI_CUDA(c, cudaStreamSynchronize(c->st));
             dev_free(r.H.val);
             r.H.val = val;
@@ -1141,7 +1190,7 @@ int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index)
         }
         r.H.cap = 0;
     }
-    if (!r.H.val_f32) {
+    if (!r.H.val_f32 && b->value_prec == 32) {
         int rc = 0;
         float *v = (float *)dev_alloc(c, std::max<int64_t>(r.H.nnz, 1) * 4, &rc);
         if (rc) return rc;
@@ -1165,6 +1214,14 @@ int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index)
     b->tuned_variant = -1;
     free_solve(b);
     if (index) *index = (int32_t)(b->blocks.size() - 1);
+    return PCI_OK;
+}
+
+int pci_batch_set_value_prec(pci_batch_t *b, int32_t value_prec)
+{
+    if (!b) return PCI_E_INPUT;
+    if (value_prec != 32 && value_prec != 64) return set_err(&b->core, PCI_E_INPUT, "value_prec must be 32 or 64");
+    b->value_prec = value_prec;
     return PCI_OK;
 }
 
@@ -1202,7 +1259,7 @@ int pci_batch_tune(pci_batch_t *b, int32_t nv, const char *cache_path, int32_t *
 {
     if (!b) return PCI_E_INPUT;
     pci_gpu *h = &b->core;
-    if (nv < 1 || nv > BT_LV) return set_err(h, PCI_E_INPUT, "nv must be 1..8");
+    if (nv < 1 || nv > BT_LV) return set_err(h, PCI_E_INPUT, "nv must be 1..12");
     int rc = prepare(b, nv);
     if (rc) return rc;
     const std::string key = tune_key(b, nv);
@@ -1215,7 +1272,7 @@ int pci_batch_tune(pci_batch_t *b, int32_t nv, const char *cache_path, int32_t *
         int v;
         double t;
         while (f >> tag >> k >> v >> t)
-            if (tag == "pci_batch_spmm" && k == key && v >= 0 && v < N_VARIANTS) { best = v; best_ms = t; cached = 1; }
+            if (tag == "pci_batch_spmm" && k == key && variant_ok(nv, v)) { best = v; best_ms = t; cached = 1; }
     }
     if (best < 0) {
         // every block running, P = 1
@@ -1227,6 +1284,7 @@ int pci_batch_tune(pci_batch_t *b, int32_t nv, const char *cache_path, int32_t *
             PCI_CUDA(h, cudaStreamSynchronize(h->st));
         }
         for (int v = 0; v < N_VARIANTS; v++) {
+            if (!variant_ok(nv, v)) continue;
             double t = 0.0;
             if ((rc = time_spmm(b, nv, v, 3, &t))) return rc;
             if (best < 0 || t < best_ms) { best = v; best_ms = t; }
@@ -1251,11 +1309,12 @@ int pci_batch_davidson(pci_batch_t *b, const pci_batch_params *p, double *E, dou
     if (!b || !p) return PCI_E_INPUT;
     pci_gpu *h = &b->core;
     const int nlv = p->nlv;
-    if (nlv < 1 || nlv > BT_LV) return set_err(h, PCI_E_INPUT, "nlv must be 1..8");
+    if (nlv < 1 || nlv > BT_LV) return set_err(h, PCI_E_INPUT, "nlv must be 1..12");
     if (p->max_sub < 2 * nlv || p->max_sub > BT_MS) return set_err(h, PCI_E_INPUT, "max_sub must be 2*nlv..64");
     if (p->keep < nlv || p->keep > p->max_sub - nlv) return set_err(h, PCI_E_INPUT, "keep must be nlv..max_sub-nlv");
     if (p->max_it < 1 || p->it_per_graph < 1 || !(p->tol > 0.0)) return set_err(h, PCI_E_INPUT, "bad max_it/it_per_graph/tol");
-    if (p->spmm_variant >= N_VARIANTS) return set_err(h, PCI_E_INPUT, "unknown SpMM variant");
+    if (p->spmm_variant >= 0 && !variant_ok(nlv, p->spmm_variant))
+        return set_err(h, PCI_E_INPUT, "unknown SpMM variant, or fewer lanes per row than vectors");
     for (const BlockRec &r : b->blocks)
         if (r.nd < nlv) return set_err(h, PCI_E_INPUT, "a block has fewer rows than nlv");
     auto t0 = std::chrono::steady_clock::now();

@@ -141,6 +141,33 @@ def test_batch_generated_blocks():
         assert np.abs(r["E"][i] - w).max() <= 1e-9, i
 
 
+def test_batch_fp64_values_ten_roots(blocks):
+    """FP64 values kept (pci_batch_set_value_prec 64) and ten roots per block:
+    the levels of the unrounded oracle matrices."""
+    from pci_b200.capi import Batch
+    nlv = 10
+    names = ["cfg1", "small3", "small4"]
+    with Batch(0) as b:
+        b.set_value_prec(64)
+        Hs = []
+        for name, s, rp, col, val in blocks:
+            if name in names:
+                b.add_csr(rp, col, val)
+                H = np.zeros((s.nd, s.nd))
+                rows = np.repeat(np.arange(s.nd), np.diff(rp))
+                H[rows, np.asarray(col) - 1] = val
+                Hs.append(H + np.tril(H, -1).T)
+        r = b.davidson(nlv=nlv, max_sub=64, keep=24, max_it=400, tol=TOL)
+        assert np.all(r["status"] == 1)
+        for i, H in enumerate(Hs):
+            w = np.linalg.eigvalsh(H)[:nlv]
+            assert np.abs(r["E"][i] - w).max() <= 1e-9, names[i]
+            X = b.vectors(i)
+            assert np.linalg.norm(H @ X - X * r["E"][i], axis=0).max() <= 2 * TOL
+        with pytest.raises(Exception):
+            b.davidson(nlv=nlv, spmm_variant=8)    # 8 lanes per row cannot hold 10 vectors
+
+
 def test_batch_iteration_limit(blocks):
     with _batch(blocks, names=["small3"]) as b:
         r = b.davidson(nlv=6, max_it=3, tol=TOL)
@@ -171,7 +198,7 @@ def test_batch_errors(blocks):
             b.davidson(nlv=4)                      # no blocks
     with _batch(blocks, names=["tiny"]) as b:
         with pytest.raises(PciError):
-            b.davidson(nlv=9)                      # more roots than supported
+            b.davidson(nlv=13)                     # more roots than supported
         with pytest.raises(PciError):
             b.davidson(nlv=6, max_sub=10)          # subspace below 2*nlv
         with pytest.raises(PciError):
