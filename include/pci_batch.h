@@ -32,7 +32,7 @@ extern "C" {
 typedef struct pci_batch pci_batch_t;
 
 #define PCI_BATCH_MAX_LV   12   /* roots per block */
-#define PCI_BATCH_MAX_SUB  64   /* subspace vectors per block */
+#define PCI_BATCH_MAX_SUB  96   /* subspace vectors per block */
 
 typedef struct {
     int32_t nlv;            /* roots per block, 1..PCI_BATCH_MAX_LV (Nlv) */

@@ -50,6 +50,7 @@ constexpr int BT_MS = PCI_BATCH_MAX_SUB;
 constexpr int BT_LV = PCI_BATCH_MAX_LV;
 constexpr int BT_PW = BT_MS * BT_LV;                         // partial words per chunk
 constexpr int BT_ROT_THREADS = 128;
+constexpr int BT_FIN_THREADS = 512;                          // threads of the per-block reductions
 
 struct BlkCsr {
     const int64_t *rowptr;
@@ -603,7 +604,7 @@ __device__ int chol_drop(const double *S, int k, double thr, double *M)
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(256) kb_fin(const int64_t *__restrict__ cb, BState *bst, Bufs B)
+__global__ void __launch_bounds__(BT_FIN_THREADS) kb_fin(const int64_t *__restrict__ cb, BState *bst, Bufs B)
 {
     const int b = blockIdx.x, t = threadIdx.x;
     BState &s = bst[b];
@@ -618,9 +619,17 @@ __global__ void __launch_bounds__(256) kb_fin(const int64_t *__restrict__ cb, BS
     const int ne = ma * kb;
     const int64_t c0 = cb[b], c1 = cb[b + 1];
     for (int e = t; e < ne; e += blockDim.x) {
-        double acc = 0.0;
-        for (int64_t c = c0; c < c1; c++) acc += B.part[c * BT_PW + e];
-        res[e] = acc;
+        // four running sums over the chunks (more loads in flight), added in a fixed order
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        int64_t c = c0;
+        for (; c + 3 < c1; c += 4) {
+            a0 += B.part[c * BT_PW + e];
+            a1 += B.part[(c + 1) * BT_PW + e];
+            a2 += B.part[(c + 2) * BT_PW + e];
+            a3 += B.part[(c + 3) * BT_PW + e];
+        }
+        for (; c < c1; c++) a0 += B.part[c * BT_PW + e];
+        res[e] = (a0 + a1) + (a2 + a3);
     }
     __syncthreads();
     double *coef = B.coef + (int64_t)b * BT_PW;
@@ -999,25 +1008,25 @@ static int enqueue_iteration(pci_batch *b, const Bufs &B, int variant, int nv)
     kb_pack<<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
     launch_spmm(nv, variant, b->nsm, st, b->d_blk, b->d_row_blk, b->d_st, b->rows, B.P, B.Q);
     kb_tn<TN_GRAM><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
-    kb_fin<FIN_GRAM><<<nblk, 256, 0, st>>>(b->d_cb, b->d_st, B);
+    kb_fin<FIN_GRAM><<<nblk, BT_FIN_THREADS, 0, st>>>(b->d_cb, b->d_st, B);
     kb_eig<<<nblk, 256, 2 * BT_MS * BT_MS * 8, st>>>(b->d_st, B);
     kb_resid<<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
-    kb_fin<FIN_RESID><<<nblk, 256, 0, st>>>(b->d_cb, b->d_st, B);
+    kb_fin<FIN_RESID><<<nblk, BT_FIN_THREADS, 0, st>>>(b->d_cb, b->d_st, B);
     kb_rotate<<<nch, BT_ROT_THREADS, (BT_MS * BT_MS + BT_MS * BT_ROT_THREADS) * 8, st>>>(b->d_chunks, b->d_st, B);
     kb_correct<<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
     kb_tn<TN_TT><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
-    kb_fin<FIN_NORM><<<nblk, 256, 0, st>>>(b->d_cb, b->d_st, B);
+    kb_fin<FIN_NORM><<<nblk, BT_FIN_THREADS, 0, st>>>(b->d_cb, b->d_st, B);
     kb_tn<TN_VT><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
-    kb_fin<FIN_VT1><<<nblk, 256, 0, st>>>(b->d_cb, b->d_st, B);
+    kb_fin<FIN_VT1><<<nblk, BT_FIN_THREADS, 0, st>>>(b->d_cb, b->d_st, B);
     kb_proj<<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
     kb_tn<TN_VT><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
-    kb_fin<FIN_VT2><<<nblk, 256, 0, st>>>(b->d_cb, b->d_st, B);
+    kb_fin<FIN_VT2><<<nblk, BT_FIN_THREADS, 0, st>>>(b->d_cb, b->d_st, B);
     kb_proj<<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
     kb_tn<TN_TT><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
-    kb_fin<FIN_CHOL1><<<nblk, 256, 0, st>>>(b->d_cb, b->d_st, B);
+    kb_fin<FIN_CHOL1><<<nblk, BT_FIN_THREADS, 0, st>>>(b->d_cb, b->d_st, B);
     kb_tri<1><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
     kb_tn<TN_T2><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
-    kb_fin<FIN_CHOL2><<<nblk, 256, 0, st>>>(b->d_cb, b->d_st, B);
+    kb_fin<FIN_CHOL2><<<nblk, BT_FIN_THREADS, 0, st>>>(b->d_cb, b->d_st, B);
     kb_tri<2><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
     kb_commit<<<(nblk + 127) / 128, 128, 0, st>>>(b->d_st, nblk);
     kb_count<<<1, 256, 0, st>>>(b->d_st, nblk, b->d_ndone);
@@ -1310,7 +1319,7 @@ int pci_batch_davidson(pci_batch_t *b, const pci_batch_params *p, double *E, dou
     pci_gpu *h = &b->core;
     const int nlv = p->nlv;
     if (nlv < 1 || nlv > BT_LV) return set_err(h, PCI_E_INPUT, "nlv must be 1..12");
-    if (p->max_sub < 2 * nlv || p->max_sub > BT_MS) return set_err(h, PCI_E_INPUT, "max_sub must be 2*nlv..64");
+    if (p->max_sub < 2 * nlv || p->max_sub > BT_MS) return set_err(h, PCI_E_INPUT, "max_sub must be 2*nlv..96");
     if (p->keep < nlv || p->keep > p->max_sub - nlv) return set_err(h, PCI_E_INPUT, "keep must be nlv..max_sub-nlv");
     if (p->max_it < 1 || p->it_per_graph < 1 || !(p->tol > 0.0)) return set_err(h, PCI_E_INPUT, "bad max_it/it_per_graph/tol");
     if (p->spmm_variant >= 0 && !variant_ok(nlv, p->spmm_variant))
