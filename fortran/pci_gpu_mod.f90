@@ -1,6 +1,6 @@
 ! ISO_C_BINDING interface to libpci_gpu.so (include/pci_gpu.h) for pconf.
 ! Use it under #ifdef PCI_GPU in place of the FormH / FormJ / Diag4 calls at
-! pconf.F90:217-238 (see INTEGRATION.md for the call sites).  Indices and
+! pconf.F90:217-238 (FormH + RedistributeHamCSR, FormJ, Diag4).  Indices and
 ! arrays are passed exactly as pconf holds them (1-based, column-major).
 module pci_gpu_mod
   use, intrinsic :: iso_c_binding

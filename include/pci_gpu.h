@@ -142,14 +142,18 @@ int pci_gpu_j_av(pci_gpu_t *h, const double *X, int32_t nv, int64_t nlim, double
  * its own pool or a framework's caching allocator, or a path where
  * cudaMalloc's implicit synchronisation is not acceptable).  Every array is
  * device memory the caller already holds: the J^2 matrix in the
- * pci_gpu_get_csr layout (rowptr[nrows+1] 0-based prefix, col 1-based, val),
- * X column-major with leading dimension ldx >= nrows, and Tj[nv] for the
- * result.  No handle and no allocation: the only scratch is a static device
+ * pci_gpu_get_csr layout (rowptr[nrows+1] 0-based prefix, col 1-based, val
+ * the FP64 values pci_gpu_get_csr(h, PCI_MAT_J2, ...) returns -- an FP32
+ * copy is read as doubles and gives wrong J), X column-major with leading
+ * dimension ldx >= nrows, and Tj[nv] for the result.  No handle and no allocation: the only scratch is a static device
  * array of 64 doubles, so nv is limited to 1..64 (larger nv returns
  * PCI_E_INPUT).  Work is enqueued on `stream` (NULL = default stream) and not
  * waited for.  All calls on a device share the scratch; calls that overlap on
  * the GPU race.  The first call on a device resolves the scratch address and
- * should come before any stream capture.  On error, errbuf (errlen bytes, may
+ * should come before any stream capture; that address belongs to the device's
+ * primary context and stays valid until the process exits or the device is
+ * reset (after cudaDeviceReset, or under another driver context, do not call
+ * this entry point again in the same process).  On error, errbuf (errlen bytes, may
  * be NULL) receives a message. */
 int pci_gpu_j_av_noalloc(const int64_t *rowptr, const int32_t *col, const double *val, int64_t nrows,
                          const double *X, int64_t ldx, int32_t nv, int64_t nlim, double *Tj,

@@ -235,7 +235,7 @@ def test_davidson_matches_dense(name):
 
 
 def test_reference_davidson_stalls_on_synthetic_small3():
-    """The finding recorded in DESIGN.md: on small3 the reference's restarted
+    """On small3 with the synthetic integrals, the reference's restarted
     Davidson (subspace 2*Nlv) is still far from Crt4 after 60 iterations while
     the dense eigenvalues are well separated."""
     s = get_system("small3")

@@ -19,16 +19,23 @@ from conftest import get_system
 pytestmark = pytest.mark.gpu
 
 
-def _noalloc(L, rowptr, col, val, X, nlim, nv, out, errbuf):
-    import torch
+def _noalloc(L, rowptr, col, val, X, nlim, nv, out, errbuf, stream=None):
     return L.pci_gpu_j_av_noalloc(C.c_void_p(rowptr.data_ptr()), C.c_void_p(col.data_ptr()),
                                   C.c_void_p(val.data_ptr()), rowptr.numel() - 1,
                                   C.c_void_p(X.data_ptr()), X.shape[1], nv, nlim,
-                                  C.c_void_p(out.data_ptr()), None, errbuf, len(errbuf))
+                                  C.c_void_p(out.data_ptr()),
+                                  None if stream is None else C.c_void_p(stream.cuda_stream),
+                                  errbuf, len(errbuf))
 
 
-@pytest.mark.parametrize("name", ["tiny", "small3"])
-def test_noalloc_matches_j_av(name):
+@pytest.mark.parametrize("name,nv,half,use_stream", [
+    ("tiny", 7, False, False),
+    ("small3", 7, False, False),
+    ("small3", 1, True, False),      # column filter k < nlim and row limit n < nlim
+    ("small3", 64, True, True),      # the edge of the static scratch, on a side stream
+    ("cfg1", 64, False, True),
+])
+def test_noalloc_matches_j_av(name, nv, half, use_stream):
     import torch
     from pci_b200.capi import Engine, load
     s = get_system(name)
@@ -38,10 +45,9 @@ def test_noalloc_matches_j_av(name):
         e.form_j()
         rp, col, val = e.get_csr(1)
         rng = np.random.default_rng(11)
-        nv = 7
         X = rng.standard_normal((s.nd, nv))
         X /= np.linalg.norm(X, axis=0)
-        nlim = s.nd
+        nlim = s.nd // 2 if half else s.nd
         ref = e.j_av(X, nlim)
     dev = torch.device("cuda:0")
     d_rp = torch.from_numpy(rp).to(dev)
@@ -49,10 +55,15 @@ def test_noalloc_matches_j_av(name):
     d_val = torch.from_numpy(val).to(dev)
     d_X = torch.from_numpy(np.ascontiguousarray(X.T)).to(dev)   # column-major Nd x nv, ldx = Nd
     errbuf = C.create_string_buffer(256)
+    stream = torch.cuda.Stream(device=dev) if use_stream else None
+    torch.cuda.synchronize()
     for _ in range(2):
         out = torch.full((nv,), float("nan"), dtype=torch.float64, device=dev)
-        rc = _noalloc(L, d_rp, d_col, d_val, d_X, nlim, nv, out, errbuf)
+        torch.cuda.synchronize()
+        rc = _noalloc(L, d_rp, d_col, d_val, d_X, nlim, nv, out, errbuf, stream)
         assert rc == 0, errbuf.value
+        if stream is not None:
+            stream.synchronize()
         torch.cuda.synchronize()
         assert np.allclose(out.cpu().numpy(), ref, rtol=1e-12, atol=1e-12)
 
