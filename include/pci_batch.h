@@ -34,6 +34,19 @@ typedef struct pci_batch pci_batch_t;
 #define PCI_BATCH_MAX_LV   12   /* roots per block */
 #define PCI_BATCH_MAX_SUB  96   /* subspace vectors per block */
 
+#define PCI_BATCH_FP64  0   /* SpMM on FP64 vectors with FP64 sums throughout */
+#define PCI_BATCH_MIXED 1   /* SpMM on FP32 vectors with FP32 sums (FP32 values) until every root of a
+                               block is at or below switch_tol, or the largest residual stops dropping
+                               (stall_max iterations without a 10% drop); then a restart on the Ritz
+                               vectors and the FP64 SpMM (FP64 values, or hi + lo of a split block) to
+                               tol.  Basis, projections, eigensolve and residual norms stay FP64. */
+
+#define PCI_BATCH_CORR_DIAG    0   /* t = r / (theta - H_nn), as Dvdsn (davidson.f90:436-570) */
+#define PCI_BATCH_CORR_LEARNED 1   /* t = output of the attached model (pci_batch_set_correction_model)
+                                      per row; a root whose residual does not drop from one iteration
+                                      to the next takes the diagonal correction for the rest of the
+                                      solve */
+
 typedef struct {
     int32_t nlv;            /* roots per block, 1..PCI_BATCH_MAX_LV (Nlv) */
     int32_t max_sub;        /* subspace size at which a block restarts, 2*nlv..PCI_BATCH_MAX_SUB */
@@ -42,20 +55,41 @@ typedef struct {
     double tol;             /* residual 2-norm per root (Crt4) */
     int32_t it_per_graph;   /* iterations captured in one CUDA graph, >= 1 */
     int32_t spmm_variant;   /* SpMM variant (pci_batch_tune), -1 = tuned or default */
+    int32_t precision;      /* PCI_BATCH_FP64 or PCI_BATCH_MIXED */
+    int32_t stall_max;      /* PCI_BATCH_MIXED: see above; 0 = 8 */
+    double switch_tol;      /* PCI_BATCH_MIXED: residual that ends the FP32 phase (>= tol) */
+    int32_t correction;     /* PCI_BATCH_CORR_DIAG or PCI_BATCH_CORR_LEARNED */
+    int32_t pad;
 } pci_batch_params;
+
+/* One sample for training the learned correction: the state of one root of
+ * one block at one iteration, seen at one sampled row. */
+typedef struct {
+    int32_t blk, iter, root, phase;   /* block, iteration (1-based), root, SpMM phase */
+    int64_t row;                      /* row within the block, 0-based */
+    double x;                         /* entry of the root's Ritz vector at this iteration */
+    double r;                         /* entry of its residual H x - theta x */
+    double theta;                     /* Ritz value */
+    double rnorm;                     /* residual 2-norm */
+    double diag;                      /* H_nn */
+} pci_batch_sample;
 
 int pci_batch_create(int32_t device, pci_batch_t **out);
 
 /* Append the Hamiltonian resident in `h` as the next block and take it over
  * (h keeps its basis and integrals but no longer holds H).  FP64 values are
- * rounded to FP32 unless pci_batch_set_value_prec(b, 64) was called.
- * *index receives the block's index. */
+ * rounded to FP32, kept, or split into FP32 pairs as pci_batch_set_value_prec
+ * says.  When h holds a determinant basis, the occupied orbitals of every row
+ * are kept as the learned correction's inputs.  *index receives the block's
+ * index. */
 int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index);
 
 /* Value precision of blocks added from now on: 32 (default) rounds FP64
  * values to FP32 when a block is added; 64 keeps each block's values as its
- * handle built them (FP64 from pci_gpu_form_h with value_prec 64).  The
- * vectors and all sums are FP64 either way. */
+ * handle built them (FP64 from pci_gpu_form_h with value_prec 64); 48 splits
+ * each FP64 value v in place into the FP32 pair hi = fl(v), lo = fl(v - hi)
+ * (same memory as FP64; hi + lo = v to about 2^-48 relative): the FP32 SpMM
+ * of PCI_BATCH_MIXED reads hi, the FP64 SpMM hi + lo. */
 int pci_batch_set_value_prec(pci_batch_t *b, int32_t value_prec);
 
 /* Storage of the blocks' matrices for the solve: 0 (default) = lower
@@ -95,10 +129,31 @@ int pci_batch_davidson(pci_batch_t *b, const pci_batch_params *p, double *E, dou
 int pci_batch_vectors(pci_batch_t *b, int32_t blk, double *X);
 
 /* Timings of the last solve: out[0] total ms, [1] iterations (largest over
- * blocks), [2] SpMM ms per call (measured outside the graph), [3] SpMM
- * variant used, [4] setup ms, [5] kernel launches per iteration, [6] share of
- * the lower-triangle elements held as full copies; n <= 7. */
+ * blocks), [2] SpMM ms per call on FP64 vectors (measured outside the
+ * graph), [3] SpMM variant used, [4] setup ms, [5] kernel launches per
+ * iteration, [6] share of the lower-triangle elements held as full copies,
+ * [7] SpMM ms per call on FP32 vectors (PCI_BATCH_MIXED), [8] largest number
+ * of FP32-phase iterations of a block, [9] blocks that reached the FP64
+ * phase (PCI_BATCH_MIXED); n <= 10. */
 int pci_batch_stats(pci_batch_t *b, double *out, int32_t n);
+
+/* Attach a trained model (pci_gpu.h) for correction = PCI_BATCH_CORR_LEARNED;
+ * NULL detaches.  Its first nin - 2 inputs are the occupation counts of the
+ * orbitals, input nin - 2 is H_nn - theta and input nin - 1 the residual
+ * entry times sqrt(nd) / |r|; every block must come from a handle with a
+ * basis of at most nin - 2 orbitals.  The model must outlive its use.  No
+ * counterpart in the reference, whose only correction is Dvdsn's diagonal one
+ * (davidson.f90:436-570). */
+int pci_batch_set_correction_model(pci_batch_t *b, pci_mlp_t *m);
+
+/* Record training samples in the next solves: rows_per_block rows of every
+ * block (all rows of smaller blocks) drawn with `seed`, up to `capacity`
+ * samples (later ones are counted, not kept); 0 rows switches it off. */
+int pci_batch_set_harvest(pci_batch_t *b, int32_t rows_per_block, int64_t capacity, int32_t seed);
+
+/* Samples of the last solve: up to cap into out (may be NULL); *count
+ * receives the number recorded (above the capacity, the rest were dropped). */
+int pci_batch_harvest(pci_batch_t *b, pci_batch_sample *out, int64_t cap, int64_t *count);
 
 const char *pci_batch_last_error(pci_batch_t *b);
 void pci_batch_destroy(pci_batch_t *b);

@@ -111,6 +111,15 @@ int pci_gpu_csr_info(pci_gpu_t *h, int32_t which, int64_t *nrows, int64_t *nnz);
  * double.  Any pointer may be NULL to skip that array. */
 int pci_gpu_get_csr(pci_gpu_t *h, int32_t which, int64_t *rowptr, int32_t *col, double *val);
 
+/* Replaces: the row range of Hamil%col/val that one rank holds after
+ * RedistributeHamCSR (matrix_io.f90:260-502) and streams to pCONF.HIJ.
+ * Copies rows row_lo..row_hi (1-based, inclusive) of the resident matrix:
+ * rowptr[row_hi-row_lo+2] as a 0-based prefix within the range, col 1-based,
+ * val as double.  col and val may be NULL (size them from rowptr's last
+ * entry first). */
+int pci_gpu_get_csr_rows(pci_gpu_t *h, int32_t which, int64_t row_lo, int64_t row_hi, int64_t *rowptr, int32_t *col,
+                         double *val);
+
 /* Replaces: ReadMatrixCSR (matrix_io.f90:801-939) for Kl = 1 restarts:
  * uploads a lower-triangle CSR (same layout as pci_gpu_get_csr) and its Hmin. */
 int pci_gpu_set_csr(pci_gpu_t *h, int32_t which, int64_t Nd, int64_t nnz, const int64_t *rowptr,
@@ -180,6 +189,14 @@ int pci_mlp_set_params(pci_mlp_t *m, const float *p, int64_t n);
 int pci_mlp_get_params(pci_mlp_t *m, float *p, int64_t n);
 /* y[n] from X[n x nin] (host arrays). */
 int pci_mlp_forward(pci_mlp_t *m, const float *X, int64_t n, float *y);
+/* y[n] from the compact inputs the solver uses, on the tensor-core path of
+ * the batched solver's learned correction: orbs[n x 8] holds each row's
+ * occupied orbitals (0-based, an orbital listed once per electron in it,
+ * 0xff = empty slot; these are the non-zero occupation counts of inputs
+ * 0..nin-3), f0[n] and f1[n] inputs nin-2 and nin-1 (host arrays).  The
+ * hidden activations are rounded to BF16 for the tensor-core products, so
+ * y agrees with pci_mlp_forward on the same rows to about 1e-2 relative. */
+int pci_mlp_forward_occ(pci_mlp_t *m, const uint8_t *orbs, const float *f0, const float *f1, int64_t n, float *y);
 /* Mean squared error against T[n] and its gradient (length num_params,
  * may be NULL) for X[n x nin] (host arrays). */
 int pci_mlp_loss_grad(pci_mlp_t *m, const float *X, const float *T, int64_t n, float *loss, float *grad);

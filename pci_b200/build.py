@@ -35,7 +35,7 @@ UNITS = [("hbuild", "hbuild.cu", NOFMA)] + \
     [("spmm", "spmm.cu", []), ("davidson", "davidson.cu", []), ("pci_gpu", "pci_gpu.cu", []),
      ("noalloc", "noalloc.cu", []), ("pci_io", "pci_io.cpp", []), ("mlp", "mlp.cu", []),
      ("batch", "batch.cu", [])]
-HEADERS = ["pci_internal.h", "hbuild_impl.cuh", os.path.join("..", "..", "include", "pci_gpu.h"),
+HEADERS = ["pci_internal.h", "hbuild_impl.cuh", "mlp_tc.cuh", os.path.join("..", "..", "include", "pci_gpu.h"),
            os.path.join("..", "..", "include", "pci_io.h"), os.path.join("..", "..", "include", "pci_batch.h")]
 
 

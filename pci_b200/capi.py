@@ -24,17 +24,26 @@ EXPORTS = ["pci_gpu_create", "pci_gpu_set_basis", "pci_gpu_set_integrals", "pci_
            "pci_gpu_davidson", "pci_gpu_j_av", "pci_gpu_j_av_noalloc", "pci_gpu_jterms", "pci_gpu_stats",
            "pci_gpu_last_error", "pci_gpu_destroy", "pci_mlp_create", "pci_mlp_num_params", "pci_mlp_set_params",
            "pci_mlp_get_params", "pci_mlp_forward", "pci_mlp_loss_grad", "pci_mlp_train", "pci_mlp_last_error",
-           "pci_mlp_destroy", "pci_gpu_set_correction_model", "pci_gpu_davidson_harvest"]
+           "pci_mlp_destroy", "pci_gpu_set_correction_model", "pci_gpu_davidson_harvest", "pci_mlp_forward_occ",
+           "pci_gpu_get_csr_rows"]
 BATCH_EXPORTS = ["pci_batch_create", "pci_batch_add_block", "pci_batch_set_storage", "pci_batch_set_value_prec",
                  "pci_batch_info", "pci_batch_tune",
                  "pci_batch_variant", "pci_batch_davidson", "pci_batch_vectors", "pci_batch_stats",
-                 "pci_batch_last_error", "pci_batch_destroy"]
+                 "pci_batch_last_error", "pci_batch_destroy", "pci_batch_set_correction_model",
+                 "pci_batch_set_harvest", "pci_batch_harvest"]
+PCI_BATCH_FP64, PCI_BATCH_MIXED = 0, 1
+PCI_BATCH_CORR_DIAG, PCI_BATCH_CORR_LEARNED = 0, 1
+SAMPLE_DTYPE = np.dtype([("blk", np.int32), ("iter", np.int32), ("root", np.int32), ("phase", np.int32),
+                         ("row", np.int64), ("x", np.float64), ("r", np.float64), ("theta", np.float64),
+                         ("rnorm", np.float64), ("diag", np.float64)])
 BATCH_STATUS = {1: "converged", 2: "iteration limit", 3: "no new direction"}
 
 
 class BatchParams(C.Structure):
     _fields_ = [("nlv", C.c_int32), ("max_sub", C.c_int32), ("keep", C.c_int32), ("max_it", C.c_int32),
-                ("tol", C.c_double), ("it_per_graph", C.c_int32), ("spmm_variant", C.c_int32)]
+                ("tol", C.c_double), ("it_per_graph", C.c_int32), ("spmm_variant", C.c_int32),
+                ("precision", C.c_int32), ("stall_max", C.c_int32), ("switch_tol", C.c_double),
+                ("correction", C.c_int32), ("pad", C.c_int32)]
 
 
 class PciError(RuntimeError):
@@ -110,6 +119,11 @@ def load(path: str = LIB):
     L.pci_batch_last_error.restype = C.c_char_p
     L.pci_batch_destroy.argtypes = [P]
     L.pci_batch_destroy.restype = None
+    L.pci_batch_set_correction_model.argtypes = [P, P]
+    L.pci_batch_set_harvest.argtypes = [P, i32, i64, i32]
+    L.pci_batch_harvest.argtypes = [P, P, i64, C.POINTER(i64)]
+    L.pci_mlp_forward_occ.argtypes = [P, P, P, P, i64, P]
+    L.pci_gpu_get_csr_rows.argtypes = [P, i32, i64, i64, P, P, P]
     _lib = L
     return L
 
@@ -194,6 +208,17 @@ class Engine:
         col = np.zeros(nnz.value, np.int32)
         val = np.zeros(nnz.value, np.float64)
         self._check(self.L.pci_gpu_get_csr(self.h, which, _p(rowptr), _p(col), _p(val)))
+        return rowptr, col, val
+
+    def get_csr_rows(self, which: int, row_lo: int, row_hi: int):
+        """Rows row_lo..row_hi (1-based, inclusive) of a resident matrix:
+        (rowptr from 0, 1-based col, val as double)."""
+        n = row_hi - row_lo + 1
+        rowptr = np.zeros(n + 1, np.int64)
+        self._check(self.L.pci_gpu_get_csr_rows(self.h, which, row_lo, row_hi, _p(rowptr), None, None))
+        col = np.zeros(rowptr[-1], np.int32)
+        val = np.zeros(rowptr[-1], np.float64)
+        self._check(self.L.pci_gpu_get_csr_rows(self.h, which, row_lo, row_hi, _p(rowptr), _p(col), _p(val)))
         return rowptr, col, val
 
     def set_csr(self, which, rowptr, col, val, hmin=0.0):
@@ -302,6 +327,15 @@ class Mlp:
         self._check(self.L.pci_mlp_forward(self.m, _p(X), X.shape[0], _p(y)))
         return y
 
+    def forward_occ(self, orbs, f0, f1):
+        """Tensor-core forward from compact inputs: orbs [n, 8] uint8 (0xff empty), f0, f1 [n]."""
+        orbs = np.ascontiguousarray(orbs, np.uint8)
+        f0 = np.ascontiguousarray(f0, np.float32)
+        f1 = np.ascontiguousarray(f1, np.float32)
+        y = np.zeros(orbs.shape[0], np.float32)
+        self._check(self.L.pci_mlp_forward_occ(self.m, _p(orbs), _p(f0), _p(f1), orbs.shape[0], _p(y)))
+        return y
+
     def loss_grad(self, X, T):
         X = np.ascontiguousarray(X, np.float32)
         T = np.ascontiguousarray(T, np.float32)
@@ -382,7 +416,8 @@ class Batch:
             return self.add_engine(e)
 
     def set_value_prec(self, value_prec: int):
-        """32: blocks rounded to FP32 when added (default); 64: kept as built."""
+        """32: blocks rounded to FP32 when added (default); 64: kept as built;
+        48: split into FP32 hi + lo pairs (for the mixed-precision form)."""
         self._check(self.L.pci_batch_set_value_prec(self.b, value_prec))
 
     def set_storage(self, mode: int):
@@ -400,10 +435,11 @@ class Batch:
                                           C.byref(ms), C.byref(fc)))
         return v.value, ms.value, bool(fc.value)
 
-    def davidson(self, nlv=6, max_sub=48, keep=None, max_it=300, tol=1e-8, it_per_graph=4, spmm_variant=-1):
+    def davidson(self, nlv=6, max_sub=48, keep=None, max_it=300, tol=1e-8, it_per_graph=4, spmm_variant=-1,
+                 precision=PCI_BATCH_FP64, switch_tol=1e-5, stall_max=0, correction=PCI_BATCH_CORR_DIAG):
         nblk = len(self.sizes)
         p = BatchParams(nlv, max_sub, keep if keep is not None else 2 * nlv, max_it, tol, it_per_graph,
-                        spmm_variant)
+                        spmm_variant, precision, stall_max, switch_tol, correction, 0)
         E = np.zeros((nblk, nlv))
         rn = np.zeros((nblk, nlv))
         it = np.zeros(nblk, np.int32)
@@ -419,11 +455,29 @@ class Batch:
         return X.T
 
     def stats(self):
-        out = np.zeros(7)
-        self._check(self.L.pci_batch_stats(self.b, _p(out), 7))
+        out = np.zeros(10)
+        self._check(self.L.pci_batch_stats(self.b, _p(out), 10))
         keys = ["total_ms", "iterations", "spmm_ms", "spmm_variant", "setup_ms", "launches_per_iteration",
-                "full_share"]
+                "full_share", "spmm32_ms", "fp32_iterations", "switched_blocks"]
         return dict(zip(keys, out.tolist()))
+
+    def set_correction_model(self, mlp):
+        """Attach a trained Mlp for correction=PCI_BATCH_CORR_LEARNED (None detaches)."""
+        self._check(self.L.pci_batch_set_correction_model(self.b, mlp.m if mlp is not None else None))
+        self._model = mlp
+
+    def set_harvest(self, rows_per_block, capacity, seed=0):
+        """Record training samples in the next solves (0 rows: off)."""
+        self._check(self.L.pci_batch_set_harvest(self.b, rows_per_block, capacity, seed))
+
+    def harvest(self):
+        """Samples of the last solve as a structured array (SAMPLE_DTYPE) and the number recorded."""
+        cnt = C.c_int64()
+        self._check(self.L.pci_batch_harvest(self.b, None, 0, C.byref(cnt)))
+        out = np.zeros(cnt.value, SAMPLE_DTYPE)
+        if cnt.value:
+            self._check(self.L.pci_batch_harvest(self.b, out.ctypes.data_as(C.c_void_p), cnt.value, C.byref(cnt)))
+        return out[:min(cnt.value, out.size)], int(cnt.value)
 
     def close(self):
         if self.b:

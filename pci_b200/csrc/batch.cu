@@ -38,6 +38,7 @@
 #include <vector>
 
 #include "pci_internal.h"
+#include "mlp_tc.cuh"
 #include "../../include/pci_batch.h"
 
 #define FULL_MASK 0xffffffffu
@@ -55,10 +56,13 @@ constexpr int BT_FIN_THREADS = 512;                          // threads of the p
 struct BlkCsr {
     const int64_t *rowptr;
     const int32_t *col;
-    const void *val;   // float, or double when f64
+    const void *val;   // float, double when f64, or (hi, lo) float pairs when split
     int64_t r0, nd;
     int32_t full;      // 1: both triangles stored (row-wise gather, no reductions)
     int32_t f64;
+    int32_t split;     // 1: val holds float2 {hi, lo} with hi + lo = the FP64 value to 2^-48
+    int32_t pad;
+    const uint8_t *orbs;   // [nd][8] occupied orbitals of each row (0xff = empty), or null
 };
 
 struct Chunk {
@@ -76,18 +80,28 @@ struct BState {
     int base;     // basis vectors the corrections are orthogonalised against
     int kk;       // corrections formed this iteration
     int k1, k2;   // corrections left after the first and second Cholesky-QR
-    int pad;
+    int phase;    // 0: SpMM on FP32 vectors with FP32 sums; 1: FP64 SpMM
+    int sw;       // this iteration ends phase 0: restart on the Ritz vectors, recompute H V in FP64
+    int it32;     // iterations spent in phase 0
+    int stall;    // phase-0 iterations without a 10% drop of the largest residual
+    int swit;     // iteration at which phase 0 ended
+    double best;  // smallest largest-residual seen in phase 0
     int jsel[BT_LV];
+    int lrn[BT_LV];          // learned correction still used for root j
     double theta[BT_LV];
     double rnorm[BT_LV];
+    double prev[BT_LV];      // residual of root j at the previous iteration
     double scale[BT_LV];
 };
 
 struct Bufs {
     double *V, *W, *R, *T, *T2, *P, *Q, *G, *EV, *EW, *part, *coef, *D;
+    float *P32, *Q32;
+    double *Xk;   // Ritz vectors of the iteration (written only while harvesting samples)
     int64_t ld;
     int msub, nlv, keep, max_it;
-    double tol;
+    double tol, swtol;
+    int stall_max;
 };
 
 enum { TN_GRAM = 0, TN_TT = 1, TN_VT = 2, TN_T2 = 3 };
@@ -101,6 +115,18 @@ __global__ void k_to_f32(const double *a, float *b, int64_t n)
         b[i] = (float)a[i];
 }
 
+// In place: a[i] (double) becomes the float pair {hi, lo}, hi = fl32(a[i]),
+// lo = fl32(a[i] - hi), so hi + lo equals a[i] to about 2^-48 relative.
+__global__ void k_split(double *a, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = a[i];
+        const float hi = (float)v;
+        const float lo = (float)(v - (double)hi);
+        reinterpret_cast<float2 *>(a)[i] = make_float2(hi, lo);
+    }
+}
+
 __global__ void kb_diag(const BlkCsr *blks, const int32_t *row_blk, int64_t rows, double *D)
 {
     for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < rows; n += (int64_t)gridDim.x * blockDim.x) {
@@ -109,7 +135,11 @@ __global__ void kb_diag(const BlkCsr *blks, const int32_t *row_blk, int64_t rows
         double d = 0.0;
         for (int64_t l = B.rowptr[ln + 1] - 1; l >= B.rowptr[ln]; l--)
             if (B.col[l] == ln) {
-                d = B.f64 ? ((const double *)B.val)[l] : (double)((const float *)B.val)[l];
+                if (B.f64) d = ((const double *)B.val)[l];
+                else if (B.split) {
+                    const float2 hl = ((const float2 *)B.val)[l];
+                    d = (double)hl.x + (double)hl.y;
+                } else d = (double)((const float *)B.val)[l];
                 break;
             }
         D[n] = d;
@@ -124,50 +154,58 @@ __global__ void kb_set_units(double *V, int64_t ld, const int64_t *pos, int n)
 
 // ------------------------------------------------------------- SpMM ---
 
-// Y = H X over the rows of every running block, X and Y row-major with NV
-// vectors.  A team of SUB lanes owns a row; within it NV lanes share one
-// stored element (lane v takes vector v) and SUB/NV elements go per step.
-// Lower-triangle blocks: the transpose part of each element goes to Y as a
-// global reduction, and so does the row part (other rows add into it), so Y
-// starts at zero.  Blocks stored with both triangles: a plain row gather and
-// store, with no reductions.
+// Value of stored element l as the arithmetic type XT of the SpMM: FP32
+// vectors take the FP32 value (hi of a split pair), FP64 vectors the FP64
+// value (hi + lo of a split pair).
+template <typename XT>
+__device__ __forceinline__ XT blk_val(const BlkCsr &B, int64_t l)
+{
+    if (B.f64) return (XT)__ldg(&((const double *)B.val)[l]);
+    if (B.split) {
+        const float2 hl = __ldg(&((const float2 *)B.val)[l]);
+        if (sizeof(XT) == 4) return (XT)hl.x;
+        return (XT)((double)hl.x + (double)hl.y);
+    }
+    return (XT)__ldg(&((const float *)B.val)[l]);
+}
+
 // Row n (local row ln) of block B for vector v: the row part of the product
 // (returned; both triangles for a full copy) and, for a lower triangle, the
-// transpose part added to Y by global reductions.
-template <int NV, int G, typename VT>
-__device__ __forceinline__ double spmm_row(const BlkCsr &B, int64_t ln, int64_t n, int g, int v,
-                                           const double *__restrict__ X, double *Y)
+// transpose part added to Y by global reductions.  XT is the vector and sum
+// type (double, or float in the first phase of the mixed-precision form).
+template <int NV, int G, typename XT>
+__device__ __forceinline__ XT spmm_row(const BlkCsr &B, int64_t ln, int64_t n, int g, int v,
+                                       const XT *__restrict__ X, XT *Y)
 {
-    const VT *__restrict__ val = (const VT *)B.val;
     const int64_t l0 = __ldg(&B.rowptr[ln]), l1 = __ldg(&B.rowptr[ln + 1]);
-    double acc = 0.0;
+    XT acc = 0;
     int64_t l = l0 + g;
     if (B.full) {
         for (; l + 3 * G < l1; l += 4 * G) {
             int k[4];
-            double t[4], xk[4];
+            XT t[4], xk[4];
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 k[u] = __ldg(&B.col[l + u * G]);
-                t[u] = (double)__ldg(&val[l + u * G]);
+                t[u] = blk_val<XT>(B, l + u * G);
             }
 #pragma unroll
             for (int u = 0; u < 4; u++) xk[u] = __ldg(&X[(B.r0 + k[u]) * NV + v]);
 #pragma unroll
             for (int u = 0; u < 4; u++) acc += t[u] * xk[u];
         }
-        for (; l < l1; l += G) acc += (double)__ldg(&val[l]) * __ldg(&X[(B.r0 + __ldg(&B.col[l])) * NV + v]);
+        for (; l < l1; l += G) acc += blk_val<XT>(B, l) * __ldg(&X[(B.r0 + __ldg(&B.col[l])) * NV + v]);
         return acc;
     }
-    const double xn = __ldg(&X[n * NV + v]);
+    const XT xn = __ldg(&X[n * NV + v]);
     // four elements per step: their loads are issued before any use
     for (; l + 3 * G < l1; l += 4 * G) {
         int k[4];
-        double t[4], xk[4];
+        XT t[4], xk[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
             k[u] = __ldg(&B.col[l + u * G]);
-            t[u] = (double)__ldg(&val[l + u * G]);
+            t[u] = blk_val<XT>(B, l + u * G);
         }
 #pragma unroll
         for (int u = 0; u < 4; u++) xk[u] = __ldg(&X[(B.r0 + k[u]) * NV + v]);
@@ -179,7 +217,7 @@ __device__ __forceinline__ double spmm_row(const BlkCsr &B, int64_t ln, int64_t 
     }
     for (; l < l1; l += G) {
         const int k = __ldg(&B.col[l]);
-        const double t = (double)__ldg(&val[l]);
+        const XT t = blk_val<XT>(B, l);
         const int64_t kg = B.r0 + k;
         if (k != ln) atomicAdd(&Y[kg * NV + v], t * xn);
         acc += t * __ldg(&X[kg * NV + v]);
@@ -187,17 +225,18 @@ __device__ __forceinline__ double spmm_row(const BlkCsr &B, int64_t ln, int64_t 
     return acc;
 }
 
-// Y = H X over the rows of every running block, X and Y row-major with NV
+// Y = H X over the rows of every running block in SpMM phase `phase`
+// (blocks in the other phase are skipped), X and Y row-major with NV
 // vectors.  A team of SUB lanes owns a row; within it NV lanes share one
 // stored element (lane v takes vector v) and SUB/NV elements go per step.
 // Lower-triangle blocks: the transpose part of each element goes to Y as a
 // global reduction, and so does the row part (other rows add into it), so Y
 // starts at zero.  Blocks stored with both triangles: a plain row gather and
 // store, with no reductions.
-template <int NV, int SUB>
+template <int NV, int SUB, typename XT>
 __global__ void __launch_bounds__(256) kb_spmm(const BlkCsr *__restrict__ blks, const int32_t *__restrict__ row_blk,
-                                               const BState *__restrict__ bst, int64_t rows,
-                                               const double *__restrict__ X, double *Y)
+                                               const BState *__restrict__ bst, int64_t rows, int phase,
+                                               const XT *__restrict__ X, XT *Y)
 {
     constexpr int G = SUB / NV;
     constexpr int TPW = 32 / SUB;
@@ -212,18 +251,17 @@ __global__ void __launch_bounds__(256) kb_spmm(const BlkCsr *__restrict__ blks, 
         const int64_t n = n0 + lane / SUB;
         bool ok = n < rows;
         const int b = ok ? __ldg(&row_blk[n]) : 0;
-        ok = ok && bst[b].done == 0;
-        double acc = 0.0;
+        ok = ok && bst[b].done == 0 && bst[b].phase == phase;
+        XT acc = 0;
         bool full = false;
         if (ok && act) {
             const BlkCsr B = blks[b];
             full = B.full != 0;
-            acc = B.f64 ? spmm_row<NV, G, double>(B, n - B.r0, n, g, v, X, Y)
-                        : spmm_row<NV, G, float>(B, n - B.r0, n, g, v, X, Y);
+            acc = spmm_row<NV, G, XT>(B, n - B.r0, n, g, v, X, Y);
         }
 #pragma unroll
         for (int gg = 1; gg < G; gg++) {
-            const double o = __shfl_sync(FULL_MASK, acc, g == 0 ? lane + gg * NV : lane);
+            const XT o = __shfl_sync(FULL_MASK, acc, g == 0 ? lane + gg * NV : lane);
             if (g == 0) acc += o;
         }
         if (ok && act && g == 0) {
@@ -239,14 +277,14 @@ constexpr int CTAS[N_CTAS] = {4, 8, 16, 32};
 constexpr int N_VARIANTS = N_SUB * N_CTAS;
 constexpr int DEFAULT_VARIANT = 2;   // 32 lanes per row, 16 blocks per SM
 
-template <int NV>
+template <int NV, typename XT>
 void launch_spmm_nv(int sub, int grid, cudaStream_t st, const BlkCsr *blks, const int32_t *row_blk, const BState *bst,
-                    int64_t rows, const double *X, double *Y)
+                    int64_t rows, int phase, const XT *X, XT *Y)
 {
-    if (sub == 32) kb_spmm<NV, 32><<<grid, 256, 0, st>>>(blks, row_blk, bst, rows, X, Y);
+    if (sub == 32) kb_spmm<NV, 32, XT><<<grid, 256, 0, st>>>(blks, row_blk, bst, rows, phase, X, Y);
     else if constexpr (NV <= 16) {
-        if (sub == 16) kb_spmm<NV, 16><<<grid, 256, 0, st>>>(blks, row_blk, bst, rows, X, Y);
-        else if constexpr (NV <= 8) kb_spmm<NV, 8><<<grid, 256, 0, st>>>(blks, row_blk, bst, rows, X, Y);
+        if (sub == 16) kb_spmm<NV, 16, XT><<<grid, 256, 0, st>>>(blks, row_blk, bst, rows, phase, X, Y);
+        else if constexpr (NV <= 8) kb_spmm<NV, 8, XT><<<grid, 256, 0, st>>>(blks, row_blk, bst, rows, phase, X, Y);
     }
 }
 
@@ -255,36 +293,49 @@ bool variant_ok(int nv, int variant)
     return variant >= 0 && variant < N_VARIANTS && SUBS[variant / N_CTAS] >= nv;
 }
 
+// One SpMM launch of every running block in `phase` (1: FP64 vectors X, Y;
+// 0: FP32 vectors X, Y).
+template <typename XT>
 void launch_spmm(int nv, int variant, int nsm, cudaStream_t st, const BlkCsr *blks, const int32_t *row_blk,
-                 const BState *bst, int64_t rows, const double *X, double *Y)
+                 const BState *bst, int64_t rows, int phase, const XT *X, XT *Y)
 {
     const int sub = SUBS[variant / N_CTAS];
     const int grid = nsm * CTAS[variant % N_CTAS];
     switch (nv) {
-    case 1: launch_spmm_nv<1>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
-    case 2: launch_spmm_nv<2>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
-    case 3: launch_spmm_nv<3>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
-    case 4: launch_spmm_nv<4>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
-    case 5: launch_spmm_nv<5>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
-    case 6: launch_spmm_nv<6>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
-    case 7: launch_spmm_nv<7>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
-    case 8: launch_spmm_nv<8>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
-    case 9: launch_spmm_nv<9>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
-    case 10: launch_spmm_nv<10>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
-    case 11: launch_spmm_nv<11>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
-    default: launch_spmm_nv<12>(sub, grid, st, blks, row_blk, bst, rows, X, Y); break;
+    case 1: launch_spmm_nv<1, XT>(sub, grid, st, blks, row_blk, bst, rows, phase, X, Y); break;
+    case 2: launch_spmm_nv<2, XT>(sub, grid, st, blks, row_blk, bst, rows, phase, X, Y); break;
+    case 3: launch_spmm_nv<3, XT>(sub, grid, st, blks, row_blk, bst, rows, phase, X, Y); break;
+    case 4: launch_spmm_nv<4, XT>(sub, grid, st, blks, row_blk, bst, rows, phase, X, Y); break;
+    case 5: launch_spmm_nv<5, XT>(sub, grid, st, blks, row_blk, bst, rows, phase, X, Y); break;
+    case 6: launch_spmm_nv<6, XT>(sub, grid, st, blks, row_blk, bst, rows, phase, X, Y); break;
+    case 7: launch_spmm_nv<7, XT>(sub, grid, st, blks, row_blk, bst, rows, phase, X, Y); break;
+    case 8: launch_spmm_nv<8, XT>(sub, grid, st, blks, row_blk, bst, rows, phase, X, Y); break;
+    case 9: launch_spmm_nv<9, XT>(sub, grid, st, blks, row_blk, bst, rows, phase, X, Y); break;
+    case 10: launch_spmm_nv<10, XT>(sub, grid, st, blks, row_blk, bst, rows, phase, X, Y); break;
+    case 11: launch_spmm_nv<11, XT>(sub, grid, st, blks, row_blk, bst, rows, phase, X, Y); break;
+    default: launch_spmm_nv<12, XT>(sub, grid, st, blks, row_blk, bst, rows, phase, X, Y); break;
     }
 }
 
 // ------------------------------------------------------ per-row steps ---
 
 // P[n, s] = V[n, m-knew+s] (s < knew), 0 otherwise; Q = 0 for the SpMM.
+// Blocks in phase 0 pack FP32 copies into P32 / Q32.
 __global__ void kb_pack(const Chunk *__restrict__ chunks, const BState *__restrict__ bst, Bufs B)
 {
     const Chunk ch = chunks[blockIdx.x];
     const BState &s = bst[ch.blk];
     if (s.done) return;
     const int c0 = s.m - s.knew, kn = s.knew, nv = B.nlv;
+    if (s.phase == 0) {
+        for (int64_t n = ch.row0 + threadIdx.x; n < ch.row1; n += blockDim.x) {
+            for (int c = 0; c < nv; c++) {
+                B.P32[n * nv + c] = c < kn ? (float)B.V[(int64_t)(c0 + c) * B.ld + n] : 0.f;
+                B.Q32[n * nv + c] = 0.f;
+            }
+        }
+        return;
+    }
     for (int64_t n = ch.row0 + threadIdx.x; n < ch.row1; n += blockDim.x) {
         for (int c = 0; c < nv; c++) {
             B.P[n * nv + c] = c < kn ? B.V[(int64_t)(c0 + c) * B.ld + n] : 0.0;
@@ -339,7 +390,7 @@ __global__ void __launch_bounds__(256) kb_tn(const Chunk *__restrict__ chunks, c
             double v = 0.0;
             if (r < nr) {
                 if (MODE == TN_GRAM) {
-                    v = Bm[(r0 + r) * B.nlv + c];
+                    v = s.phase == 0 ? (double)B.Q32[(r0 + r) * B.nlv + c] : Bm[(r0 + r) * B.nlv + c];
                     B.W[(int64_t)(b0 + c) * ld + r0 + r] = v;
                 } else {
                     v = Bm[(int64_t)(b0 + c) * ld + r0 + r];
@@ -421,6 +472,7 @@ __global__ void __launch_bounds__(256) kb_resid(const Chunk *__restrict__ chunks
             if (j < nlv) {
                 const double r = hx[j] - th[j] * x[j];
                 B.R[(int64_t)j * B.ld + n] = r;
+                if (B.Xk) B.Xk[(int64_t)j * B.ld + n] = x[j];
                 ss[j] += r * r;
             }
         }
@@ -479,6 +531,102 @@ __global__ void kb_correct(const Chunk *__restrict__ chunks, const BState *__res
             B.T[(int64_t)c * B.ld + n] = B.R[(int64_t)j * B.ld + n] / d;
         }
     }
+}
+
+// Learned correction: T[:, c] = MLP(features of row n) for the correction
+// slots whose root still uses it (lrn); kb_correct's diagonal correction
+// stays in the other slots.  Features of row n for root j: the occupied
+// orbitals of its determinant, H_nn - theta_j and r_jn sqrt(nd) / |r_j|.
+// One warp evaluates 16 rows of one slot on the tensor cores (mlp_tc.cuh);
+// work items are (chunk, 16-row tile, slot) in a grid-stride loop.
+__global__ void __launch_bounds__(256, 2) kb_learned(const Chunk *__restrict__ chunks, int nch,
+                                                     const BlkCsr *__restrict__ blks, const BState *__restrict__ bst,
+                                                     Bufs B, mlptc::Weights W)
+{
+    extern __shared__ double smw[];
+    const mlptc::Smem S = mlptc::load(W, reinterpret_cast<unsigned char *>(smw));
+    const int lane = threadIdx.x & 31, g = lane >> 2;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    constexpr int TILES = BT_CH / 16;
+    const int64_t nitems = (int64_t)nch * TILES * BT_LV;
+    for (int64_t it = warp; it < nitems; it += nwarps) {
+        const int c = (int)(it % BT_LV);
+        const int64_t q = it / BT_LV;
+        const int sub = (int)(q % TILES);
+        const Chunk ch = chunks[q / TILES];
+        const BState &s = bst[ch.blk];
+        if (s.done || c >= s.kk) continue;
+        const int j = s.jsel[c];
+        if (!s.lrn[j]) continue;
+        const int64_t r0 = ch.row0 + (int64_t)sub * 16;
+        if (r0 >= ch.row1) continue;
+        const BlkCsr &Bk = blks[ch.blk];
+        const double fs = sqrt((double)Bk.nd) / fmax(s.rnorm[j], 1e-300);
+        const double th = s.theta[j];
+        uint8_t o[2][mlptc::MAXOCC];
+        float a[2], b[2], out[2];
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const int64_t n = r0 + g + 8 * r;
+            const bool ok = n < ch.row1;
+            const uint8_t *src = Bk.orbs + (ok ? (n - Bk.r0) * mlptc::MAXOCC : 0);
+#pragma unroll
+            for (int e = 0; e < mlptc::MAXOCC; e++) o[r][e] = ok ? src[e] : (uint8_t)0xff;
+            a[r] = ok ? (float)(B.D[n] - th) : 0.f;
+            b[r] = ok ? (float)(B.R[(int64_t)j * B.ld + n] * fs) : 0.f;
+        }
+        mlptc::tile(S, W.nin, o, a, b, out);
+        if ((lane & 3) == 0) {
+#pragma unroll
+            for (int r = 0; r < 2; r++) {
+                const int64_t n = r0 + g + 8 * r;
+                if (n < ch.row1) B.T[(int64_t)c * B.ld + n] = (double)out[r];
+            }
+        }
+    }
+}
+
+// Samples for training the learned correction: for every sampled row and
+// every root still above the criterion of a running block, the Ritz vector
+// and residual entries with the Ritz value, residual norm and H_nn.
+__global__ void kb_harvest(const int64_t *__restrict__ rows, int64_t nrows, const int32_t *__restrict__ row_blk,
+                           const BlkCsr *__restrict__ blks, const BState *__restrict__ bst, Bufs B,
+                           pci_batch_sample *out, int64_t cap, unsigned long long *count)
+{
+    const int nlv = B.nlv;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nrows * nlv;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e / nlv;
+        const int j = (int)(e - i * nlv);
+        const int64_t n = rows[i];
+        const int b = row_blk[n];
+        const BState &s = bst[b];
+        if (s.done || !(s.rnorm[j] > B.tol)) continue;
+        const unsigned long long pos = atomicAdd(count, 1ULL);
+        if ((int64_t)pos >= cap) continue;
+        pci_batch_sample rec;
+        rec.blk = b;
+        rec.iter = s.iters;
+        rec.root = j;
+        rec.phase = s.phase;
+        rec.row = n - blks[b].r0;
+        rec.x = B.Xk[(int64_t)j * B.ld + n];
+        rec.r = B.R[(int64_t)j * B.ld + n];
+        rec.theta = s.theta[j];
+        rec.rnorm = s.rnorm[j];
+        rec.diag = B.D[n];
+        out[pos] = rec;
+    }
+}
+
+// Occupied orbitals (0-based) of every determinant: orbs[n][e] = orbital of
+// m-state occ[n][e], 0xff past the Ne electrons.
+__global__ void kb_row_orbs(const uint16_t *occ, const int16_t *ms_orb, int ne, int64_t nd, uint8_t *orbs)
+{
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nd; n += (int64_t)gridDim.x * blockDim.x)
+        for (int e = 0; e < mlptc::MAXOCC; e++)
+            orbs[n * mlptc::MAXOCC + e] = e < ne ? (uint8_t)ms_orb[occ[n * ne + e]] : (uint8_t)0xff;
 }
 
 // T[:, s] = scale_s T[:, s] - V[:, :base] C[:, s].
@@ -661,23 +809,54 @@ __global__ void __launch_bounds__(BT_FIN_THREADS) kb_fin(const int64_t *__restri
     } else {   // FIN_RESID: convergence, corrections to form, restart
         __shared__ int sh_base, sh_restart;
         if (t == 0) {
-            int nconv = 0;
+            int nconv = 0, nsw = 0;
+            double mx = 0.0;
             for (int j = 0; j < B.nlv; j++) {
                 const double rn = sqrt(fmax(res[j], 0.0));
+                s.prev[j] = s.rnorm[j];
                 s.rnorm[j] = rn;
                 nconv += rn <= B.tol;
+                nsw += rn <= B.swtol;
+                mx = fmax(mx, rn);
             }
             s.iters += 1;
             sh_restart = 0;
             sh_base = 0;
-            if (nconv == B.nlv) {
+            // judge of the learned correction: a root whose residual did not drop
+            // since the previous iteration takes the diagonal correction from now on
+            // (not right after the end of the FP32 phase, whose restart recomputes H V)
+            if (s.iters >= 2 && s.iters != s.swit + 1)
+                for (int j = 0; j < B.nlv; j++)
+                    if (s.lrn[j] && s.rnorm[j] >= s.prev[j]) s.lrn[j] = 0;
+            const bool p0 = s.phase == 0;
+            if (p0) {
+                s.it32 += 1;
+                if (mx < 0.9 * s.best) {
+                    s.best = mx;
+                    s.stall = 0;
+                } else {
+                    s.stall += 1;
+                }
+            }
+            if (!p0 && nconv == B.nlv) {
                 s.done = 1;
             } else if (s.iters >= B.max_it) {
                 s.done = 2;
+            } else if (p0 && (nsw == B.nlv || s.stall >= B.stall_max)) {
+                // end of the FP32 phase: restart on the nlv Ritz vectors; the next
+                // iteration recomputes their H V with the FP64 SpMM
+                s.kk = 0;
+                s.sw = 1;
+                s.swit = s.iters;
+                sh_base = B.nlv;
+                sh_restart = 1;
+                s.base = sh_base;
+                s.restart = sh_restart;
             } else {
+                const double thr = p0 ? B.swtol : B.tol;
                 int kk = 0;
                 for (int j = 0; j < B.nlv; j++)
-                    if (!(s.rnorm[j] <= B.tol)) s.jsel[kk++] = j;
+                    if (!(s.rnorm[j] <= thr)) s.jsel[kk++] = j;
                 s.kk = kk;
                 if (s.m + kk > B.msub) {
                     sh_base = min(B.keep, s.m);
@@ -815,10 +994,26 @@ __global__ void kb_commit(BState *bst, int nblk)
     if (b >= nblk) return;
     BState &s = bst[b];
     if (s.done) return;
+    s.restart = 0;
+    if (s.sw) {   // FP64 from now on, every basis vector's H V recomputed
+        s.m = s.base;
+        s.knew = s.base;
+        s.phase = 1;
+        s.sw = 0;
+        return;
+    }
     s.m = s.base + s.k2;
     s.knew = s.k2;
-    s.restart = 0;
-    if (s.k2 == 0) s.done = 3;
+    if (s.k2 == 0) {
+        // no direction left: with learned corrections in use, fall back to the
+        // diagonal ones for every root and go on; otherwise stop
+        bool any = false;
+        for (int j = 0; j < BT_LV; j++) {
+            any = any || s.lrn[j] != 0;
+            s.lrn[j] = 0;
+        }
+        if (!any) s.done = 3;
+    }
 }
 
 __global__ void kb_count(const BState *bst, int nblk, int *ndone)
@@ -840,6 +1035,9 @@ struct BlockRec {
     Csr H;            // lower triangle (freed once a full copy exists)
     Csr F;            // both triangles, or empty
     int64_t r0 = 0, nd = 0, nnz = 0;   // rows and stored lower-triangle elements
+    int split = 0;    // H.val holds {hi, lo} float pairs (value precision 48)
+    uint8_t *orbs = nullptr;   // [nd][8] occupied orbitals of each row (from the handle's basis), or null
+    int nsu = 0;               // orbitals of the block's basis (0 without a basis)
 };
 
 struct pci_batch {
@@ -860,16 +1058,26 @@ struct pci_batch {
     int cap_nlv = 0;
     double *d_V = nullptr, *d_W = nullptr, *d_R = nullptr, *d_T = nullptr, *d_T2 = nullptr, *d_P = nullptr,
            *d_Q = nullptr, *d_G = nullptr, *d_EV = nullptr, *d_EW = nullptr, *d_part = nullptr, *d_coef = nullptr;
+    float *d_P32 = nullptr, *d_Q32 = nullptr;
     BState *d_st = nullptr;
     int *d_ndone = nullptr;
     int last_nlv = 0;
     int storage = 0;          // 1: full copies where memory allows, 0: lower triangles only
-    int value_prec = 32;      // 32: blocks rounded to FP32 when added; 64: kept as built
+    int value_prec = 32;      // 32: blocks rounded to FP32 when added; 64: kept as built; 48: hi/lo split
     bool storage_done = false;
     int64_t full_nnz = 0;     // lower-triangle elements of the blocks held as full copies
     int tuned_variant = -1, tuned_nv = 0;
+    pci_mlp *model = nullptr;                 // learned correction (not owned)
+    // samples for the learned correction
+    int hv_per_block = 0, hv_seed = 0;
+    int64_t hv_cap = 0, hv_n = 0, hv_last = 0;
+    int64_t *d_hv_rows = nullptr;
+    pci_batch_sample *d_hv = nullptr;
+    unsigned long long *d_hv_count = nullptr;
+    double *d_Xk = nullptr;
     double tuned_ms = 0.0;
     double st_total = 0, st_iters = 0, st_spmm = 0, st_variant = 0, st_setup = 0, st_launches = 0;
+    double st_spmm32 = 0, st_it32 = 0, st_switched = 0;
 };
 
 static void free_solve(pci_batch *b)
@@ -877,6 +1085,9 @@ static void free_solve(pci_batch *b)
     double **bufs[] = {&b->d_V, &b->d_W, &b->d_R, &b->d_T, &b->d_T2, &b->d_P, &b->d_Q,
                        &b->d_G, &b->d_EV, &b->d_EW, &b->d_part, &b->d_coef};
     for (double **p : bufs) { dev_free(*p); *p = nullptr; }
+    dev_free(b->d_P32);
+    dev_free(b->d_Q32);
+    b->d_P32 = b->d_Q32 = nullptr;
     dev_free(b->d_st);
     b->d_st = nullptr;
     dev_free(b->d_ndone);
@@ -914,7 +1125,8 @@ static int build_tables(pci_batch *b)
     for (int i = 0; i < nblk; i++) {
         const BlockRec &r = b->blocks[i];
         const Csr &M = r.F.rowptr ? r.F : r.H;
-        tab[i] = BlkCsr{M.rowptr, M.col, M.val, r.r0, r.nd, r.F.rowptr ? 1 : 0, M.val_f32 ? 0 : 1};
+        tab[i] = BlkCsr{M.rowptr, M.col, M.val, r.r0, r.nd, r.F.rowptr ? 1 : 0,
+                        (M.val_f32 || r.split) ? 0 : 1, r.split ? 1 : 0, 0, r.orbs};
         std::fill(rb.begin() + r.r0, rb.begin() + r.r0 + r.nd, i);
         cb[i] = (int64_t)ch.size();
         for (int64_t s = 0; s < r.nd; s += BT_CH)
@@ -961,6 +1173,8 @@ static int ensure_solve(pci_batch *b, int nlv)
     al(&b->d_T2, R * nlv);
     al(&b->d_P, R * nlv);
     al(&b->d_Q, R * nlv);
+    if (!rc) b->d_P32 = (float *)dev_alloc(h, 4 * std::max<int64_t>(R * nlv, 1), &rc);
+    if (!rc) b->d_Q32 = (float *)dev_alloc(h, 4 * std::max<int64_t>(R * nlv, 1), &rc);
     al(&b->d_G, nblk * BT_MS * BT_MS);
     al(&b->d_EV, nblk * BT_MS * BT_MS);
     al(&b->d_EW, nblk * BT_MS);
@@ -981,12 +1195,16 @@ static Bufs make_bufs(pci_batch *b, const pci_batch_params *p)
     Bufs B;
     B.V = b->d_V; B.W = b->d_W; B.R = b->d_R; B.T = b->d_T; B.T2 = b->d_T2; B.P = b->d_P; B.Q = b->d_Q;
     B.G = b->d_G; B.EV = b->d_EV; B.EW = b->d_EW; B.part = b->d_part; B.coef = b->d_coef; B.D = b->d_D;
+    B.P32 = b->d_P32; B.Q32 = b->d_Q32;
+    B.Xk = nullptr;
     B.ld = b->rows;
     B.msub = p ? p->max_sub : BT_MS;
     B.nlv = p ? p->nlv : b->cap_nlv;
     B.keep = p ? p->keep : 0;
     B.max_it = p ? p->max_it : 0;
     B.tol = p ? p->tol : 0.0;
+    B.swtol = p ? p->switch_tol : 0.0;
+    B.stall_max = p ? (p->stall_max > 0 ? p->stall_max : 8) : 8;
     return B;
 }
 
@@ -996,24 +1214,36 @@ static int set_attrs(pci_batch *b)
     PCI_CUDA(h, cudaFuncSetAttribute(kb_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * BT_MS * BT_MS * 8));
     PCI_CUDA(h, cudaFuncSetAttribute(kb_rotate, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (BT_MS * BT_MS + BT_MS * BT_ROT_THREADS) * 8));
+    if (b->model)
+        PCI_CUDA(h, cudaFuncSetAttribute(kb_learned, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)mlptc::smem_bytes(mlp_num_inputs(b->model))));
     return PCI_OK;
 }
 
-// One iteration of every running block (26 launches, no host synchronisation).
-static int enqueue_iteration(pci_batch *b, const Bufs &B, int variant, int nv)
+// One iteration of every running block (25 launches, one more for the FP32
+// SpMM of the mixed-precision form, one more for the learned correction and
+// one more while harvesting samples; no host synchronisation).
+static int enqueue_iteration(pci_batch *b, const Bufs &B, int variant, int nv, bool mixed, bool learned)
 {
     pci_gpu *h = &b->core;
     cudaStream_t st = h->st;
     const int nch = b->nch, nblk = (int)b->blocks.size();
     kb_pack<<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
-    launch_spmm(nv, variant, b->nsm, st, b->d_blk, b->d_row_blk, b->d_st, b->rows, B.P, B.Q);
+    if (mixed) launch_spmm<float>(nv, variant, b->nsm, st, b->d_blk, b->d_row_blk, b->d_st, b->rows, 0, B.P32, B.Q32);
+    launch_spmm<double>(nv, variant, b->nsm, st, b->d_blk, b->d_row_blk, b->d_st, b->rows, 1, B.P, B.Q);
     kb_tn<TN_GRAM><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
     kb_fin<FIN_GRAM><<<nblk, BT_FIN_THREADS, 0, st>>>(b->d_cb, b->d_st, B);
     kb_eig<<<nblk, 256, 2 * BT_MS * BT_MS * 8, st>>>(b->d_st, B);
     kb_resid<<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
     kb_fin<FIN_RESID><<<nblk, BT_FIN_THREADS, 0, st>>>(b->d_cb, b->d_st, B);
+    if (B.Xk)
+        kb_harvest<<<b->nsm * 4, 256, 0, st>>>(b->d_hv_rows, b->hv_n, b->d_row_blk, b->d_blk, b->d_st, B, b->d_hv,
+                                               b->hv_cap, b->d_hv_count);
     kb_rotate<<<nch, BT_ROT_THREADS, (BT_MS * BT_MS + BT_MS * BT_ROT_THREADS) * 8, st>>>(b->d_chunks, b->d_st, B);
     kb_correct<<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
+    if (learned)
+        kb_learned<<<b->nsm * 2, 256, mlptc::smem_bytes(mlp_num_inputs(b->model)), st>>>(
+            b->d_chunks, nch, b->d_blk, b->d_st, B, mlp_tc_weights(b->model));
     kb_tn<TN_TT><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
     kb_fin<FIN_NORM><<<nblk, BT_FIN_THREADS, 0, st>>>(b->d_cb, b->d_st, B);
     kb_tn<TN_VT><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
@@ -1035,28 +1265,83 @@ static int enqueue_iteration(pci_batch *b, const Bufs &B, int variant, int nv)
 }
 
 static const int ITER_LAUNCHES = 25;
+static const int LEARNED_LAUNCHES = 1;
 
-// One SpMM of every block with the given variant on P (all blocks running),
-// timed with events; average ms over `reps`.
-static int time_spmm(pci_batch *b, int nv, int variant, int reps, double *ms)
+static int prepare_harvest(pci_batch *b, Bufs &B, int nlv);
+
+// The learned correction needs a model whose inputs cover every block's
+// orbitals, and every block's determinant basis.
+static int learned_ready(pci_batch *b)
 {
     pci_gpu *h = &b->core;
-    cudaEvent_t e0, e1;
-    PCI_CUDA(h, cudaEventCreate(&e0));
-    PCI_CUDA(h, cudaEventCreate(&e1));
-    launch_spmm(nv, variant, b->nsm, h->st, b->d_blk, b->d_row_blk, b->d_st, b->rows, b->d_P, b->d_Q);
-    PCI_CUDA(h, cudaEventRecord(e0, h->st));
-    for (int r = 0; r < reps; r++) {
-        PCI_CUDA(h, cudaMemsetAsync(b->d_Q, 0, 8 * b->rows * nv, h->st));
-        launch_spmm(nv, variant, b->nsm, h->st, b->d_blk, b->d_row_blk, b->d_st, b->rows, b->d_P, b->d_Q);
+    if (!b->model) return set_err(h, PCI_E_STATE, "learned correction requested without a model");
+    const int nin = mlp_num_inputs(b->model);
+    for (const BlockRec &r : b->blocks) {
+        if (!r.orbs) return set_err(h, PCI_E_INPUT, "a block has no determinant basis (added from a CSR)");
+        if (r.nsu > nin - 2) return set_err(h, PCI_E_INPUT, "a block has more orbitals than the model's inputs");
     }
-    PCI_CUDA(h, cudaEventRecord(e1, h->st));
+    return PCI_OK;
+}
+
+// CUDA events released when the scope ends, on every return path.
+struct EventPair {
+    cudaEvent_t a = nullptr, b = nullptr;
+    ~EventPair()
+    {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+    cudaError_t create()
+    {
+        cudaError_t e = cudaEventCreate(&a);
+        return e != cudaSuccess ? e : cudaEventCreate(&b);
+    }
+};
+
+// Device memory released when the scope ends.
+struct DevBuf {
+    void *p = nullptr;
+    ~DevBuf() { dev_free(p); }
+};
+
+// Every block running and in SpMM phase `phase` (the state of a solve is
+// overwritten: used before a solve, for timing).
+__global__ void kb_set_phase(BState *bst, int nblk, int phase)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < nblk) {
+        bst[b].done = 0;
+        bst[b].phase = phase;
+    }
+}
+
+// One SpMM of every block with the given variant on P (FP64 vectors, phase 1)
+// or P32 (FP32 vectors, phase 0), timed with events; average ms over `reps`.
+static int time_spmm(pci_batch *b, int nv, int variant, int reps, int phase, double *ms)
+{
+    pci_gpu *h = &b->core;
+    const int nblk = (int)b->blocks.size();
+    EventPair ev;
+    PCI_CUDA(h, ev.create());
+    kb_set_phase<<<(nblk + 127) / 128, 128, 0, h->st>>>(b->d_st, nblk, phase);
+    auto one = [&]() {
+        if (phase) launch_spmm<double>(nv, variant, b->nsm, h->st, b->d_blk, b->d_row_blk, b->d_st, b->rows, 1,
+                                       b->d_P, b->d_Q);
+        else launch_spmm<float>(nv, variant, b->nsm, h->st, b->d_blk, b->d_row_blk, b->d_st, b->rows, 0, b->d_P32,
+                                b->d_Q32);
+    };
+    one();
+    PCI_CUDA(h, cudaEventRecord(ev.a, h->st));
+    for (int r = 0; r < reps; r++) {
+        if (phase) PCI_CUDA(h, cudaMemsetAsync(b->d_Q, 0, 8 * b->rows * nv, h->st));
+        else PCI_CUDA(h, cudaMemsetAsync(b->d_Q32, 0, 4 * b->rows * nv, h->st));
+        one();
+    }
+    PCI_CUDA(h, cudaEventRecord(ev.b, h->st));
     PCI_CUDA(h, cudaGetLastError());
-    PCI_CUDA(h, cudaEventSynchronize(e1));
+    PCI_CUDA(h, cudaEventSynchronize(ev.b));
     float f = 0.f;
-    cudaEventElapsedTime(&f, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    PCI_CUDA(h, cudaEventElapsedTime(&f, ev.a, ev.b));
     *ms = f / reps;
     return PCI_OK;
 }
@@ -1095,7 +1380,7 @@ static int choose_storage(pci_batch *b)
     const size_t margin = (size_t)4 << 30;
     for (int i : order) {
         BlockRec &r = b->blocks[i];
-        if (r.F.rowptr) continue;
+        if (r.F.rowptr || r.split) continue;
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
         // the copy (both triangles, FP32 + int32) and its build scratch
@@ -1124,7 +1409,7 @@ static int prepare(pci_batch *b, int nlv)
 
 // Revision of the SpMM kernels, part of the cache key: cached picks of an
 // older kernel are not reused.
-static const int SPMM_REV = 4;
+static const int SPMM_REV = 5;
 
 static std::string tune_key(pci_batch *b, int nv)
 {
@@ -1132,9 +1417,13 @@ static std::string tune_key(pci_batch *b, int nv)
     std::string dn = b->devname;
     for (char &c : dn)
         if (c == ' ') c = '_';
-    int f64 = 0;
-    for (const BlockRec &r : b->blocks) f64 += (r.F.rowptr ? !r.F.val_f32 : !r.H.val_f32);
+    int f64 = 0, split = 0;
+    for (const BlockRec &r : b->blocks) {
+        f64 += (r.F.rowptr ? !r.F.val_f32 : !r.H.val_f32) && !r.split;
+        split += r.split;
+    }
     k << dn << "|rev=" << SPMM_REV << "|storage=" << b->storage << "|full=" << b->full_nnz << "|f64=" << f64
+      << "|split=" << split
       << "|blocks=" << b->blocks.size() << "|rows=" << b->rows << "|nnz=" << b->nnz << "|nv=" << nv;
     return k.str();
 }
@@ -1173,6 +1462,16 @@ int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index)
     r.r0 = b->rows;
     r.nd = r.H.nrows;
     r.nnz = r.H.nnz;
+    if (h->have_basis && h->d_occ && h->d_ms_orb && h->nd == r.nd && h->nsu <= 254 && h->ne <= mlptc::MAXOCC) {
+        // the occupied orbitals of every row: inputs of the learned correction
+        int rc = 0;
+        r.orbs = (uint8_t *)dev_alloc(c, (size_t)std::max<int64_t>(r.nd, 1) * mlptc::MAXOCC, &rc);
+        if (rc) return rc;
+        kb_row_orbs<<<b->nsm * 4, 256, 0, c->st>>>(h->d_occ, h->d_ms_orb, h->ne, r.nd, r.orbs);
+        PCI_CUDA(c, cudaGetLastError());
+        PCI_CUDA(c, cudaStreamSynchronize(c->st));
+        r.nsu = h->nsu;
+    }
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
     if (r.H.cap > r.H.nnz && (size_t)r.H.nnz * 8 + ((size_t)1 << 30) < fr) {
@@ -1187,7 +1486,7 @@ int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index)
         dev_free(r.H.col);
         r.H.col = col;
         h->H.col = col;
-        if (r.H.val_f32 || b->value_prec == 64) {
+        if (r.H.val_f32 || b->value_prec != 32) {
             const size_t vb = r.H.val_f32 ? 4 : 8;
             void *val = dev_alloc(c, n * vb, &rc);
             if (rc) return rc;
@@ -1198,6 +1497,13 @@ int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index)
             h->H.val = val;
         }
         r.H.cap = 0;
+    }
+    if (!r.H.val_f32 && b->value_prec == 48) {
+        // in place: each FP64 value becomes {hi, lo} = {(float)v, (float)(v - hi)}
+        k_split<<<b->nsm * 8, 256, 0, c->st>>>((double *)r.H.val, r.H.nnz);
+        PCI_CUDA(c, cudaGetLastError());
+        PCI_CUDA(c, cudaStreamSynchronize(c->st));
+        r.split = 1;
     }
     if (!r.H.val_f32 && b->value_prec == 32) {
         int rc = 0;
@@ -1229,7 +1535,8 @@ int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index)
 int pci_batch_set_value_prec(pci_batch_t *b, int32_t value_prec)
 {
     if (!b) return PCI_E_INPUT;
-    if (value_prec != 32 && value_prec != 64) return set_err(&b->core, PCI_E_INPUT, "value_prec must be 32 or 64");
+    if (value_prec != 32 && value_prec != 64 && value_prec != 48)
+        return set_err(&b->core, PCI_E_INPUT, "value_prec must be 32, 48 (FP32 hi + lo) or 64");
     b->value_prec = value_prec;
     return PCI_OK;
 }
@@ -1295,7 +1602,7 @@ int pci_batch_tune(pci_batch_t *b, int32_t nv, const char *cache_path, int32_t *
         for (int v = 0; v < N_VARIANTS; v++) {
             if (!variant_ok(nv, v)) continue;
             double t = 0.0;
-            if ((rc = time_spmm(b, nv, v, 3, &t))) return rc;
+            if ((rc = time_spmm(b, nv, v, 3, 1, &t))) return rc;
             if (best < 0 || t < best_ms) { best = v; best_ms = t; }
         }
         if (cache_path) {
@@ -1322,6 +1629,12 @@ int pci_batch_davidson(pci_batch_t *b, const pci_batch_params *p, double *E, dou
     if (p->max_sub < 2 * nlv || p->max_sub > BT_MS) return set_err(h, PCI_E_INPUT, "max_sub must be 2*nlv..96");
     if (p->keep < nlv || p->keep > p->max_sub - nlv) return set_err(h, PCI_E_INPUT, "keep must be nlv..max_sub-nlv");
     if (p->max_it < 1 || p->it_per_graph < 1 || !(p->tol > 0.0)) return set_err(h, PCI_E_INPUT, "bad max_it/it_per_graph/tol");
+    if (p->precision != PCI_BATCH_FP64 && p->precision != PCI_BATCH_MIXED)
+        return set_err(h, PCI_E_INPUT, "precision must be PCI_BATCH_FP64 or PCI_BATCH_MIXED");
+    const bool mixed = p->precision == PCI_BATCH_MIXED;
+    if (mixed && !(p->switch_tol >= p->tol)) return set_err(h, PCI_E_INPUT, "switch_tol must be >= tol");
+    if (p->correction != PCI_BATCH_CORR_DIAG && p->correction != PCI_BATCH_CORR_LEARNED)
+        return set_err(h, PCI_E_INPUT, "correction must be PCI_BATCH_CORR_DIAG or PCI_BATCH_CORR_LEARNED");
     if (p->spmm_variant >= 0 && !variant_ok(nlv, p->spmm_variant))
         return set_err(h, PCI_E_INPUT, "unknown SpMM variant, or fewer lanes per row than vectors");
     for (const BlockRec &r : b->blocks)
@@ -1329,21 +1642,24 @@ int pci_batch_davidson(pci_batch_t *b, const pci_batch_params *p, double *E, dou
     auto t0 = std::chrono::steady_clock::now();
     int rc = prepare(b, nlv);
     if (rc) return rc;
+    const bool learned = p->correction == PCI_BATCH_CORR_LEARNED;
+    if (learned && (rc = learned_ready(b))) return rc;
     const int nblk = (int)b->blocks.size();
     const int variant = p->spmm_variant >= 0 ? p->spmm_variant
                         : (b->tuned_variant >= 0 && b->tuned_nv == nlv ? b->tuned_variant : DEFAULT_VARIANT);
     Bufs B = make_bufs(b, p);
     b->last_nlv = nlv;
+    if ((rc = prepare_harvest(b, B, nlv))) return rc;
 
-    // SpMM time per call, outside the solve
-    PCI_CUDA(h, cudaMemsetAsync(b->d_st, 0, sizeof(BState) * nblk, h->st));
+    // SpMM time per call (FP64 vectors, and FP32 vectors for the mixed form), outside the solve
     PCI_CUDA(h, cudaMemsetAsync(b->d_P, 0, 8 * b->rows * nlv, h->st));
-    double spmm_ms = 0.0;
-    if ((rc = time_spmm(b, nlv, variant, 2, &spmm_ms))) return rc;
+    PCI_CUDA(h, cudaMemsetAsync(b->d_P32, 0, 4 * b->rows * nlv, h->st));
+    double spmm_ms = 0.0, spmm32_ms = 0.0;
+    if ((rc = time_spmm(b, nlv, variant, 2, 1, &spmm_ms))) return rc;
+    if (mixed && (rc = time_spmm(b, nlv, variant, 2, 0, &spmm32_ms))) return rc;
 
-    cudaEvent_t e0, e1;
-    PCI_CUDA(h, cudaEventCreate(&e0));
-    PCI_CUDA(h, cudaEventCreate(&e1));
+    EventPair ev;
+    PCI_CUDA(h, ev.create());
     // initial basis: unit vectors at the nlv lowest diagonal elements of each block
     std::vector<double> D(b->rows);
     PCI_CUDA(h, cudaMemcpy(D.data(), b->d_D, 8 * b->rows, cudaMemcpyDeviceToHost));
@@ -1361,26 +1677,30 @@ int pci_batch_davidson(pci_batch_t *b, const pci_batch_params *p, double *E, dou
         BState s{};
         s.m = nlv;
         s.knew = nlv;
+        s.phase = mixed ? 0 : 1;
+        s.best = 1e300;
+        for (int j = 0; j < BT_LV; j++) s.lrn[j] = learned ? 1 : 0;
         st0[i] = s;
     }
-    int64_t *d_pos = (int64_t *)dev_alloc(h, 8 * pos.size(), &rc);
+    DevBuf d_pos;
+    d_pos.p = dev_alloc(h, 8 * pos.size(), &rc);
     if (rc) return rc;
-    PCI_CUDA(h, cudaEventRecord(e0, h->st));
-    PCI_CUDA(h, cudaMemcpyAsync(d_pos, pos.data(), 8 * pos.size(), cudaMemcpyHostToDevice, h->st));
+    PCI_CUDA(h, cudaEventRecord(ev.a, h->st));
+    PCI_CUDA(h, cudaMemcpyAsync(d_pos.p, pos.data(), 8 * pos.size(), cudaMemcpyHostToDevice, h->st));
     PCI_CUDA(h, cudaMemcpyAsync(b->d_st, st0.data(), sizeof(BState) * nblk, cudaMemcpyHostToDevice, h->st));
     PCI_CUDA(h, cudaMemsetAsync(b->d_V, 0, 8 * b->rows * BT_MS, h->st));
     PCI_CUDA(h, cudaMemsetAsync(b->d_G, 0, 8 * (int64_t)nblk * BT_MS * BT_MS, h->st));
-    kb_set_units<<<((int)pos.size() + 255) / 256, 256, 0, h->st>>>(b->d_V, b->rows, d_pos, (int)pos.size());
+    kb_set_units<<<((int)pos.size() + 255) / 256, 256, 0, h->st>>>(b->d_V, b->rows, (const int64_t *)d_pos.p,
+                                                                   (int)pos.size());
     PCI_CUDA(h, cudaGetLastError());
     PCI_CUDA(h, cudaStreamSynchronize(h->st));
-    dev_free(d_pos);
     auto t1 = std::chrono::steady_clock::now();
 
     // capture it_per_graph iterations once, replay until every block is done
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     PCI_CUDA(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
-    for (int i = 0; i < p->it_per_graph && !rc; i++) rc = enqueue_iteration(b, B, variant, nlv);
+    for (int i = 0; i < p->it_per_graph && !rc; i++) rc = enqueue_iteration(b, B, variant, nlv, mixed, learned);
     cudaError_t ce = cudaStreamEndCapture(h->st, &graph);
     if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
     if (ce != cudaSuccess) return cuda_err(h, ce, "cudaStreamEndCapture");
@@ -1402,15 +1722,18 @@ int pci_batch_davidson(pci_batch_t *b, const pci_batch_params *p, double *E, dou
     if (ce != cudaSuccess) return cuda_err(h, ce, "graph replay");
     kb_ritz<<<b->nch, 256, 0, h->st>>>(b->d_chunks, b->d_st, B);
     PCI_CUDA(h, cudaGetLastError());
-    PCI_CUDA(h, cudaEventRecord(e1, h->st));
+    PCI_CUDA(h, cudaEventRecord(ev.b, h->st));
     std::vector<BState> sf(nblk);
     PCI_CUDA(h, cudaMemcpyAsync(sf.data(), b->d_st, sizeof(BState) * nblk, cudaMemcpyDeviceToHost, h->st));
     PCI_CUDA(h, cudaStreamSynchronize(h->st));
     float total = 0.f;
-    cudaEventElapsedTime(&total, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    int maxit = 0;
+    PCI_CUDA(h, cudaEventElapsedTime(&total, ev.a, ev.b));
+    if (B.Xk) {
+        unsigned long long cnt = 0;
+        PCI_CUDA(h, cudaMemcpy(&cnt, b->d_hv_count, 8, cudaMemcpyDeviceToHost));
+        b->hv_last = (int64_t)cnt;
+    }
+    int maxit = 0, maxit32 = 0, switched = 0;
     for (int i = 0; i < nblk; i++) {
         for (int j = 0; j < nlv; j++) {
             if (E) E[(int64_t)i * nlv + j] = sf[i].theta[j];
@@ -1419,16 +1742,103 @@ int pci_batch_davidson(pci_batch_t *b, const pci_batch_params *p, double *E, dou
         if (iters) iters[i] = sf[i].iters;
         if (status) status[i] = sf[i].done;
         maxit = std::max(maxit, sf[i].iters);
+        maxit32 = std::max(maxit32, sf[i].it32);
+        switched += sf[i].phase == 1 && mixed;
     }
     if (graph_launches) *graph_launches = replays;
     b->st_total = total;
     b->st_iters = maxit;
     b->st_spmm = spmm_ms;
+    b->st_spmm32 = spmm32_ms;
+    b->st_it32 = maxit32;
+    b->st_switched = switched;
     b->st_variant = variant;
     b->st_setup = std::chrono::duration<double, std::milli>(t1 - t0).count();
-    b->st_launches = ITER_LAUNCHES;
+    b->st_launches = ITER_LAUNCHES + (mixed ? 1 : 0) + (learned ? LEARNED_LAUNCHES : 0);
     return ndone == nblk ? PCI_OK : set_err(h, PCI_E_NOT_CONVERGED, "graph replays ended before every block stopped");
 }
+
+int pci_batch_set_correction_model(pci_batch_t *b, pci_mlp_t *m)
+{
+    if (!b) return PCI_E_INPUT;
+    if (m && mlp_num_inputs(m) < 3) return set_err(&b->core, PCI_E_INPUT, "the model needs at least 3 inputs");
+    b->model = m;
+    return PCI_OK;
+}
+
+int pci_batch_set_harvest(pci_batch_t *b, int32_t rows_per_block, int64_t capacity, int32_t seed)
+{
+    if (!b) return PCI_E_INPUT;
+    if (rows_per_block < 0 || capacity < 0) return set_err(&b->core, PCI_E_INPUT, "negative harvest size");
+    b->hv_per_block = rows_per_block;
+    b->hv_cap = rows_per_block ? capacity : 0;
+    b->hv_seed = seed;
+    return PCI_OK;
+}
+
+int pci_batch_harvest(pci_batch_t *b, pci_batch_sample *out, int64_t cap, int64_t *count)
+{
+    if (!b) return PCI_E_INPUT;
+    pci_gpu *h = &b->core;
+    if (count) *count = b->hv_last;
+    if (!out || cap <= 0 || !b->d_hv) return PCI_OK;
+    const int64_t n = std::min<int64_t>(std::min<int64_t>(cap, b->hv_last), b->hv_cap);
+    if (n > 0) PCI_CUDA(h, cudaMemcpy(out, b->d_hv, (size_t)n * sizeof(pci_batch_sample), cudaMemcpyDeviceToHost));
+    return PCI_OK;
+}
+
+}  // extern "C"
+
+// Sampled rows of every block (seeded, ascending) and the sample buffers for
+// a solve that harvests; B.Xk set so kb_resid keeps the Ritz vectors.
+static int prepare_harvest(pci_batch *b, Bufs &B, int nlv)
+{
+    pci_gpu *h = &b->core;
+    B.Xk = nullptr;
+    b->hv_last = 0;
+    if (!b->hv_per_block || !b->hv_cap) return PCI_OK;
+    std::vector<int64_t> rows;
+    uint64_t st = 0x853C49E6748FEA9BULL ^ (uint64_t)(uint32_t)b->hv_seed;
+    for (const BlockRec &r : b->blocks) {
+        const int64_t k = std::min<int64_t>(b->hv_per_block, r.nd);
+        std::vector<int64_t> pick;
+        if (k == r.nd) {
+            for (int64_t n = 0; n < r.nd; n++) pick.push_back(n);
+        } else {   // Floyd's sampling of k distinct rows
+            std::vector<int64_t> chosen;
+            for (int64_t j = r.nd - k; j < r.nd; j++) {
+                st ^= st << 13; st ^= st >> 7; st ^= st << 17;
+                const int64_t t = (int64_t)(st % (uint64_t)(j + 1));
+                if (std::find(chosen.begin(), chosen.end(), t) == chosen.end()) chosen.push_back(t);
+                else chosen.push_back(j);
+            }
+            pick = chosen;
+            std::sort(pick.begin(), pick.end());
+        }
+        for (int64_t n : pick) rows.push_back(r.r0 + n);
+    }
+    int rc = 0;
+    dev_free(b->d_hv_rows);
+    dev_free(b->d_Xk);
+    b->d_hv_rows = (int64_t *)dev_alloc(h, 8 * std::max<size_t>(rows.size(), 1), &rc);
+    if (rc) return rc;
+    b->d_Xk = (double *)dev_alloc(h, 8 * (size_t)std::max<int64_t>(b->rows * nlv, 1), &rc);
+    if (rc) return rc;
+    if (!b->d_hv_count) {
+        b->d_hv_count = (unsigned long long *)dev_alloc(h, 16, &rc);
+        if (rc) return rc;
+    }
+    dev_free(b->d_hv);
+    b->d_hv = (pci_batch_sample *)dev_alloc(h, sizeof(pci_batch_sample) * (size_t)b->hv_cap, &rc);
+    if (rc) return rc;
+    PCI_CUDA(h, cudaMemcpy(b->d_hv_rows, rows.data(), 8 * rows.size(), cudaMemcpyHostToDevice));
+    PCI_CUDA(h, cudaMemset(b->d_hv_count, 0, 16));
+    b->hv_n = (int64_t)rows.size();
+    B.Xk = b->d_Xk;
+    return PCI_OK;
+}
+
+extern "C" {
 
 int pci_batch_vectors(pci_batch_t *b, int32_t blk, double *X)
 {
@@ -1446,9 +1856,10 @@ int pci_batch_vectors(pci_batch_t *b, int32_t blk, double *X)
 int pci_batch_stats(pci_batch_t *b, double *out, int32_t n)
 {
     if (!b || !out || n < 0) return PCI_E_INPUT;
-    const double v[7] = {b->st_total, b->st_iters, b->st_spmm, b->st_variant, b->st_setup, b->st_launches,
-                         b->nnz ? (double)b->full_nnz / (double)b->nnz : 0.0};
-    for (int i = 0; i < n && i < 7; i++) out[i] = v[i];
+    const double v[10] = {b->st_total, b->st_iters, b->st_spmm, b->st_variant, b->st_setup, b->st_launches,
+                          b->nnz ? (double)b->full_nnz / (double)b->nnz : 0.0, b->st_spmm32, b->st_it32,
+                          b->st_switched};
+    for (int i = 0; i < n && i < 10; i++) out[i] = v[i];
     return PCI_OK;
 }
 
@@ -1465,7 +1876,12 @@ void pci_batch_destroy(pci_batch_t *b)
     for (BlockRec &r : b->blocks) {
         csr_free(r.H);
         csr_free(r.F);
+        dev_free(r.orbs);
     }
+    dev_free(b->d_hv_rows);
+    dev_free(b->d_hv);
+    dev_free(b->d_hv_count);
+    dev_free(b->d_Xk);
     free_solve(b);
     free_tables(b);
     dev_free(b->core.d_tmp);

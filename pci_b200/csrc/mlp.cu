@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "pci_internal.h"
+#include "mlp_tc.cuh"
 
 namespace {
 
@@ -145,6 +146,35 @@ __global__ void k_to_bf16(const float *p, __nv_bfloat16 *pb, int64_t n)
 {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         pb[i] = __float2bfloat16(p[i]);
+}
+
+// Tensor-core forward pass over n rows given in compact form: orbs[i][8]
+// (occupied orbitals, 0xff = empty), f0[i], f1[i] (the last two inputs).
+__global__ void __launch_bounds__(256) k_forward_tc(mlptc::Weights W, const uint8_t *orbs, const float *f0,
+                                                    const float *f1, int64_t n, float *y)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
+    const mlptc::Smem S = mlptc::load(W, sm);
+    const int lane = threadIdx.x & 31, g = lane >> 2;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r0 = warp * 16; r0 < n; r0 += nwarps * 16) {
+        uint8_t o[2][mlptc::MAXOCC];
+        float a[2], b[2], out[2];
+        for (int r = 0; r < 2; r++) {
+            const int64_t i = r0 + g + 8 * r;
+            const bool ok = i < n;
+            for (int e = 0; e < mlptc::MAXOCC; e++) o[r][e] = ok ? orbs[i * mlptc::MAXOCC + e] : 0xff;
+            a[r] = ok ? f0[i] : 0.f;
+            b[r] = ok ? f1[i] : 0.f;
+        }
+        mlptc::tile(S, W.nin, o, a, b, out);
+        if ((lane & 3) == 0)
+            for (int r = 0; r < 2; r++) {
+                const int64_t i = r0 + g + 8 * r;
+                if (i < n) y[i] = out[r];
+            }
+    }
 }
 
 }  // namespace
@@ -460,4 +490,49 @@ int mlp_forward_device(pci_mlp *m, const float *dX, int64_t n, float *dy, cudaSt
 int mlp_num_inputs(const pci_mlp *m)
 {
     return m->nin;
+}
+
+mlptc::Weights mlp_tc_weights(const pci_mlp *m)
+{
+    mlptc::Weights W;
+    W.pb = m->pb;
+    W.p = m->p;
+    W.nin = m->nin;
+    for (int l = 0; l < NLAYER; l++) {
+        W.woff[l] = m->woff[l];
+        W.boff[l] = m->boff[l];
+    }
+    return W;
+}
+
+extern "C" int pci_mlp_forward_occ(pci_mlp_t *m, const uint8_t *orbs, const float *f0, const float *f1, int64_t n,
+                                   float *y)
+{
+    if (!m || !orbs || !f0 || !f1 || !y || n < 1) return mlp_fail(m, PCI_E_INPUT, "forward_occ: bad arguments");
+    if (m->nin < 3) return mlp_fail(m, PCI_E_INPUT, "forward_occ: the model needs nin >= 3");
+    cudaSetDevice(m->device);
+    uint8_t *d_o = nullptr;
+    float *d_a = nullptr, *d_b = nullptr, *d_y = nullptr;
+    int rc = PCI_OK;
+    const size_t sb = mlptc::smem_bytes(m->nin);
+    if (cudaMalloc(&d_o, (size_t)n * mlptc::MAXOCC) != cudaSuccess || cudaMalloc(&d_a, (size_t)n * 4) != cudaSuccess ||
+        cudaMalloc(&d_b, (size_t)n * 4) != cudaSuccess || cudaMalloc(&d_y, (size_t)n * 4) != cudaSuccess) {
+        rc = mlp_fail(m, PCI_E_OOM, "forward_occ: device allocation failed");
+    } else if (cudaFuncSetAttribute(k_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb) != cudaSuccess) {
+        rc = mlp_fail(m, PCI_E_CUDA, "forward_occ: shared memory attribute");
+    } else {
+        cudaMemcpyAsync(d_o, orbs, (size_t)n * mlptc::MAXOCC, cudaMemcpyHostToDevice, m->st);
+        cudaMemcpyAsync(d_a, f0, (size_t)n * 4, cudaMemcpyHostToDevice, m->st);
+        cudaMemcpyAsync(d_b, f1, (size_t)n * 4, cudaMemcpyHostToDevice, m->st);
+        k_forward_tc<<<148, 256, sb, m->st>>>(mlp_tc_weights(m), d_o, d_a, d_b, n, d_y);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(y, d_y, (size_t)n * 4, cudaMemcpyDeviceToHost, m->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(m->st);
+        if (e != cudaSuccess) rc = mlp_fail(m, PCI_E_CUDA, std::string("forward_occ: ") + cudaGetErrorString(e));
+    }
+    cudaFree(d_o);
+    cudaFree(d_a);
+    cudaFree(d_b);
+    cudaFree(d_y);
+    return rc;
 }

@@ -384,6 +384,35 @@ int pci_gpu_get_csr(pci_gpu_t *h, int32_t which, int64_t *rowptr, int32_t *col, 
     return PCI_OK;
 }
 
+int pci_gpu_get_csr_rows(pci_gpu_t *h, int32_t which, int64_t row_lo, int64_t row_hi, int64_t *rowptr, int32_t *col,
+                         double *val)
+{
+    if (!h) return PCI_E_INPUT;
+    cudaSetDevice(h->device);
+    const Csr &c = which == PCI_MAT_J2 ? h->J : h->H;
+    if (!c.rowptr) return set_err(h, PCI_E_STATE, "matrix not formed");
+    if (!rowptr || row_lo < 1 || row_hi < row_lo || row_hi > c.nrows)
+        return set_err(h, PCI_E_INPUT, "get_csr_rows: need 1 <= row_lo <= row_hi <= Nd and rowptr");
+    const int64_t n = row_hi - row_lo + 1;
+    PCI_CUDA(h, cudaMemcpy(rowptr, c.rowptr + (row_lo - 1), (n + 1) * 8, cudaMemcpyDeviceToHost));
+    const int64_t base = rowptr[0], cnt = rowptr[n] - base;
+    for (int64_t i = 0; i <= n; i++) rowptr[i] -= base;
+    if (col && cnt) {
+        PCI_CUDA(h, cudaMemcpy(col, c.col + base, cnt * 4, cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < cnt; i++) col[i] += 1;   // Fortran 1-based columns
+    }
+    if (val && cnt) {
+        if (c.val_f32) {
+            std::vector<float> tmp(cnt);
+            PCI_CUDA(h, cudaMemcpy(tmp.data(), (const float *)c.val + base, cnt * 4, cudaMemcpyDeviceToHost));
+            for (int64_t i = 0; i < cnt; i++) val[i] = tmp[i];
+        } else {
+            PCI_CUDA(h, cudaMemcpy(val, (const double *)c.val + base, cnt * 8, cudaMemcpyDeviceToHost));
+        }
+    }
+    return PCI_OK;
+}
+
 int pci_gpu_set_csr(pci_gpu_t *h, int32_t which, int64_t Nd, int64_t nnz, const int64_t *rowptr, const int32_t *col,
                     const double *val, double Hmin)
 {

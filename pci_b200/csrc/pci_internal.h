@@ -109,6 +109,8 @@ struct pci_gpu {
 // learned correction model (mlp.cu)
 int mlp_forward_device(pci_mlp *m, const float *dX, int64_t n, float *dy, cudaStream_t st);
 int mlp_num_inputs(const pci_mlp *m);
+namespace mlptc { struct Weights; }
+mlptc::Weights mlp_tc_weights(const pci_mlp *m);
 
 // error helpers
 int set_err(pci_gpu *h, int code, const std::string &msg);

@@ -481,6 +481,20 @@ def cfg2(seed=2):
 
 
 @_register
+def cfg3(seed=3, max_nd=1300000):
+    """Precision-form system: 4 valence electrons, 140 orbitals (n <= 24, l <= 4), even
+    parity, M_J = 0, singles + doubles from 8 reference configurations, 10 roots.  The
+    full singles-and-doubles space (well over 5M determinants) holds a Hamiltonian far
+    beyond one GPU, so the configuration list is cut at max_nd determinants: the largest
+    system whose FP64 lower triangle (about 1.1e10 stored elements) fits one B200 beside
+    the solver's buffers."""
+    shells = _shells({0: (3, 24), 1: (3, 19), 2: (3, 17), 3: (4, 16), 4: (5, 18)})
+    refs = _random_refs(shells, 4, 0, 8, 28, seed)
+    return dict(name="cfg3", shells=shells, ne=4, mj=0, parity=0, refs=refs, seed=seed, max_nd=max_nd,
+                params=dict(Nlv=10, MaxNd0=3000))
+
+
+@_register
 def mid(seed=2):
     """A config-2-like system at about 1/12 the size (3 electrons, 71 orbitals,
     ~86k determinants); used for profiling captures."""

@@ -68,9 +68,10 @@ def test_batch_header_exported_and_bound():
 
 
 def test_batch_params_layout():
-    """pci_batch_params: 4 int32, a double, 2 int32 (32 bytes, no padding)."""
+    """pci_batch_params: 4 int32, a double, 4 int32, a double, 2 int32 (56
+    bytes, no padding), field for field as the header declares them."""
     from pci_b200.capi import BatchParams
-    assert C.sizeof(BatchParams) == 32
+    assert C.sizeof(BatchParams) == 56
     hdr = open(os.path.join(ROOT, "include", "pci_batch.h")).read()
     body = hdr[hdr.index("typedef struct {"):hdr.index("} pci_batch_params;")]
     fields = re.findall(r"(int32_t|double)\s+(\w+);", body)
@@ -90,3 +91,16 @@ def test_batch_variants_and_no_device():
     rc = L.pci_batch_create(0, C.byref(b))
     assert rc == 6 and b"CUDA" in L.pci_batch_last_error(b)
     L.pci_batch_destroy(b)
+
+
+def test_batch_sample_layout():
+    """pci_batch_sample: 4 int32, an int64 and 5 doubles (64 bytes), in the
+    order of the header, as the numpy record type of the binding reads it."""
+    from pci_b200.capi import SAMPLE_DTYPE
+    assert SAMPLE_DTYPE.itemsize == 64
+    hdr = open(os.path.join(ROOT, "include", "pci_batch.h")).read()
+    body = hdr[hdr.index("typedef struct {", hdr.index("} pci_batch_params;")):hdr.index("} pci_batch_sample;")]
+    names = []
+    for typ, rest in re.findall(r"(int32_t|int64_t|double)\s+([\w, ]+);", body):
+        names += [x.strip() for x in rest.split(",")]
+    assert names == list(SAMPLE_DTYPE.names)
