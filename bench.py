@@ -62,6 +62,12 @@ def parse():
     ap.add_argument("--no-batched", dest="batched", action="store_false", help="skip the batched form")
     ap.add_argument("--no-roots", dest="roots", action="store_false",
                     help="skip the time-to-roots solves of the configuration")
+    ap.add_argument("--roots-config", default="cfg3", help="configuration of the time-to-roots section")
+    ap.add_argument("--no-learned", dest="learned", action="store_false",
+                    help="skip the learned form of the time-to-roots section")
+    ap.add_argument("--learn-nd", type=int, default=30000,
+                    help="determinants of each training system of the learned correction")
+    ap.add_argument("--switch-tol", type=float, default=1e-5, help="residual that ends the FP32 phase")
     ap.add_argument("--batch-blocks", type=int, default=64)
     ap.add_argument("--batch-variant", type=int, default=-1, help="SpMM variant of the batched form "
                     "(-1: from the tuning cache, tuned when absent)")
@@ -343,11 +349,13 @@ def run_ours(args):
         line["cpu_baseline"] = {"value": n / t, "unit": "nnz/s", "cores": os.cpu_count() or 1, "kind": "port",
                                 "sample": f"{r} random rows of FormH ({n} non-zeros, {t:.1f} s), oracle "
                                           f"restatement of src/pconf.F90:1227-1290 with OpenMP"}
-    if args.roots:
-        line["time_to_roots"] = time_to_roots(args, eng, sysm, local, dist, peak, peak_kind)
     eng.close()
+    if args.roots:
+        flush = None
+        torch.cuda.empty_cache()
+        line["time_to_roots"] = time_to_roots(args, local, dist, peak, peak_kind)
     if args.batched:
-        del flush
+        flush = None
         torch.cuda.empty_cache()
         line["batched"] = run_batched(args, local, rank, world, dist, peak, peak_kind)
     if rank == 0:
@@ -357,42 +365,147 @@ def run_ours(args):
     return 0
 
 
-def time_to_roots(args, eng, sysm, local, dist, peak, peak_kind):
-    """The configuration's Nlv roots to a residual 2-norm of 1e-8 through the
-    batched solver with one block (the reference's restarted Davidson stalls
-    on these inputs): H formed on the device in FP64 (plain) and in FP32
-    (mixed: FP32 values, FP64 vectors and sums), each timed as FormH + solve."""
-    from pci_b200.capi import Batch
+def spmm_bytes(numh, nd, nlv, value_bytes, vec_bytes):
+    """Algorithmic bytes of one lower-triangle SpMM over nlv vectors: every stored
+    element (column index + value) read once, X read once, Y written once."""
+    return numh * (4 + value_bytes) + (nd + 1) * 8 + 2 * nd * nlv * vec_bytes
+
+
+def cpu_solve_estimate(sysm, nlv, iterations, numh, seed, threads):
+    """CPU time to the roots on the host cores, from a bounded sample: the
+    oracle's FormH over sampled rows (its nnz/s) and its Mxmpy over the sampled
+    rows' CSR for nlv vectors (stored elements per second), scaled to the full
+    matrix with the GPU run's iteration count (same algorithm and basis)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ctypes as C
+    import oracle as O
+    o = O.Oracle(sysm)
+    rng = np.random.default_rng(seed)
+    wins = sorted(rng.choice(np.arange(1, sysm.nd - 40), 40, replace=False))
+    t0 = time.perf_counter()
+    parts = [o.form_h(int(a), int(a) + 39, threads=threads) for a in wins]
+    t_build = time.perf_counter() - t0
+    n_build = sum(int(p[0][-1]) for p in parts)
+    # Mxmpy over the sampled rows, full-length vectors, all host cores
+    rows = np.concatenate([np.arange(int(a), int(a) + 40, dtype=np.int64) for a in wins])
+    rp = np.concatenate([[0], np.cumsum(np.concatenate([np.diff(p[0]) for p in parts]))]).astype(np.int64)
+    col = np.ascontiguousarray(np.concatenate([p[1] for p in parts]).astype(np.int32))
+    val = np.ascontiguousarray(np.concatenate([p[2] for p in parts]))
+    X = np.ascontiguousarray(rng.standard_normal((nlv, sysm.nd)))
+    Y = np.zeros((nlv, sysm.nd))
+    L = O.lib()
+    f = L.orc_mxmpy_rows
+    f.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                  C.c_void_p, C.c_int]
+    t0 = time.perf_counter()
+    reps = 0
+    while time.perf_counter() - t0 < 3.0:
+        f(sysm.nd, rows.size, rows.ctypes.data, rp.ctypes.data, col.ctypes.data, val.ctypes.data, nlv,
+          X.ctypes.data, Y.ctypes.data, threads)
+        reps += 1
+    t_mx = (time.perf_counter() - t0) / reps
+    build_rate = n_build / t_build
+    mx_rate = col.size / t_mx
+    est_s = numh / build_rate + iterations * numh / mx_rate
+    return {"value_ms": 1e3 * est_s, "unit": "ms (estimate from a sample)", "cores": threads, "kind": "port",
+            "formh_nnz_per_s": build_rate, "mxmpy_elements_per_s": mx_rate, "iterations": iterations,
+            "sample": f"FormH of 40 windows of 40 rows ({n_build} non-zeros, {t_build:.1f} s) and Mxmpy of those "
+                      f"rows for {nlv} vectors ({reps} passes), oracle restatements of src/pconf.F90:1227-1290 and "
+                      f"src/davidson.f90:572-647 with OpenMP; scaled to NumH = {numh} and the GPU run's "
+                      f"{iterations} iterations"}
+
+
+def train_correction(args, sysm_kw, nlv, local):
+    """The learned correction's network for a configuration: samples harvested
+    from the solver's own converged FP64 runs of smaller systems on the same
+    orbital basis at other seeds (100-103), trained on the GPU."""
+    from pci_b200 import learned as LR
+    from pci_b200 import system as S
+    t0 = time.perf_counter()
+    systems = []
+    for sd in range(100, 104):
+        kw = dict(sysm_kw)
+        kw.update(seed=sd, max_nd=args.learn_nd)
+        systems.append(S.make_system(**kw))
+    F, T, info = LR.harvest(systems, nlv=nlv, rows_per_block=4000, device=local, max_sub=96, keep=48)
+    model, loss = LR.train(F, T, device=local, epochs=4)
+    return model, {"train_systems": f"{len(systems)} systems, seeds 100-103, {args.learn_nd} determinants each "
+                                    f"(same orbital basis)", "samples": int(F.shape[0]), "loss": loss,
+                   "seconds": time.perf_counter() - t0}
+
+
+def time_to_roots(args, local, dist, peak, peak_kind):
+    """The configuration's Nlv roots to a residual 2-norm of 1e-8 against the
+    FP64 Hamiltonian through the batched solver with one block, in three
+    forms, each timed as FormH + solve (device time):
+      fp64           FP64 H, FP64 SpMM, diagonal correction (plain);
+      mixed          H split into FP32 hi + lo, FP32 SpMM phase, FP64 phase to the criterion;
+      learned_mixed  the mixed form with the learned correction."""
+    from pci_b200 import system as S
+    from pci_b200.capi import PCI_BATCH_CORR_LEARNED, PCI_BATCH_FP64, PCI_BATCH_MIXED, Batch, Engine
+    kw = S.CONFIGS[args.roots_config]()
+    sysm = S.make_system(**kw)
     nlv = int(sysm.params["Nlv"])
-    out = {"workload": f"{args.config}: Nd={sysm.nd}, {nlv} roots, residual 2-norm <= 1e-8 per root",
+    out = {"workload": f"{args.roots_config}: Nd={sysm.nd}, Ne={sysm.ne}, Nsu={sysm.nsu}, {nlv} roots, residual "
+                       f"2-norm <= 1e-8 per root against the FP64 H",
            "metric": "time to all roots (FormH + solve), ms", "solver": "batched block Davidson, one block, "
            "subspace 96, 48 kept at a restart"}
+    model = None
+    if args.learned:
+        model, out["learned_training"] = train_correction(args, kw, nlv, local)
+    forms = [("fp64", 64, PCI_BATCH_FP64, None), ("mixed", 48, PCI_BATCH_MIXED, None)]
+    if model is not None:
+        forms.append(("learned_mixed", 48, PCI_BATCH_MIXED, model))
     E = {}
-    for prec, key in ((64, "fp64"), (32, "mixed_fp32_h")):
-        numh, _, _ = eng.form_h(prec)
-        fh = eng.stats()["formh_ms"]
-        b = Batch(local)
-        b.set_value_prec(prec)
-        b.add_engine(eng)
-        variant, tune_ms, cached = b.tune(nlv, tune_cache_path(args.tune_cache))
-        # subspace 96 with 48 kept at a restart: config 2 measured 26.5 s against
-        # 27.6 s for 96/36, 28.3 s for 96/24 and 32.6 s for 64/24 (FP32 H)
-        r = b.davidson(nlv=nlv, max_sub=96, keep=48, max_it=400, tol=1e-8, it_per_graph=4)
+    launches = 0
+    for key, vp, prec, mdl in forms:
+        with Engine(local) as e:
+            e.load_system(sysm)
+            numh, _, _ = e.form_h(64)
+            st_h = e.stats()
+            fh = st_h["formh_ms"]
+            launches += int(st_h["formh_launches"]) + 1
+            b = Batch(local)
+            b.set_value_prec(vp)
+            b.add_engine(e)
+        kwd = dict(nlv=nlv, max_sub=96, keep=48, max_it=400, tol=1e-8, it_per_graph=4, precision=prec,
+                   switch_tol=args.switch_tol)
+        if mdl is not None:
+            b.set_correction_model(mdl)
+            kwd["correction"] = PCI_BATCH_CORR_LEARNED
+        r = b.davidson(**kwd)
         st = b.stats()
         b.close()
         solve = max_over_ranks(st["total_ms"], dist, device=f"cuda:{local}")
         fh = max_over_ranks(fh, dist, device=f"cuda:{local}")
-        sp_bytes = numh * (4 + prec // 8) + sysm.nd * 12 + 2 * sysm.nd * nlv * 8
-        ach = sp_bytes / (st["spmm_ms"] * 1e-3) / 1e9
+        launches += int(r["graph_launches"]) * kwd["it_per_graph"] * int(st["launches_per_iteration"])
+        sp = spmm_bytes(numh, sysm.nd, nlv, 8, 8)
+        ach = sp / (st["spmm_ms"] * 1e-3) / 1e9
         E[key] = r["E"][0]
-        out[key] = {"value_ms": fh + solve, "formh_ms": fh, "solve_ms": solve, "iterations": int(r["iters"][0]),
-                    "converged": bool(r["status"][0] == 1), "max_residual": float(np.max(r["rnorm"])),
-                    "spmm_ms_per_call": st["spmm_ms"], "spmm_variant": variant,
-                    "spmm_roofline": {"bound": "hbm", "kernel": "kb_spmm", "achieved": ach, "peak": peak,
-                                      "peak_kind": peak_kind, "unit": "GB/s", "frac": ach / peak,
-                                      "algorithmic_bytes": int(sp_bytes)}}
-    out["abs_dE_mixed_vs_fp64_per_root"] = [float(x) for x in np.abs(E["mixed_fp32_h"] - E["fp64"])]
-    out["speedup_mixed_vs_fp64"] = out["fp64"]["value_ms"] / out["mixed_fp32_h"]["value_ms"]
+        rec = {"value_ms": fh + solve, "formh_ms": fh, "solve_ms": solve, "iterations": int(r["iters"][0]),
+               "converged": bool(r["status"][0] == 1), "max_residual": float(np.max(r["rnorm"])),
+               "spmm_ms_per_call": st["spmm_ms"], "numh": int(numh),
+               "spmm_roofline": {"bound": "hbm", "kernel": "SpMM, FP64 vectors", "achieved": ach, "peak": peak,
+                                 "peak_kind": peak_kind, "unit": "GB/s", "frac": ach / peak,
+                                 "algorithmic_bytes": int(sp)}}
+        if prec == PCI_BATCH_MIXED:
+            sp32 = spmm_bytes(numh, sysm.nd, nlv, 4, 4)
+            a32 = sp32 / (st["spmm32_ms"] * 1e-3) / 1e9
+            rec.update(fp32_iterations=int(st["fp32_iterations"]), spmm32_ms_per_call=st["spmm32_ms"],
+                       spmm32_roofline={"bound": "hbm", "kernel": "SpMM, FP32 vectors and hi values", "achieved": a32,
+                                        "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": a32 / peak,
+                                        "algorithmic_bytes": int(sp32)})
+        out[key] = rec
+    for key in E:
+        if key != "fp64":
+            out[f"abs_dE_{key}_vs_fp64_per_root"] = [float(x) for x in np.abs(E[key] - E["fp64"])]
+            out[f"speedup_{key}_vs_fp64"] = out["fp64"]["value_ms"] / out[key]["value_ms"]
+    if model is not None:
+        model.close()
+    out["gpu_launches"] = launches
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_solve_estimate(sysm, nlv, out["fp64"]["iterations"], out["fp64"]["numh"], 11,
+                                                 os.cpu_count() or 1)
     return out
 
 

@@ -580,6 +580,37 @@ void orc_mxmpy_block(int64_t nd, const int64_t *rowptr, const int32_t *col, cons
     free(buf);
 }
 
+/* Mxmpy (src/davidson.f90:572-647) over a subset of rows, for the timed CPU
+ * baseline: rows[0..nrows) (1-based) with their CSR slices rp[nrows+1] into
+ * col (1-based) / val, nv vectors column-major [nd, nv].  OpenMP over the
+ * rows; the row part goes to the row's own entry, the transpose part is added
+ * atomically into the full-length vectors. */
+void orc_mxmpy_rows(int64_t nd, int64_t nrows, const int64_t *rows, const int64_t *rp, const int32_t *col,
+                    const double *val, int nv, const double *x, double *y, int nthreads)
+{
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t i = 0; i < nrows; i++) {
+        const int64_t n = rows[i];
+        for (int64_t l = rp[i]; l < rp[i + 1]; l++) {
+            const int64_t k = col[l];
+            const double t = val[l];
+            for (int v = 0; v < nv; v++) {
+                const double a = t * x[(size_t)v * nd + k - 1];
+#pragma omp atomic
+                y[(size_t)v * nd + n - 1] += a;
+                if (n != k) {
+                    const double b = t * x[(size_t)v * nd + n - 1];
+#pragma omp atomic
+                    y[(size_t)v * nd + k - 1] += b;
+                }
+            }
+        }
+    }
+}
+
 /* J_av, src/formj2.f90:355-387: <x|J^2|x> over rows/cols <= nx, returned as J. */
 double orc_j_av(int64_t nd, const int64_t *rowptr, const int32_t *col, const double *val,
                 const double *x, int64_t nx)

@@ -127,19 +127,19 @@ __global__ void k_split(double *a, int64_t n)
     }
 }
 
-__global__ void kb_diag(const BlkCsr *blks, const int32_t *row_blk, int64_t rows, double *D)
+// Diagonal of one block's lower-triangle CSR (values FP64, FP32 or split pairs).
+__global__ void kb_diag_blk(const int64_t *rowptr, const int32_t *col, const void *val, int f64, int split, int64_t nd,
+                            double *D)
 {
-    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < rows; n += (int64_t)gridDim.x * blockDim.x) {
-        const BlkCsr B = blks[row_blk[n]];
-        const int64_t ln = n - B.r0;
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nd; n += (int64_t)gridDim.x * blockDim.x) {
         double d = 0.0;
-        for (int64_t l = B.rowptr[ln + 1] - 1; l >= B.rowptr[ln]; l--)
-            if (B.col[l] == ln) {
-                if (B.f64) d = ((const double *)B.val)[l];
-                else if (B.split) {
-                    const float2 hl = ((const float2 *)B.val)[l];
+        for (int64_t l = rowptr[n + 1] - 1; l >= rowptr[n]; l--)
+            if (col[l] == n) {
+                if (f64) d = ((const double *)val)[l];
+                else if (split) {
+                    const float2 hl = ((const float2 *)val)[l];
                     d = (double)hl.x + (double)hl.y;
-                } else d = (double)((const float *)B.val)[l];
+                } else d = (double)((const float *)val)[l];
                 break;
             }
         D[n] = d;
@@ -157,16 +157,18 @@ __global__ void kb_set_units(double *V, int64_t ld, const int64_t *pos, int n)
 // Value of stored element l as the arithmetic type XT of the SpMM: FP32
 // vectors take the FP32 value (hi of a split pair), FP64 vectors the FP64
 // value (hi + lo of a split pair).
+// The matrix is read once per SpMM: its loads are streaming (evict-first),
+// so the vectors X and Y stay in L2 while the stored elements pass through.
 template <typename XT>
 __device__ __forceinline__ XT blk_val(const BlkCsr &B, int64_t l)
 {
-    if (B.f64) return (XT)__ldg(&((const double *)B.val)[l]);
+    if (B.f64) return (XT)__ldcs(&((const double *)B.val)[l]);
     if (B.split) {
-        const float2 hl = __ldg(&((const float2 *)B.val)[l]);
+        const float2 hl = __ldcs(&((const float2 *)B.val)[l]);
         if (sizeof(XT) == 4) return (XT)hl.x;
         return (XT)((double)hl.x + (double)hl.y);
     }
-    return (XT)__ldg(&((const float *)B.val)[l]);
+    return (XT)__ldcs(&((const float *)B.val)[l]);
 }
 
 // Row n (local row ln) of block B for vector v: the row part of the product
@@ -186,7 +188,7 @@ __device__ __forceinline__ XT spmm_row(const BlkCsr &B, int64_t ln, int64_t n, i
             XT t[4], xk[4];
 #pragma unroll
             for (int u = 0; u < 4; u++) {
-                k[u] = __ldg(&B.col[l + u * G]);
+                k[u] = __ldcs(&B.col[l + u * G]);
                 t[u] = blk_val<XT>(B, l + u * G);
             }
 #pragma unroll
@@ -194,7 +196,7 @@ __device__ __forceinline__ XT spmm_row(const BlkCsr &B, int64_t ln, int64_t n, i
 #pragma unroll
             for (int u = 0; u < 4; u++) acc += t[u] * xk[u];
         }
-        for (; l < l1; l += G) acc += blk_val<XT>(B, l) * __ldg(&X[(B.r0 + __ldg(&B.col[l])) * NV + v]);
+        for (; l < l1; l += G) acc += blk_val<XT>(B, l) * __ldg(&X[(B.r0 + __ldcs(&B.col[l])) * NV + v]);
         return acc;
     }
     const XT xn = __ldg(&X[n * NV + v]);
@@ -204,7 +206,7 @@ __device__ __forceinline__ XT spmm_row(const BlkCsr &B, int64_t ln, int64_t n, i
         XT t[4], xk[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-            k[u] = __ldg(&B.col[l + u * G]);
+            k[u] = __ldcs(&B.col[l + u * G]);
             t[u] = blk_val<XT>(B, l + u * G);
         }
 #pragma unroll
@@ -216,7 +218,7 @@ __device__ __forceinline__ XT spmm_row(const BlkCsr &B, int64_t ln, int64_t n, i
         }
     }
     for (; l < l1; l += G) {
-        const int k = __ldg(&B.col[l]);
+        const int k = __ldcs(&B.col[l]);
         const XT t = blk_val<XT>(B, l);
         const int64_t kg = B.r0 + k;
         if (k != ln) atomicAdd(&Y[kg * NV + v], t * xn);
@@ -1038,6 +1040,7 @@ struct BlockRec {
     int split = 0;    // H.val holds {hi, lo} float pairs (value precision 48)
     uint8_t *orbs = nullptr;   // [nd][8] occupied orbitals of each row (from the handle's basis), or null
     int nsu = 0;               // orbitals of the block's basis (0 without a basis)
+    double *D = nullptr;       // diagonal H_nn
 };
 
 struct pci_batch {
@@ -1149,8 +1152,10 @@ static int build_tables(pci_batch *b)
     PCI_CUDA(h, cudaMemcpy(b->d_chunks, ch.data(), sizeof(Chunk) * ch.size(), cudaMemcpyHostToDevice));
     PCI_CUDA(h, cudaMemcpy(b->d_cb, cb.data(), 8 * cb.size(), cudaMemcpyHostToDevice));
     b->nch = (int)ch.size();
-    kb_diag<<<b->nsm * 8, 256, 0, h->st>>>(b->d_blk, b->d_row_blk, b->rows, b->d_D);
-    PCI_CUDA(h, cudaGetLastError());
+    for (int i = 0; i < nblk; i++) {
+        const BlockRec &r = b->blocks[i];
+        PCI_CUDA(h, cudaMemcpyAsync(b->d_D + r.r0, r.D, 8 * r.nd, cudaMemcpyDeviceToDevice, h->st));
+    }
     PCI_CUDA(h, cudaStreamSynchronize(h->st));
     b->dirty = false;
     return PCI_OK;
@@ -1220,6 +1225,14 @@ static int set_attrs(pci_batch *b)
     return PCI_OK;
 }
 
+// One SpMM of every running block in `phase`.
+template <typename XT>
+static cudaError_t spmm_all(pci_batch *b, int nv, int variant, cudaStream_t st, int phase, const XT *X, XT *Y)
+{
+    launch_spmm<XT>(nv, variant, b->nsm, st, b->d_blk, b->d_row_blk, b->d_st, b->rows, phase, X, Y);
+    return cudaGetLastError();
+}
+
 // One iteration of every running block (25 launches, one more for the FP32
 // SpMM of the mixed-precision form, one more for the learned correction and
 // one more while harvesting samples; no host synchronisation).
@@ -1229,8 +1242,8 @@ static int enqueue_iteration(pci_batch *b, const Bufs &B, int variant, int nv, b
     cudaStream_t st = h->st;
     const int nch = b->nch, nblk = (int)b->blocks.size();
     kb_pack<<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
-    if (mixed) launch_spmm<float>(nv, variant, b->nsm, st, b->d_blk, b->d_row_blk, b->d_st, b->rows, 0, B.P32, B.Q32);
-    launch_spmm<double>(nv, variant, b->nsm, st, b->d_blk, b->d_row_blk, b->d_st, b->rows, 1, B.P, B.Q);
+    if (mixed) PCI_CUDA(h, spmm_all<float>(b, nv, variant, st, 0, B.P32, B.Q32));
+    PCI_CUDA(h, spmm_all<double>(b, nv, variant, st, 1, B.P, B.Q));
     kb_tn<TN_GRAM><<<nch, 256, 0, st>>>(b->d_chunks, b->d_st, B);
     kb_fin<FIN_GRAM><<<nblk, BT_FIN_THREADS, 0, st>>>(b->d_cb, b->d_st, B);
     kb_eig<<<nblk, 256, 2 * BT_MS * BT_MS * 8, st>>>(b->d_st, B);
@@ -1325,17 +1338,15 @@ static int time_spmm(pci_batch *b, int nv, int variant, int reps, int phase, dou
     PCI_CUDA(h, ev.create());
     kb_set_phase<<<(nblk + 127) / 128, 128, 0, h->st>>>(b->d_st, nblk, phase);
     auto one = [&]() {
-        if (phase) launch_spmm<double>(nv, variant, b->nsm, h->st, b->d_blk, b->d_row_blk, b->d_st, b->rows, 1,
-                                       b->d_P, b->d_Q);
-        else launch_spmm<float>(nv, variant, b->nsm, h->st, b->d_blk, b->d_row_blk, b->d_st, b->rows, 0, b->d_P32,
-                                b->d_Q32);
+        return phase ? spmm_all<double>(b, nv, variant, h->st, 1, b->d_P, b->d_Q)
+                     : spmm_all<float>(b, nv, variant, h->st, 0, b->d_P32, b->d_Q32);
     };
-    one();
+    PCI_CUDA(h, one());
     PCI_CUDA(h, cudaEventRecord(ev.a, h->st));
     for (int r = 0; r < reps; r++) {
         if (phase) PCI_CUDA(h, cudaMemsetAsync(b->d_Q, 0, 8 * b->rows * nv, h->st));
         else PCI_CUDA(h, cudaMemsetAsync(b->d_Q32, 0, 4 * b->rows * nv, h->st));
-        one();
+        PCI_CUDA(h, one());
     }
     PCI_CUDA(h, cudaEventRecord(ev.b, h->st));
     PCI_CUDA(h, cudaGetLastError());
@@ -1409,7 +1420,7 @@ static int prepare(pci_batch *b, int nlv)
 
 // Revision of the SpMM kernels, part of the cache key: cached picks of an
 // older kernel are not reused.
-static const int SPMM_REV = 5;
+static const int SPMM_REV = 7;
 
 static std::string tune_key(pci_batch *b, int nv)
 {
@@ -1517,6 +1528,15 @@ int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index)
         r.H.val_f32 = 1;
         h->H.val = v;
         h->H.val_f32 = 1;
+    }
+    {   // the block's diagonal, while its CSR columns are there
+        int rc = 0;
+        r.D = (double *)dev_alloc(c, 8 * (size_t)std::max<int64_t>(r.nd, 1), &rc);
+        if (rc) return rc;
+        kb_diag_blk<<<b->nsm * 8, 256, 0, c->st>>>(r.H.rowptr, r.H.col, r.H.val, (r.H.val_f32 || r.split) ? 0 : 1,
+                                                   r.split, r.nd, r.D);
+        PCI_CUDA(c, cudaGetLastError());
+        PCI_CUDA(c, cudaStreamSynchronize(c->st));
     }
     h->H = Csr();
     csr_free(h->Hfull);
@@ -1877,6 +1897,7 @@ void pci_batch_destroy(pci_batch_t *b)
         csr_free(r.H);
         csr_free(r.F);
         dev_free(r.orbs);
+        dev_free(r.D);
     }
     dev_free(b->d_hv_rows);
     dev_free(b->d_hv);
