@@ -439,8 +439,13 @@ def time_to_roots(args, local, dist, peak, peak_kind):
     FP64 Hamiltonian through the batched solver with one block, in three
     forms, each timed as FormH + solve (device time):
       fp64           FP64 H, FP64 SpMM, diagonal correction (plain);
-      mixed          H split into FP32 hi + lo, FP32 SpMM phase, FP64 phase to the criterion;
-      learned_mixed  the mixed form with the learned correction."""
+      mixed          FP64 H; SpMM on FP32 vectors with FP32 sums and the values rounded to
+                     FP32 while every residual is above switch_tol (or until the FP32 sums
+                     stop it dropping), then FP64 SpMM to the criterion;
+      learned_mixed  the mixed form with the learned correction.
+    Each SpMM is also set against the measured throughput of its transpose
+    part's global FP64 reductions (pci_batch_probe_reduction), the limit it
+    actually meets: nnz x vectors reduced words per call."""
     from pci_b200 import system as S
     from pci_b200.capi import PCI_BATCH_CORR_LEARNED, PCI_BATCH_FP64, PCI_BATCH_MIXED, Batch, Engine
     kw = S.CONFIGS[args.roots_config]()
@@ -453,9 +458,12 @@ def time_to_roots(args, local, dist, peak, peak_kind):
     model = None
     if args.learned:
         model, out["learned_training"] = train_correction(args, kw, nlv, local)
-    forms = [("fp64", 64, PCI_BATCH_FP64, None), ("mixed", 48, PCI_BATCH_MIXED, None)]
+    forms = [("fp64", 64, PCI_BATCH_FP64, None), ("mixed", 64, PCI_BATCH_MIXED, None)]
     if model is not None:
-        forms.append(("learned_mixed", 48, PCI_BATCH_MIXED, model))
+        forms.append(("learned_mixed", 64, PCI_BATCH_MIXED, model))
+    from pci_b200.capi import probe_reduction
+    red_peak = probe_reduction(local, sysm.nd, nlv)
+    out["l2_reduction_peak_gbs"] = red_peak
     E = {}
     launches = 0
     for key, vp, prec, mdl in forms:
@@ -482,12 +490,16 @@ def time_to_roots(args, local, dist, peak, peak_kind):
         sp = spmm_bytes(numh, sysm.nd, nlv, 8, 8)
         ach = sp / (st["spmm_ms"] * 1e-3) / 1e9
         E[key] = r["E"][0]
+        red = numh * nlv * 8 / (st["spmm_ms"] * 1e-3) / 1e9
         rec = {"value_ms": fh + solve, "formh_ms": fh, "solve_ms": solve, "iterations": int(r["iters"][0]),
                "converged": bool(r["status"][0] == 1), "max_residual": float(np.max(r["rnorm"])),
                "spmm_ms_per_call": st["spmm_ms"], "numh": int(numh),
                "spmm_roofline": {"bound": "hbm", "kernel": "SpMM, FP64 vectors", "achieved": ach, "peak": peak,
                                  "peak_kind": peak_kind, "unit": "GB/s", "frac": ach / peak,
-                                 "algorithmic_bytes": int(sp)}}
+                                 "algorithmic_bytes": int(sp)},
+               "spmm_l2_reduction": {"bound": "L2 reductions", "achieved": red, "peak": red_peak,
+                                     "peak_kind": "measured (pci_batch_probe_reduction)", "unit": "GB/s",
+                                     "frac": red / red_peak, "reduced_bytes": int(numh * nlv * 8)}}
         if prec == PCI_BATCH_MIXED:
             sp32 = spmm_bytes(numh, sysm.nd, nlv, 4, 4)
             a32 = sp32 / (st["spmm32_ms"] * 1e-3) / 1e9

@@ -138,10 +138,12 @@ int pci_batch_vectors(pci_batch_t *b, int32_t blk, double *X);
 int pci_batch_stats(pci_batch_t *b, double *out, int32_t n);
 
 /* Attach a trained model (pci_gpu.h) for correction = PCI_BATCH_CORR_LEARNED;
- * NULL detaches.  Its first nin - 2 inputs are the occupation counts of the
- * orbitals, input nin - 2 is H_nn - theta and input nin - 1 the residual
- * entry times sqrt(nd) / |r|; every block must come from a handle with a
- * basis of at most nin - 2 orbitals.  The model must outlive its use.  No
+ * NULL detaches.  Its first nin - 3 inputs are the occupation counts of the
+ * orbitals; with s = sqrt(nd) / |r|, input nin - 3 is H_nn - theta, input
+ * nin - 2 the residual entry r_n s and input nin - 1 the diagonal correction
+ * r_n s / (theta - H_nn) (denominator at least 1e-8 in size, value clipped to
+ * +-1e4); every block must come from a handle with a basis of at most
+ * nin - 3 orbitals.  The model must outlive its use.  No
  * counterpart in the reference, whose only correction is Dvdsn's diagonal one
  * (davidson.f90:436-570). */
 int pci_batch_set_correction_model(pci_batch_t *b, pci_mlp_t *m);
@@ -154,6 +156,13 @@ int pci_batch_set_harvest(pci_batch_t *b, int32_t rows_per_block, int64_t capaci
 /* Samples of the last solve: up to cap into out (may be NULL); *count
  * receives the number recorded (above the capacity, the rest were dropped). */
 int pci_batch_harvest(pci_batch_t *b, pci_batch_sample *out, int64_t cap, int64_t *count);
+
+/* Measured throughput of the SpMM's transpose part on this device: FP64
+ * reductions by teams of nv lanes onto nv consecutive words at random rows of
+ * a rows x nv array (rows = the SpMM's row count), as GB/s of reduced data.
+ * The lower-triangle SpMM adds nnz * nv such words per call, so this is the
+ * roofline that bounds it.  Allocates rows * nv * 8 bytes for the probe. */
+int pci_batch_probe_reduction(int32_t device, int64_t rows, int32_t nv, double *gbs);
 
 const char *pci_batch_last_error(pci_batch_t *b);
 void pci_batch_destroy(pci_batch_t *b);

@@ -193,10 +193,10 @@ int pci_mlp_forward(pci_mlp_t *m, const float *X, int64_t n, float *y);
  * the batched solver's learned correction: orbs[n x 8] holds each row's
  * occupied orbitals (0-based, an orbital listed once per electron in it,
  * 0xff = empty slot; these are the non-zero occupation counts of inputs
- * 0..nin-3), f0[n] and f1[n] inputs nin-2 and nin-1 (host arrays).  The
+ * 0..nin-4), f[n x 3] inputs nin-3, nin-2 and nin-1 (host arrays).  The
  * hidden activations are rounded to BF16 for the tensor-core products, so
  * y agrees with pci_mlp_forward on the same rows to about 1e-2 relative. */
-int pci_mlp_forward_occ(pci_mlp_t *m, const uint8_t *orbs, const float *f0, const float *f1, int64_t n, float *y);
+int pci_mlp_forward_occ(pci_mlp_t *m, const uint8_t *orbs, const float *f, int64_t n, float *y);
 /* Mean squared error against T[n] and its gradient (length num_params,
  * may be NULL) for X[n x nin] (host arrays). */
 int pci_mlp_loss_grad(pci_mlp_t *m, const float *X, const float *T, int64_t n, float *loss, float *grad);

@@ -39,6 +39,26 @@ int pci_io_read_csr_header(const char *path, int64_t *nd, int64_t *nnz, int32_t 
 int pci_io_read_csr(const char *path, int64_t nd, int64_t nnz, int64_t *rowptr, int32_t *col, void *val,
                     int32_t val_bytes, char *errbuf, int32_t errlen);
 
+/* ---- CONF.HIJ / CONF.JJJ (stream) ------------------------------------------
+ * The sorted element stream that pCI's sort program writes from pconf's
+ * parallel matrix file (src/sort.f90:16-80) and that pol / ine read
+ * (ReadHIJ, src/pol.f90:766-797): int64 count, then count records of int32
+ * row, int32 column (1-based, column <= row) and real64 value, rows
+ * ascending and columns ascending within a row, exact zeros left out.
+ * rowptr/col/val are a lower-triangle CSR as pci_gpu_get_csr returns it
+ * (0-based row prefix, 1-based columns). */
+int pci_io_write_hij(const char *path, int64_t nd, const int64_t *rowptr, const int32_t *col, const double *val,
+                     char *errbuf, int32_t errlen);
+/* The same stream written in row ranges (to stream a matrix too large for
+ * host memory, e.g. from pci_gpu_get_csr_rows): rows row0+1 .. row0+nrows of
+ * a CSR slice (rowptr[nrows+1], any base; col/val indexed from rowptr[0]).
+ * row0 = 0 creates the file; later ranges must follow in row order. */
+int pci_io_append_hij(const char *path, int64_t row0, int64_t nrows, const int64_t *rowptr, const int32_t *col,
+                      const double *val, char *errbuf, int32_t errlen);
+/* *count = the file's record count; up to cap records into row/col/val. */
+int pci_io_read_hij(const char *path, int64_t cap, int32_t *row, int32_t *col, double *val, int64_t *count,
+                    char *errbuf, int32_t errlen);
+
 /* ---- CONF.XIJ (sequential) -----------------------------------------------
  * One record per level n: Tk(n) (r8), Tj(n) (r8), Nd (i4), x(1:Nd) (r8), as
  * WriteXIJ / WriteFinalXIJ write them (src/pconf.F90:2536-2602).  X is

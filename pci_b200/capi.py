@@ -30,7 +30,7 @@ BATCH_EXPORTS = ["pci_batch_create", "pci_batch_add_block", "pci_batch_set_stora
                  "pci_batch_info", "pci_batch_tune",
                  "pci_batch_variant", "pci_batch_davidson", "pci_batch_vectors", "pci_batch_stats",
                  "pci_batch_last_error", "pci_batch_destroy", "pci_batch_set_correction_model",
-                 "pci_batch_set_harvest", "pci_batch_harvest"]
+                 "pci_batch_set_harvest", "pci_batch_harvest", "pci_batch_probe_reduction"]
 PCI_BATCH_FP64, PCI_BATCH_MIXED = 0, 1
 PCI_BATCH_CORR_DIAG, PCI_BATCH_CORR_LEARNED = 0, 1
 SAMPLE_DTYPE = np.dtype([("blk", np.int32), ("iter", np.int32), ("root", np.int32), ("phase", np.int32),
@@ -122,7 +122,8 @@ def load(path: str = LIB):
     L.pci_batch_set_correction_model.argtypes = [P, P]
     L.pci_batch_set_harvest.argtypes = [P, i32, i64, i32]
     L.pci_batch_harvest.argtypes = [P, P, i64, C.POINTER(i64)]
-    L.pci_mlp_forward_occ.argtypes = [P, P, P, P, i64, P]
+    L.pci_batch_probe_reduction.argtypes = [i32, i64, i32, C.POINTER(f64)]
+    L.pci_mlp_forward_occ.argtypes = [P, P, P, i64, P]
     L.pci_gpu_get_csr_rows.argtypes = [P, i32, i64, i64, P, P, P]
     _lib = L
     return L
@@ -209,6 +210,12 @@ class Engine:
         val = np.zeros(nnz.value, np.float64)
         self._check(self.L.pci_gpu_get_csr(self.h, which, _p(rowptr), _p(col), _p(val)))
         return rowptr, col, val
+
+    def csr_info(self, which: int = PCI_MAT_H):
+        """(rows, stored elements) of a resident matrix."""
+        nrows, nnz = C.c_int64(), C.c_int64()
+        self._check(self.L.pci_gpu_csr_info(self.h, which, C.byref(nrows), C.byref(nnz)))
+        return nrows.value, nnz.value
 
     def get_csr_rows(self, which: int, row_lo: int, row_hi: int):
         """Rows row_lo..row_hi (1-based, inclusive) of a resident matrix:
@@ -327,13 +334,12 @@ class Mlp:
         self._check(self.L.pci_mlp_forward(self.m, _p(X), X.shape[0], _p(y)))
         return y
 
-    def forward_occ(self, orbs, f0, f1):
-        """Tensor-core forward from compact inputs: orbs [n, 8] uint8 (0xff empty), f0, f1 [n]."""
+    def forward_occ(self, orbs, f):
+        """Tensor-core forward from compact inputs: orbs [n, 8] uint8 (0xff empty), f [n, 3]."""
         orbs = np.ascontiguousarray(orbs, np.uint8)
-        f0 = np.ascontiguousarray(f0, np.float32)
-        f1 = np.ascontiguousarray(f1, np.float32)
+        f = np.ascontiguousarray(f, np.float32)
         y = np.zeros(orbs.shape[0], np.float32)
-        self._check(self.L.pci_mlp_forward_occ(self.m, _p(orbs), _p(f0), _p(f1), orbs.shape[0], _p(y)))
+        self._check(self.L.pci_mlp_forward_occ(self.m, _p(orbs), _p(f), orbs.shape[0], _p(y)))
         return y
 
     def loss_grad(self, X, T):
@@ -362,6 +368,16 @@ class Mlp:
             self.close()
         except Exception:
             pass
+
+
+def probe_reduction(device, rows, nv):
+    """Measured GB/s of random FP64 reductions in the SpMM's transpose-part pattern."""
+    L = load()
+    g = C.c_double()
+    rc = L.pci_batch_probe_reduction(device, rows, nv, C.byref(g))
+    if rc != PCI_OK:
+        raise PciError(rc, "pci_batch_probe_reduction failed")
+    return g.value
 
 
 def batch_variants():

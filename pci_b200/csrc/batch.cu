@@ -157,18 +157,16 @@ __global__ void kb_set_units(double *V, int64_t ld, const int64_t *pos, int n)
 // Value of stored element l as the arithmetic type XT of the SpMM: FP32
 // vectors take the FP32 value (hi of a split pair), FP64 vectors the FP64
 // value (hi + lo of a split pair).
-// The matrix is read once per SpMM: its loads are streaming (evict-first),
-// so the vectors X and Y stay in L2 while the stored elements pass through.
 template <typename XT>
 __device__ __forceinline__ XT blk_val(const BlkCsr &B, int64_t l)
 {
-    if (B.f64) return (XT)__ldcs(&((const double *)B.val)[l]);
+    if (B.f64) return (XT)__ldg(&((const double *)B.val)[l]);
     if (B.split) {
-        const float2 hl = __ldcs(&((const float2 *)B.val)[l]);
+        const float2 hl = __ldg(&((const float2 *)B.val)[l]);
         if (sizeof(XT) == 4) return (XT)hl.x;
         return (XT)((double)hl.x + (double)hl.y);
     }
-    return (XT)__ldcs(&((const float *)B.val)[l]);
+    return (XT)__ldg(&((const float *)B.val)[l]);
 }
 
 // Row n (local row ln) of block B for vector v: the row part of the product
@@ -188,7 +186,7 @@ __device__ __forceinline__ XT spmm_row(const BlkCsr &B, int64_t ln, int64_t n, i
             XT t[4], xk[4];
 #pragma unroll
             for (int u = 0; u < 4; u++) {
-                k[u] = __ldcs(&B.col[l + u * G]);
+                k[u] = __ldg(&B.col[l + u * G]);
                 t[u] = blk_val<XT>(B, l + u * G);
             }
 #pragma unroll
@@ -196,7 +194,7 @@ __device__ __forceinline__ XT spmm_row(const BlkCsr &B, int64_t ln, int64_t n, i
 #pragma unroll
             for (int u = 0; u < 4; u++) acc += t[u] * xk[u];
         }
-        for (; l < l1; l += G) acc += blk_val<XT>(B, l) * __ldg(&X[(B.r0 + __ldcs(&B.col[l])) * NV + v]);
+        for (; l < l1; l += G) acc += blk_val<XT>(B, l) * __ldg(&X[(B.r0 + __ldg(&B.col[l])) * NV + v]);
         return acc;
     }
     const XT xn = __ldg(&X[n * NV + v]);
@@ -206,7 +204,7 @@ __device__ __forceinline__ XT spmm_row(const BlkCsr &B, int64_t ln, int64_t n, i
         XT t[4], xk[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-            k[u] = __ldcs(&B.col[l + u * G]);
+            k[u] = __ldg(&B.col[l + u * G]);
             t[u] = blk_val<XT>(B, l + u * G);
         }
 #pragma unroll
@@ -218,7 +216,7 @@ __device__ __forceinline__ XT spmm_row(const BlkCsr &B, int64_t ln, int64_t n, i
         }
     }
     for (; l < l1; l += G) {
-        const int k = __ldcs(&B.col[l]);
+        const int k = __ldg(&B.col[l]);
         const XT t = blk_val<XT>(B, l);
         const int64_t kg = B.r0 + k;
         if (k != ln) atomicAdd(&Y[kg * NV + v], t * xn);
@@ -358,6 +356,20 @@ __device__ __forceinline__ void tn_dims(int mode, const BState &s, const Bufs &B
 // Per-chunk partial of A[:, :ma]^T B[:, b0:b0+kb] over the chunk's rows.  In
 // TN_GRAM mode B is the SpMM output Q (row-major) and the kernel also stores
 // it as W's new columns.
+// D (8 x 8, FP64) += A (8 x 4) B (4 x 8) on the FP64 tensor cores.
+__device__ __forceinline__ void dmma884(double (&d)[2], double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+// Per-chunk partial of A[:, :ma]^T B[:, b0:b0+kb] over the chunk's rows, on
+// the FP64 tensor cores: the chunk's rows pass through shared memory 32 at a
+// time (zero-padded to whole 8 x 8 output tiles) and each warp owns up to
+// three 8 x 8 tiles of the ma x kb product, eight m8n8k4 steps per 32 rows.
+// In TN_GRAM mode B is the SpMM output Q (row-major) and the kernel also
+// stores it as W's new columns.
 template <int MODE>
 __global__ void __launch_bounds__(256) kb_tn(const Chunk *__restrict__ chunks, const BState *__restrict__ bst, Bufs B)
 {
@@ -367,30 +379,24 @@ __global__ void __launch_bounds__(256) kb_tn(const Chunk *__restrict__ chunks, c
     const double *A, *Bm;
     int ma, b0, kb;
     tn_dims(MODE, s, B, A, ma, Bm, b0, kb);
-    __shared__ double As[BT_TR][BT_MS + 1];
-    __shared__ double Bs[BT_TR][BT_LV + 1];
-    constexpr int OPT = (BT_PW + 255) / 256;   // outputs per thread
-    const int ne = ma * kb, t = threadIdx.x;
-    int ii[OPT], cc[OPT];
-    double acc[OPT];
-#pragma unroll
-    for (int o = 0; o < OPT; o++) {
-        const int e = t + 256 * o;
-        ii[o] = kb ? e / kb : 0;
-        cc[o] = kb ? e % kb : 0;
-        acc[o] = 0.0;
-    }
+    constexpr int MT = BT_MS / 8, NT = (BT_LV + 7) / 8;
+    __shared__ double As[BT_TR][MT * 8 + 1];
+    __shared__ double Bs[BT_TR][NT * 8 + 1];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int mt = (ma + 7) / 8, nt = (kb + 7) / 8, ntile = mt * nt;
+    const int map = mt * 8, kbp = nt * 8;
+    double acc[3][2] = {};
     const int64_t ld = B.ld;
     for (int64_t r0 = ch.row0; r0 < ch.row1; r0 += BT_TR) {
         const int nr = (int)min((int64_t)BT_TR, ch.row1 - r0);
-        for (int idx = t; idx < BT_TR * ma; idx += blockDim.x) {
+        for (int idx = t; idx < BT_TR * map; idx += blockDim.x) {
             const int r = idx % BT_TR, i = idx / BT_TR;
-            As[r][i] = r < nr ? A[(int64_t)i * ld + r0 + r] : 0.0;
+            As[r][i] = (r < nr && i < ma) ? A[(int64_t)i * ld + r0 + r] : 0.0;
         }
-        for (int idx = t; idx < BT_TR * kb; idx += blockDim.x) {
+        for (int idx = t; idx < BT_TR * kbp; idx += blockDim.x) {
             const int r = idx % BT_TR, c = idx / BT_TR;
             double v = 0.0;
-            if (r < nr) {
+            if (r < nr && c < kb) {
                 if (MODE == TN_GRAM) {
                     v = s.phase == 0 ? (double)B.Q32[(r0 + r) * B.nlv + c] : Bm[(r0 + r) * B.nlv + c];
                     B.W[(int64_t)(b0 + c) * ld + r0 + r] = v;
@@ -402,18 +408,32 @@ __global__ void __launch_bounds__(256) kb_tn(const Chunk *__restrict__ chunks, c
         }
         __syncthreads();
 #pragma unroll
-        for (int o = 0; o < OPT; o++) {
-            if (t + 256 * o < ne) {
-#pragma unroll 8
-                for (int r = 0; r < BT_TR; r++) acc[o] += As[r][ii[o]] * Bs[r][cc[o]];
+        for (int q = 0; q < 3; q++) {
+            const int tile = w + 8 * q;
+            if (tile < ntile) {
+                const int mi = tile / nt, ni = tile - mi * nt;
+                const int ka = lane & 3, row = lane >> 2;
+#pragma unroll
+                for (int k0 = 0; k0 < BT_TR; k0 += 4)
+                    dmma884(acc[q], As[k0 + ka][mi * 8 + row], Bs[k0 + ka][ni * 8 + row]);
             }
         }
         __syncthreads();
     }
     double *out = B.part + (int64_t)blockIdx.x * BT_PW;
 #pragma unroll
-    for (int o = 0; o < OPT; o++)
-        if (t + 256 * o < ne) out[t + 256 * o] = acc[o];
+    for (int q = 0; q < 3; q++) {
+        const int tile = w + 8 * q;
+        if (tile < ntile) {
+            const int mi = tile / nt, ni = tile - mi * nt;
+            const int i = mi * 8 + (lane >> 2);
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const int c = ni * 8 + 2 * (lane & 3) + u;
+                if (i < ma && c < kb) out[i * kb + c] = acc[q][u];
+            }
+        }
+    }
 }
 
 // Sum of up to BT_LV per-thread values over the thread block into out[0..n).
@@ -538,7 +558,9 @@ __global__ void kb_correct(const Chunk *__restrict__ chunks, const BState *__res
 // Learned correction: T[:, c] = MLP(features of row n) for the correction
 // slots whose root still uses it (lrn); kb_correct's diagonal correction
 // stays in the other slots.  Features of row n for root j: the occupied
-// orbitals of its determinant, H_nn - theta_j and r_jn sqrt(nd) / |r_j|.
+// orbitals of its determinant, H_nn - theta_j, s r_jn and s r_jn / (theta_j
+// - H_nn) (the diagonal correction, its denominator kept away from zero as in
+// kb_correct, clipped to +-1e4), with s = sqrt(nd) / |r_j|.
 // One warp evaluates 16 rows of one slot on the tensor cores (mlp_tc.cuh);
 // work items are (chunk, 16-row tile, slot) in a grid-stride loop.
 __global__ void __launch_bounds__(256, 2) kb_learned(const Chunk *__restrict__ chunks, int nch,
@@ -567,7 +589,7 @@ __global__ void __launch_bounds__(256, 2) kb_learned(const Chunk *__restrict__ c
         const double fs = sqrt((double)Bk.nd) / fmax(s.rnorm[j], 1e-300);
         const double th = s.theta[j];
         uint8_t o[2][mlptc::MAXOCC];
-        float a[2], b[2], out[2];
+        float f[2][mlptc::NSCAL], out[2];
 #pragma unroll
         for (int r = 0; r < 2; r++) {
             const int64_t n = r0 + g + 8 * r;
@@ -575,10 +597,14 @@ __global__ void __launch_bounds__(256, 2) kb_learned(const Chunk *__restrict__ c
             const uint8_t *src = Bk.orbs + (ok ? (n - Bk.r0) * mlptc::MAXOCC : 0);
 #pragma unroll
             for (int e = 0; e < mlptc::MAXOCC; e++) o[r][e] = ok ? src[e] : (uint8_t)0xff;
-            a[r] = ok ? (float)(B.D[n] - th) : 0.f;
-            b[r] = ok ? (float)(B.R[(int64_t)j * B.ld + n] * fs) : 0.f;
+            const double dn = ok ? B.D[n] : 0.0, rn = ok ? B.R[(int64_t)j * B.ld + n] * fs : 0.0;
+            double den = th - dn;
+            if (fabs(den) < 1e-8) den = den < 0.0 ? -1e-8 : 1e-8;
+            f[r][0] = ok ? (float)(dn - th) : 0.f;
+            f[r][1] = (float)rn;
+            f[r][2] = ok ? (float)fmax(-1e4, fmin(1e4, rn / den)) : 0.f;
         }
-        mlptc::tile(S, W.nin, o, a, b, out);
+        mlptc::tile(S, W.nin, o, f, out);
         if ((lane & 3) == 0) {
 #pragma unroll
             for (int r = 0; r < 2; r++) {
@@ -1291,7 +1317,7 @@ static int learned_ready(pci_batch *b)
     const int nin = mlp_num_inputs(b->model);
     for (const BlockRec &r : b->blocks) {
         if (!r.orbs) return set_err(h, PCI_E_INPUT, "a block has no determinant basis (added from a CSR)");
-        if (r.nsu > nin - 2) return set_err(h, PCI_E_INPUT, "a block has more orbitals than the model's inputs");
+        if (r.nsu > nin - mlptc::NSCAL) return set_err(h, PCI_E_INPUT, "a block has more orbitals than the model's inputs");
     }
     return PCI_OK;
 }
@@ -1781,7 +1807,8 @@ int pci_batch_davidson(pci_batch_t *b, const pci_batch_params *p, double *E, dou
 int pci_batch_set_correction_model(pci_batch_t *b, pci_mlp_t *m)
 {
     if (!b) return PCI_E_INPUT;
-    if (m && mlp_num_inputs(m) < 3) return set_err(&b->core, PCI_E_INPUT, "the model needs at least 3 inputs");
+    if (m && mlp_num_inputs(m) < mlptc::NSCAL + 1)
+        return set_err(&b->core, PCI_E_INPUT, "the model needs at least 4 inputs");
     b->model = m;
     return PCI_OK;
 }
@@ -1859,6 +1886,54 @@ static int prepare_harvest(pci_batch *b, Bufs &B, int nlv)
 }
 
 extern "C" {
+
+}  // extern "C"
+
+namespace {
+// Random FP64 reductions in teams of nv lanes onto nv consecutive words of a
+// rows x nv array: the access pattern of the SpMM's transpose part.
+__global__ void kb_red_probe(double *Y, uint32_t rows, int nv, int iters)
+{
+    const int lane = threadIdx.x & 31;
+    const int teams = 32 / nv, team = lane / nv, v = lane - team * nv;
+    if (team >= teams) return;
+    uint32_t x = (uint32_t)((blockIdx.x * blockDim.x + threadIdx.x) / 32 * teams + team) * 2654435761u + 12345u;
+    for (int i = 0; i < iters; i++) {
+        x ^= x << 13; x ^= x >> 17; x ^= x << 5;
+        atomicAdd(&Y[(size_t)(x % rows) * nv + v], 1.0);
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int pci_batch_probe_reduction(int32_t device, int64_t rows, int32_t nv, double *gbs)
+{
+    if (!gbs || rows < 1 || nv < 1 || nv > 32) return PCI_E_INPUT;
+    if (cudaSetDevice(device) != cudaSuccess) return PCI_E_CUDA;
+    double *Y = nullptr;
+    if (cudaMalloc(&Y, (size_t)rows * nv * 8) != cudaSuccess) return PCI_E_OOM;
+    cudaMemset(Y, 0, (size_t)rows * nv * 8);
+    cudaDeviceProp prop;
+    int nsm = 148;
+    if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) nsm = prop.multiProcessorCount;
+    const int grid = nsm * 8, block = 256, iters = 400;
+    EventPair ev;
+    int rc = PCI_OK;
+    if (ev.create() != cudaSuccess) rc = PCI_E_CUDA;
+    if (!rc) {
+        kb_red_probe<<<grid, block>>>(Y, (uint32_t)std::min<int64_t>(rows, UINT32_MAX), nv, 20);
+        cudaEventRecord(ev.a);
+        kb_red_probe<<<grid, block>>>(Y, (uint32_t)std::min<int64_t>(rows, UINT32_MAX), nv, iters);
+        cudaEventRecord(ev.b);
+        float ms = 0.f;
+        if (cudaEventSynchronize(ev.b) != cudaSuccess || cudaEventElapsedTime(&ms, ev.a, ev.b) != cudaSuccess) rc = PCI_E_CUDA;
+        const double reds = (double)grid * (block / 32) * (32 / nv) * nv * iters;
+        if (!rc) *gbs = reds * 8.0 / (ms * 1e-3) / 1e9;
+    }
+    cudaFree(Y);
+    return rc;
+}
 
 int pci_batch_vectors(pci_batch_t *b, int32_t blk, double *X)
 {

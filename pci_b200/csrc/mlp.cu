@@ -149,9 +149,9 @@ __global__ void k_to_bf16(const float *p, __nv_bfloat16 *pb, int64_t n)
 }
 
 // Tensor-core forward pass over n rows given in compact form: orbs[i][8]
-// (occupied orbitals, 0xff = empty), f0[i], f1[i] (the last two inputs).
-__global__ void __launch_bounds__(256) k_forward_tc(mlptc::Weights W, const uint8_t *orbs, const float *f0,
-                                                    const float *f1, int64_t n, float *y)
+// (occupied orbitals, 0xff = empty), f[i][NSCAL] (the last NSCAL inputs).
+__global__ void __launch_bounds__(256) k_forward_tc(mlptc::Weights W, const uint8_t *orbs, const float *f, int64_t n,
+                                                    float *y)
 {
     extern __shared__ __align__(16) unsigned char sm[];
     const mlptc::Smem S = mlptc::load(W, sm);
@@ -160,15 +160,14 @@ __global__ void __launch_bounds__(256) k_forward_tc(mlptc::Weights W, const uint
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t r0 = warp * 16; r0 < n; r0 += nwarps * 16) {
         uint8_t o[2][mlptc::MAXOCC];
-        float a[2], b[2], out[2];
+        float fs[2][mlptc::NSCAL], out[2];
         for (int r = 0; r < 2; r++) {
             const int64_t i = r0 + g + 8 * r;
             const bool ok = i < n;
             for (int e = 0; e < mlptc::MAXOCC; e++) o[r][e] = ok ? orbs[i * mlptc::MAXOCC + e] : 0xff;
-            a[r] = ok ? f0[i] : 0.f;
-            b[r] = ok ? f1[i] : 0.f;
+            for (int j = 0; j < mlptc::NSCAL; j++) fs[r][j] = ok ? f[i * mlptc::NSCAL + j] : 0.f;
         }
-        mlptc::tile(S, W.nin, o, a, b, out);
+        mlptc::tile(S, W.nin, o, fs, out);
         if ((lane & 3) == 0)
             for (int r = 0; r < 2; r++) {
                 const int64_t i = r0 + g + 8 * r;
@@ -505,34 +504,31 @@ mlptc::Weights mlp_tc_weights(const pci_mlp *m)
     return W;
 }
 
-extern "C" int pci_mlp_forward_occ(pci_mlp_t *m, const uint8_t *orbs, const float *f0, const float *f1, int64_t n,
-                                   float *y)
+extern "C" int pci_mlp_forward_occ(pci_mlp_t *m, const uint8_t *orbs, const float *f, int64_t n, float *y)
 {
-    if (!m || !orbs || !f0 || !f1 || !y || n < 1) return mlp_fail(m, PCI_E_INPUT, "forward_occ: bad arguments");
-    if (m->nin < 3) return mlp_fail(m, PCI_E_INPUT, "forward_occ: the model needs nin >= 3");
+    if (!m || !orbs || !f || !y || n < 1) return mlp_fail(m, PCI_E_INPUT, "forward_occ: bad arguments");
+    if (m->nin < mlptc::NSCAL + 1) return mlp_fail(m, PCI_E_INPUT, "forward_occ: the model needs nin >= 4");
     cudaSetDevice(m->device);
     uint8_t *d_o = nullptr;
-    float *d_a = nullptr, *d_b = nullptr, *d_y = nullptr;
+    float *d_f = nullptr, *d_y = nullptr;
     int rc = PCI_OK;
     const size_t sb = mlptc::smem_bytes(m->nin);
-    if (cudaMalloc(&d_o, (size_t)n * mlptc::MAXOCC) != cudaSuccess || cudaMalloc(&d_a, (size_t)n * 4) != cudaSuccess ||
-        cudaMalloc(&d_b, (size_t)n * 4) != cudaSuccess || cudaMalloc(&d_y, (size_t)n * 4) != cudaSuccess) {
+    if (cudaMalloc(&d_o, (size_t)n * mlptc::MAXOCC) != cudaSuccess ||
+        cudaMalloc(&d_f, (size_t)n * mlptc::NSCAL * 4) != cudaSuccess || cudaMalloc(&d_y, (size_t)n * 4) != cudaSuccess) {
         rc = mlp_fail(m, PCI_E_OOM, "forward_occ: device allocation failed");
     } else if (cudaFuncSetAttribute(k_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb) != cudaSuccess) {
         rc = mlp_fail(m, PCI_E_CUDA, "forward_occ: shared memory attribute");
     } else {
         cudaMemcpyAsync(d_o, orbs, (size_t)n * mlptc::MAXOCC, cudaMemcpyHostToDevice, m->st);
-        cudaMemcpyAsync(d_a, f0, (size_t)n * 4, cudaMemcpyHostToDevice, m->st);
-        cudaMemcpyAsync(d_b, f1, (size_t)n * 4, cudaMemcpyHostToDevice, m->st);
-        k_forward_tc<<<148, 256, sb, m->st>>>(mlp_tc_weights(m), d_o, d_a, d_b, n, d_y);
+        cudaMemcpyAsync(d_f, f, (size_t)n * mlptc::NSCAL * 4, cudaMemcpyHostToDevice, m->st);
+        k_forward_tc<<<148, 256, sb, m->st>>>(mlp_tc_weights(m), d_o, d_f, n, d_y);
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaMemcpyAsync(y, d_y, (size_t)n * 4, cudaMemcpyDeviceToHost, m->st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(m->st);
         if (e != cudaSuccess) rc = mlp_fail(m, PCI_E_CUDA, std::string("forward_occ: ") + cudaGetErrorString(e));
     }
     cudaFree(d_o);
-    cudaFree(d_a);
-    cudaFree(d_b);
+    cudaFree(d_f);
     cudaFree(d_y);
     return rc;
 }

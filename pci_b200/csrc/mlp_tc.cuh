@@ -2,7 +2,7 @@
 // ReLU) for 16 rows per warp.
 //
 // The first layer's input is sparse: the occupation counts of the orbitals
-// (at most PCI_NE_MAX non-zero entries per determinant) and two scalars, so it
+// (at most PCI_NE_MAX non-zero entries per determinant) and NSCAL scalars, so it
 // is evaluated as a sum of rows of W1 on the CUDA cores.  The two 128 x 128
 // hidden layers run as mma.sync m16n8k16 BF16 products with FP32 accumulation:
 // a layer's accumulator fragments are, after bias and ReLU, exactly the next
@@ -23,6 +23,7 @@ namespace mlptc {
 constexpr int HID = 128;
 constexpr int WPAD = HID + 8;   // row stride (bf16) of the transposed hidden weights in shared memory
 constexpr int MAXOCC = 8;       // orbital slots per determinant (PCI_NE_MAX)
+constexpr int NSCAL = 3;        // scalar inputs after the occupation counts
 
 // Where the parameters live (device pointers into the model, layer by layer:
 // W (din x dout, row-major) then b (dout)).
@@ -133,12 +134,12 @@ __device__ __forceinline__ void hidden(const uint32_t (&A)[8][4], const __nv_bfl
 
 // MLP output for the 16 rows of a warp.  Lane (g = lane / 4, t = lane % 4)
 // supplies rows g (index 0) and g + 8 (index 1): up to MAXOCC orbital indices
-// each (entries >= nin - 2 ignored, so 0xff marks an empty slot; an orbital
-// listed twice counts twice) and the two scalar inputs f0 (input nin - 2) and
-// f1 (input nin - 1).  All 32 lanes must call it; out[i] receives row i's
+// each (entries >= nin - NSCAL ignored, so 0xff marks an empty slot; an
+// orbital listed twice counts twice) and the scalar inputs f[r][j] (input
+// nin - NSCAL + j).  All 32 lanes must call it; out[i] receives row i's
 // output (replicated over the four lanes of the group).
-__device__ inline void tile(const Smem &S, int nin, const uint8_t (&orb)[2][MAXOCC], const float (&f0)[2],
-                            const float (&f1)[2], float (&out)[2])
+__device__ inline void tile(const Smem &S, int nin, const uint8_t (&orb)[2][MAXOCC], const float (&f)[2][NSCAL],
+                            float (&out)[2])
 {
     const int lane = threadIdx.x & 31, t = lane & 3;
     float C[16][4];
@@ -151,23 +152,23 @@ __device__ inline void tile(const Smem &S, int nin, const uint8_t (&orb)[2][MAXO
     }
 #pragma unroll
     for (int r = 0; r < 2; r++) {
-        for (int e = 0; e < MAXOCC + 2; e++) {
+        for (int e = 0; e < MAXOCC + NSCAL; e++) {
             int wrow;
-            float f;
+            float fe;
             if (e < MAXOCC) {
                 wrow = orb[r][e];
-                f = 1.f;
-                if (wrow >= nin - 2) continue;
+                fe = 1.f;
+                if (wrow >= nin - NSCAL) continue;
             } else {
-                wrow = nin - 2 + (e - MAXOCC);
-                f = e == MAXOCC ? f0[r] : f1[r];
+                wrow = nin - NSCAL + (e - MAXOCC);
+                fe = f[r][e - MAXOCC];
             }
             const __nv_bfloat16 *w = S.w1 + (size_t)wrow * HID + 2 * t;
 #pragma unroll
             for (int j = 0; j < 16; j++) {
                 const __nv_bfloat162 v = *reinterpret_cast<const __nv_bfloat162 *>(w + 8 * j);
-                C[j][2 * r] += f * __low2float(v);
-                C[j][2 * r + 1] += f * __high2float(v);
+                C[j][2 * r] += fe * __low2float(v);
+                C[j][2 * r + 1] += fe * __high2float(v);
             }
         }
     }

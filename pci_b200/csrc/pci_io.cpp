@@ -205,6 +205,98 @@ int pci_io_read_csr(const char *path, int64_t nd, int64_t nnz, int64_t *rowptr, 
     return PCI_OK;
 }
 
+// ----------------------------------------------------- CONF.HIJ / CONF.JJJ ---
+
+// Appends the records of rows row0+1 .. row0+n (1-based) of a CSR slice:
+// (int32 row, int32 col, real64 value) per non-zero element.
+static bool hij_records(FILE *f, int64_t row0, int64_t n, const int64_t *rowptr, const int32_t *col, const double *val,
+                        int64_t *written)
+{
+    struct Rec {
+        int32_t r, c;
+        double v;
+    };
+    static_assert(sizeof(Rec) == 16, "record layout");
+    std::vector<Rec> buf;
+    buf.reserve(1 << 16);
+    for (int64_t i = 0; i < n; i++) {
+        for (int64_t l = rowptr[i] - rowptr[0]; l < rowptr[i + 1] - rowptr[0]; l++) {
+            if (val[l] == 0.0) continue;   // sort.f90 drops exact zeros
+            buf.push_back(Rec{(int32_t)(row0 + i + 1), col[l], val[l]});
+            if (buf.size() == buf.capacity()) {
+                if (fwrite(buf.data(), sizeof(Rec), buf.size(), f) != buf.size()) return false;
+                *written += (int64_t)buf.size();
+                buf.clear();
+            }
+        }
+    }
+    if (!buf.empty() && fwrite(buf.data(), sizeof(Rec), buf.size(), f) != buf.size()) return false;
+    *written += (int64_t)buf.size();
+    return true;
+}
+
+int pci_io_write_hij(const char *path, int64_t nd, const int64_t *rowptr, const int32_t *col, const double *val,
+                     char *errbuf, int32_t errlen)
+{
+    if (nd < 0 || nd > INT32_MAX || !rowptr || (rowptr[nd] > rowptr[0] && (!col || !val)))
+        return fail(errbuf, errlen, "write_hij: bad arguments (Nd must fit a 4-byte integer)");
+    File F(path, "wb");
+    if (!F.ok()) return fail(errbuf, errlen, "write_hij: cannot open %s", path ? path : "(null)");
+    int64_t count = 0;
+    if (fwrite(&count, 8, 1, F.f) != 1) return fail(errbuf, errlen, "write_hij: write to %s failed", path);
+    if (!hij_records(F.f, 0, nd, rowptr, col, val, &count))
+        return fail(errbuf, errlen, "write_hij: write to %s failed", path);
+    if (fseeko(F.f, 0, SEEK_SET) != 0 || fwrite(&count, 8, 1, F.f) != 1)
+        return fail(errbuf, errlen, "write_hij: cannot write the count of %s", path);
+    return PCI_OK;
+}
+
+int pci_io_append_hij(const char *path, int64_t row0, int64_t nrows, const int64_t *rowptr, const int32_t *col,
+                      const double *val, char *errbuf, int32_t errlen)
+{
+    if (row0 < 0 || nrows < 0 || row0 + nrows > INT32_MAX || !rowptr || (rowptr[nrows] > rowptr[0] && (!col || !val)))
+        return fail(errbuf, errlen, "append_hij: bad arguments");
+    File F(path, row0 == 0 ? "wb+" : "rb+");
+    if (!F.ok()) return fail(errbuf, errlen, "append_hij: cannot open %s", path ? path : "(null)");
+    int64_t count = 0;
+    if (row0 == 0) {
+        if (fwrite(&count, 8, 1, F.f) != 1) return fail(errbuf, errlen, "append_hij: write to %s failed", path);
+    } else {
+        if (fread(&count, 8, 1, F.f) != 1 || count < 0) return fail(errbuf, errlen, "append_hij: %s has no count", path);
+        if (fseeko(F.f, 0, SEEK_END) != 0) return fail(errbuf, errlen, "append_hij: cannot seek %s", path);
+        if ((int64_t)ftello(F.f) != 8 + 16 * count)
+            return fail(errbuf, errlen, "append_hij: %s is not a complete record stream", path);
+    }
+    if (!hij_records(F.f, row0, nrows, rowptr, col, val, &count))
+        return fail(errbuf, errlen, "append_hij: write to %s failed", path);
+    if (fseeko(F.f, 0, SEEK_SET) != 0 || fwrite(&count, 8, 1, F.f) != 1)
+        return fail(errbuf, errlen, "append_hij: cannot write the count of %s", path);
+    return PCI_OK;
+}
+
+int pci_io_read_hij(const char *path, int64_t cap, int32_t *row, int32_t *col, double *val, int64_t *count,
+                    char *errbuf, int32_t errlen)
+{
+    File F(path, "rb");
+    if (!F.ok()) return fail(errbuf, errlen, "read_hij: cannot open %s", path ? path : "(null)");
+    int64_t n = 0;
+    if (fread(&n, 8, 1, F.f) != 1 || n < 0) return fail(errbuf, errlen, "read_hij: %s has no count", path);
+    if (count) *count = n;
+    if (cap <= 0) return PCI_OK;
+    if (!row || !col || !val) return fail(errbuf, errlen, "read_hij: null array");
+    const int64_t m = std::min(cap, n);
+    for (int64_t i = 0; i < m; i++) {
+        int32_t rc[2];
+        double v;
+        if (fread(rc, 4, 2, F.f) != 2 || fread(&v, 8, 1, F.f) != 1)
+            return fail(errbuf, errlen, "read_hij: %s ended at record %" PRId64, path, i + 1);
+        row[i] = rc[0];
+        col[i] = rc[1];
+        val[i] = v;
+    }
+    return PCI_OK;
+}
+
 // -------------------------------------------------------------- CONF.XIJ ---
 
 int pci_io_write_xij(const char *path, int32_t nlv, int64_t nd, const double *Tk, const double *Tj, const double *X,

@@ -52,6 +52,9 @@ def lib():
         "pci_io_read_int": [s, C.POINTER(IntHeader), P, P, P, P, P, P, P, P, i32],
         "pci_io_write_int": [s, C.POINTER(IntHeader), P, P, P, P, P, P, P, P, i32],
         "pci_io_hint_lut": [i32, P, P, i32, P],
+        "pci_io_write_hij": [s, i64, P, P, P, P, i32],
+        "pci_io_append_hij": [s, i64, i64, P, P, P, P, i32],
+        "pci_io_read_hij": [s, i64, P, P, P, P, P, i32],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -65,7 +68,7 @@ EXPORTS = ["pci_io_write_csr", "pci_io_read_csr_header", "pci_io_read_csr", "pci
            "pci_io_read_xij", "pci_io_write_res", "pci_io_write_det", "pci_io_read_det_header",
            "pci_io_read_det", "pci_io_write_gnt", "pci_io_read_gnt_header", "pci_io_read_gnt",
            "pci_io_gaunt_lut", "pci_io_read_int_header", "pci_io_read_int", "pci_io_write_int",
-           "pci_io_hint_lut"]
+           "pci_io_hint_lut", "pci_io_write_hij", "pci_io_append_hij", "pci_io_read_hij"]
 
 
 def _p(a):
@@ -110,6 +113,42 @@ def read_csr(path):
     val = np.empty(nnz.value, np.float64 if vb.value == 8 else np.float32)
     _call(L.pci_io_read_csr, _path(path), nd.value, nnz.value, _p(rowptr), _p(col), _p(val), vb.value)
     return rowptr, col, val
+
+
+# ------------------------------------------------------- CONF.HIJ / JJJ ---
+
+def write_hij(path, rowptr, col, val):
+    """CONF.HIJ / CONF.JJJ record stream from a lower-triangle CSR (0-based
+    rowptr, 1-based col, float64 val)."""
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.int64)
+    col = np.ascontiguousarray(col, dtype=np.int32)
+    val = np.ascontiguousarray(val, dtype=np.float64)
+    _call(lib().pci_io_write_hij, _path(path), rowptr.size - 1, _p(rowptr), _p(col), _p(val))
+
+
+def write_hij_from_engine(path, eng, which=0, rows_per_chunk=1 << 16):
+    """CONF.HIJ (which 0) or CONF.JJJ (which 1) streamed from a device-resident
+    matrix in row ranges, so the host never holds the whole matrix."""
+    nd = eng.csr_info(which)[0]
+    L = lib()
+    for r0 in range(0, nd, rows_per_chunk):
+        r1 = min(nd, r0 + rows_per_chunk)
+        rp, col, val = eng.get_csr_rows(which, r0 + 1, r1)
+        _call(L.pci_io_append_hij, _path(path), r0, r1 - r0, _p(rp), _p(col), _p(val))
+    if nd == 0:
+        write_hij(path, np.zeros(1, np.int64), np.zeros(0, np.int32), np.zeros(0))
+
+
+def read_hij(path):
+    """(row int32, col int32, val float64) records of a CONF.HIJ stream."""
+    L = lib()
+    n = C.c_int64()
+    _call(L.pci_io_read_hij, _path(path), 0, None, None, None, C.byref(n))
+    row = np.empty(n.value, np.int32)
+    col = np.empty(n.value, np.int32)
+    val = np.empty(n.value, np.float64)
+    _call(L.pci_io_read_hij, _path(path), n.value, _p(row), _p(col), _p(val), C.byref(n))
+    return row, col, val
 
 
 # ------------------------------------------------------------------ XIJ ---

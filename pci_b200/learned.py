@@ -9,12 +9,15 @@ x* is the converged vector of the root that x_k is closest to: the exact
 expansion vector that would finish the root in one Rayleigh-Ritz step.  The
 network sees per row
 
-* the occupation counts of the orbitals (inputs 0 .. nin-3),
-* H_nn - theta (input nin-2),
-* r_k[n] * sqrt(Nd) / |r_k| (input nin-1),
+* the occupation counts of the orbitals (inputs 0 .. nin-4),
+* H_nn - theta (input nin-3),
+* r_k[n] * s with s = sqrt(Nd) / |r_k| (input nin-2),
+* the diagonal correction r_k[n] * s / (theta - H_nn) of the reference's
+  Dvdsn (input nin-1; denominator at least 1e-8 in size, clipped to +-1e4),
 
-and predicts (x* - x_k)[n] in units of its RMS over the sampled rows of that
-root and iteration (signs of x_k and r_k aligned with x*).  The solver uses
+and predicts (x* - x_k)[n], scaled so its RMS over the sampled rows of that
+root and iteration equals that of the diagonal-correction input (signs of x_k
+and r_k aligned with x*).  The solver uses
 the prediction as the expansion direction of the root (its length does not
 matter: corrections are normalised), with the diagonal correction of the
 reference's Dvdsn (davidson.f90:436-570) as the fallback of every root whose
@@ -26,12 +29,13 @@ import numpy as np
 
 from .capi import PCI_BATCH_CORR_LEARNED, PCI_BATCH_FP64, Batch, Engine, Mlp
 
-NIN_DEFAULT = 142   # 140 orbitals (the largest basis of the workloads) + 2 scalars
+NSCAL = 3
+NIN_DEFAULT = 143   # 140 orbitals (the largest basis of the workloads) + 3 scalars
 
 
 def occupation_counts(sysm, rows, nin=NIN_DEFAULT):
-    """Occupation counts of the orbitals for determinant rows (0-based), [n, nin-2]."""
-    norb = nin - 2
+    """Occupation counts of the orbitals for determinant rows (0-based), [n, nin-3]."""
+    norb = nin - NSCAL
     if sysm.nsu > norb:
         raise ValueError(f"{sysm.nsu} orbitals exceed the model's {norb} occupation inputs")
     orb = sysm.nh[sysm.iarr[rows] - 1] - 1            # [n, Ne] 0-based orbitals
@@ -72,11 +76,20 @@ def samples_to_training(sysm, recs, X, nin=NIN_DEFAULT, blk=0):
         if not np.isfinite(rms) or rms <= 0:
             continue
         f = np.empty((b - a, nin), np.float32)
-        f[:, :nin - 2] = occ_all[a:b]
-        f[:, nin - 2] = g["diag"] - g["theta"]
-        f[:, nin - 1] = sgn * g["r"] * np.sqrt(nd) / g["rnorm"]
+        f[:, :nin - NSCAL] = occ_all[a:b]
+        f[:, nin - 3] = g["diag"] - g["theta"]
+        rs = sgn * g["r"] * np.sqrt(nd) / g["rnorm"]
+        den = g["theta"] - g["diag"]
+        den = np.where(np.abs(den) < 1e-8, np.where(den < 0, -1e-8, 1e-8), den)
+        f[:, nin - 2] = rs
+        d = np.clip(rs / den, -1e4, 1e4)
+        f[:, nin - 1] = d
+        drms = np.sqrt(np.mean(d * d))
+        if not np.isfinite(drms) or drms <= 0:
+            continue
         feats.append(f)
-        targs.append((t / rms).astype(np.float32))
+        # on the scale of the diagonal-correction input, so the network can keep it
+        targs.append((t / rms * drms).astype(np.float32))
     if not feats:
         return np.zeros((0, nin), np.float32), np.zeros(0, np.float32)
     return np.concatenate(feats), np.concatenate(targs)
@@ -110,7 +123,7 @@ def harvest(systems, nlv, rows_per_block=2000, nin=NIN_DEFAULT, device=0, max_su
     return F, T, dict(result=r, recorded=count)
 
 
-def train(F, T, nin=NIN_DEFAULT, device=0, epochs=4, batch=4096, lr=1e-3, seed=0, clip=8.0):
+def train(F, T, nin=NIN_DEFAULT, device=0, epochs=4, batch=4096, lr=1e-3, seed=0, clip=1e3):
     """A fresh model trained on (F, T) on the GPU (targets clipped to +-clip)."""
     m = Mlp(nin, device, seed)
     T = np.clip(T, -clip, clip).astype(np.float32)

@@ -93,7 +93,7 @@ def test_tensor_core_forward_matches_forward():
     """pci_mlp_forward_occ (mma.sync BF16 hidden layers, the solver's path)
     against pci_mlp_forward (FP32 activations) on the same inputs."""
     from pci_b200.capi import Mlp
-    nin = 42
+    nin = 43
     m = Mlp(nin, 0, seed=5)
     rng = np.random.default_rng(3)
     n = 1000
@@ -101,15 +101,13 @@ def test_tensor_core_forward_matches_forward():
     X = np.zeros((n, nin), np.float32)
     for i in range(n):
         ne = rng.integers(1, 9)
-        o = rng.integers(0, nin - 2, ne)
+        o = rng.integers(0, nin - 3, ne)
         orbs[i, :ne] = o
         np.add.at(X[i], o, 1.0)
-    f0 = rng.normal(0, 1, n).astype(np.float32)
-    f1 = rng.normal(0, 3, n).astype(np.float32)
-    X[:, nin - 2] = f0
-    X[:, nin - 1] = f1
+    f = rng.normal(0, 2, (n, 3)).astype(np.float32)
+    X[:, nin - 3:] = f
     y = m.forward(X)
-    yt = m.forward_occ(orbs, f0, f1)
+    yt = m.forward_occ(orbs, f)
     scale = np.abs(y).max()
     assert scale > 0
     assert np.abs(yt - y).max() <= 2e-2 * scale

@@ -2,7 +2,9 @@
 
 Every writer is checked twice: by its own reader (round trip) and by an
 independent parse of the bytes that follows the layouts of the reference's
-writers -- WriteMatrixCSR (src/matrix_io.f90:689-799) for pCONF.HIJ,
+writers -- WriteMatrixCSR (src/matrix_io.f90:689-799) for pCONF.HIJ, the
+sort program's record stream (src/sort.f90:16-80, read by ReadHIJ,
+src/pol.f90:766-797) for CONF.HIJ,
 WriteFinalXIJ (src/pconf.F90:2566-2602) for CONF.XIJ, PrintEnergies
 (src/pconf.F90:3152-3242) for CONF.RES, Wdet (src/determinants.f90:448-460)
 for CONF.DET, the CONF.GNT records of src/breit.f90:96-101 and the CONF.INT
@@ -89,6 +91,45 @@ def test_csr_stream_errors(tmp_path):
         f.truncate(os.path.getsize(p) - 3)
     with pytest.raises(capi.PciError):
         files.read_csr(p)
+
+
+def _hij_parse(path):
+    """The CONF.HIJ bytes as ReadHIJ reads them: int64 count, then (int32, int32, real64) records."""
+    b = open(path, "rb").read()
+    (n,) = struct.unpack_from("<q", b, 0)
+    assert len(b) == 8 + 16 * n
+    rec = np.frombuffer(b, np.dtype([("r", "<i4"), ("c", "<i4"), ("v", "<f8")]), n, 8)
+    return n, rec
+
+
+def test_hij_stream(tmp_path):
+    """Whole-matrix and row-range writers give the same bytes: rows ascending,
+    columns ascending within a row (the order sort.f90's quicksort leaves),
+    exact zeros dropped, column <= row."""
+    rowptr, col, val = _csr(5)
+    val[::7] = 0.0
+    p1, p2 = tmp_path / "CONF.HIJ", tmp_path / "CONF2.HIJ"
+    files.write_hij(p1, rowptr, col, val)
+    n, rec = _hij_parse(p1)
+    rows = np.repeat(np.arange(1, rowptr.size), np.diff(rowptr))
+    keep = val != 0.0
+    assert n == keep.sum()
+    assert np.array_equal(rec["r"], rows[keep]) and np.array_equal(rec["c"], col[keep])
+    assert np.array_equal(rec["v"], val[keep])
+    assert np.all(rec["c"] <= rec["r"])
+    key = rec["r"].astype(np.int64) * (1 << 32) + rec["c"]
+    assert np.all(np.diff(key) > 0)
+    # the same stream in row ranges of 10
+    nd = rowptr.size - 1
+    L = files.lib()
+    for r0 in range(0, nd, 10):
+        r1 = min(nd, r0 + 10)
+        rp = rowptr[r0:r1 + 1]
+        files._call(L.pci_io_append_hij, files._path(p2), r0, r1 - r0, files._p(np.ascontiguousarray(rp)),
+                    files._p(col[rp[0]:]), files._p(val[rp[0]:]))
+    assert open(p1, "rb").read() == open(p2, "rb").read()
+    r, c, v = files.read_hij(p1)
+    assert np.array_equal(r, rec["r"]) and np.array_equal(c, rec["c"]) and np.array_equal(v, rec["v"])
 
 
 def test_xij(tmp_path):
