@@ -68,6 +68,9 @@ def parse():
     ap.add_argument("--learn-nd", type=int, default=30000,
                     help="determinants of each training system of the learned correction")
     ap.add_argument("--switch-tol", type=float, default=1e-5, help="residual that ends the FP32 phase")
+    ap.add_argument("--profile-case", default=None,
+                    help="only a short batched solve of this configuration, for profiler captures")
+    ap.add_argument("--case-iters", type=int, default=6, help="iterations of --profile-case")
     ap.add_argument("--batch-blocks", type=int, default=64)
     ap.add_argument("--batch-variant", type=int, default=-1, help="SpMM variant of the batched form "
                     "(-1: from the tuning cache, tuned when absent)")
@@ -605,8 +608,37 @@ def run_batched(args, local, rank, world, dist, peak, peak_kind):
     return out
 
 
+def run_profile_case(args):
+    """A short batched solve for profiler captures: the configuration's FP64 H
+    built on the device, then args.case_iters iterations of the batched solver
+    with the learned correction (a freshly initialised network), so every
+    kernel of an iteration (SpMM, tensor-core Gram products, tensor-core
+    network) runs."""
+    from pci_b200 import learned as LR
+    from pci_b200 import system as S
+    from pci_b200.capi import PCI_BATCH_CORR_LEARNED, Batch, Engine, Mlp
+    sysm = S.make_system(**S.CONFIGS[args.profile_case]())
+    m = Mlp(LR.NIN_DEFAULT, 0, seed=1)
+    with Engine(0) as e:
+        e.load_system(sysm)
+        e.form_h(64)
+        b = Batch(0)
+        b.set_value_prec(64)
+        b.add_engine(e)
+    b.set_correction_model(m)
+    r = b.davidson(nlv=int(sysm.params["Nlv"]), max_sub=96, keep=48, max_it=args.case_iters, tol=1e-8,
+                   correction=PCI_BATCH_CORR_LEARNED, spmm_variant=0)
+    print(json.dumps({"profile_case": args.profile_case, "Nd": sysm.nd, "iterations": int(r["iters"][0]),
+                      "stats": b.stats()}), flush=True)
+    b.close()
+    m.close()
+    return 0
+
+
 def main():
     args = parse()
+    if args.profile_case:
+        return run_profile_case(args)
     if args.tune_cache is None:
         args.tune_cache = TUNE_CACHE
     if args.impl == "reference":

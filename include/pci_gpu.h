@@ -168,6 +168,24 @@ int pci_gpu_j_av_noalloc(const int64_t *rowptr, const int32_t *col, const double
                          const double *X, int64_t ldx, int32_t nv, int64_t nlim, double *Tj,
                          void *stream, char *errbuf, int32_t errlen);
 
+/* Replaces: FormBarr (src/determinants.f90:839-864), the bit-string form of
+ * the determinant list that pconf builds when Ne >= num_ints_bit_rep or
+ * CONF_USE_BIT_DET is set: Barr(nint, Nd), nint = ceil(Nst / 32), bit
+ * (m-1) mod 32 of word (m-1)/32 + 1 set for every occupied m-state m.  Kept
+ * on the device; *nint receives nint; barr (nint x Nd int32, may be NULL)
+ * receives a copy. */
+int pci_gpu_form_barr(pci_gpu_t *h, int32_t *nint, int32_t *barr);
+
+/* Replaces: compare_bit_dets + get_det_indexes (src/determinants.f90:933-1034)
+ * on the device for n determinant pairs (pairs[2i], pairs[2i+1], 1-based):
+ * ndiffs (3 for three or more), the phase is and the differing m-states
+ * idx1[3i..3i+2], idx2[3i..3i+2] of each determinant in the reference's slot
+ * order (slot 1 unused, 0 where absent).  The reference's phase rule is kept
+ * as it is, including its disagreement with Rspq on some single
+ * differences.  Needs pci_gpu_form_barr. */
+int pci_gpu_bit_compare(pci_gpu_t *h, int64_t n, const int64_t *pairs, int32_t *ndiffs, int32_t *is, int32_t *idx1,
+                        int32_t *idx2);
+
 /* Jt(1:Njd) of the basis set by pci_gpu_set_basis: the sorted 2J values of
  * the terms its configurations hold, as Dinit lists them
  * (src/determinants.f90:227-325); Prj_J of the Kv = 3 Davidson filters

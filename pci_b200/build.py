@@ -65,8 +65,7 @@ def build(verbose: bool = False, force: bool = False, extra: list | None = None,
             for f in [ex.submit(run, c) for c in todo]:
                 f.result()
     if force or _mtime(LIB) < max(_mtime(o) for o in objs):
-        run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs +
-            ["-lcusolver", "-lcublas", "-Xlinker", f"-rpath,{CUDA_HOME}/lib64"])
+        run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-Xlinker", f"-rpath,{CUDA_HOME}/lib64"])
     return LIB
 
 

@@ -25,7 +25,7 @@ EXPORTS = ["pci_gpu_create", "pci_gpu_set_basis", "pci_gpu_set_integrals", "pci_
            "pci_gpu_last_error", "pci_gpu_destroy", "pci_mlp_create", "pci_mlp_num_params", "pci_mlp_set_params",
            "pci_mlp_get_params", "pci_mlp_forward", "pci_mlp_loss_grad", "pci_mlp_train", "pci_mlp_last_error",
            "pci_mlp_destroy", "pci_gpu_set_correction_model", "pci_gpu_davidson_harvest", "pci_mlp_forward_occ",
-           "pci_gpu_get_csr_rows"]
+           "pci_gpu_get_csr_rows", "pci_gpu_form_barr", "pci_gpu_bit_compare"]
 BATCH_EXPORTS = ["pci_batch_create", "pci_batch_add_block", "pci_batch_set_storage", "pci_batch_set_value_prec",
                  "pci_batch_info", "pci_batch_tune",
                  "pci_batch_variant", "pci_batch_davidson", "pci_batch_vectors", "pci_batch_stats",
@@ -125,6 +125,8 @@ def load(path: str = LIB):
     L.pci_batch_probe_reduction.argtypes = [i32, i64, i32, C.POINTER(f64)]
     L.pci_mlp_forward_occ.argtypes = [P, P, P, i64, P]
     L.pci_gpu_get_csr_rows.argtypes = [P, i32, i64, i64, P, P, P]
+    L.pci_gpu_form_barr.argtypes = [P, C.POINTER(i32), P]
+    L.pci_gpu_bit_compare.argtypes = [P, i64, P, P, P, P, P]
     _lib = L
     return L
 
@@ -176,6 +178,7 @@ class Engine:
                                       _p(k["iarr"]), _p(k["nh"]), _p(k["jz"]), _p(k["nn"]), _p(k["kk"]),
                                       _p(k["ll"]), _p(k["jj"]), sysm.nc, _p(k["ndc"]), float(sysm.gj))
         self._check(rc)
+        self._nd = int(sysm.nd)
 
     def set_integrals(self, sysm):
         hl = np.ascontiguousarray(sysm.hint_lut, np.float64)
@@ -210,6 +213,29 @@ class Engine:
         val = np.zeros(nnz.value, np.float64)
         self._check(self.L.pci_gpu_get_csr(self.h, which, _p(rowptr), _p(col), _p(val)))
         return rowptr, col, val
+
+    def form_barr(self, copy=True):
+        """FormBarr on the device; returns Barr as [Nd, nint] int32 (None without copy)."""
+        nint = C.c_int32()
+        self._check(self.L.pci_gpu_form_barr(self.h, C.byref(nint), None))
+        if not copy:
+            return None
+        nd = self._nd
+        out = np.zeros((nd, nint.value), np.int32)
+        self._check(self.L.pci_gpu_form_barr(self.h, C.byref(nint), _p(out)))
+        return out
+
+    def bit_compare(self, pairs):
+        """compare_bit_dets + get_det_indexes on the device for 1-based pairs [n, 2]:
+        (ndiffs, is, idx1 [n, 3], idx2 [n, 3])."""
+        pairs = np.ascontiguousarray(pairs, np.int64)
+        n = pairs.shape[0]
+        nf = np.zeros(n, np.int32)
+        isg = np.zeros(n, np.int32)
+        i1 = np.zeros((n, 3), np.int32)
+        i2 = np.zeros((n, 3), np.int32)
+        self._check(self.L.pci_gpu_bit_compare(self.h, n, _p(pairs), _p(nf), _p(isg), _p(i1), _p(i2)))
+        return nf, isg, i1, i2
 
     def csr_info(self, which: int = PCI_MAT_H):
         """(rows, stored elements) of a resident matrix."""

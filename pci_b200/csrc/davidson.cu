@@ -10,8 +10,6 @@
 // (convergence flags, the projected eigensolve) are taken on the host from a
 // few scalars copied back per iteration; the orthogonalisation's pass logic
 // runs in a one-thread kernel so an Ortn call needs no host round trip.
-#include <cublas_v2.h>
-#include <cusolverDn.h>
 
 #include <algorithm>
 #include <cmath>
@@ -249,6 +247,175 @@ __global__ void __launch_bounds__(256) k_resid(double *A, int ld, int64_t nd, in
             part[(size_t)blockIdx.x * nlv + j] = s;
         }
         __syncthreads();
+    }
+}
+
+// D[m + n ldd] += sum_k A(m, k) B(k, n) for m < M, n < N (N <= 16), k < K,
+// with A(m, k) = A[m am + k ak] and B(k, n) = B[k + n ldb]: the two products
+// of the Z1 projector (src/davidson.f90:526-544, DGEMV per level in the
+// reference, here batched over the levels).  FP64 tensor cores (mma m8n8k4):
+// one warp per 8 rows of D, K cut into gridDim.y slices added into D (zeroed
+// by the caller) with atomics.
+__global__ void __launch_bounds__(256) k_gemm_dmma(int M, int N, int K, const double *__restrict__ A, int64_t am,
+                                                   int64_t ak, const double *__restrict__ B, int64_t ldb, double *D,
+                                                   int64_t ldd)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int m0 = (int)(warp * 8);
+    if (m0 >= M) return;
+    const int kc = (K + gridDim.y - 1) / gridDim.y;
+    const int kb = blockIdx.y * kc, ke = min(K, kb + kc);
+    const int rw = lane >> 2, kq = lane & 3;
+    const int m = m0 + rw;
+    double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll 4
+    for (int k0 = kb; k0 < ke; k0 += 4) {
+        const int k = k0 + kq;
+        const bool kin = k < ke;
+        const double a = (m < M && kin) ? A[(int64_t)m * am + (int64_t)k * ak] : 0.0;
+#pragma unroll
+        for (int nt = 0; nt < 2; nt++) {
+            const int n = nt * 8 + rw;
+            const double b = (n < N && kin) ? B[k + (int64_t)n * ldb] : 0.0;
+            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                         : "+d"(acc[nt][0]), "+d"(acc[nt][1])
+                         : "d"(a), "d"(b));
+        }
+    }
+#pragma unroll
+    for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int n = nt * 8 + 2 * kq + u;
+            if (m < M && n < N) atomicAdd(&D[m + (int64_t)n * ldd], acc[nt][u]);
+        }
+}
+
+// D (M x N, column-major, leading dimension ldd) = A B in slices of 16 columns.
+static cudaError_t gemm_dmma(cudaStream_t st, int M, int N, int K, const double *A, int64_t am, int64_t ak,
+                             const double *B, int64_t ldb, double *D, int64_t ldd)
+{
+    for (int n = 0; n < N; n++) {
+        cudaError_t e = cudaMemsetAsync(D + (int64_t)n * ldd, 0, (size_t)M * 8, st);
+        if (e != cudaSuccess) return e;
+    }
+    const int warps = (M + 7) / 8;
+    const dim3 grid((warps + 7) / 8, (unsigned)std::max(1, std::min(32, K / 256)));
+    for (int n0 = 0; n0 < N; n0 += 16)
+        k_gemm_dmma<<<grid, 256, 0, st>>>(M, std::min(16, N - n0), K, A, am, ak, B + (int64_t)n0 * ldb, ldb,
+                                          D + (int64_t)n0 * ldd, ldd);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------- eigenpairs of the initial block ---
+// The reference diagonalises the Nd0 x Nd0 initial block with LAPACK DSYEVD
+// (src/pconf.F90:1874-1889).  Here: one-sided cyclic Jacobi (Hestenes) on the
+// block shifted to be positive definite (the shift is the Gershgorin bound
+// max_i sum_j |a_ij|), whose right singular vectors are the eigenvectors and
+// whose column norms, minus the shift, the eigenvalues.  Every round rotates
+// n/2 disjoint column pairs (round-robin tournament order), one thread block
+// per pair; a sweep is n - 1 rounds, replayed from a CUDA graph until no pair
+// is rotated.
+
+// Gershgorin bound of the column-major n x n block: bound = max over columns
+// (the block is symmetric) of the absolute column sums.
+__global__ void kj_gersh(const double *A, int n, double *colsum)
+{
+    const int j = blockIdx.x;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += fabs(A[i + (int64_t)j * n]);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    __shared__ double red[8];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+        colsum[j] = t;
+    }
+}
+
+// A += shift I; V = I.
+__global__ void kj_init(double *A, double *V, int n, double shift)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < (int64_t)n * n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e % n, j = e / n;
+        if (i == j) A[e] += shift;
+        V[e] = i == j ? 1.0 : 0.0;
+    }
+}
+
+__device__ __forceinline__ double block_sum256(double v, double *red)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int w = 0; w < 8; w++) t += red[w];
+    __syncthreads();
+    return t;
+}
+
+// Round r of a sweep over np (n rounded up to even) indices: pair t of the
+// tournament; the index n (odd n) is a dummy.  Rotates columns p, q of U and V
+// when their cosine |u_p . u_q| / (|u_p| |u_q|) exceeds tol; flag records it.
+__global__ void __launch_bounds__(256) kj_round(double *U, double *V, int n, int np, int r, double tol, int *flag)
+{
+    __shared__ double red[8];
+    const int t = blockIdx.x;
+    int p, q;
+    if (t == 0) { p = np - 1; q = r; }
+    else { p = (r + t) % (np - 1); q = (r - t + np - 1) % (np - 1); }
+    if (p > q) { const int x = p; p = q; q = x; }
+    if (q >= n) return;
+    double *up = U + (int64_t)p * n, *uq = U + (int64_t)q * n;
+    double a = 0.0, b = 0.0, g = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double x = up[i], y = uq[i];
+        a += x * x;
+        b += y * y;
+        g += x * y;
+    }
+    a = block_sum256(a, red);
+    b = block_sum256(b, red);
+    g = block_sum256(g, red);
+    if (!(fabs(g) > tol * sqrt(a * b))) return;
+    if (threadIdx.x == 0) *flag = 1;
+    const double zeta = (b - a) / (2.0 * g);
+    const double tt = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+    const double c = 1.0 / sqrt(1.0 + tt * tt), sn = c * tt;
+    double *vp = V + (int64_t)p * n, *vq = V + (int64_t)q * n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double x = up[i], y = uq[i];
+        up[i] = c * x - sn * y;
+        uq[i] = sn * x + c * y;
+        const double xv = vp[i], yv = vq[i];
+        vp[i] = c * xv - sn * yv;
+        vq[i] = sn * xv + c * yv;
+    }
+}
+
+// Column norms of U.
+__global__ void kj_norms(const double *U, int n, double *out)
+{
+    __shared__ double red[8];
+    const int j = blockIdx.x;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double x = U[i + (int64_t)j * n];
+        s += x * x;
+    }
+    s = block_sum256(s, red);
+    if (threadIdx.x == 0) out[j] = sqrt(s);
+}
+
+// Z[:, k] = V[:, perm[k]].
+__global__ void kj_gather(const double *V, int n, const int *perm, double *Z)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < (int64_t)n * n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e % n, k = e / n;
+        Z[e] = V[i + (int64_t)perm[k] * n];
     }
 }
 
@@ -490,8 +657,6 @@ struct Dvd {
     OrtnState *ost = nullptr;
     int *iconv_d = nullptr, *jsel_d = nullptr;
     std::vector<int> iconv;
-    cublasHandle_t cub = nullptr;
-    cusolverDnHandle_t sol = nullptr;
     int blocks = 148 * 4;
     float spmm_ms = 0;
     int spmm_calls = 0;
@@ -564,13 +729,81 @@ void free_dvd(Dvd &d)
     dev_free(d.A); dev_free(d.D); dev_free(d.Z1); dev_free(d.E1); dev_free(d.C); dev_free(d.Bz); dev_free(d.Sz);
     dev_free(d.part); dev_free(d.small); dev_free(d.ost); dev_free(d.iconv_d); dev_free(d.jsel_d);
     dev_free(d.xp); dev_free(d.yp); dev_free(d.feat); dev_free(d.yout); dev_free(d.ycol);
-    if (d.cub) cublasDestroy(d.cub);
-    if (d.sol) cusolverDnDestroy(d.sol);
     if (d.ea) cudaEventDestroy(d.ea);
     if (d.eb) cudaEventDestroy(d.eb);
 }
 
 }  // namespace
+
+// Device memory released when the scope ends (allocation skipped once rc is set).
+struct DevBlock {
+    void *p = nullptr;
+    DevBlock(pci_gpu *h, size_t bytes, int &rc)
+    {
+        if (!rc) p = dev_alloc(h, bytes, &rc);
+    }
+    ~DevBlock() { dev_free(p); }
+};
+
+// All eigenpairs of the symmetric n x n block A (column-major, device):
+// on return A holds the eigenvectors as columns and E1 (host and E1_dev)
+// the eigenvalues, ascending -- what DSYEVD returns (src/pconf.F90:1874-1889).
+static int block_eigen(pci_gpu *h, cudaStream_t st, double *A, int n, double *E1_dev, std::vector<double> &E1)
+{
+    if (n <= 0) return PCI_OK;
+    int rc = 0;
+    DevBlock V(h, (size_t)n * n * 8, rc), tmp(h, (size_t)n * 8, rc), flag(h, 16, rc), perm(h, (size_t)n * 4, rc);
+    if (rc) return rc;
+    kj_gersh<<<n, 256, 0, st>>>(A, n, (double *)tmp.p);
+    std::vector<double> cs(n);
+    PCI_CUDA(h, cudaMemcpyAsync(cs.data(), tmp.p, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+    PCI_CUDA(h, cudaStreamSynchronize(st));
+    double shift = 0.0;
+    for (double x : cs) shift = std::max(shift, x);
+    shift = shift > 0.0 ? 1.01 * shift : 1.0;
+    kj_init<<<148 * 4, 256, 0, st>>>(A, (double *)V.p, n, shift);
+    PCI_CUDA(h, cudaGetLastError());
+    const int np = n + (n & 1);
+    const double tol = std::max(1e-15, std::sqrt((double)n) * 2.3e-16);
+    bool converged = n == 1;
+    if (!converged) {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        PCI_CUDA(h, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        for (int r = 0; r < np - 1; r++)
+            kj_round<<<np / 2, 256, 0, st>>>(A, (double *)V.p, n, np, r, tol, (int *)flag.p);
+        cudaError_t ce = cudaStreamEndCapture(st, &graph);
+        if (ce != cudaSuccess) return cuda_err(h, ce, "Jacobi sweep capture");
+        ce = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) return cuda_err(h, ce, "Jacobi sweep instantiate");
+        for (int sweep = 0; sweep < 60 && ce == cudaSuccess; sweep++) {
+            int f = 0;
+            ce = cudaMemsetAsync(flag.p, 0, 4, st);
+            if (ce == cudaSuccess) ce = cudaGraphLaunch(exec, st);
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(&f, flag.p, 4, cudaMemcpyDeviceToHost, st);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+            if (ce == cudaSuccess && !f) converged = true;
+            if (converged) break;
+        }
+        cudaGraphExecDestroy(exec);
+        if (ce != cudaSuccess) return cuda_err(h, ce, "Jacobi sweeps");
+    }
+    if (!converged) return set_err(h, PCI_E_CUDA, "eigenpairs of the initial block: Jacobi did not converge in 60 sweeps");
+    kj_norms<<<n, 256, 0, st>>>(A, n, (double *)tmp.p);
+    PCI_CUDA(h, cudaMemcpyAsync(cs.data(), tmp.p, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+    PCI_CUDA(h, cudaStreamSynchronize(st));
+    std::vector<int> order(n);
+    for (int j = 0; j < n; j++) order[j] = j;
+    for (int j = 0; j < n; j++) cs[j] -= shift;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cs[x] < cs[y]; });
+    for (int j = 0; j < n; j++) E1[j] = cs[order[j]];
+    PCI_CUDA(h, cudaMemcpyAsync(perm.p, order.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st));
+    kj_gather<<<148 * 4, 256, 0, st>>>((const double *)V.p, n, (const int *)perm.p, A);
+    PCI_CUDA(h, cudaMemcpyAsync(E1_dev, E1.data(), (size_t)n * 8, cudaMemcpyHostToDevice, st));
+    PCI_CUDA(h, cudaStreamSynchronize(st));
+    return PCI_OK;
+}
 
 int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out, double *Tj_out,
            int32_t *Iconverge_out, double *X_out, int32_t *iters_out, double *resid_out, DvdHarvest *hv)
@@ -643,10 +876,6 @@ int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out
     ALLOC(d.xp, double, nd * Nlv);
     ALLOC(d.yp, double, nd * Nlv);
 #undef ALLOC
-    if (cublasCreate(&d.cub) != CUBLAS_STATUS_SUCCESS) { free_dvd(d); return set_err(h, PCI_E_CUDA, "cublasCreate failed"); }
-    cublasSetStream(d.cub, d.st);
-    if (cusolverDnCreate(&d.sol) != CUSOLVER_STATUS_SUCCESS) { free_dvd(d); return set_err(h, PCI_E_CUDA, "cusolverDnCreate failed"); }
-    cusolverDnSetStream(d.sol, d.st);
     // the SpMM picks the full symmetric copy or the lower-triangle kernel by free memory
     PCI_CUDA(h, cudaMemsetAsync(d.A, 0, (size_t)nd * d.ld * 8, d.st));
     PCI_CUDA(h, cudaMemsetAsync(d.iconv_d, 0, 16 * 4, d.st));
@@ -661,19 +890,7 @@ int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out
         PCI_CUDA(h, cudaMemsetAsync(d.Z1, 0, (size_t)nd0 * nd0 * 8, d.st));
         if (H.val_f32) k_extract_z1<float><<<d.blocks, 256, 0, d.st>>>(H.rowptr, H.col, (const float *)H.val, h->hmin, nd0, d.Z1);
         else k_extract_z1<double><<<d.blocks, 256, 0, d.st>>>(H.rowptr, H.col, (const double *)H.val, h->hmin, nd0, d.Z1);
-        int lwork = 0;
-        cusolverDnDsyevd_bufferSize(d.sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nd0, d.Z1, nd0, d.E1, &lwork);
-        double *work = (double *)dev_alloc(h, (size_t)std::max(lwork, 1) * 8 + 16, &rc);
-        if (rc) { free_dvd(d); return rc; }
-        int *info = (int *)(work + std::max(lwork, 1));
-        cusolverStatus_t cs = cusolverDnDsyevd(d.sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nd0, d.Z1, nd0,
-                                               d.E1, work, lwork, info);
-        int hinfo = 0;
-        cudaMemcpyAsync(&hinfo, info, 4, cudaMemcpyDeviceToHost, d.st);
-        cudaMemcpyAsync(E1.data(), d.E1, (size_t)nd0 * 8, cudaMemcpyDeviceToHost, d.st);
-        cudaStreamSynchronize(d.st);
-        dev_free(work);
-        if (cs != CUSOLVER_STATUS_SUCCESS || hinfo != 0) { free_dvd(d); return set_err(h, PCI_E_CUDA, "DSYEVD of the initial block failed"); }
+        if ((rc = block_eigen(h, d.st, d.Z1, nd0, d.E1, E1))) { free_dvd(d); return rc; }
     }
     cudaEventRecord(t1, d.st);
     // FormB0 (src/davidson.f90:75-193): initial vectors from the Nd0 block;
@@ -833,11 +1050,11 @@ int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out
                 PCI_CUDA(h, cudaMemcpyAsync(d.Bz + (size_t)q * nd0, d.C + (size_t)jsel[q] * nd0, (size_t)nd0 * 8,
                                             cudaMemcpyDeviceToDevice, d.st));
             if (nz > 0 && nd0 > 0) {
-                const double one = 1.0, zero = 0.0;
                 const double *Z1s = d.Z1 + (size_t)(n01 - 1) * nd0;
-                cublasDgemm(d.cub, CUBLAS_OP_T, CUBLAS_OP_N, nz, nj, nd0, &one, Z1s, nd0, d.Bz, nd0, &zero, d.Sz, nz);
+                // Sz = Z1s^T Bz, scaled by 1 / (theta - E1), then Bz = Z1s Sz
+                PCI_CUDA(h, gemm_dmma(d.st, nz, nj, nd0, Z1s, nd0, 1, d.Bz, nd0, d.Sz, nz));
                 k_zscale<<<(nz * nj + 255) / 256, 256, 0, d.st>>>(d.Sz, nz, nj, d.E1 + (n01 - 1), d.small + SM_TSEL);
-                cublasDgemm(d.cub, CUBLAS_OP_N, CUBLAS_OP_N, nd0, nj, nz, &one, Z1s, nd0, d.Sz, nz, &zero, d.Bz, nd0);
+                PCI_CUDA(h, gemm_dmma(d.st, nd0, nj, nz, Z1s, 1, nd0, d.Sz, nz, d.Bz, nd0));
             } else if (nd0 > 0) {
                 PCI_CUDA(h, cudaMemsetAsync(d.Bz, 0, (size_t)nd0 * nj * 8, d.st));
             }

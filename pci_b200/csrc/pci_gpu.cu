@@ -93,7 +93,10 @@ static void free_basis(pci_gpu *h)
     dev_free(h->d_occ); dev_free(h->d_conf_of); dev_free(h->d_conf_start); dev_free(h->d_conf_orb);
     dev_free(h->d_adj_ptr); dev_free(h->d_adj); dev_free(h->d_ms_orb); dev_free(h->d_ms_jz);
     dev_free(h->d_ms_type); dev_free(h->d_orb_l); dev_free(h->d_orb_j); dev_free(h->d_msd);
+    dev_free(h->d_barr);
     h->d_msd = nullptr;
+    h->d_barr = nullptr;
+    h->nint = 0;
     h->d_occ = nullptr; h->d_conf_of = nullptr; h->d_conf_start = nullptr; h->d_conf_orb = nullptr;
     h->d_adj_ptr = nullptr; h->d_adj = nullptr; h->d_ms_orb = nullptr; h->d_ms_jz = nullptr;
     h->d_ms_type = nullptr; h->d_orb_l = nullptr; h->d_orb_j = nullptr;
@@ -519,6 +522,150 @@ int32_t pci_gpu_stats(pci_gpu_t *h, double *out, int32_t n)
 const char *pci_gpu_last_error(pci_gpu_t *h)
 {
     return h ? h->err.c_str() : "null handle";
+}
+
+// ----------------------------------------------------- bit-string path ---
+
+// FormBarr (src/determinants.f90:839-864): bit m-1 of determinant n's bit
+// string is set for each occupied m-state m (1-based): word (m-1)/32, bit
+// (m-1) mod 32; Barr is nint x Nd, column-major.
+__global__ void k_form_barr(const uint16_t *occ, int ne, int64_t nd, int nint, int32_t *barr)
+{
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nd; n += (int64_t)gridDim.x * blockDim.x) {
+        int32_t *b = barr + n * nint;
+        for (int w = 0; w < nint; w++) b[w] = 0;
+        for (int e = 0; e < ne; e++) {
+            const int m = occ[n * ne + e];   // 0-based m-state = (1-based) - 1
+            b[m >> 5] |= (int32_t)(1u << (m & 31));
+        }
+    }
+}
+
+// compare_bit_dets + get_det_indexes (src/determinants.f90:933-1034) for
+// one pair of bit strings, step for step: the difference count from the
+// popcount of the XOR (3 when it reaches 6 differing bits), then for 1 or 2
+// differences the differing positions (1-based) of each determinant and the
+// phase from the positions less the zero bits seen after the first occupied
+// one.  The early exit leaves only the bit loop of the current word, as the
+// reference's `exit` does, so later words still add to the zero-bit count.
+__device__ void d_bit_compare(const int32_t *b1, const int32_t *b2, int nint, int &ndiffs, int &is, int *d1, int *d2)
+{
+    int nf = 0;
+    ndiffs = -1;
+    for (int w = 0; w < nint; w++) {
+        if (b1[w] != 0 || b2[w] != 0) {
+            nf += __popc((uint32_t)(b1[w] ^ b2[w]));
+            if (nf >= 6) {
+                ndiffs = 3;
+                break;
+            }
+        }
+    }
+    if (ndiffs < 0) ndiffs = (nf + 1) / 2;
+    d1[0] = d1[1] = d1[2] = 0;
+    d2[0] = d2[1] = d2[2] = 0;
+    is = 1;
+    if (ndiffs > 2 || ndiffs == 0) return;
+    int i1 = 1, j1 = 1, nzb = 0, first = 0, l1[2] = {0, 0}, l2[2] = {0, 0};
+    for (int w = 0; w < nint; w++) {
+        const uint32_t x1 = (uint32_t)b1[w], x2 = (uint32_t)b2[w];
+        if (x1 == 0 && x2 == 0) continue;
+        for (int bit = 0; bit < 32; bit++) {
+            const int bt1 = (x1 >> bit) & 1, bt2 = (x2 >> bit) & 1;
+            if (bt1 || bt2) first = 1;
+            if (!bt1 && !bt2) {
+                if (first) nzb++;
+            } else if (bt1 != bt2) {
+                const int pos = 32 * w + bit + 1;
+                if (bt1) {
+                    i1++;
+                    if (i1 <= 3) { d1[i1 - 1] = pos; l1[i1 - 2] = pos - nzb; }
+                }
+                if (bt2) {
+                    j1++;
+                    if (j1 <= 3) { d2[j1 - 1] = pos; l2[j1 - 2] = pos - nzb; }
+                }
+                if ((ndiffs == 1 && i1 == 2 && j1 == 2) || (ndiffs == 2 && i1 == 3 && j1 == 3)) break;
+            }
+        }
+    }
+    if (ndiffs == 1) {
+        if (nzb > 0 && abs(l2[0] - l1[0] - 1) % 2 == 1) is = -is;
+    } else {
+        if (abs(l2[0] - l1[0] - nzb % 2) % 2 == 1) is = -is;
+        if (abs(l2[1] - l1[1] - nzb % 2) % 2 == 1) is = -is;
+        int t = d2[1]; d2[1] = d2[2]; d2[2] = t;
+        t = d1[1]; d1[1] = d1[2]; d1[2] = t;
+    }
+}
+
+__global__ void k_bit_compare(const int32_t *barr, int nint, int64_t nd, const int64_t *pairs, int64_t n, int32_t *ndiffs,
+                              int32_t *is, int32_t *idx1, int32_t *idx2, unsigned *err)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t a = pairs[2 * t] - 1, b = pairs[2 * t + 1] - 1;
+        if (a < 0 || a >= nd || b < 0 || b >= nd) {
+            atomicOr(err, DERR_BAD_INDEX);
+            continue;
+        }
+        int nf, s, d1[3], d2[3];
+        d_bit_compare(barr + a * nint, barr + b * nint, nint, nf, s, d1, d2);
+        ndiffs[t] = nf;
+        is[t] = s;
+        for (int q = 0; q < 3; q++) {
+            idx1[3 * t + q] = d1[q];
+            idx2[3 * t + q] = d2[q];
+        }
+    }
+}
+
+int pci_gpu_form_barr(pci_gpu_t *h, int32_t *nint_out, int32_t *barr)
+{
+    if (!h) return PCI_E_INPUT;
+    cudaSetDevice(h->device);
+    if (!h->have_basis) return set_err(h, PCI_E_STATE, "form_barr before set_basis");
+    const int nint = (h->nst + 31) / 32;
+    if (!h->d_barr) {
+        int rc = 0;
+        h->d_barr = (int32_t *)dev_alloc(h, (size_t)nint * std::max<int64_t>(h->nd, 1) * 4, &rc);
+        if (rc) return rc;
+        h->nint = nint;
+        k_form_barr<<<148 * 4, 256, 0, h->st>>>(h->d_occ, h->ne, h->nd, nint, h->d_barr);
+        PCI_CUDA(h, cudaGetLastError());
+    }
+    if (nint_out) *nint_out = nint;
+    if (barr) PCI_CUDA(h, cudaMemcpyAsync(barr, h->d_barr, (size_t)nint * h->nd * 4, cudaMemcpyDeviceToHost, h->st));
+    PCI_CUDA(h, cudaStreamSynchronize(h->st));
+    return PCI_OK;
+}
+
+int pci_gpu_bit_compare(pci_gpu_t *h, int64_t n, const int64_t *pairs, int32_t *ndiffs, int32_t *is, int32_t *idx1,
+                        int32_t *idx2)
+{
+    if (!h || n < 0 || (n && (!pairs || !ndiffs || !is || !idx1 || !idx2))) return PCI_E_INPUT;
+    cudaSetDevice(h->device);
+    if (!h->d_barr) return set_err(h, PCI_E_STATE, "bit_compare before form_barr");
+    if (n == 0) return PCI_OK;
+    int rc = 0;
+    char *buf = (char *)dev_alloc(h, (size_t)n * (16 + 4 * 8), &rc);
+    if (rc) return rc;
+    int64_t *dp = (int64_t *)buf;
+    int32_t *dn = (int32_t *)(buf + n * 16), *ds = dn + n, *d1 = ds + n, *d2 = d1 + 3 * n;
+    PCI_CUDA(h, cudaMemsetAsync(h->d_err, 0, 4, h->st));
+    PCI_CUDA(h, cudaMemcpyAsync(dp, pairs, (size_t)n * 16, cudaMemcpyHostToDevice, h->st));
+    k_bit_compare<<<148 * 4, 256, 0, h->st>>>(h->d_barr, h->nint, h->nd, dp, n, dn, ds, d1, d2, h->d_err);
+    unsigned e = 0;
+    cudaError_t ce = cudaGetLastError();
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(ndiffs, dn, (size_t)n * 4, cudaMemcpyDeviceToHost, h->st);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(is, ds, (size_t)n * 4, cudaMemcpyDeviceToHost, h->st);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(idx1, d1, (size_t)n * 12, cudaMemcpyDeviceToHost, h->st);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(idx2, d2, (size_t)n * 12, cudaMemcpyDeviceToHost, h->st);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(&e, h->d_err, 4, cudaMemcpyDeviceToHost, h->st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->st);
+    dev_free(buf);
+    if (ce != cudaSuccess) return cuda_err(h, ce, "bit_compare");
+    if (e) return set_err(h, PCI_E_INPUT, "bit_compare: determinant index out of 1..Nd");
+    return PCI_OK;
 }
 
 void pci_gpu_destroy(pci_gpu_t *h)

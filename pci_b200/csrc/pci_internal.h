@@ -69,6 +69,8 @@ struct pci_gpu {
     std::vector<int32_t> h_jterms;    // Jt(1:Njd): sorted 2J of the terms present
     std::vector<unsigned long long> h_rowwork;   // determinant pairs per row, per configuration
     uint32_t *d_msd = nullptr;                   // packed m-state descriptors
+    int32_t *d_barr = nullptr;                   // Barr(nint, Nd) bit strings (pci_gpu_form_barr), or null
+    int nint = 0;
     uint16_t *d_occ = nullptr;
     int32_t *d_conf_of = nullptr;
     int64_t *d_conf_start = nullptr;
