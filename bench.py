@@ -71,6 +71,7 @@ def parse():
     ap.add_argument("--profile-case", default=None,
                     help="only a short batched solve of this configuration, for profiler captures")
     ap.add_argument("--case-iters", type=int, default=6, help="iterations of --profile-case")
+    ap.add_argument("--case-train", type=int, default=0, help="training epochs before --profile-case's solve")
     ap.add_argument("--batch-blocks", type=int, default=64)
     ap.add_argument("--batch-variant", type=int, default=-1, help="SpMM variant of the batched form "
                     "(-1: from the tuning cache, tuned when absent)")
@@ -619,6 +620,11 @@ def run_profile_case(args):
     from pci_b200.capi import PCI_BATCH_CORR_LEARNED, Batch, Engine, Mlp
     sysm = S.make_system(**S.CONFIGS[args.profile_case]())
     m = Mlp(LR.NIN_DEFAULT, 0, seed=1)
+    if args.case_train > 0:   # training steps on random samples (the network's tensor-core GEMMs)
+        rng = np.random.default_rng(5)
+        F = rng.standard_normal((16384, LR.NIN_DEFAULT)).astype(np.float32)
+        T = rng.standard_normal(16384).astype(np.float32)
+        m.train(F, T, epochs=args.case_train, batch=4096, lr=1e-3, seed=1)
     with Engine(0) as e:
         e.load_system(sysm)
         e.form_h(64)

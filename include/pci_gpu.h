@@ -195,8 +195,9 @@ int32_t pci_gpu_jterms(pci_gpu_t *h, int32_t *out, int32_t cap);
 
 /* ---- Learned Davidson correction ------------------------------------------
  * A small MLP (nin -> 128 -> 128 -> 128 -> 1, ReLU) whose forward and
- * backward kernels read BF16 weights and accumulate in FP32, with FP32
- * master weights and Adam moments; trained on the GPU.  No counterpart in
+ * backward products run on the tensor cores with BF16 weights, FP32
+ * activations split into two BF16 terms (hi + lo) and FP32 accumulation, with
+ * FP32 master weights and Adam moments; trained on the GPU.  No counterpart in
  * the reference, which has only the diagonal correction of Dvdsn
  * (davidson.f90:436-570).  Parameters are laid out layer by layer as
  * W (din x dout, row-major) then b (dout). */

@@ -1,8 +1,9 @@
 // Learned Davidson correction: a small MLP (nin -> 128 -> 128 -> 128 -> 1,
 // ReLU) with BF16 weights used by the forward and backward kernels and FP32
 // master weights, activations, gradients and Adam moments.  Trained on the
-// GPU by the kernels of this file; evaluated per determinant by the
-// Davidson's learned mode.
+// GPU by the kernels of this file, whose products run on the tensor cores
+// (split-BF16 mma.sync with FP32 accumulation); evaluated per determinant by
+// the Davidson's learned mode (mlp_tc.cuh).
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -19,54 +20,87 @@ namespace {
 constexpr int HID = 128;
 constexpr int NLAYER = 4;   // three hidden layers and the output layer
 constexpr int TB = 64;      // GEMM tile (rows and columns)
-constexpr int TKK = 16;     // GEMM tile depth
 
-// C[i][j] (+)= sum_p A(i,p) B(p,j), A(i,p) = A[i*ars + p*acs], B(p,j) =
-// B[p*brs + j*bcs]; a 64 x 64 tile per block, 4 x 4 outputs per thread,
-// the reduction split over gridDim.z with atomic adds when split.
-template <typename BT>
-__global__ void __launch_bounds__(256) k_gemm(int M, int N, int K, const float *A, int64_t ars, int64_t acs,
-                                              const BT *B, int64_t brs, int64_t bcs, float *C, int64_t ldc,
-                                              int accumulate)
+// C[i][j] = sum_p A(i,p) B(p,j) on the tensor cores (mma.sync m16n8k16, BF16
+// in, FP32 accumulate), A(i,p) = A[i*ars + p*acs], B(p,j) = B[p*brs + j*bcs].
+// An FP32 operand is split into hi = bf16(x) and lo = bf16(x - hi) and the
+// products hi*hi + hi*lo + lo*hi are summed (split-BF16: about 16 bits of
+// each FP32 operand kept); a BF16 operand (the weights) is exact.  A 64 x 64
+// tile per block of 4 warps (32 x 32 each), 16-deep steps through shared
+// memory; the reduction is split over gridDim.z with atomic adds when split.
+template <typename AT, typename BT>
+__global__ void __launch_bounds__(128) k_gemm_tc(int M, int N, int K, const AT *A, int64_t ars, int64_t acs,
+                                                 const BT *B, int64_t brs, int64_t bcs, float *C, int64_t ldc)
 {
-    __shared__ float As[TKK][TB + 1];
-    __shared__ float Bs[TKK][TB + 1];
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    __shared__ float As[16][TB + 4];
+    __shared__ float Bs[16][TB + 4];
+    constexpr bool ASPLIT = sizeof(AT) == 4, BSPLIT = sizeof(BT) == 4;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int g = lane >> 2, q = lane & 3;
+    const int wm = (w >> 1) * 32, wn = (w & 1) * 32;
     const int i0 = blockIdx.y * TB, j0 = blockIdx.x * TB;
     const int kchunk = (K + gridDim.z - 1) / gridDim.z;
     const int kbeg = blockIdx.z * kchunk, kend = min(K, kbeg + kchunk);
-    float acc[4][4] = {};
-    for (int p0 = kbeg; p0 < kend; p0 += TKK) {
-        for (int t = threadIdx.x; t < TKK * TB; t += 256) {
-            const int pp = t / TB, ii = t % TB;
+    float acc[2][4][4] = {};
+    for (int p0 = kbeg; p0 < kend; p0 += 16) {
+        for (int e = t; e < 16 * TB; e += 128) {
+            const int pp = e / TB, ii = e % TB;
             const int p = p0 + pp;
-            As[pp][ii] = (i0 + ii < M && p < kend) ? A[(int64_t)(i0 + ii) * ars + (int64_t)p * acs] : 0.0f;
+            As[pp][ii] = (i0 + ii < M && p < kend) ? (float)A[(int64_t)(i0 + ii) * ars + (int64_t)p * acs] : 0.0f;
             Bs[pp][ii] = (j0 + ii < N && p < kend) ? (float)B[(int64_t)p * brs + (int64_t)(j0 + ii) * bcs] : 0.0f;
         }
         __syncthreads();
+        uint32_t ah[2][4], al[2][4];
 #pragma unroll
-        for (int pp = 0; pp < TKK; pp++) {
-            float a[4], b[4];
+        for (int mt = 0; mt < 2; mt++) {
+            const int r0 = wm + mt * 16 + g;
+            const float v[8] = {As[2 * q][r0],     As[2 * q + 1][r0],     As[2 * q][r0 + 8],     As[2 * q + 1][r0 + 8],
+                                As[2 * q + 8][r0], As[2 * q + 9][r0],     As[2 * q + 8][r0 + 8], As[2 * q + 9][r0 + 8]};
 #pragma unroll
-            for (int u = 0; u < 4; u++) { a[u] = As[pp][ty * 4 + u]; b[u] = Bs[pp][tx * 4 + u]; }
+            for (int u = 0; u < 4; u++) {
+                const float x0 = v[2 * u], x1 = v[2 * u + 1];
+                ah[mt][u] = mlptc::pack2(x0, x1);
+                if (ASPLIT) {
+                    const __nv_bfloat162 hh = *reinterpret_cast<const __nv_bfloat162 *>(&ah[mt][u]);
+                    al[mt][u] = mlptc::pack2(x0 - __low2float(hh), x1 - __high2float(hh));
+                }
+            }
+        }
 #pragma unroll
-            for (int u = 0; u < 4; u++)
+        for (int nt = 0; nt < 4; nt++) {
+            const int c0 = wn + nt * 8 + g;
+            const float v[4] = {Bs[2 * q][c0], Bs[2 * q + 1][c0], Bs[2 * q + 8][c0], Bs[2 * q + 9][c0]};
+            const uint32_t bh0 = mlptc::pack2(v[0], v[1]), bh1 = mlptc::pack2(v[2], v[3]);
+            uint32_t bl0 = 0, bl1 = 0;
+            if (BSPLIT) {
+                const __nv_bfloat162 h0 = *reinterpret_cast<const __nv_bfloat162 *>(&bh0);
+                const __nv_bfloat162 h1 = *reinterpret_cast<const __nv_bfloat162 *>(&bh1);
+                bl0 = mlptc::pack2(v[0] - __low2float(h0), v[1] - __high2float(h0));
+                bl1 = mlptc::pack2(v[2] - __low2float(h1), v[3] - __high2float(h1));
+            }
 #pragma unroll
-                for (int w = 0; w < 4; w++) acc[u][w] += a[u] * b[w];
+            for (int mt = 0; mt < 2; mt++) {
+                mlptc::mma16816(acc[mt][nt], ah[mt], bh0, bh1);
+                if (BSPLIT) mlptc::mma16816(acc[mt][nt], ah[mt], bl0, bl1);
+                if (ASPLIT) mlptc::mma16816(acc[mt][nt], al[mt], bh0, bh1);
+            }
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int u = 0; u < 4; u++)
+    for (int mt = 0; mt < 2; mt++)
 #pragma unroll
-        for (int w = 0; w < 4; w++) {
-            const int i = i0 + ty * 4 + u, j = j0 + tx * 4 + w;
-            if (i < M && j < N) {
-                float *c = &C[(int64_t)i * ldc + j];
-                if (gridDim.z > 1) atomicAdd(c, acc[u][w]);
-                else *c = accumulate ? *c + acc[u][w] : acc[u][w];
+        for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int i = i0 + wm + mt * 16 + g + (u >= 2 ? 8 : 0);
+                const int j = j0 + wn + nt * 8 + 2 * q + (u & 1);
+                if (i < M && j < N) {
+                    float *c = &C[(int64_t)i * ldc + j];
+                    if (gridDim.z > 1) atomicAdd(c, acc[mt][nt][u]);
+                    else *c = acc[mt][nt][u];
+                }
             }
-        }
 }
 
 // Z += bias (per column), A = relu(Z) when relu
@@ -230,18 +264,20 @@ static int mlp_reserve(pci_mlp *m, int64_t n)
     return PCI_OK;
 }
 
+// Activations x BF16 weights (forward, and the backward's dA = dZ W^T).
 static void gemm(cudaStream_t st, int M, int N, int K, const float *A, int64_t ars, int64_t acs, const __nv_bfloat16 *B,
                  int64_t brs, int64_t bcs, float *C, int64_t ldc, int split)
 {
     dim3 grid((N + TB - 1) / TB, (M + TB - 1) / TB, split);
-    k_gemm<__nv_bfloat16><<<grid, 256, 0, st>>>(M, N, K, A, ars, acs, B, brs, bcs, C, ldc, 0);
+    k_gemm_tc<float, __nv_bfloat16><<<grid, 128, 0, st>>>(M, N, K, A, ars, acs, B, brs, bcs, C, ldc);
 }
 
+// FP32 x FP32 (the weight gradients in^T dZ), both operands split.
 static void gemm_f(cudaStream_t st, int M, int N, int K, const float *A, int64_t ars, int64_t acs, const float *B,
                    int64_t brs, int64_t bcs, float *C, int64_t ldc, int split)
 {
     dim3 grid((N + TB - 1) / TB, (M + TB - 1) / TB, split);
-    k_gemm<float><<<grid, 256, 0, st>>>(M, N, K, A, ars, acs, B, brs, bcs, C, ldc, 0);
+    k_gemm_tc<float, float><<<grid, 128, 0, st>>>(M, N, K, A, ars, acs, B, brs, bcs, C, ldc);
 }
 
 // Forward pass over n rows of m->x; output (pre-activation of the last
@@ -268,7 +304,7 @@ static int mlp_backward_dev(pci_mlp *m, int64_t n, float *loss_host)
     MLP_CUDA(m, cudaMemsetAsync(m->g, 0, (size_t)m->nparam * 4, m->st));
     k_mse<<<148 * 4, 256, 0, m->st>>>(m->A[NLAYER - 1], m->t, n, m->dA, m->loss);
     float *dZ = m->dA, *dnext = m->dB;
-    const int split = (int)std::min<int64_t>(148, std::max<int64_t>(1, n / 2048));
+    const int split = (int)std::min<int64_t>(148, std::max<int64_t>(1, n / 256));
     for (int l = NLAYER - 1; l >= 0; l--) {
         const int K = m->din[l], N = m->dout[l];
         const float *in = l ? m->A[l - 1] : m->x;
