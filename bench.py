@@ -15,9 +15,15 @@ lower-triangle CSR (NumH non-zeros).  Metric: H-build nnz/s.
   --impl reference -- the oracle (C restatement of the reference's FormH) on
             the host cores, rows sampled per step.
 
-Time to roots (key "time_to_roots", skipped with --no-roots): the
-configuration's Nlv roots to residual 1e-8 through the batched solver with
-one block, H formed in FP64 (plain) and in FP32 (mixed), FormH + solve each.
+Time to roots (key "time_to_roots", skipped with --no-roots): the config-3
+system's 10 roots (4 valence electrons, 140 orbitals, Nd 1.3M) to residual
+1e-8 against the FP64 H through the batched solver with one block, FormH +
+solve each, in three forms: fp64 (FP64 SpMM, diagonal correction), mixed
+(FP32 SpMM phase, then FP64 to the criterion) and learned_mixed (the mixed
+form with the learned correction, trained first on the solver's own runs of
+four smaller systems of the same orbital basis; skipped with --no-learned).
+Each SpMM is set against HBM and against the measured L2 reduction
+throughput that bounds it.
 
 Batched form (key "batched", skipped with --no-batched): 64 synthetic ions
 (seeds 1000-1063; 2-4 valence electrons, 30-120 orbitals, mixed M and
@@ -546,17 +552,9 @@ def run_batched(args, local, rank, world, dist, peak, peak_kind):
     from pci_b200 import system as S
     from pci_b200.capi import Batch, Engine
     blocks = S.make_batch(args.batch_blocks)
-    order = sorted(range(len(blocks)), key=lambda i: -blocks[i].nd)
     # with several GPUs the blocks are split over the ranks (largest first to
     # the least loaded rank by determinants), no communication
-    load = [0] * world
-    mine = []
-    for i in order:
-        rk = min(range(world), key=lambda q: (load[q], q))
-        load[rk] += blocks[i].nd
-        if rk == rank:
-            mine.append(i)
-    order = mine
+    order = S.split_blocks([blk.nd for blk in blocks], world, rank)
     b = Batch(local)
     formh_ms = 0.0
     launches = 0

@@ -47,6 +47,35 @@ module pci_gpu_mod
        import; type(c_ptr), value :: h; real(c_double) :: X(*), Tj(*)
        integer(c_int32_t), value :: nv; integer(c_int64_t), value :: nlim
      end function
+     integer(c_int) function pci_gpu_csr_info(h, which, nrows, nnz) bind(C)
+       import; type(c_ptr), value :: h; integer(c_int32_t), value :: which
+       integer(c_int64_t) :: nrows, nnz
+     end function
+     ! one rank's row range of H (which 0) or J^2 (which 1), as RedistributeHamCSR leaves it
+     integer(c_int) function pci_gpu_get_csr_rows(h, which, row_lo, row_hi, rowptr, col, val) bind(C)
+       import; type(c_ptr), value :: h; integer(c_int32_t), value :: which
+       integer(c_int64_t), value :: row_lo, row_hi
+       integer(c_int64_t) :: rowptr(*)
+       type(c_ptr), value :: col, val
+     end function
+     ! FormBarr: Barr(nint, Nd) of the basis (barr may be c_null_ptr)
+     integer(c_int) function pci_gpu_form_barr(h, nint, barr) bind(C)
+       import; type(c_ptr), value :: h; integer(c_int32_t) :: nint
+       type(c_ptr), value :: barr
+     end function
+     ! compare_bit_dets + get_det_indexes for n pairs (pairs(2, n), 1-based)
+     integer(c_int) function pci_gpu_bit_compare(h, n, pairs, ndiffs, is, idx1, idx2) bind(C)
+       import; type(c_ptr), value :: h; integer(c_int64_t), value :: n
+       integer(c_int64_t) :: pairs(*)
+       integer(c_int32_t) :: ndiffs(*), is(*), idx1(*), idx2(*)
+     end function
+     ! CONF.HIJ / CONF.JJJ record stream (sort.f90), written in row ranges
+     integer(c_int) function pci_io_append_hij(path, row0, nrows, rowptr, col, val, errbuf, errlen) bind(C)
+       import; character(kind=c_char) :: path(*), errbuf(*)
+       integer(c_int64_t), value :: row0, nrows
+       integer(c_int64_t) :: rowptr(*); integer(c_int32_t) :: col(*); real(c_double) :: val(*)
+       integer(c_int32_t), value :: errlen
+     end function
      type(c_ptr) function pci_gpu_last_error(h) bind(C)
        import; type(c_ptr), value :: h
      end function

@@ -511,15 +511,19 @@ class Batch:
     def set_harvest(self, rows_per_block, capacity, seed=0):
         """Record training samples in the next solves (0 rows: off)."""
         self._check(self.L.pci_batch_set_harvest(self.b, rows_per_block, capacity, seed))
+        self._hv_cap = int(capacity) if rows_per_block > 0 else 0
 
     def harvest(self):
-        """Samples of the last solve as a structured array (SAMPLE_DTYPE) and the number recorded."""
+        """Samples of the last solve as a structured array (SAMPLE_DTYPE), and the
+        number the solve produced (above the capacity given to set_harvest, the
+        samples past the capacity were dropped and are not in the array)."""
         cnt = C.c_int64()
         self._check(self.L.pci_batch_harvest(self.b, None, 0, C.byref(cnt)))
-        out = np.zeros(cnt.value, SAMPLE_DTYPE)
-        if cnt.value:
-            self._check(self.L.pci_batch_harvest(self.b, out.ctypes.data_as(C.c_void_p), cnt.value, C.byref(cnt)))
-        return out[:min(cnt.value, out.size)], int(cnt.value)
+        n = min(cnt.value, getattr(self, "_hv_cap", 0))
+        out = np.zeros(n, SAMPLE_DTYPE)
+        if n:
+            self._check(self.L.pci_batch_harvest(self.b, out.ctypes.data_as(C.c_void_p), n, C.byref(cnt)))
+        return out, int(cnt.value)
 
     def close(self):
         if self.b:

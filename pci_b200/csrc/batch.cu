@@ -154,29 +154,41 @@ __global__ void kb_set_units(double *V, int64_t ld, const int64_t *pos, int n)
 
 // ------------------------------------------------------------- SpMM ---
 
+// Stored value kinds of a block: FP32, FP64, or split FP32 pairs.
+enum { VK_F32 = 0, VK_F64 = 1, VK_SPLIT = 2 };
+
 // Value of stored element l as the arithmetic type XT of the SpMM: FP32
 // vectors take the FP32 value (hi of a split pair), FP64 vectors the FP64
-// value (hi + lo of a split pair).
-template <typename XT>
-__device__ __forceinline__ XT blk_val(const BlkCsr &B, int64_t l)
+// value (hi + lo of a split pair).  The kind is a template parameter so the
+// element loop has no branch on it and its loads issue back to back.
+template <typename XT, int VK>
+__device__ __forceinline__ XT blk_val(const void *val, int64_t l)
 {
-    if (B.f64) return (XT)__ldg(&((const double *)B.val)[l]);
-    if (B.split) {
-        const float2 hl = __ldg(&((const float2 *)B.val)[l]);
-        if (sizeof(XT) == 4) return (XT)hl.x;
-        return (XT)((double)hl.x + (double)hl.y);
+    if constexpr (VK == VK_F64) {
+        return (XT)__ldg(&((const double *)val)[l]);
+    } else if constexpr (VK == VK_SPLIT) {
+        const float2 hl = __ldg(&((const float2 *)val)[l]);
+        if constexpr (sizeof(XT) == 4) return (XT)hl.x;
+        else return (XT)((double)hl.x + (double)hl.y);
+    } else {
+        return (XT)__ldg(&((const float *)val)[l]);
     }
-    return (XT)__ldg(&((const float *)B.val)[l]);
+}
+
+__device__ __forceinline__ int blk_kind(const BlkCsr &B)
+{
+    return B.f64 ? VK_F64 : (B.split ? VK_SPLIT : VK_F32);
 }
 
 // Row n (local row ln) of block B for vector v: the row part of the product
 // (returned; both triangles for a full copy) and, for a lower triangle, the
 // transpose part added to Y by global reductions.  XT is the vector and sum
 // type (double, or float in the first phase of the mixed-precision form).
-template <int NV, int G, typename XT>
+template <int NV, int G, typename XT, int VK>
 __device__ __forceinline__ XT spmm_row(const BlkCsr &B, int64_t ln, int64_t n, int g, int v,
                                        const XT *__restrict__ X, XT *Y)
 {
+    const void *val = B.val;
     const int64_t l0 = __ldg(&B.rowptr[ln]), l1 = __ldg(&B.rowptr[ln + 1]);
     XT acc = 0;
     int64_t l = l0 + g;
@@ -187,14 +199,14 @@ __device__ __forceinline__ XT spmm_row(const BlkCsr &B, int64_t ln, int64_t n, i
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 k[u] = __ldg(&B.col[l + u * G]);
-                t[u] = blk_val<XT>(B, l + u * G);
+                t[u] = blk_val<XT, VK>(val, l + u * G);
             }
 #pragma unroll
             for (int u = 0; u < 4; u++) xk[u] = __ldg(&X[(B.r0 + k[u]) * NV + v]);
 #pragma unroll
             for (int u = 0; u < 4; u++) acc += t[u] * xk[u];
         }
-        for (; l < l1; l += G) acc += blk_val<XT>(B, l) * __ldg(&X[(B.r0 + __ldg(&B.col[l])) * NV + v]);
+        for (; l < l1; l += G) acc += blk_val<XT, VK>(val, l) * __ldg(&X[(B.r0 + __ldg(&B.col[l])) * NV + v]);
         return acc;
     }
     const XT xn = __ldg(&X[n * NV + v]);
@@ -205,7 +217,7 @@ __device__ __forceinline__ XT spmm_row(const BlkCsr &B, int64_t ln, int64_t n, i
 #pragma unroll
         for (int u = 0; u < 4; u++) {
             k[u] = __ldg(&B.col[l + u * G]);
-            t[u] = blk_val<XT>(B, l + u * G);
+            t[u] = blk_val<XT, VK>(val, l + u * G);
         }
 #pragma unroll
         for (int u = 0; u < 4; u++) xk[u] = __ldg(&X[(B.r0 + k[u]) * NV + v]);
@@ -217,7 +229,7 @@ __device__ __forceinline__ XT spmm_row(const BlkCsr &B, int64_t ln, int64_t n, i
     }
     for (; l < l1; l += G) {
         const int k = __ldg(&B.col[l]);
-        const XT t = blk_val<XT>(B, l);
+        const XT t = blk_val<XT, VK>(val, l);
         const int64_t kg = B.r0 + k;
         if (k != ln) atomicAdd(&Y[kg * NV + v], t * xn);
         acc += t * __ldg(&X[kg * NV + v]);
@@ -257,7 +269,10 @@ __global__ void __launch_bounds__(256) kb_spmm(const BlkCsr *__restrict__ blks, 
         if (ok && act) {
             const BlkCsr B = blks[b];
             full = B.full != 0;
-            acc = spmm_row<NV, G, XT>(B, n - B.r0, n, g, v, X, Y);
+            const int vk = blk_kind(B);
+            if (vk == VK_F64) acc = spmm_row<NV, G, XT, VK_F64>(B, n - B.r0, n, g, v, X, Y);
+            else if (vk == VK_SPLIT) acc = spmm_row<NV, G, XT, VK_SPLIT>(B, n - B.r0, n, g, v, X, Y);
+            else acc = spmm_row<NV, G, XT, VK_F32>(B, n - B.r0, n, g, v, X, Y);
         }
 #pragma unroll
         for (int gg = 1; gg < G; gg++) {
@@ -1446,7 +1461,7 @@ static int prepare(pci_batch *b, int nlv)
 
 // Revision of the SpMM kernels, part of the cache key: cached picks of an
 // older kernel are not reused.
-static const int SPMM_REV = 7;
+static const int SPMM_REV = 8;
 
 static std::string tune_key(pci_batch *b, int nv)
 {

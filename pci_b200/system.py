@@ -555,6 +555,23 @@ def _make_block(kw):
     return make_system(**kw)
 
 
+def split_blocks(nds, world, rank):
+    """Indices of the blocks rank `rank` of `world` solves: blocks taken largest
+    first (by determinant count), each to the rank with the fewest determinants
+    so far (lowest rank on ties).  Every rank computes the same split from the
+    same counts, so no communication is needed; the ranks' sets partition the
+    blocks."""
+    order = sorted(range(len(nds)), key=lambda i: (-int(nds[i]), i))
+    load = [0] * world
+    mine = []
+    for i in order:
+        rk = min(range(world), key=lambda q: (load[q], q))
+        load[rk] += int(nds[i])
+        if rk == rank:
+            mine.append(i)
+    return mine
+
+
 def make_batch(nblocks=64, seed0=1000, nd_lo=2000, nd_hi=400000, workers=None):
     """Every block of the batched workload as a CISystem, generated in a pool
     of spawned worker processes (safe to start after CUDA is initialised)."""

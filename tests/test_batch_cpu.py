@@ -33,3 +33,49 @@ def test_truncated_block_reaches_its_count():
     assert s.nd - int(s.ndc[-1]) < kw["max_nd"]
     assert s.ne == kw["ne"] and s.mj == kw["mj"]
     assert s.nsu <= sum(1 if l == 0 else 2 for _, l in kw["shells"])
+
+
+def test_split_blocks_partitions_and_balances():
+    nds = [kw["max_nd"] for kw in S.batch_blocks()]
+    for world in (1, 2, 4, 8):
+        parts = [S.split_blocks(nds, world, r) for r in range(world)]
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(len(nds)))              # every block once
+        loads = [sum(nds[i] for i in p) for p in parts]
+        # greedy largest-first: no rank exceeds the lightest by more than the largest block
+        assert max(loads) - min(loads) <= max(nds)
+    assert S.split_blocks(nds, 1, 0)[0] == int(np.argmax(nds))
+
+
+def _split_worker(rank, port, q):
+    import os
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=2)
+    nds = [kw["max_nd"] for kw in S.batch_blocks()]
+    mine = S.split_blocks(nds, 2, rank)
+    got = [None, None]
+    dist.all_gather_object(got, mine)
+    q.put((rank, got))
+    dist.destroy_process_group()
+
+
+def test_split_blocks_two_gloo_ranks():
+    """Two ranks compute their shares independently; gathered over gloo, the
+    shares agree between ranks and partition the 64 blocks."""
+    import multiprocessing as mp
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    ps = [ctx.Process(target=_split_worker, args=(r, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    for p in ps:
+        p.join(120)
+    res = dict(q.get(timeout=10) for _ in range(2))
+    assert res[0] == res[1]
+    assert sorted(res[0][0] + res[0][1]) == list(range(64))
+    assert not set(res[0][0]) & set(res[0][1])

@@ -353,3 +353,21 @@ def test_j_av_matches_oracle(engine, name):
         got = engine.j_av(X, nlim)
         ref = np.array([O.j_av(jr, jc, jv, X[:, v], nlim) for v in range(5)])
         assert np.allclose(got, ref, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("name", ["small3", "cfg1"])
+def test_hij_streamed_from_device(engine, name, tmp_path):
+    """CONF.HIJ and CONF.JJJ (src/sort.f90:16-80) streamed from the resident
+    matrices in row ranges (pci_gpu_get_csr_rows + pci_io_append_hij) are the
+    same bytes as the stream written from the oracle's FormH / FormJ CSR."""
+    from pci_b200 import files
+    s = get_system(name)
+    (rp, col, val, *_), (jr, jc, jv) = oracle_h(name)
+    _load(engine, s)
+    engine.form_h(64)
+    engine.form_j()
+    for which, (r, c, v) in ((0, (rp, col, val)), (1, (jr, jc, jv))):
+        got, want = tmp_path / f"dev{which}.HIJ", tmp_path / f"orc{which}.HIJ"
+        files.write_hij_from_engine(got, engine, which, rows_per_chunk=97)
+        files.write_hij(want, np.asarray(r, np.int64), np.asarray(c, np.int32), np.asarray(v, np.float64))
+        assert got.read_bytes() == want.read_bytes()
