@@ -942,7 +942,6 @@ int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out
     int it_done = 0, n1 = 2 * Nlv;
     const int n01 = (p->Kl4 == 2 || p->Kl4 == -2) ? 1 : Nlv + 1;
     const int nz = nd0 - n01 + 1;
-    bool converged = false;
     for (int it = 1; it <= p->N_it; it++) {
         if (!(ax > crit)) continue;
         it_done = it;
@@ -1157,11 +1156,9 @@ int dv_run(pci_gpu *h, const pci_dvd_params *p, const double *X0, double *Tk_out
         } else {
             if (it == 1)
                 for (int k = 0; k < Nlv; k++) Tk[k] = E[k];
-            converged = true;
             break;
         }
     }
-    (void)converged;
     if (hv) {
         // targets of the recorded samples: the converged vector minus the vector of
         // that iteration (signs aligned), in units of the residual scale

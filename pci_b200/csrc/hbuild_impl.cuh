@@ -879,14 +879,16 @@ __global__ void __launch_bounds__(WARPS * 32, PCI_TILES_MIN_BLOCKS) k_tiles(DevS
                         ws->u.t.tcol[i] = (uint8_t)((__ldg(&S.msd[m]) >> 10) & 63u);
                     }
                     __syncwarp();
+                    // pair idx = r * nkc + kk, lane + 32 s at step s: (r, kk) advance
+                    // by (32 / nkc, 32 % nkc) per step with a carry, no division
                     const int np = nrc * nkc;
+                    const int dr = 32 / nkc, dk = 32 - dr * nkc;
+                    int r = lane / nkc;
+                    int kk = lane - r * nkc;
                     int qn = 0;
                     for (int base = 0; base < np; base += 32) {
-                        const int idx = base + lane;
-                        const int r = idx / nkc;
-                        const int kk = idx - r * nkc;
                         bool cand = false;
-                        if (idx < np && !(diag && k0 + kc + kk > rb + r)) {
+                        if (base + lane < np && !(diag && k0 + kc + kk > rb + r)) {
                             ty.nscan++;
                             uint16_t d1[NE], d2[NE];
 #pragma unroll
@@ -910,6 +912,9 @@ __global__ void __launch_bounds__(WARPS * 32, PCI_TILES_MIN_BLOCKS) k_tiles(DevS
                             qn -= 32;
                             __syncwarp();
                         }
+                        r += dr;
+                        kk += dk;
+                        if (kk >= nkc) { kk -= nkc; r++; }
                     }
                     if (qn > 0) eval_queue<NE, KIND, FILL, VT>(S, ws, tkind, qn, rb, k0 + kc, col, val, ty, lane);
                 }
