@@ -437,7 +437,7 @@ def train_correction(args, sysm_kw, nlv, local):
         kw = dict(sysm_kw)
         kw.update(seed=sd, max_nd=args.learn_nd)
         systems.append(S.make_system(**kw))
-    F, T, info = LR.harvest(systems, nlv=nlv, rows_per_block=4000, device=local, max_sub=96, keep=48)
+    F, T, info = LR.harvest(systems, nlv=nlv, rows_per_block=4000, device=local, max_sub=112, keep=48)
     model, loss = LR.train(F, T, device=local, epochs=4)
     return model, {"train_systems": f"{len(systems)} systems, seeds 100-103, {args.learn_nd} determinants each "
                                     f"(same orbital basis)", "samples": int(F.shape[0]), "loss": loss,
@@ -464,7 +464,7 @@ def time_to_roots(args, local, dist, peak, peak_kind):
     out = {"workload": f"{args.roots_config}: Nd={sysm.nd}, Ne={sysm.ne}, Nsu={sysm.nsu}, {nlv} roots, residual "
                        f"2-norm <= 1e-8 per root against the FP64 H",
            "metric": "time to all roots (FormH + solve), ms", "solver": "batched block Davidson, one block, "
-           "subspace 96, 48 kept at a restart"}
+           "subspace 112, 48 kept at a restart"}
     model = None
     if args.learned:
         model, out["learned_training"] = train_correction(args, kw, nlv, local)
@@ -486,7 +486,7 @@ def time_to_roots(args, local, dist, peak, peak_kind):
             b = Batch(local)
             b.set_value_prec(vp)
             b.add_engine(e)
-        kwd = dict(nlv=nlv, max_sub=96, keep=48, max_it=400, tol=1e-8, it_per_graph=4, precision=prec,
+        kwd = dict(nlv=nlv, max_sub=112, keep=48, max_it=400, tol=1e-8, it_per_graph=4, precision=prec,
                    switch_tol=args.switch_tol)
         if mdl is not None:
             b.set_correction_model(mdl)

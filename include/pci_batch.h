@@ -32,7 +32,8 @@ extern "C" {
 typedef struct pci_batch pci_batch_t;
 
 #define PCI_BATCH_MAX_LV   12   /* roots per block */
-#define PCI_BATCH_MAX_SUB  96   /* subspace vectors per block */
+#define PCI_BATCH_MAX_SUB  112  /* subspace vectors per block (the projected eigensolve keeps two
+                                   112 x 112 FP64 arrays in shared memory) */
 
 #define PCI_BATCH_FP64  0   /* SpMM on FP64 vectors with FP64 sums throughout */
 #define PCI_BATCH_MIXED 1   /* SpMM on FP32 vectors with FP32 sums (FP32 values) until every root of a

@@ -381,8 +381,8 @@ __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b)
 
 // Per-chunk partial of A[:, :ma]^T B[:, b0:b0+kb] over the chunk's rows, on
 // the FP64 tensor cores: the chunk's rows pass through shared memory 32 at a
-// time (zero-padded to whole 8 x 8 output tiles) and each warp owns up to
-// three 8 x 8 tiles of the ma x kb product, eight m8n8k4 steps per 32 rows.
+// time (zero-padded to whole 8 x 8 output tiles) and each of the 8 warps owns
+// up to QT 8 x 8 tiles of the ma x kb product, eight m8n8k4 steps per 32 rows.
 // In TN_GRAM mode B is the SpMM output Q (row-major) and the kernel also
 // stores it as W's new columns.
 template <int MODE>
@@ -394,13 +394,14 @@ __global__ void __launch_bounds__(256) kb_tn(const Chunk *__restrict__ chunks, c
     const double *A, *Bm;
     int ma, b0, kb;
     tn_dims(MODE, s, B, A, ma, Bm, b0, kb);
-    constexpr int MT = BT_MS / 8, NT = (BT_LV + 7) / 8;
+    constexpr int MT = BT_MS / 8, NT = (BT_LV + 7) / 8, QT = (MT * NT + 7) / 8;
+    static_assert(BT_MS % 8 == 0, "subspace maximum must be a multiple of 8");
     __shared__ double As[BT_TR][MT * 8 + 1];
     __shared__ double Bs[BT_TR][NT * 8 + 1];
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     const int mt = (ma + 7) / 8, nt = (kb + 7) / 8, ntile = mt * nt;
     const int map = mt * 8, kbp = nt * 8;
-    double acc[3][2] = {};
+    double acc[QT][2] = {};
     const int64_t ld = B.ld;
     for (int64_t r0 = ch.row0; r0 < ch.row1; r0 += BT_TR) {
         const int nr = (int)min((int64_t)BT_TR, ch.row1 - r0);
@@ -423,7 +424,7 @@ __global__ void __launch_bounds__(256) kb_tn(const Chunk *__restrict__ chunks, c
         }
         __syncthreads();
 #pragma unroll
-        for (int q = 0; q < 3; q++) {
+        for (int q = 0; q < QT; q++) {
             const int tile = w + 8 * q;
             if (tile < ntile) {
                 const int mi = tile / nt, ni = tile - mi * nt;
@@ -437,7 +438,7 @@ __global__ void __launch_bounds__(256) kb_tn(const Chunk *__restrict__ chunks, c
     }
     double *out = B.part + (int64_t)blockIdx.x * BT_PW;
 #pragma unroll
-    for (int q = 0; q < 3; q++) {
+    for (int q = 0; q < QT; q++) {
         const int tile = w + 8 * q;
         if (tile < ntile) {
             const int mi = tile / nt, ni = tile - mi * nt;
@@ -1687,7 +1688,7 @@ int pci_batch_davidson(pci_batch_t *b, const pci_batch_params *p, double *E, dou
     pci_gpu *h = &b->core;
     const int nlv = p->nlv;
     if (nlv < 1 || nlv > BT_LV) return set_err(h, PCI_E_INPUT, "nlv must be 1..12");
-    if (p->max_sub < 2 * nlv || p->max_sub > BT_MS) return set_err(h, PCI_E_INPUT, "max_sub must be 2*nlv..96");
+    if (p->max_sub < 2 * nlv || p->max_sub > BT_MS) return set_err(h, PCI_E_INPUT, "max_sub must be 2*nlv..PCI_BATCH_MAX_SUB");
     if (p->keep < nlv || p->keep > p->max_sub - nlv) return set_err(h, PCI_E_INPUT, "keep must be nlv..max_sub-nlv");
     if (p->max_it < 1 || p->it_per_graph < 1 || !(p->tol > 0.0)) return set_err(h, PCI_E_INPUT, "bad max_it/it_per_graph/tol");
     if (p->precision != PCI_BATCH_FP64 && p->precision != PCI_BATCH_MIXED)

@@ -202,6 +202,8 @@ def test_batch_errors(blocks):
         with pytest.raises(PciError):
             b.davidson(nlv=6, max_sub=10)          # subspace below 2*nlv
         with pytest.raises(PciError):
+            b.davidson(nlv=6, max_sub=120)         # above PCI_BATCH_MAX_SUB
+        with pytest.raises(PciError):
             b.davidson(nlv=4, spmm_variant=99)
         with pytest.raises(PciError):
             b.set_storage(2)

@@ -74,19 +74,21 @@ def test_mixed_stall_switch(systems):
             assert np.abs(r["E"][i] - np.linalg.eigvalsh(H)[:nlv]).max() <= 1e-9, name
 
 
-def test_largest_subspace_with_restarts(systems):
-    """max_sub 96 with 48 kept and 12 roots (the kernels' shared-memory
-    limits), forcing restarts on small3, against the dense levels."""
+@pytest.mark.parametrize("msub,keep", [(96, 48), (112, 48), (112, 100)])
+def test_largest_subspace_with_restarts(systems, msub, keep):
+    """Subspaces up to PCI_BATCH_MAX_SUB (112: the kernels' shared-memory
+    limits) with 12 roots, forcing restarts on small3, against the dense
+    levels."""
     nlv = 12
     sub = [x for x in systems if x[0] in ("small3", "small4")]
     with _batch(sub, 64) as b:
-        r = b.davidson(nlv=nlv, max_sub=96, keep=48, max_it=400, tol=TOL)
+        r = b.davidson(nlv=nlv, max_sub=msub, keep=keep, max_it=400, tol=TOL)
         assert np.all(r["status"] == 1)
         for i, (name, s, rp, col, val, H) in enumerate(sub):
             assert np.abs(r["E"][i] - np.linalg.eigvalsh(H)[:nlv]).max() <= 1e-9, name
             X = b.vectors(i)
             assert np.linalg.norm(H @ X - X * r["E"][i], axis=0).max() <= 2 * TOL
-    assert r["iters"].max() * nlv > 96 - nlv   # more directions than fit: restarted
+    assert r["iters"].max() * nlv > msub - nlv   # more directions than fit: restarted
 
 
 def test_tensor_core_forward_matches_forward():
