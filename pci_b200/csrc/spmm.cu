@@ -533,9 +533,10 @@ static int spmm_lower_red_dispatch(pci_gpu *h, const XT *X, int ldx, XT *Y, int 
     const Csr &L = h->H;
     k_zero_block<<<148 * 8, 256, 0, st>>>(Y, ldy, L.nrows, nv);
     const VT *val = (const VT *)L.val;
+    // 4 thread blocks per SM (measured 1.5% faster than 16 on config 2)
 #define CASE(N)                                                                                               \
     case N:                                                                                                   \
-        k_spmm_lower_red<N, VT, XT><<<148 * 16, 256, 0, st>>>(L.rowptr, L.col, val, L.nrows, h->hmin, X, ldx, Y, ldy); \
+        k_spmm_lower_red<N, VT, XT><<<148 * 4, 256, 0, st>>>(L.rowptr, L.col, val, L.nrows, h->hmin, X, ldx, Y, ldy); \
         break;
     switch (nv) {
         CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8)
