@@ -78,7 +78,8 @@ typedef struct {
 int pci_batch_create(int32_t device, pci_batch_t **out);
 
 /* Append the Hamiltonian resident in `h` as the next block and take it over
- * (h keeps its basis and integrals but no longer holds H).  FP64 values are
+ * (h keeps its basis and integrals but no longer holds H; on an error return
+ * the matrix is released and h no longer holds it either).  FP64 values are
  * rounded to FP32, kept, or split into FP32 pairs as pci_batch_set_value_prec
  * says.  When h holds a determinant basis, the occupied orbitals of every row
  * are kept as the learned correction's inputs.  *index receives the block's

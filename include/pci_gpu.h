@@ -95,7 +95,12 @@ int pci_gpu_set_integrals(pci_gpu_t *h, const double *HintLUT, int32_t Nlx,
  * npes = 1 semantics, pconf.F90:1259) as device-resident CSR with values in
  * FP64 (value_prec = 64) or FP32 (32).  Returns NumH (stored elements),
  * numzero (difference <= 2 pairs whose element is exactly 0) and Hmin (the
- * minimum stored value, Hamil%minval). */
+ * minimum stored value, Hamil%minval).  A matrix the handle held before
+ * (from an earlier pci_gpu_form_h, dropped by pci_gpu_set_basis or
+ * pci_gpu_set_integrals) lends its device buffers to the new one when they
+ * fit, instead of being freed and allocated again; buffers left over are
+ * freed when the build ends, and any allocation that fails first frees them
+ * and retries. */
 int pci_gpu_form_h(pci_gpu_t *h, int32_t value_prec, int64_t *NumH, int64_t *numzero, double *Hmin);
 
 /* Replaces: Call FormJ + RedistributeJsqCSR (pconf.F90:224-225).  J^2 in units

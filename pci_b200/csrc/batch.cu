@@ -1512,9 +1512,22 @@ int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index)
     cudaSetDevice(c->device);
     BlockRec r;
     r.H = h->H;
+    h->H = Csr();   // the batch owns the matrix from here on, error paths included
     r.r0 = b->rows;
     r.nd = r.H.nrows;
     r.nnz = r.H.nnz;
+    // on an error return the block's device buffers are released
+    struct Release {
+        BlockRec *r;
+        bool armed = true;
+        ~Release()
+        {
+            if (!armed) return;
+            csr_free(r->H);
+            dev_free(r->orbs);
+            dev_free(r->D);
+        }
+    } release{&r};
     if (h->have_basis && h->d_occ && h->d_ms_orb && h->nd == r.nd && h->nsu <= 254 && h->ne <= mlptc::MAXOCC) {
         // the occupied orbitals of every row: inputs of the learned correction
         int rc = 0;
@@ -1538,7 +1551,6 @@ int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index)
         PCI_CUDA(c, cudaStreamSynchronize(c->st));
         dev_free(r.H.col);
         r.H.col = col;
-        h->H.col = col;
         if (r.H.val_f32 || b->value_prec != 32) {
             const size_t vb = r.H.val_f32 ? 4 : 8;
             void *val = dev_alloc(c, n * vb, &rc);
@@ -1547,7 +1559,6 @@ int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index)
             PCI_CUDA(c, cudaStreamSynchronize(c->st));
             dev_free(r.H.val);
             r.H.val = val;
-            h->H.val = val;
         }
         r.H.cap = 0;
     }
@@ -1568,8 +1579,6 @@ int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index)
         dev_free(r.H.val);
         r.H.val = v;
         r.H.val_f32 = 1;
-        h->H.val = v;
-        h->H.val_f32 = 1;
     }
     {   // the block's diagonal, while its CSR columns are there
         int rc = 0;
@@ -1580,7 +1589,7 @@ int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index)
         PCI_CUDA(c, cudaGetLastError());
         PCI_CUDA(c, cudaStreamSynchronize(c->st));
     }
-    h->H = Csr();
+    release.armed = false;
     csr_free(h->Hfull);
     h->h_from_tiles = false;
     b->blocks.push_back(r);

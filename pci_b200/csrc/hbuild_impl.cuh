@@ -1107,6 +1107,17 @@ static inline int formh_mode_env()
 // Compaction buffer of the padded build, in entries.
 constexpr int64_t COMPACT_CHUNK = 1LL << 24;
 
+// Buffer `which` (0 rowptr, 1 col, 2 val) of the H being built: the retired
+// H's buffer when it fits, else a new allocation.
+static inline void *csr_buf(pci_gpu *h, int which, size_t bytes, int *rc)
+{
+    if (void *p = spare_take(h, which, bytes)) {
+        *rc = PCI_OK;
+        return p;
+    }
+    return dev_alloc(h, bytes, rc);
+}
+
 template <int NE, int KIND>
 static int rows_impl(pci_gpu *h, int value_prec, Csr &out, RowStats *hs)
 {
@@ -1114,7 +1125,8 @@ static int rows_impl(pci_gpu *h, int value_prec, Csr &out, RowStats *hs)
     DevSys S = make_devsys(h);
     const int64_t nd = h->nd;
     const int vb = value_prec == 32 ? 4 : 8;
-    csr_free(out);
+    if (KIND == 0) csr_retire(h, out);
+    else csr_free(out);
     out.nrows = nd;
     int64_t *cnt = nullptr, *pptr = nullptr;
     RowStats *d_stats = nullptr;
@@ -1122,13 +1134,14 @@ static int rows_impl(pci_gpu *h, int value_prec, Csr &out, RowStats *hs)
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
     auto cleanup = [&](int code) {
         dev_free(cnt); dev_free(pptr); dev_free(d_stats); dev_free(d_items);
+        if (KIND == 0) spare_release(h);   // what the new H did not reuse
         if (e0) cudaEventDestroy(e0);
         if (e1) cudaEventDestroy(e1);
         if (e2) cudaEventDestroy(e2);
         if (e3) cudaEventDestroy(e3);
         return code;
     };
-    out.rowptr = (int64_t *)dev_alloc(h, (nd + 1) * 8, &rc);
+    out.rowptr = (int64_t *)(KIND == 0 ? csr_buf(h, 0, (nd + 1) * 8, &rc) : dev_alloc(h, (nd + 1) * 8, &rc));
     if (rc) return cleanup(rc);
     cnt = (int64_t *)dev_alloc(h, (nd + 1) * 8, &rc);
     if (rc) return cleanup(rc);
@@ -1205,14 +1218,15 @@ static int rows_impl(pci_gpu *h, int value_prec, Csr &out, RowStats *hs)
         PCI_CUDA(h, cudaStreamSynchronize(h->st));
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
+        fr += h->spare.col_bytes + h->spare.val_bytes;   // the retired H's buffers count as free
         const int64_t chunk = std::min<int64_t>(COMPACT_CHUNK, std::max<int64_t>(ncand, 1));
         const double need = (double)(ncand + chunk) * (4 + vb) + (double)(nd + 1) * 8 + (512.0 * (1 << 20));
         if (forced == 1 || need <= (double)fr) {
             out.nnz = ncand;
             out.val_f32 = value_prec == 32;
-            out.col = (int32_t *)dev_alloc(h, std::max<int64_t>(ncand, 1) * 4, &rc);
+            out.col = (int32_t *)csr_buf(h, 1, std::max<int64_t>(ncand, 1) * 4, &rc);
             if (rc) return cleanup(rc);
-            out.val = dev_alloc(h, std::max<int64_t>(ncand, 1) * vb, &rc);
+            out.val = csr_buf(h, 2, std::max<int64_t>(ncand, 1) * vb, &rc);
             if (rc) return cleanup(rc);
             out.cap = ncand;
             cudaEventRecord(e1, h->st);
@@ -1256,9 +1270,11 @@ static int rows_impl(pci_gpu *h, int value_prec, Csr &out, RowStats *hs)
         if ((rc = check_derr())) return cleanup(rc);
         out.nnz = nnz;
         out.val_f32 = value_prec == 32;
-        out.col = (int32_t *)dev_alloc(h, std::max<int64_t>(nnz, 1) * 4, &rc);
+        out.col = (int32_t *)(KIND == 0 ? csr_buf(h, 1, std::max<int64_t>(nnz, 1) * 4, &rc)
+                                        : dev_alloc(h, std::max<int64_t>(nnz, 1) * 4, &rc));
         if (rc) return cleanup(rc);
-        out.val = dev_alloc(h, std::max<int64_t>(nnz, 1) * vb, &rc);
+        out.val = KIND == 0 ? csr_buf(h, 2, std::max<int64_t>(nnz, 1) * vb, &rc)
+                            : dev_alloc(h, std::max<int64_t>(nnz, 1) * vb, &rc);
         if (rc) return cleanup(rc);
         if ((rc = launch_fill(out.rowptr, nullptr, nullptr))) return cleanup(rc);
         cudaEventRecord(e2, h->st);

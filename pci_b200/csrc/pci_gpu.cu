@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -27,6 +28,12 @@ void *dev_alloc(pci_gpu *h, size_t bytes, int *rc)
 {
     void *p = nullptr;
     cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+    if (e != cudaSuccess && h && spare_bytes(h) > 0) {
+        // the buffers kept for reuse give way to any other allocation
+        cudaGetLastError();
+        spare_release(h);
+        e = cudaMalloc(&p, bytes ? bytes : 16);
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
         *rc = set_err(h, PCI_E_OOM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
@@ -179,44 +186,59 @@ static std::vector<int32_t> compute_jterms(int Ne, int Nc, const int32_t *Ndc, c
     int jmax = 1;
     for (int o = 0; o < Nsu; o++) jmax = std::max(jmax, (int)Jj[o]);
     const int OFF = Ne * jmax;  // |2M| <= Ne * max(2j)
+    // The terms of a configuration depend only on its (2j, occupation) groups:
+    // configurations with the same groups share one computation.
+    std::map<std::vector<int>, std::vector<int32_t>> memo;
     for (int c = 0; c < Nc; c++) {
         if (Ndc[c] == 0) continue;
         std::vector<int> orbs(conf_orb.begin() + (size_t)c * Ne, conf_orb.begin() + (size_t)(c + 1) * Ne);
         std::sort(orbs.begin(), orbs.end());
-        std::vector<int64_t> dist(2 * OFF + 1, 0);
-        dist[OFF] = 1;
+        std::vector<int> key;   // (2j, q) of each orbital group, sorted
         for (size_t i = 0; i < orbs.size();) {
             size_t j = i;
             while (j < orbs.size() && orbs[j] == orbs[i]) j++;
-            const int q = (int)(j - i), j2 = Jj[orbs[i]];
-            // ways[k][s]: k of the m values -j2, -j2+2, ..., j2 chosen with 2M sum s
-            std::vector<std::vector<int64_t>> ways(q + 1, std::vector<int64_t>(2 * OFF + 1, 0));
-            ways[0][OFF] = 1;
-            for (int m = -j2; m <= j2; m += 2)
-                for (int k = q; k >= 1; k--)
-                    for (int sidx = 0; sidx <= 2 * OFF; sidx++)
-                        if (ways[k - 1][sidx] && sidx + m >= 0 && sidx + m <= 2 * OFF) ways[k][sidx + m] += ways[k - 1][sidx];
-            std::vector<int64_t> nd2(2 * OFF + 1, 0);
-            for (int a = 0; a <= 2 * OFF; a++)
-                if (dist[a])
-                    for (int b = 0; b <= 2 * OFF; b++)
-                        if (ways[q][b] && a + b - OFF >= 0 && a + b - OFF <= 2 * OFF) nd2[a + b - OFF] += dist[a] * ways[q][b];
-            dist.swap(nd2);
+            key.push_back(Jj[orbs[i]] * 16 + (int)(j - i));
             i = j;
         }
-        if (Mj + OFF < 0 || Mj + OFF > 2 * OFF || dist[Mj + OFF] == 0) continue;
-        std::vector<int64_t> nmj(1, 0);   // nmj[im], im >= 1
-        for (int m2 = Mj; m2 + OFF <= 2 * OFF; m2 += 2) nmj.push_back(dist[m2 + OFF]);
-        int imax = (int)nmj.size() - 1;
-        while (imax > 1 && nmj[imax] == 0) imax--;
-        for (int im = imax; im >= 1; im--) {
-            const int64_t n = nmj[im];
-            if (n != 0) {
-                const int mt = (im - 1) * 2 + Mj;
-                for (int k = 1; k <= im; k++) nmj[k] -= n;
-                if (std::find(jt.begin(), jt.end(), mt) == jt.end()) jt.push_back(mt);
+        std::sort(key.begin(), key.end());
+        auto it = memo.find(key);
+        if (it == memo.end()) {
+            std::vector<int64_t> dist(2 * OFF + 1, 0);
+            dist[OFF] = 1;
+            for (int kq : key) {
+                const int q = kq % 16, j2 = kq / 16;
+                // ways[k][s]: k of the m values -j2, -j2+2, ..., j2 chosen with 2M sum s
+                std::vector<std::vector<int64_t>> ways(q + 1, std::vector<int64_t>(2 * OFF + 1, 0));
+                ways[0][OFF] = 1;
+                for (int m = -j2; m <= j2; m += 2)
+                    for (int k = q; k >= 1; k--)
+                        for (int sidx = 0; sidx <= 2 * OFF; sidx++)
+                            if (ways[k - 1][sidx] && sidx + m >= 0 && sidx + m <= 2 * OFF) ways[k][sidx + m] += ways[k - 1][sidx];
+                std::vector<int64_t> nd2(2 * OFF + 1, 0);
+                for (int a = 0; a <= 2 * OFF; a++)
+                    if (dist[a])
+                        for (int b = 0; b <= 2 * OFF; b++)
+                            if (ways[q][b] && a + b - OFF >= 0 && a + b - OFF <= 2 * OFF) nd2[a + b - OFF] += dist[a] * ways[q][b];
+                dist.swap(nd2);
             }
+            std::vector<int32_t> mts;
+            if (Mj + OFF >= 0 && Mj + OFF <= 2 * OFF && dist[Mj + OFF] != 0) {
+                std::vector<int64_t> nmj(1, 0);   // nmj[im], im >= 1
+                for (int m2 = Mj; m2 + OFF <= 2 * OFF; m2 += 2) nmj.push_back(dist[m2 + OFF]);
+                int imax = (int)nmj.size() - 1;
+                while (imax > 1 && nmj[imax] == 0) imax--;
+                for (int im = imax; im >= 1; im--) {
+                    const int64_t n = nmj[im];
+                    if (n != 0) {
+                        for (int k = 1; k <= im; k++) nmj[k] -= n;
+                        mts.push_back((im - 1) * 2 + Mj);
+                    }
+                }
+            }
+            it = memo.emplace(key, std::move(mts)).first;
         }
+        for (int32_t mt : it->second)
+            if (std::find(jt.begin(), jt.end(), mt) == jt.end()) jt.push_back(mt);
     }
     std::sort(jt.begin(), jt.end());
     return jt;
@@ -257,7 +279,7 @@ int pci_gpu_set_basis(pci_gpu_t *h, int32_t Ne, int64_t Nd, int32_t Nst, int32_t
     }
     if (Nsu - Nso > Nx) return set_err(h, PCI_E_INPUT, "Nsu - Nso exceeds Nx");
     free_basis(h);
-    csr_free(h->H); csr_free(h->J); csr_free(h->Hfull);
+    csr_retire(h, h->H); csr_free(h->J); csr_free(h->Hfull);
     h->ne = Ne; h->nd = Nd; h->nst = Nst; h->nsu = Nsu; h->nso = Nso; h->nx = Nx; h->mj = Mj; h->nc = Nc; h->gj = Gj;
     h->h_ndc.assign(Ndc, Ndc + Nc);
     h->h_orb_j.assign(Jj, Jj + Nsu);
@@ -335,7 +357,7 @@ int pci_gpu_set_integrals(pci_gpu_t *h, const double *HintLUT, int32_t Nlx, int6
     int rc;
     if ((rc = build_tables(h, HintLUT, Nlx, nGauntLUT, GauntLUT))) return rc;
     if ((rc = hb_build_hash(h, Ngint, kbrt, r2_is_f64, Rint2, Iint2, Iint3))) return rc;
-    csr_free(h->H); csr_free(h->J); csr_free(h->Hfull);
+    csr_retire(h, h->H); csr_free(h->J); csr_free(h->Hfull);
     h->have_ints = true;
     return PCI_OK;
 }
@@ -675,6 +697,7 @@ void pci_gpu_destroy(pci_gpu_t *h)
     if (h->st) cudaStreamSynchronize(h->st);
     free_basis(h);
     csr_free(h->H); csr_free(h->J); csr_free(h->Hfull);
+    spare_release(h);
     dev_free(h->d_h1); dev_free(h->d_gaunt); dev_free(h->d_htab);
     dev_free(h->d_err); dev_free(h->d_tmp);
     if (h->st) cudaStreamDestroy(h->st);

@@ -91,6 +91,13 @@ struct pci_gpu {
     unsigned long long hcap = 0;
     // matrices
     Csr H, J, Hfull;
+    // device buffers of the last retired H (csr_retire), reused by the next
+    // FormH instead of a cudaFree and cudaMalloc of the whole CSR; released
+    // by dev_alloc when an allocation fails, and by pci_gpu_destroy
+    struct Spare {
+        void *rowptr = nullptr, *col = nullptr, *val = nullptr;
+        size_t rowptr_bytes = 0, col_bytes = 0, val_bytes = 0;
+    } spare;
     double hmin = 0.0;
     int64_t numh = 0, numzero = 0, numj = 0;
     unsigned int *d_err = nullptr;
@@ -155,6 +162,13 @@ int sp_spmm_f32(pci_gpu *h, const float *X, int ldx, float *Y, int ldy, int nv, 
 int sp_jav(pci_gpu *h, const double *X, int ldx, int nv, int64_t nlim, double *out_host);
 int sp_jav_strided(pci_gpu *h, const double *X, int64_t sn, int64_t sv, int nv, int64_t nlim, double *out_host);
 void csr_free(Csr &c);
+// Free c, keeping its buffers in h->spare (releasing what the spare held).
+void csr_retire(pci_gpu *h, Csr &c);
+// A spare buffer of at least `bytes` (0: rowptr, 1: col, 2: val), taken out of
+// the spare, or nullptr.
+void *spare_take(pci_gpu *h, int which, size_t bytes);
+void spare_release(pci_gpu *h);
+size_t spare_bytes(const pci_gpu *h);
 
 // davidson.cu
 // Samples of the learned correction recorded during a solve (features of

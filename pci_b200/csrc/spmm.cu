@@ -32,6 +32,48 @@ void csr_free(Csr &c)
     c.nrows = c.nnz = 0;
 }
 
+void spare_release(pci_gpu *h)
+{
+    dev_free(h->spare.rowptr);
+    dev_free(h->spare.col);
+    dev_free(h->spare.val);
+    h->spare = pci_gpu::Spare();
+}
+
+size_t spare_bytes(const pci_gpu *h)
+{
+    return h->spare.rowptr_bytes + h->spare.col_bytes + h->spare.val_bytes;
+}
+
+void csr_retire(pci_gpu *h, Csr &c)
+{
+    if (!c.col) {
+        csr_free(c);
+        return;
+    }
+    spare_release(h);
+    const int64_t slots = std::max(c.cap, c.nnz);
+    h->spare.rowptr = c.rowptr;
+    h->spare.rowptr_bytes = c.rowptr ? (size_t)(c.nrows + 1) * 8 : 0;
+    h->spare.col = c.col;
+    h->spare.col_bytes = (size_t)slots * 4;
+    h->spare.val = c.val;
+    h->spare.val_bytes = (size_t)slots * (c.val_f32 ? 4 : 8);
+    c = Csr();
+}
+
+void *spare_take(pci_gpu *h, int which, size_t bytes)
+{
+    void **p = which == 0 ? &h->spare.rowptr : which == 1 ? &h->spare.col : &h->spare.val;
+    size_t *n = which == 0 ? &h->spare.rowptr_bytes : which == 1 ? &h->spare.col_bytes : &h->spare.val_bytes;
+    // reused only when at most about twice the size asked for
+    if (!*p || *n < bytes || *n > 2 * bytes + ((size_t)64 << 20)) return nullptr;
+    void *r = *p;
+    *p = nullptr;
+    *n = 0;
+    return r;
+}
+
 // --------------------------------------------------------- full CSR ---
 
 __global__ void k_count_upper(const int64_t *rowptr, const int32_t *col, int64_t nd, unsigned int *cntU)
