@@ -83,6 +83,7 @@ def parse():
                     "(-1: from the tuning cache, tuned when absent)")
     ap.add_argument("--tune-cache", default=None, help="SpMM tuning cache of the batched form "
                     "(default: ~/.cache/pci_b200/spmm_tune_cache.txt; empty string = tune every run)")
+    ap.add_argument("--no-lsj", action="store_true", help="skip the LSJ section")
     ap.add_argument("--davidson-iters", type=int, default=2,
                     help="plain FP64 Davidson iterations timed after the H-build (0 skips)")
     return ap.parse_args()
@@ -312,6 +313,8 @@ def run_ours(args):
         "clocks": clk,
         "e2e": e2e,
     }
+    if not args.no_lsj:
+        line["lsj"] = lsj_section(args, eng, sysm)
     if args.davidson_iters > 0:
         eng.form_j()
         nlv = int(sysm.params["Nlv"])
@@ -373,6 +376,40 @@ def run_ours(args):
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+def lsj_section(args, eng, sysm):
+    """LSJ (the kLSJ = 1 step, src/pconf.F90:2672-2962) of 10 normalised
+    vectors of the configuration through pci_gpu_lsj (host call, vectors from
+    host memory), against the oracle's restatement of calcLSJ on one core over
+    the first configurations, scaled to all of them by calcLSJ's work per
+    configuration (its determinants times the configurations after it)."""
+    rng = np.random.default_rng(21)
+    X = rng.standard_normal((sysm.nd, 10))
+    X /= np.linalg.norm(X, axis=0)
+    ts = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        xj, xl, xs = eng.lsj(X)
+        ts.append(time.perf_counter() - t0)
+    out = {"workload": f"{args.config}: J, L, S of 10 normalised random vectors (Nd={sysm.nd})",
+           "gpu_ms": 1e3 * ts[-1], "J_range": [float(xj.min()), float(xj.max())]}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        o = O.Oracle(sysm)
+        ndc = np.asarray(sysm.ndc, np.float64)
+        w = ndc * (sysm.nc - np.arange(sysm.nc))           # calcLSJ's CompNRC checks per configuration
+        k = int(np.searchsorted(np.cumsum(w), 4e8)) + 1     # about 10 s of oracle work
+        k = max(1, min(k, sysm.nc))
+        t0 = time.perf_counter()
+        o.lsj_sums(X, 1, k)
+        tc = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value_ms": 1e3 * tc * w.sum() / w[:k].sum(), "unit": "ms (estimate from a sample)",
+                               "cores": 1, "kind": "port",
+                               "sample": f"oracle calcLSJ over configurations 1..{k} of {sysm.nc} "
+                                         f"({tc:.1f} s), scaled by determinants x later configurations"}
+    return out
 
 
 def spmm_bytes(numh, nd, nlv, value_bytes, vec_bytes):

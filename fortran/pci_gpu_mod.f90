@@ -58,6 +58,11 @@ module pci_gpu_mod
        integer(c_int64_t) :: rowptr(*)
        type(c_ptr), value :: col, val
      end function
+     ! kLSJ = 1 (lsj, pconf.F90:2672-2962): J, L, S of nv vectors X(Nd, nv)
+     integer(c_int) function pci_gpu_lsj(h, X, nv, xj, xl, xs) bind(C)
+       import; type(c_ptr), value :: h; real(c_double) :: X(*), xj(*), xl(*), xs(*)
+       integer(c_int32_t), value :: nv
+     end function
      ! FormBarr: Barr(nint, Nd) of the basis (barr may be c_null_ptr)
      integer(c_int) function pci_gpu_form_barr(h, nint, barr) bind(C)
        import; type(c_ptr), value :: h; integer(c_int32_t) :: nint

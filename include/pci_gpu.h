@@ -151,6 +151,15 @@ int pci_gpu_davidson(pci_gpu_t *h, const pci_dvd_params *p, const double *X0,
  * J = (sqrt(1 + <x|J^2|x>) - 1) / 2. */
 int pci_gpu_j_av(pci_gpu_t *h, const double *X, int32_t nv, int64_t nlim, double *Tj);
 
+/* Replaces: lsj / calcLSJ / lsj_det (pconf.F90:2672-2962), the kLSJ = 1
+ * step: for each vector the quantum numbers J, L, S from <x|X^2|x> over the
+ * determinant pairs of equal non-relativistic configuration (CompNRC = 0)
+ * and relativistic CompC <= 2, x = (sqrt(<X^2> + 1) - 1) / 2.  X is Nd x nv
+ * column-major on the host (1 <= nv <= 64), normalised as the caller wants
+ * (the reference passes the eigenvectors).  Needs the principal numbers Nn
+ * passed to pci_gpu_set_basis (PCI_E_STATE without them). */
+int pci_gpu_lsj(pci_gpu_t *h, const double *X, int32_t nv, double *xj, double *xl, double *xs);
+
 /* No counterpart in the reference.  The J_av of pci_gpu_j_av for callers that
  * cannot allocate device memory (a host that owns all device memory through
  * its own pool or a framework's caching allocator, or a path where

@@ -77,6 +77,7 @@ def lib():
         L.orc_gint.restype = C.c_double
         L.orc_hint.argtypes = [C.POINTER(OrcSys), C.c_int, C.c_int]
         L.orc_hint.restype = C.c_double
+        L.orc_lsj.argtypes = [C.POINTER(OrcSys), P, C.c_int, C.c_int, C.c_int, P]
         _lib = L
     return _lib
 
@@ -186,6 +187,25 @@ class Oracle:
             nnz += L.orc_form_h(C.byref(self.s), lo, hi, _ptr(cnt), None, None, None,
                                 C.byref(nz), C.byref(hmin), C.byref(pairs), threads)
         return time.perf_counter() - t0, nnz, pairs.value
+
+    def lsj_sums(self, X, ic_lo=1, ic_hi=None):
+        """calcLSJ (src/pconf.F90:2805-2863) over configurations ic_lo..ic_hi
+        (1-based): the sums of c_n c_k t for J, L, S, shape [3, nv]."""
+        X = np.asarray(X, np.float64)
+        if X.ndim == 1:
+            X = X[:, None]
+        nv = X.shape[1]
+        xc = np.ascontiguousarray(X.T)
+        out = np.zeros(3 * nv)
+        lib().orc_lsj(C.byref(self.s), _ptr(xc), nv, ic_lo, self.sys.nc if ic_hi is None else ic_hi, _ptr(out))
+        return out.reshape(3, nv)
+
+    def lsj(self, X):
+        """(J, L, S) of each column of X, lsj's final step
+        (src/pconf.F90:2798-2800): x = (sqrt(<X^2> + 1) - 1) / 2."""
+        t = self.lsj_sums(X)
+        x = 0.5 * (np.sqrt(t + 1) - 1)
+        return x[0], x[1], x[2]
 
     def form_j(self):
         L = lib()

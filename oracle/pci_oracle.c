@@ -630,3 +630,206 @@ double orc_j_av(int64_t nd, const int64_t *rowptr, const int32_t *col, const dou
     }
     return 0.5 * (sqrt(1.0 + xj) - 1.0);
 }
+
+/* ---------------------------------------------------------------- LSJ --- */
+
+/* Plus_j, src/pconf.F90:3129-3140 (Plj). */
+static double orc_plus_j(const orc_sys *s, int ia, int ib)
+{
+    double t = 0.0;
+    int na = s->nh[ia - 1], nb = s->nh[ib - 1];
+    if (na == nb) {
+        int ma = s->jz[ia - 1], mb = s->jz[ib - 1];
+        if (ma == mb + 2) {
+            int ja = s->jj[na - 1];
+            t = sqrt(ja * (ja + 2) - ma * mb + 0.0);
+        }
+    }
+    return t;
+}
+
+/* plus_s, src/pconf.F90:2964-2997. */
+static double orc_plus_s(const orc_sys *s, int ia, int ib)
+{
+    double t = 0.0, ta, tb;
+    if (s->jz[ia - 1] != s->jz[ib - 1] + 2) return t;
+    int na = s->nh[ia - 1], nb = s->nh[ib - 1];
+    if (s->nn[na - 1] != s->nn[nb - 1]) return t;
+    if (s->ll[na - 1] != s->ll[nb - 1]) return t;
+    int ja = s->jj[na - 1], jb = s->jj[nb - 1], la = s->ll[na - 1], lb = s->ll[nb - 1];
+    int msa = 1, mja = s->jz[ia - 1], mjb = s->jz[ib - 1];
+    int mla = (mja - msa) / 2;
+    if (abs(mla) > la) return t;
+    ta = 0.0;
+    if (ja == 2 * la + 1) ta = sqrt((ja + mja) / (2.0 * ja));
+    if (ja == 2 * la - 1) ta = -sqrt((ja - mja + 2.0) / (2.0 * ja + 4.0));
+    tb = 0.0;
+    if (jb == 2 * lb + 1) tb = sqrt((jb - mjb) / (2.0 * jb));
+    if (jb == 2 * lb - 1) tb = sqrt((jb + mjb + 2.0) / (2.0 * jb + 4.0));
+    t = -sqrt(0.5) * ta * tb;
+    return t;
+}
+
+/* ta / tb factors of plus_l, p0_s, p0_l for spin projection msa. */
+static void orc_lsj_tatb(int ja, int la, int mja, int jb, int lb, int mjb, int msa, double *ta, double *tb)
+{
+    *ta = 0.0;
+    *tb = 0.0;
+    if (msa == 1) {
+        if (ja == 2 * la + 1) *ta = sqrt((ja + mja) / (2.0 * ja));
+        if (ja == 2 * la - 1) *ta = -sqrt((ja - mja + 2.0) / (2.0 * ja + 4.0));
+        if (jb == 2 * lb + 1) *tb = sqrt((jb + mjb) / (2.0 * jb));
+        if (jb == 2 * lb - 1) *tb = -sqrt((jb - mjb + 2.0) / (2.0 * jb + 4.0));
+    }
+    if (msa == -1) {
+        if (ja == 2 * la + 1) *ta = sqrt((ja - mja) / (2.0 * ja));
+        if (ja == 2 * la - 1) *ta = sqrt((ja + mja + 2.0) / (2.0 * ja + 4.0));
+        if (jb == 2 * lb + 1) *tb = sqrt((jb - mjb) / (2.0 * jb));
+        if (jb == 2 * lb - 1) *tb = sqrt((jb + mjb + 2.0) / (2.0 * jb + 4.0));
+    }
+}
+
+/* plus_l (src/pconf.F90:2999-3042, kind 0), p0_s (3044-3086, kind 1),
+ * p0_l (3088-3127, kind 2). */
+static double orc_lsj_one(const orc_sys *s, int ia, int ib, int kind)
+{
+    double t = 0.0, ta, tb;
+    int mja = s->jz[ia - 1], mjb = s->jz[ib - 1];
+    if (kind == 0 ? (mja != mjb + 2) : (mja != mjb)) return t;
+    int na = s->nh[ia - 1], nb = s->nh[ib - 1];
+    if (s->nn[na - 1] != s->nn[nb - 1]) return t;
+    if (s->ll[na - 1] != s->ll[nb - 1]) return t;
+    int ja = s->jj[na - 1], jb = s->jj[nb - 1], la = s->ll[na - 1], lb = s->ll[nb - 1];
+    for (int msa = -1; msa <= 1; msa += 2) {
+        int mla = (mja - msa) / 2;
+        int mlb = kind == 0 ? (mjb - msa) / 2 : mla;
+        if (abs(mla) > la) continue;
+        if (kind == 0 && abs(mlb) > lb) continue;
+        orc_lsj_tatb(ja, la, mja, jb, lb, mjb, msa, &ta, &tb);
+        if (kind == 0) t = t - sqrt(0.5 * (lb * (lb + 1.0) - mlb * (mlb + 1.0))) * ta * tb;
+        else if (kind == 1) t = t + 0.5 * msa * (ta * tb);
+        else t = t + mla * (ta * tb);
+    }
+    return t;
+}
+
+#define PLJ(a, b) orc_plus_j(s, a, b)
+#define PLS(a, b) orc_plus_s(s, a, b)
+#define PLL(a, b) orc_lsj_one(s, a, b, 0)
+#define P0S(a, b) orc_lsj_one(s, a, b, 1)
+#define P0L(a, b) orc_lsj_one(s, a, b, 2)
+
+/* lsj_det, src/pconf.F90:2865-2962. */
+void orc_lsj_det(const orc_sys *s, const int32_t *d1, const int32_t *d2, double *tj_, double *tl_, double *ts_)
+{
+    double tj = 0.0, tl = 0.0, ts = 0.0;
+    int is, nf, ii[3], jj[3];
+    orc_rspq(d1, d2, s->ne, &is, &nf, ii, jj);
+    /* Rspq(idet1,idet2,is,nf,i1,j1,i2,j2): i2/j2 the later difference */
+    int i1 = ii[2], j1 = jj[2], i2 = ii[1], j2 = jj[1];
+    if (nf == 0) {
+        tj = s->mj * s->mj;
+        for (int iq = 0; iq < s->ne; iq++) {
+            int ia = d1[iq], na = s->nh[ia - 1], ja = s->jj[na - 1], la = s->ll[na - 1], ma = s->jz[ia - 1];
+            tj = tj + (ja * (ja + 2) - ma * ma);
+            ts = ts + 0.75;
+            tl = tl + la * (la + 1);
+            for (int jq = iq + 1; jq < s->ne; jq++) {
+                int ib = d1[jq];
+                tj = tj - pow(PLJ(ia, ib), 2) - pow(PLJ(ib, ia), 2);
+                ts = ts + 2 * (P0S(ia, ia) * P0S(ib, ib) - pow(P0S(ia, ib), 2));
+                ts = ts - 2 * (pow(PLS(ia, ib), 2) + pow(PLS(ib, ia), 2));
+                tl = tl + 2 * (P0L(ia, ia) * P0L(ib, ib) - pow(P0L(ia, ib), 2));
+                tl = tl - 2 * (pow(PLL(ia, ib), 2) + pow(PLL(ib, ia), 2));
+            }
+        }
+    }
+    if (nf == 1) {
+        int ia = i2, ib = j2;
+        int ka = s->nh[ia - 1], kb = s->nh[ib - 1];
+        if (s->nn[ka - 1] == s->nn[kb - 1]) {
+            for (int iq = 0; iq < s->ne; iq++) {
+                int ic = d1[iq];
+                if (ic == i2) continue;
+                ts = ts + 2 * (P0S(ia, ib) * P0S(ic, ic) - P0S(ia, ic) * P0S(ib, ic));
+                ts = ts - 2 * (PLS(ia, ic) * PLS(ib, ic) + PLS(ic, ia) * PLS(ic, ib));
+                tl = tl + 2 * (P0L(ia, ib) * P0L(ic, ic) - P0L(ia, ic) * P0L(ib, ic));
+                tl = tl - 2 * (PLL(ia, ic) * PLL(ib, ic) + PLL(ic, ia) * PLL(ic, ib));
+            }
+            ts = ts * is;
+            tl = tl * is;
+        }
+    }
+    if (nf == 2) {
+        int ia = i1, ic = j1, ib = i2, id = j2;
+        int na = s->nn[s->nh[ia - 1] - 1], nc = s->nn[s->nh[ic - 1] - 1];
+        int nb = s->nn[s->nh[ib - 1] - 1], nd = s->nn[s->nh[id - 1] - 1];
+        if ((na == nc && nb == nd) || (na == nd && nb == nc)) {
+            tj = PLJ(ia, ic) * PLJ(id, ib) + PLJ(ic, ia) * PLJ(ib, id) - PLJ(ia, id) * PLJ(ic, ib) - PLJ(id, ia) * PLJ(ib, ic);
+            ts = ts + 2 * (P0S(ia, ic) * P0S(id, ib) - P0S(ia, id) * P0S(ic, ib));
+            ts = ts + 2 * (PLS(ia, ic) * PLS(id, ib) + PLS(ic, ia) * PLS(ib, id) - PLS(ia, id) * PLS(ic, ib) -
+                           PLS(id, ia) * PLS(ib, ic));
+            tl = tl + 2 * (P0L(ia, ic) * P0L(id, ib) - P0L(ia, id) * P0L(ic, ib));
+            tl = tl + 2 * (PLL(ia, ic) * PLL(id, ib) + PLL(ic, ia) * PLL(ib, id) - PLL(ia, id) * PLL(ic, ib) -
+                           PLL(id, ia) * PLL(ib, ic));
+            tj = tj * is;
+            ts = ts * is;
+            tl = tl * is;
+        }
+    }
+    *tj_ = tj;
+    *tl_ = tl * 4;
+    *ts_ = ts * 4;
+}
+
+/* calcLSJ, src/pconf.F90:2805-2863, for configurations ic_lo..ic_hi
+ * (1-based): the sums sum[q*nv + m] (q = J, L, S) of c_n c_k t over the
+ * pairs n <= k (doubled for n /= k); X is Nd x nv column-major.  CompNRC
+ * compares the non-relativistic orbitals Nh0 (src/determinants.f90:62-82)
+ * and CompC the relativistic ones. */
+void orc_lsj(const orc_sys *s, const double *X, int nv, int ic_lo, int ic_hi, double *sum)
+{
+    int ne = s->ne;
+    int *nh0 = (int *)malloc(sizeof(int) * (size_t)s->nst);
+    for (int i = 0; i < s->nst; i++) {
+        int ni = s->nh[i];
+        int nrorb = ni > 1 && s->nn[ni - 2] == s->nn[ni - 1] && s->ll[ni - 2] == s->ll[ni - 1];
+        nh0[i] = nrorb ? ni - 1 : ni;
+    }
+    int64_t *start = (int64_t *)malloc(sizeof(int64_t) * ((size_t)s->nc + 1));
+    start[0] = 0;
+    for (int c = 0; c < s->nc; c++) start[c + 1] = start[c] + s->ndc[c];
+    for (int q = 0; q < 3 * nv; q++) sum[q] = 0.0;
+    int32_t c1[8], c2[8];
+    for (int ic1 = ic_lo; ic1 <= ic_hi; ic1++) {
+        int64_t ndn = s->ndc[ic1 - 1], n = start[ic1 - 1];
+        for (int64_t n1 = 1; n1 <= ndn; n1++) {
+            n++;
+            const int32_t *d1 = s->iarr + (n - 1) * ne;
+            int64_t k = n - 1;
+            for (int ic2 = ic1; ic2 <= s->nc; ic2++) {
+                int64_t ndk = s->ndc[ic2 - 1], k1n = ic2 == ic1 ? n1 : 1;
+                const int32_t *d2 = s->iarr + k * ne;   /* determinant k + 1 */
+                for (int e = 0; e < ne; e++) { c1[e] = nh0[d1[e] - 1]; c2[e] = nh0[d2[e] - 1]; }
+                if (orc_compd(c1, c2, ne) > 0) { k += ndk; continue; }
+                for (int e = 0; e < ne; e++) { c1[e] = s->nh[d1[e] - 1]; c2[e] = s->nh[d2[e] - 1]; }
+                if (orc_compd(c1, c2, ne) > 2) { k += ndk; continue; }
+                for (int64_t k1 = k1n; k1 <= ndk; k1++) {
+                    k++;
+                    double tj, tl, ts;
+                    orc_lsj_det(s, d1, s->iarr + (k - 1) * ne, &tj, &tl, &ts);
+                    if (tj == 0.0 && tl == 0.0 && ts == 0.0) continue;
+                    for (int m = 0; m < nv; m++) {
+                        double ckn = X[(int64_t)m * s->nd + n - 1] * X[(int64_t)m * s->nd + k - 1];
+                        if (n != k) ckn = 2 * ckn;
+                        sum[m] = sum[m] + ckn * tj;
+                        sum[nv + m] = sum[nv + m] + ckn * tl;
+                        sum[2 * nv + m] = sum[2 * nv + m] + ckn * ts;
+                    }
+                }
+            }
+        }
+    }
+    free(start);
+    free(nh0);
+}

@@ -21,7 +21,7 @@ PCI_DVD_FP64, PCI_DVD_FP32, PCI_DVD_LEARNED = 0, 1, 2
 
 EXPORTS = ["pci_gpu_create", "pci_gpu_set_basis", "pci_gpu_set_integrals", "pci_gpu_form_h",
            "pci_gpu_form_j", "pci_gpu_csr_info", "pci_gpu_get_csr", "pci_gpu_set_csr",
-           "pci_gpu_davidson", "pci_gpu_j_av", "pci_gpu_j_av_noalloc", "pci_gpu_jterms", "pci_gpu_stats",
+           "pci_gpu_davidson", "pci_gpu_j_av", "pci_gpu_j_av_noalloc", "pci_gpu_lsj", "pci_gpu_jterms", "pci_gpu_stats",
            "pci_gpu_last_error", "pci_gpu_destroy", "pci_mlp_create", "pci_mlp_num_params", "pci_mlp_set_params",
            "pci_mlp_get_params", "pci_mlp_forward", "pci_mlp_loss_grad", "pci_mlp_train", "pci_mlp_last_error",
            "pci_mlp_destroy", "pci_gpu_set_correction_model", "pci_gpu_davidson_harvest", "pci_mlp_forward_occ",
@@ -81,6 +81,7 @@ def load(path: str = LIB):
     L.pci_gpu_set_csr.argtypes = [P, i32, i64, i64, P, P, P, f64]
     L.pci_gpu_davidson.argtypes = [P, C.POINTER(DvdParams), P, P, P, P, P, C.POINTER(i32), P]
     L.pci_gpu_j_av.argtypes = [P, P, i32, i64, P]
+    L.pci_gpu_lsj.argtypes = [P, P, i32, P, P, P]
     L.pci_gpu_j_av_noalloc.argtypes = [P, P, P, i64, P, i64, i32, i64, P, P, C.c_char_p, i32]
     L.pci_mlp_create.argtypes = [i32, i32, i32, C.POINTER(P)]
     L.pci_mlp_num_params.argtypes = [P]
@@ -287,6 +288,18 @@ class Engine:
         out = np.zeros(nv)
         self._check(self.L.pci_gpu_j_av(self.h, _p(xc), nv, nd if nlim is None else nlim, _p(out)))
         return out
+
+    def lsj(self, X):
+        """(J, L, S) of each column of X (Nd x nv), as pconf's kLSJ = 1 step
+        computes them (pci_gpu_lsj)."""
+        X = np.asarray(X, np.float64)
+        if X.ndim == 1:
+            X = X[:, None]
+        nd, nv = X.shape
+        xc = np.ascontiguousarray(X.T)        # column-major Nd x nv
+        xj, xl, xs = np.zeros(nv), np.zeros(nv), np.zeros(nv)
+        self._check(self.L.pci_gpu_lsj(self.h, _p(xc), nv, _p(xj), _p(xl), _p(xs)))
+        return xj, xl, xs
 
     def set_correction_model(self, mlp):
         """Attach a trained Mlp for mode=PCI_DVD_LEARNED (None detaches)."""

@@ -1,0 +1,388 @@
+// LSJ: per-level <J^2>, <L^2>, <S^2> of CI vectors in the determinant basis,
+// as pconf's lsj / calcLSJ / lsj_det compute them (src/pconf.F90:2672-2962)
+// for kLSJ = 1, returned as J, L, S (x = (sqrt(<X^2> + 1) - 1) / 2).
+//
+// The reference loops over every determinant n and every later determinant k
+// whose non-relativistic configuration equals n's (CompNRC = 0) and whose
+// relativistic configuration differs by at most two orbitals (CompC <= 2).
+// Here the host groups the configurations by their non-relativistic orbital
+// multiset once per call, lists the configuration pairs (c1 <= c2) of each
+// group with CompD <= 2, and one warp evaluates the determinant pairs of one
+// configuration pair: the difference of the two occupation lists (Rspq), the
+// one-electron elements of J+, S+, Sz, L+, Lz between m-states, and the
+// contributions c_n c_k t (doubled off the diagonal) to every level, summed
+// in registers and added to the result once per warp.  Compiled with
+// -fmad=false so each pair's terms follow the reference's operation order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <vector>
+
+#include "pci_internal.h"
+
+namespace {
+
+constexpr int LSJ_NVC = 8;   // levels per launch
+
+// Device memory released when the scope ends.
+struct LsjBuf {
+    void *p = nullptr;
+    ~LsjBuf() { dev_free(p); }
+};
+
+// What lsj_det needs of one m-state.
+struct LMs {
+    int orb, n, l, j2, m2;
+};
+
+__device__ __forceinline__ LMs lms(const uint32_t *msd, const int8_t *orb_n, int a)
+{
+    const uint32_t w = __ldg(&msd[a]);
+    LMs r;
+    r.orb = (int)(w & 1023u);
+    r.m2 = (int)((w >> 16) & 255u) - 128;
+    r.l = (int)((w >> 24) & 15u);
+    r.j2 = 2 * (int)((w >> 28) & 15u) + 1;
+    r.n = orb_n[r.orb];
+    return r;
+}
+
+// Plus_j (src/pconf.F90:3129-3140)
+__device__ double d_plus_j(const LMs &a, const LMs &b)
+{
+    double t = 0.0;
+    if (a.orb == b.orb && a.m2 == b.m2 + 2) t = sqrt((double)(a.j2 * (a.j2 + 2) - a.m2 * b.m2) + 0.0);
+    return t;
+}
+
+// The jj -> ls coefficients shared by plus_s, plus_l, p0_s, p0_l for spin
+// projection msa (+-1) of m-state a, with the sign convention of the
+// reference's "ta" (first) and "tb" (second) factors.
+__device__ __forceinline__ double d_ta(int j, int l, int mj, int msa)
+{
+    double t = 0.0;
+    if (msa == 1) {
+        if (j == 2 * l + 1) t = sqrt((j + mj) / (2.0 * j));
+        if (j == 2 * l - 1) t = -sqrt((j - mj + 2.0) / (2.0 * j + 4.0));
+    } else {
+        if (j == 2 * l + 1) t = sqrt((j - mj) / (2.0 * j));
+        if (j == 2 * l - 1) t = sqrt((j + mj + 2.0) / (2.0 * j + 4.0));
+    }
+    return t;
+}
+
+// plus_s (src/pconf.F90:2964-2997)
+__device__ double d_plus_s(const LMs &a, const LMs &b)
+{
+    if (a.m2 != b.m2 + 2 || a.n != b.n || a.l != b.l) return 0.0;
+    const int mla = (a.m2 - 1) / 2;
+    if (abs(mla) > a.l) return 0.0;
+    const double ta = d_ta(a.j2, a.l, a.m2, 1);
+    double tb = 0.0;   // spin down of b
+    if (b.j2 == 2 * b.l + 1) tb = sqrt((b.j2 - b.m2) / (2.0 * b.j2));
+    if (b.j2 == 2 * b.l - 1) tb = sqrt((b.j2 + b.m2 + 2.0) / (2.0 * b.j2 + 4.0));
+    return -sqrt(0.5) * ta * tb;
+}
+
+// plus_l (src/pconf.F90:2999-3042)
+__device__ double d_plus_l(const LMs &a, const LMs &b)
+{
+    if (a.m2 != b.m2 + 2 || a.n != b.n || a.l != b.l) return 0.0;
+    double t = 0.0;
+    for (int msa = -1; msa <= 1; msa += 2) {
+        const int mla = (a.m2 - msa) / 2, mlb = (b.m2 - msa) / 2;
+        if (abs(mla) > a.l || abs(mlb) > b.l) continue;
+        const double ta = d_ta(a.j2, a.l, a.m2, msa), tb = d_ta(b.j2, b.l, b.m2, msa);
+        t = t - sqrt(0.5 * (b.l * (b.l + 1.0) - mlb * (mlb + 1.0))) * ta * tb;
+    }
+    return t;
+}
+
+// p0_s (src/pconf.F90:3044-3086) and p0_l (3088-3127): Sz and Lz
+template <bool SPIN>
+__device__ double d_p0(const LMs &a, const LMs &b)
+{
+    if (a.m2 != b.m2 || a.n != b.n || a.l != b.l) return 0.0;
+    double t = 0.0;
+    for (int msa = -1; msa <= 1; msa += 2) {
+        const int mla = (a.m2 - msa) / 2;
+        if (abs(mla) > a.l) continue;
+        const double ta = d_ta(a.j2, a.l, a.m2, msa), tb = d_ta(b.j2, b.l, b.m2, msa);
+        if (SPIN) t = t + 0.5 * msa * (ta * tb);
+        else t = t + mla * (ta * tb);
+    }
+    return t;
+}
+
+// Difference of two sorted occupation lists as Rspq (src/determinants.f90:
+// 499-590) reports it: nf (3 = more than two), the differing m-states
+// (i1, i2 of det1 and j1, j2 of det2, earlier then later) and the sign.
+template <int NE>
+struct LDiff {
+    int nf, is, i1, i2, j1, j2;
+};
+
+template <int NE>
+__device__ __forceinline__ LDiff<NE> l_diff(const uint16_t *d1, const uint16_t *d2)
+{
+    unsigned ma = 0, mb = 0;
+#pragma unroll
+    for (int i = 0; i < NE; i++)
+#pragma unroll
+        for (int j = 0; j < NE; j++)
+            if (d1[i] == d2[j]) { ma |= 1u << i; mb |= 1u << j; }
+    LDiff<NE> r;
+    r.nf = NE - __popc(ma);
+    r.is = 1;
+    r.i1 = r.i2 = r.j1 = r.j2 = -1;
+    if (r.nf == 1 || r.nf == 2) {
+        const unsigned ua = (~ma) & ((1u << NE) - 1), ub = (~mb) & ((1u << NE) - 1);
+        const int ip1 = __ffs(ua) - 1, jp1 = __ffs(ub) - 1;
+        const int ip2 = 31 - __clz(ua), jp2 = 31 - __clz(ub);
+        if (r.nf == 1) {
+            r.i2 = d1[ip1];
+            r.j2 = d2[jp1];
+            r.is = ((ip1 + jp1) & 1) ? -1 : 1;
+        } else {
+            r.i1 = d1[ip1];
+            r.j1 = d2[jp1];
+            r.i2 = d1[ip2];
+            r.j2 = d2[jp2];
+            r.is = ((ip1 + jp1 + ip2 + jp2) & 1) ? -1 : 1;
+        }
+    }
+    return r;
+}
+
+// lsj_det (src/pconf.F90:2865-2962) for one determinant pair: tj, tl, ts.
+template <int NE>
+__device__ void d_lsj_det(const uint32_t *msd, const int8_t *orb_n, int mj, const uint16_t *d1, const uint16_t *d2,
+                          double &tj, double &tl, double &ts)
+{
+    tj = 0.0;
+    tl = 0.0;
+    ts = 0.0;
+    const LDiff<NE> df = l_diff<NE>(d1, d2);
+    if (df.nf == 0) {
+        tj = (double)(mj * mj);
+#pragma unroll
+        for (int iq = 0; iq < NE; iq++) {
+            const LMs a = lms(msd, orb_n, d1[iq]);
+            tj = tj + (double)(a.j2 * (a.j2 + 2) - a.m2 * a.m2);
+            ts = ts + 0.75;
+            tl = tl + (double)(a.l * (a.l + 1));
+#pragma unroll
+            for (int jq = iq + 1; jq < NE; jq++) {
+                const LMs b = lms(msd, orb_n, d1[jq]);
+                const double pj1 = d_plus_j(a, b), pj2 = d_plus_j(b, a);
+                tj = tj - pj1 * pj1 - pj2 * pj2;
+                const double sab = d_p0<true>(a, b);
+                ts = ts + 2 * (d_p0<true>(a, a) * d_p0<true>(b, b) - sab * sab);
+                const double s1 = d_plus_s(a, b), s2 = d_plus_s(b, a);
+                ts = ts - 2 * (s1 * s1 + s2 * s2);
+                const double lab = d_p0<false>(a, b);
+                tl = tl + 2 * (d_p0<false>(a, a) * d_p0<false>(b, b) - lab * lab);
+                const double l1 = d_plus_l(a, b), l2 = d_plus_l(b, a);
+                tl = tl - 2 * (l1 * l1 + l2 * l2);
+            }
+        }
+    } else if (df.nf == 1) {
+        const LMs a = lms(msd, orb_n, df.i2), b = lms(msd, orb_n, df.j2);
+        if (a.n == b.n) {
+#pragma unroll
+            for (int iq = 0; iq < NE; iq++) {
+                if (d1[iq] == df.i2) continue;
+                const LMs c = lms(msd, orb_n, d1[iq]);
+                ts = ts + 2 * (d_p0<true>(a, b) * d_p0<true>(c, c) - d_p0<true>(a, c) * d_p0<true>(b, c));
+                ts = ts - 2 * (d_plus_s(a, c) * d_plus_s(b, c) + d_plus_s(c, a) * d_plus_s(c, b));
+                tl = tl + 2 * (d_p0<false>(a, b) * d_p0<false>(c, c) - d_p0<false>(a, c) * d_p0<false>(b, c));
+                tl = tl - 2 * (d_plus_l(a, c) * d_plus_l(b, c) + d_plus_l(c, a) * d_plus_l(c, b));
+            }
+            ts = ts * df.is;
+            tl = tl * df.is;
+        }
+    } else if (df.nf == 2) {
+        // ia = i1, ic = j1, ib = i2, id = j2
+        const LMs a = lms(msd, orb_n, df.i1), c = lms(msd, orb_n, df.j1);
+        const LMs b = lms(msd, orb_n, df.i2), d = lms(msd, orb_n, df.j2);
+        if ((a.n == c.n && b.n == d.n) || (a.n == d.n && b.n == c.n)) {
+            tj = d_plus_j(a, c) * d_plus_j(d, b) + d_plus_j(c, a) * d_plus_j(b, d) - d_plus_j(a, d) * d_plus_j(c, b) -
+                 d_plus_j(d, a) * d_plus_j(b, c);
+            ts = ts + 2 * (d_p0<true>(a, c) * d_p0<true>(d, b) - d_p0<true>(a, d) * d_p0<true>(c, b));
+            ts = ts + 2 * (d_plus_s(a, c) * d_plus_s(d, b) + d_plus_s(c, a) * d_plus_s(b, d) -
+                           d_plus_s(a, d) * d_plus_s(c, b) - d_plus_s(d, a) * d_plus_s(b, c));
+            tl = tl + 2 * (d_p0<false>(a, c) * d_p0<false>(d, b) - d_p0<false>(a, d) * d_p0<false>(c, b));
+            tl = tl + 2 * (d_plus_l(a, c) * d_plus_l(d, b) + d_plus_l(c, a) * d_plus_l(b, d) -
+                           d_plus_l(a, d) * d_plus_l(c, b) - d_plus_l(d, a) * d_plus_l(b, c));
+            tj = tj * df.is;
+            ts = ts * df.is;
+            tl = tl * df.is;
+        }
+    }
+    ts = ts * 4;
+    tl = tl * 4;
+}
+
+// One warp per configuration pair (c1 <= c2 of one non-relativistic group):
+// every determinant pair n <= k, summed into out[q * nv + v] (q = J, L, S)
+// for levels v0 .. v0 + LSJ_NVC - 1 (X column-major, leading dimension nd).
+template <int NE>
+__global__ void __launch_bounds__(128) k_lsj(const uint16_t *__restrict__ occ, const int64_t *__restrict__ conf_start,
+                                             const uint32_t *__restrict__ msd, const int8_t *__restrict__ orb_n,
+                                             int mj, const int2 *__restrict__ items, int64_t nitems,
+                                             const double *__restrict__ X, int64_t nd, int nv, int v0, double *out)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int nvc = min(LSJ_NVC, nv - v0);
+    for (int64_t w = warp; w < nitems; w += nwarps) {
+        const int2 it = items[w];
+        const int64_t n0 = conf_start[it.x], nr = conf_start[it.x + 1] - n0;
+        const int64_t k0 = conf_start[it.y], nk = conf_start[it.y + 1] - k0;
+        const bool same = it.x == it.y;
+        double acc[3][LSJ_NVC];
+#pragma unroll
+        for (int q = 0; q < 3; q++)
+#pragma unroll
+            for (int v = 0; v < LSJ_NVC; v++) acc[q][v] = 0.0;
+        for (int64_t p = lane; p < nr * nk; p += 32) {
+            const int64_t a = p / nk, b = p - a * nk;
+            if (same && b < a) continue;
+            const int64_t n = n0 + a, k = k0 + b;
+            uint16_t d1[NE], d2[NE];
+#pragma unroll
+            for (int e = 0; e < NE; e++) { d1[e] = occ[n * NE + e]; d2[e] = occ[k * NE + e]; }
+            double tj, tl, ts;
+            d_lsj_det<NE>(msd, orb_n, mj, d1, d2, tj, tl, ts);
+            if (tj == 0.0 && tl == 0.0 && ts == 0.0) continue;
+#pragma unroll
+            for (int v = 0; v < LSJ_NVC; v++) {
+                if (v < nvc) {
+                    double ckn = X[(int64_t)(v0 + v) * nd + n] * X[(int64_t)(v0 + v) * nd + k];
+                    if (n != k) ckn = 2 * ckn;
+                    acc[0][v] = acc[0][v] + ckn * tj;
+                    acc[1][v] = acc[1][v] + ckn * tl;
+                    acc[2][v] = acc[2][v] + ckn * ts;
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 3; q++)
+#pragma unroll
+            for (int v = 0; v < LSJ_NVC; v++) {
+                double s = acc[q][v];
+                for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+                if (lane == 0 && v < nvc && s != 0.0) atomicAdd(&out[q * nv + v0 + v], s);
+            }
+    }
+}
+
+template <int NE>
+void launch_lsj(int blocks, cudaStream_t st, const DevSys &S, const int8_t *orb_n, const int2 *items, int64_t nitems,
+                const double *X, int nv, int v0, double *out)
+{
+    k_lsj<NE><<<blocks, 128, 0, st>>>(S.occ, S.conf_start, S.msd, orb_n, S.mj, items, nitems, X, S.nd, nv, v0, out);
+}
+
+}  // namespace
+
+// Configuration pairs (c1 <= c2) of equal non-relativistic configuration and
+// relativistic CompD <= 2, the pairs calcLSJ visits (src/pconf.F90:2805-2863).
+// A relativistic orbital that follows one of the same n and l maps to it
+// (Nh0, src/determinants.f90:62-82).
+static std::vector<int2> lsj_items(const pci_gpu *h, const std::vector<uint16_t> &conf_orb)
+{
+    const int ne = h->ne, nc = h->nc, nsu = h->nsu;
+    std::vector<int> nr(nsu);
+    for (int o = 0; o < nsu; o++)
+        nr[o] = (o > 0 && h->h_orb_n[o - 1] == h->h_orb_n[o] && h->h_orb_l[o - 1] == h->h_orb_l[o]) ? o - 1 : o;
+    std::map<std::vector<int>, std::vector<int>> groups;
+    for (int c = 0; c < nc; c++) {
+        if (h->h_ndc[c] == 0) continue;
+        std::vector<int> key(ne);
+        for (int e = 0; e < ne; e++) key[e] = nr[conf_orb[(size_t)c * ne + e]];
+        std::sort(key.begin(), key.end());
+        groups[key].push_back(c);
+    }
+    std::vector<int2> items;
+    for (const auto &g : groups) {
+        const std::vector<int> &cs = g.second;
+        for (size_t x = 0; x < cs.size(); x++)
+            for (size_t y = x; y < cs.size(); y++) {
+                const uint16_t *a = &conf_orb[(size_t)cs[x] * ne], *b = &conf_orb[(size_t)cs[y] * ne];
+                int i = 0, j = 0, ni = 0, nj = 0;
+                while (i < ne && j < ne) {
+                    if (a[i] == b[j]) { i++; j++; }
+                    else if (a[i] > b[j]) { nj++; j++; }
+                    else { ni++; i++; }
+                }
+                ni += ne - i;
+                nj += ne - j;
+                if (std::max(ni, nj) <= 2) items.push_back(make_int2(cs[x], cs[y]));
+            }
+    }
+    return items;
+}
+
+extern "C" {
+
+int pci_gpu_lsj(pci_gpu_t *h, const double *X, int32_t nv, double *xj, double *xl, double *xs)
+{
+    if (!h) return PCI_E_INPUT;
+    cudaSetDevice(h->device);
+    if (!X || !xj || !xl || !xs) return set_err(h, PCI_E_INPUT, "null array");
+    if (!h->have_basis) return set_err(h, PCI_E_STATE, "LSJ before set_basis");
+    if ((int)h->h_orb_n.size() != h->nsu) return set_err(h, PCI_E_STATE, "LSJ needs the principal numbers Nn");
+    if (nv < 1 || nv > 64) return set_err(h, PCI_E_INPUT, "LSJ: nv must be 1..64");
+    const int64_t nd = h->nd;
+    // configuration orbital lists (as set_basis built them)
+    std::vector<uint16_t> conf_orb((size_t)h->nc * h->ne);
+    PCI_CUDA(h, cudaMemcpy(conf_orb.data(), h->d_conf_orb, conf_orb.size() * 2, cudaMemcpyDeviceToHost));
+    const std::vector<int2> items = lsj_items(h, conf_orb);
+    int rc = 0;
+    LsjBuf d_items, d_x, d_out;
+    d_items.p = dev_alloc(h, std::max<size_t>(items.size(), 1) * sizeof(int2), &rc);
+    if (rc) return rc;
+    d_x.p = dev_alloc(h, (size_t)nd * nv * 8, &rc);
+    if (rc) return rc;
+    d_out.p = dev_alloc(h, (size_t)3 * nv * 8, &rc);
+    if (rc) return rc;
+    PCI_CUDA(h, cudaMemcpyAsync(d_items.p, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice, h->st));
+    PCI_CUDA(h, cudaMemcpyAsync(d_x.p, X, (size_t)nd * nv * 8, cudaMemcpyHostToDevice, h->st));
+    PCI_CUDA(h, cudaMemsetAsync(d_out.p, 0, (size_t)3 * nv * 8, h->st));
+    const DevSys S = make_devsys(h);
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+    const int blocks = nsm * 8;
+    const int64_t nit = (int64_t)items.size();
+    for (int v0 = 0; v0 < nv && nit > 0; v0 += LSJ_NVC) {
+        const int2 *it = (const int2 *)d_items.p;
+        const double *x = (const double *)d_x.p;
+        double *o = (double *)d_out.p;
+        switch (h->ne) {
+        case 1: launch_lsj<1>(blocks, h->st, S, h->d_orb_n, it, nit, x, nv, v0, o); break;
+        case 2: launch_lsj<2>(blocks, h->st, S, h->d_orb_n, it, nit, x, nv, v0, o); break;
+        case 3: launch_lsj<3>(blocks, h->st, S, h->d_orb_n, it, nit, x, nv, v0, o); break;
+        case 4: launch_lsj<4>(blocks, h->st, S, h->d_orb_n, it, nit, x, nv, v0, o); break;
+        case 5: launch_lsj<5>(blocks, h->st, S, h->d_orb_n, it, nit, x, nv, v0, o); break;
+        case 6: launch_lsj<6>(blocks, h->st, S, h->d_orb_n, it, nit, x, nv, v0, o); break;
+        case 7: launch_lsj<7>(blocks, h->st, S, h->d_orb_n, it, nit, x, nv, v0, o); break;
+        default: launch_lsj<8>(blocks, h->st, S, h->d_orb_n, it, nit, x, nv, v0, o); break;
+        }
+        PCI_CUDA(h, cudaGetLastError());
+    }
+    std::vector<double> sums((size_t)3 * nv);
+    PCI_CUDA(h, cudaMemcpyAsync(sums.data(), d_out.p, sums.size() * 8, cudaMemcpyDeviceToHost, h->st));
+    PCI_CUDA(h, cudaStreamSynchronize(h->st));
+    for (int v = 0; v < nv; v++) {
+        xj[v] = 0.5 * (sqrt(sums[v] + 1) - 1);
+        xl[v] = 0.5 * (sqrt(sums[nv + v] + 1) - 1);
+        xs[v] = 0.5 * (sqrt(sums[2 * nv + v] + 1) - 1);
+    }
+    return PCI_OK;
+}
+
+}  // extern "C"

@@ -101,6 +101,8 @@ static void free_basis(pci_gpu *h)
     dev_free(h->d_adj_ptr); dev_free(h->d_adj); dev_free(h->d_ms_orb); dev_free(h->d_ms_jz);
     dev_free(h->d_ms_type); dev_free(h->d_orb_l); dev_free(h->d_orb_j); dev_free(h->d_msd);
     dev_free(h->d_barr);
+    dev_free(h->d_orb_n);
+    h->d_orb_n = nullptr;
     h->d_msd = nullptr;
     h->d_barr = nullptr;
     h->nint = 0;
@@ -264,7 +266,6 @@ int pci_gpu_set_basis(pci_gpu_t *h, int32_t Ne, int64_t Nd, int32_t Nst, int32_t
     if (Nst < 1 || Nst > 65000) return set_err(h, PCI_E_INPUT, "Nst out of range");
     if (Nsu < 1 || Nc < 1 || Nx < 1 || Nso < 0) return set_err(h, PCI_E_INPUT, "bad Nsu/Nc/Nx/Nso");
     if (!Iarr || !Nh || !Jz || !Kk || !Ll || !Jj || !Ndc) return set_err(h, PCI_E_INPUT, "null array");
-    (void)Nn;
     int64_t sum = 0;
     for (int c = 0; c < Nc; c++) {
         if (Ndc[c] < 0) return set_err(h, PCI_E_INPUT, "negative Ndc");
@@ -285,6 +286,8 @@ int pci_gpu_set_basis(pci_gpu_t *h, int32_t Ne, int64_t Nd, int32_t Nst, int32_t
     h->h_orb_j.assign(Jj, Jj + Nsu);
     h->h_orb_l.assign(Ll, Ll + Nsu);
     h->h_orb_k.assign(Kk, Kk + Nsu);
+    if (Nn) h->h_orb_n.assign(Nn, Nn + Nsu);
+    else h->h_orb_n.clear();
     h->h_nh.assign(Nh, Nh + Nst);
     h->h_jz.assign(Jz, Jz + Nst);
     // determinants: 0-based uint16, validated sorted and configuration-consistent
@@ -339,6 +342,14 @@ int pci_gpu_set_basis(pci_gpu_t *h, int32_t Ne, int64_t Nd, int32_t Nst, int32_t
     if ((rc = upload(h, &h->d_msd, msd))) return rc;
     if ((rc = upload(h, &h->d_orb_l, orb_l))) return rc;
     if ((rc = upload(h, &h->d_orb_j, orb_j))) return rc;
+    if (Nn) {
+        std::vector<int8_t> orb_n(Nsu);
+        for (int o = 0; o < Nsu; o++) {
+            if (Nn[o] < 1 || Nn[o] > 127) return set_err(h, PCI_E_INPUT, "Nn outside 1..127");
+            orb_n[o] = (int8_t)Nn[o];
+        }
+        if ((rc = upload(h, &h->d_orb_n, orb_n))) return rc;
+    }
     PCI_CUDA(h, cudaStreamSynchronize(h->st));
     h->have_basis = true;
     h->have_ints = false;  // tables depend on the basis; integrals must be set again

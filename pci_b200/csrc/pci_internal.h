@@ -65,6 +65,8 @@ struct pci_gpu {
     bool have_basis = false, have_ints = false;
     std::vector<int32_t> h_ndc;       // host copy of Ndc
     std::vector<int32_t> h_orb_j, h_orb_l, h_orb_k;
+    std::vector<int32_t> h_orb_n;     // principal numbers Nn (empty when not given)
+    int8_t *d_orb_n = nullptr;
     std::vector<int32_t> h_nh, h_jz;
     std::vector<int32_t> h_jterms;    // Jt(1:Njd): sorted 2J of the terms present
     std::vector<unsigned long long> h_rowwork;   // determinant pairs per row, per configuration
