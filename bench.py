@@ -595,10 +595,11 @@ def run_batched(args, local, rank, world, dist, peak, peak_kind):
     b = Batch(local)
     formh_ms = 0.0
     launches = 0
+    numh_blk = []
     for i in order:
         with Engine(local) as e:
             e.load_system(blocks[i])
-            e.form_h(32)
+            numh_blk.append(e.form_h(32)[0])
             st = e.stats()
             formh_ms += st["formh_ms"]
             launches += int(st["formh_launches"]) + 1
@@ -641,6 +642,18 @@ def run_batched(args, local, rank, world, dist, peak, peak_kind):
                           "algorithmic_bytes": int(sp_bytes)},
         "gpu_launches": launches,
     }
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        # the oracle's FormH and Mxmpy rates on the largest block, applied to
+        # every block's stored elements and iteration count (blocks in sequence)
+        big = int(np.argmax(numh_blk))
+        rates = cpu_solve_estimate(blocks[order[big]], nlv, 1, numh_blk[big], 17, os.cpu_count() or 1)
+        est_s = sum(nh / rates["formh_nnz_per_s"] + int(r["iters"][j]) * nh / rates["mxmpy_elements_per_s"]
+                    for j, nh in enumerate(numh_blk))
+        out["cpu_baseline"] = {"value_ms": 1e3 * est_s, "unit": "ms (estimate from a sample)",
+                               "cores": rates["cores"], "kind": "port",
+                               "sample": "the largest block's " + rates["sample"].split(";")[0] + "; its rates "
+                                         "applied to every block's stored elements and iteration count, the "
+                                         "blocks solved one after another"}
     return out
 
 
