@@ -866,7 +866,7 @@ __global__ void __launch_bounds__(BT_FIN_THREADS) kb_fin(const int64_t *__restri
             s.iters += 1;
             sh_restart = 0;
             sh_base = 0;
-            // judge of the learned correction: a root whose residual did not drop
+            // fallback of the learned correction: a root whose residual did not drop
             // since the previous iteration takes the diagonal correction from now on
             // (not right after the end of the FP32 phase, whose restart recomputes H V)
             if (s.iters >= 2 && s.iters != s.swit + 1)

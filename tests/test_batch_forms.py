@@ -116,7 +116,7 @@ def test_tensor_core_forward_matches_forward():
     m.close()
 
 
-def test_learned_correction_converges_and_judge():
+def test_learned_correction_converges_and_falls_back():
     """The learned form on a held-out config-1 seed, with a network trained on
     samples harvested from the solver's own converged runs at other seeds:
     every root converges to the same levels as the diagonal form."""
