@@ -63,6 +63,15 @@ module pci_gpu_mod
        import; type(c_ptr), value :: h; real(c_double) :: X(*), xj(*), xl(*), xs(*)
        integer(c_int32_t), value :: nv
      end function
+     ! kCSF = 1: jbasis + formh_sym (csf.f90); the CSF H replaces H on the handle
+     integer(c_int) function pci_gpu_form_csf(h, ncsf, numh) bind(C)
+       import; type(c_ptr), value :: h; integer(c_int64_t) :: ncsf, numh
+     end function
+     ! unsym (csf.f90:1088-1134): Y(Ncsf, nv) -> X(Nd, nv)
+     integer(c_int) function pci_gpu_csf_to_det(h, Y, nv, X) bind(C)
+       import; type(c_ptr), value :: h; real(c_double) :: Y(*), X(*)
+       integer(c_int32_t), value :: nv
+     end function
      ! FormBarr: Barr(nint, Nd) of the basis (barr may be c_null_ptr)
      integer(c_int) function pci_gpu_form_barr(h, nint, barr) bind(C)
        import; type(c_ptr), value :: h; integer(c_int32_t) :: nint

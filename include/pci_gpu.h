@@ -160,6 +160,22 @@ int pci_gpu_j_av(pci_gpu_t *h, const double *X, int32_t nv, int64_t nlim, double
  * passed to pci_gpu_set_basis (PCI_E_STATE without them). */
 int pci_gpu_lsj(pci_gpu_t *h, const double *X, int32_t nv, double *xj, double *xl, double *xs);
 
+/* Replaces: the kCSF = 1 path, jbasis + formh_sym (csf.f90:17-407, 538-1006;
+ * pconf.F90:146-148, 211-214).  From the resident FP64 determinant H
+ * (pci_gpu_form_h(64)) and J^2 (pci_gpu_form_j): each configuration's CSFs
+ * are the eigenvectors of its J^2 block with 2J = Mj, and the CSF
+ * Hamiltonian C^T H C replaces H on the handle (lower triangle, FP64; CSFs
+ * in configuration order).  *ncsf receives the number of CSFs, *numh the
+ * stored elements.  Solve it with the batched solver (pci_batch_add_block);
+ * pci_gpu_davidson refuses it.  Configurations of up to 112 determinants. */
+int pci_gpu_form_csf(pci_gpu_t *h, int64_t *ncsf, int64_t *numh);
+/* CSFs of each configuration (Nc entries) after pci_gpu_form_csf. */
+int pci_gpu_csf_counts(pci_gpu_t *h, int32_t *per_conf);
+/* Replaces: unsym (csf.f90:1088-1134).  Y is Ncsf x nv column-major on the
+ * host (1 <= nv <= 64); X (Nd x nv, column-major, host) receives the
+ * determinant vectors. */
+int pci_gpu_csf_to_det(pci_gpu_t *h, const double *Y, int32_t nv, double *X);
+
 /* No counterpart in the reference.  The J_av of pci_gpu_j_av for callers that
  * cannot allocate device memory (a host that owns all device memory through
  * its own pool or a framework's caching allocator, or a path where

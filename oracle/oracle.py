@@ -560,3 +560,43 @@ def diag4(nd, H, hmin, J, params, ndc, mxmpy_threads=1, log=None, timing=None, j
                          cnorm=cnorms.copy(), converged=bool(np.all(Iconverge == 1)),
                          Nd0=Nd0, seconds=time.perf_counter() - t_start, history=hist)
     return res
+
+
+def csf_basis(sysm, J):
+    """jbasis (src/csf.f90:17-407) for every configuration, densely: the J^2
+    block of the configuration's determinants (build_j2, 409-452, from the
+    FormJ CSR J = (rowptr, col 1-based, val) lower triangle), its
+    eigenvectors (DSYEVD), and the ones with 2J = Mj kept, J from
+    (sqrt(1 + eigenvalue) - 1) / 2.  Returns (per-configuration CSF counts,
+    the block-diagonal Nd x Ncsf coefficient matrix C)."""
+    jr, jc, jv = J
+    nd = sysm.nd
+    starts = np.concatenate([[0], np.cumsum(sysm.ndc)])
+    counts, cols = [], []
+    for c in range(len(sysm.ndc)):
+        a, b = int(starts[c]), int(starts[c + 1])
+        m = b - a
+        Z = np.zeros((m, m))
+        for n in range(a, b):
+            for l in range(jr[n], jr[n + 1]):
+                k = jc[l] - 1
+                if a <= k <= n:
+                    Z[n - a, k - a] = Z[k - a, n - a] = jv[l]
+        de, zz = np.linalg.eigh(Z)
+        tj = 0.5 * (np.sqrt(1.0 + de) - 1.0)
+        jtt = np.floor(2 * tj + 0.0001).astype(int)
+        if np.any(np.abs(2 * tj - jtt) > 1e-7):
+            raise ValueError(f"jbasis: J not integer or half-integer in configuration {c + 1}")
+        sel = np.flatnonzero(jtt == sysm.mj)
+        counts.append(sel.size)
+        for s in sel:
+            v = np.zeros(nd)
+            v[a:b] = zz[:, s]
+            cols.append(v)
+    C = np.stack(cols, axis=1) if cols else np.zeros((nd, 0))
+    return np.asarray(counts), C
+
+
+def csf_hamiltonian(H_dense, C):
+    """formh_sym (src/csf.f90:538-964): the CSF-basis H = C^T H C."""
+    return C.T @ H_dense @ C

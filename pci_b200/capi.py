@@ -21,7 +21,8 @@ PCI_DVD_FP64, PCI_DVD_FP32, PCI_DVD_LEARNED = 0, 1, 2
 
 EXPORTS = ["pci_gpu_create", "pci_gpu_set_basis", "pci_gpu_set_integrals", "pci_gpu_form_h",
            "pci_gpu_form_j", "pci_gpu_csr_info", "pci_gpu_get_csr", "pci_gpu_set_csr",
-           "pci_gpu_davidson", "pci_gpu_j_av", "pci_gpu_j_av_noalloc", "pci_gpu_lsj", "pci_gpu_jterms", "pci_gpu_stats",
+           "pci_gpu_davidson", "pci_gpu_j_av", "pci_gpu_j_av_noalloc", "pci_gpu_lsj", "pci_gpu_form_csf", "pci_gpu_csf_counts",
+           "pci_gpu_csf_to_det", "pci_gpu_jterms", "pci_gpu_stats",
            "pci_gpu_last_error", "pci_gpu_destroy", "pci_mlp_create", "pci_mlp_num_params", "pci_mlp_set_params",
            "pci_mlp_get_params", "pci_mlp_forward", "pci_mlp_loss_grad", "pci_mlp_train", "pci_mlp_last_error",
            "pci_mlp_destroy", "pci_gpu_set_correction_model", "pci_gpu_davidson_harvest", "pci_mlp_forward_occ",
@@ -82,6 +83,9 @@ def load(path: str = LIB):
     L.pci_gpu_davidson.argtypes = [P, C.POINTER(DvdParams), P, P, P, P, P, C.POINTER(i32), P]
     L.pci_gpu_j_av.argtypes = [P, P, i32, i64, P]
     L.pci_gpu_lsj.argtypes = [P, P, i32, P, P, P]
+    L.pci_gpu_form_csf.argtypes = [P, P, P]
+    L.pci_gpu_csf_counts.argtypes = [P, P]
+    L.pci_gpu_csf_to_det.argtypes = [P, P, i32, P]
     L.pci_gpu_j_av_noalloc.argtypes = [P, P, P, i64, P, i64, i32, i64, P, P, C.c_char_p, i32]
     L.pci_mlp_create.argtypes = [i32, i32, i32, C.POINTER(P)]
     L.pci_mlp_num_params.argtypes = [P]
@@ -300,6 +304,31 @@ class Engine:
         xj, xl, xs = np.zeros(nv), np.zeros(nv), np.zeros(nv)
         self._check(self.L.pci_gpu_lsj(self.h, _p(xc), nv, _p(xj), _p(xl), _p(xs)))
         return xj, xl, xs
+
+    def form_csf(self):
+        """jbasis + formh_sym on the device: the CSF Hamiltonian replaces the
+        determinant one (needs form_h(64) and form_j first); (ncsf, stored
+        elements)."""
+        n, nnz = C.c_int64(), C.c_int64()
+        self._check(self.L.pci_gpu_form_csf(self.h, C.byref(n), C.byref(nnz)))
+        self._ncsf = n.value
+        return n.value, nnz.value
+
+    def csf_counts(self, nc):
+        out = np.zeros(nc, np.int32)
+        self._check(self.L.pci_gpu_csf_counts(self.h, _p(out)))
+        return out
+
+    def csf_to_det(self, Y):
+        """unsym: determinant vectors (Nd x nv) from CSF vectors (Ncsf x nv)."""
+        Y = np.asarray(Y, np.float64)
+        if Y.ndim == 1:
+            Y = Y[:, None]
+        nv = Y.shape[1]
+        yc = np.ascontiguousarray(Y.T)
+        out = np.zeros((nv, self._nd))
+        self._check(self.L.pci_gpu_csf_to_det(self.h, _p(yc), nv, _p(out)))
+        return out.T
 
     def set_correction_model(self, mlp):
         """Attach a trained Mlp for mode=PCI_DVD_LEARNED (None detaches)."""

@@ -103,6 +103,10 @@ static void free_basis(pci_gpu *h)
     dev_free(h->d_barr);
     dev_free(h->d_orb_n);
     h->d_orb_n = nullptr;
+    dev_free(h->d_csf_C); dev_free(h->d_csf_start); dev_free(h->d_csf_coff);
+    h->d_csf_C = nullptr; h->d_csf_start = nullptr; h->d_csf_coff = nullptr;
+    h->h_csf_start.clear();
+    h->ncsf = 0;
     h->d_msd = nullptr;
     h->d_barr = nullptr;
     h->nint = 0;
@@ -494,6 +498,8 @@ int pci_gpu_davidson(pci_gpu_t *h, const pci_dvd_params *p, const double *X0, do
 {
     if (!h || !p) return PCI_E_INPUT;
     cudaSetDevice(h->device);
+    if (h->H.rowptr && h->H.nrows != h->nd)
+        return set_err(h, PCI_E_STATE, "davidson: the resident matrix is the CSF one; solve it with the batched solver");
     return dv_run(h, p, X0, Tk, Tj, Iconverge, X, iters, resid);
 }
 

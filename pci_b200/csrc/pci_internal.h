@@ -67,6 +67,13 @@ struct pci_gpu {
     std::vector<int32_t> h_orb_j, h_orb_l, h_orb_k;
     std::vector<int32_t> h_orb_n;     // principal numbers Nn (empty when not given)
     int8_t *d_orb_n = nullptr;
+    // CSF basis (pci_gpu_form_csf): coefficients C_c (ndc x ncsf per
+    // configuration, column-major at csf_coff[c]) and the first CSF of each
+    // configuration
+    double *d_csf_C = nullptr;
+    int64_t *d_csf_start = nullptr, *d_csf_coff = nullptr;
+    std::vector<int64_t> h_csf_start;
+    int64_t ncsf = 0;
     std::vector<int32_t> h_nh, h_jz;
     std::vector<int32_t> h_jterms;    // Jt(1:Njd): sorted 2J of the terms present
     std::vector<unsigned long long> h_rowwork;   // determinant pairs per row, per configuration
