@@ -84,6 +84,7 @@ def parse():
     ap.add_argument("--tune-cache", default=None, help="SpMM tuning cache of the batched form "
                     "(default: ~/.cache/pci_b200/spmm_tune_cache.txt; empty string = tune every run)")
     ap.add_argument("--no-lsj", action="store_true", help="skip the LSJ section")
+    ap.add_argument("--no-csf", action="store_true", help="skip the CSF-basis section")
     ap.add_argument("--davidson-iters", type=int, default=2,
                     help="plain FP64 Davidson iterations timed after the H-build (0 skips)")
     return ap.parse_args()
@@ -315,6 +316,7 @@ def run_ours(args):
     }
     if not args.no_lsj:
         line["lsj"] = lsj_section(args, eng, sysm)
+
     if args.davidson_iters > 0:
         eng.form_j()
         nlv = int(sysm.params["Nlv"])
@@ -362,6 +364,11 @@ def run_ours(args):
         line["cpu_baseline"] = {"value": n / t, "unit": "nnz/s", "cores": os.cpu_count() or 1, "kind": "port",
                                 "sample": f"{r} random rows of FormH ({n} non-zeros, {t:.1f} s), oracle "
                                           f"restatement of src/pconf.F90:1227-1290 with OpenMP"}
+    if not args.no_csf:
+        try:
+            line["csf"] = csf_section(args, local, eng, sysm)
+        except Exception as exc:   # an optional section must not cost the bench line
+            line["csf"] = {"error": str(exc)[:300]}
     eng.close()
     if args.roots:
         flush = None
@@ -410,6 +417,34 @@ def lsj_section(args, eng, sysm):
                                "sample": f"oracle calcLSJ over configurations 1..{k} of {sysm.nc} "
                                          f"({tc:.1f} s), scaled by determinants x later configurations"}
     return out
+
+
+def csf_section(args, local, e, sysm):
+    """kCSF = 1 on the configuration, on the bench's engine (its matrix is
+    replaced): FormH (FP64) + FormJ + jbasis/formh_sym (pci_gpu_form_csf),
+    then the CSF matrix's lowest roots (the levels with 2J = Mj) to residual
+    1e-8 through the batched solver; device times, form_csf host-timed."""
+    from pci_b200.capi import Batch
+    nlv = int(sysm.params["Nlv"])
+    numh = e.form_h(64)[0]
+    e.form_j()
+    st = e.stats()
+    t0 = time.perf_counter()
+    ncsf, nnz = e.form_csf()
+    t_csf = time.perf_counter() - t0
+    b = Batch(local)
+    b.set_value_prec(64)
+    b.add_engine(e)
+    r = b.davidson(nlv=nlv, max_sub=112, keep=48, max_it=400, tol=1e-8, it_per_graph=4)
+    stb = b.stats()
+    b.close()
+    return {"workload": f"{args.config}: CSF basis (2J = Mj = {sysm.mj}), {nlv} roots to residual 1e-8",
+            "ncsf": int(ncsf), "nd": int(sysm.nd), "numh_det": int(numh), "numh_csf": int(nnz),
+            "formh_ms": st["formh_ms"], "formj_ms": st["formj_ms"], "form_csf_ms": 1e3 * t_csf,
+            "solve_ms": stb["total_ms"], "iterations": int(r["iters"][0]), "converged": bool(r["status"][0] == 1),
+            "max_residual": float(np.max(r["rnorm"])),
+            "value_ms": st["formh_ms"] + st["formj_ms"] + 1e3 * t_csf + stb["total_ms"],
+            "roots": [float(x) for x in r["E"][0]]}
 
 
 def spmm_bytes(numh, nd, nlv, value_bytes, vec_bytes):
@@ -645,15 +680,18 @@ def run_batched(args, local, rank, world, dist, peak, peak_kind):
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         # the oracle's FormH and Mxmpy rates on the largest block, applied to
         # every block's stored elements and iteration count (blocks in sequence)
-        big = int(np.argmax(numh_blk))
-        rates = cpu_solve_estimate(blocks[order[big]], nlv, 1, numh_blk[big], 17, os.cpu_count() or 1)
-        est_s = sum(nh / rates["formh_nnz_per_s"] + int(r["iters"][j]) * nh / rates["mxmpy_elements_per_s"]
-                    for j, nh in enumerate(numh_blk))
-        out["cpu_baseline"] = {"value_ms": 1e3 * est_s, "unit": "ms (estimate from a sample)",
-                               "cores": rates["cores"], "kind": "port",
-                               "sample": "the largest block's " + rates["sample"].split(";")[0] + "; its rates "
-                                         "applied to every block's stored elements and iteration count, the "
-                                         "blocks solved one after another"}
+        try:
+            big = int(np.argmax(numh_blk))
+            rates = cpu_solve_estimate(blocks[order[big]], nlv, 1, numh_blk[big], 17, os.cpu_count() or 1)
+            est_s = sum(nh / rates["formh_nnz_per_s"] + int(r["iters"][j]) * nh / rates["mxmpy_elements_per_s"]
+                        for j, nh in enumerate(numh_blk))
+            out["cpu_baseline"] = {"value_ms": 1e3 * est_s, "unit": "ms (estimate from a sample)",
+                                   "cores": rates["cores"], "kind": "port",
+                                   "sample": "the largest block's " + rates["sample"].split(";")[0] + "; its "
+                                             "rates applied to every block's stored elements and iteration count, "
+                                             "the blocks solved one after another"}
+        except Exception as exc:   # the estimate must not cost the bench line
+            out["cpu_baseline"] = {"error": str(exc)[:300]}
     return out
 
 

@@ -338,28 +338,31 @@ int pci_gpu_lsj(pci_gpu_t *h, const double *X, int32_t nv, double *xj, double *x
     if ((int)h->h_orb_n.size() != h->nsu) return set_err(h, PCI_E_STATE, "LSJ needs the principal numbers Nn");
     if (nv < 1 || nv > 64) return set_err(h, PCI_E_INPUT, "LSJ: nv must be 1..64");
     const int64_t nd = h->nd;
-    // configuration orbital lists (as set_basis built them)
-    std::vector<uint16_t> conf_orb((size_t)h->nc * h->ne);
-    PCI_CUDA(h, cudaMemcpy(conf_orb.data(), h->d_conf_orb, conf_orb.size() * 2, cudaMemcpyDeviceToHost));
-    const std::vector<int2> items = lsj_items(h, conf_orb);
     int rc = 0;
-    LsjBuf d_items, d_x, d_out;
-    d_items.p = dev_alloc(h, std::max<size_t>(items.size(), 1) * sizeof(int2), &rc);
-    if (rc) return rc;
+    if (h->lsj_nitems < 0) {
+        // the configuration pairs depend on the basis only: built once
+        std::vector<uint16_t> conf_orb((size_t)h->nc * h->ne);
+        PCI_CUDA(h, cudaMemcpy(conf_orb.data(), h->d_conf_orb, conf_orb.size() * 2, cudaMemcpyDeviceToHost));
+        const std::vector<int2> items = lsj_items(h, conf_orb);
+        h->d_lsj_items = (int2 *)dev_alloc(h, std::max<size_t>(items.size(), 1) * sizeof(int2), &rc);
+        if (rc) return rc;
+        PCI_CUDA(h, cudaMemcpy(h->d_lsj_items, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice));
+        h->lsj_nitems = (int64_t)items.size();
+    }
+    LsjBuf d_x, d_out;
     d_x.p = dev_alloc(h, (size_t)nd * nv * 8, &rc);
     if (rc) return rc;
     d_out.p = dev_alloc(h, (size_t)3 * nv * 8, &rc);
     if (rc) return rc;
-    PCI_CUDA(h, cudaMemcpyAsync(d_items.p, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice, h->st));
     PCI_CUDA(h, cudaMemcpyAsync(d_x.p, X, (size_t)nd * nv * 8, cudaMemcpyHostToDevice, h->st));
     PCI_CUDA(h, cudaMemsetAsync(d_out.p, 0, (size_t)3 * nv * 8, h->st));
     const DevSys S = make_devsys(h);
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
     const int blocks = nsm * 8;
-    const int64_t nit = (int64_t)items.size();
+    const int64_t nit = h->lsj_nitems;
     for (int v0 = 0; v0 < nv && nit > 0; v0 += LSJ_NVC) {
-        const int2 *it = (const int2 *)d_items.p;
+        const int2 *it = h->d_lsj_items;
         const double *x = (const double *)d_x.p;
         double *o = (double *)d_out.p;
         switch (h->ne) {

@@ -107,6 +107,9 @@ static void free_basis(pci_gpu *h)
     h->d_csf_C = nullptr; h->d_csf_start = nullptr; h->d_csf_coff = nullptr;
     h->h_csf_start.clear();
     h->ncsf = 0;
+    dev_free(h->d_lsj_items);
+    h->d_lsj_items = nullptr;
+    h->lsj_nitems = -1;
     h->d_msd = nullptr;
     h->d_barr = nullptr;
     h->nint = 0;

@@ -74,6 +74,9 @@ struct pci_gpu {
     int64_t *d_csf_start = nullptr, *d_csf_coff = nullptr;
     std::vector<int64_t> h_csf_start;
     int64_t ncsf = 0;
+    // LSJ's configuration pairs (pci_gpu_lsj), built once per basis
+    int2 *d_lsj_items = nullptr;
+    int64_t lsj_nitems = -1;
     std::vector<int32_t> h_nh, h_jz;
     std::vector<int32_t> h_jterms;    // Jt(1:Njd): sorted 2J of the terms present
     std::vector<unsigned long long> h_rowwork;   // determinant pairs per row, per configuration
