@@ -72,6 +72,12 @@ module pci_gpu_mod
        import; type(c_ptr), value :: h; real(c_double) :: Y(*), X(*)
        integer(c_int32_t), value :: nv
      end function
+     ! conf_pt PTE (conf_pt.f90:751-952): second-order energies dE(nv), Xpt(Nd, nv) or c_null_ptr
+     integer(c_int) function pci_gpu_pt2(h, nd1, nd0, X0, nv, E, avg_diag, dE, Xpt) bind(C)
+       import; type(c_ptr), value :: h; integer(c_int64_t), value :: nd1, nd0
+       real(c_double) :: X0(*), E(*), dE(*); integer(c_int32_t), value :: nv, avg_diag
+       type(c_ptr), value :: Xpt
+     end function
      ! FormBarr: Barr(nint, Nd) of the basis (barr may be c_null_ptr)
      integer(c_int) function pci_gpu_form_barr(h, nint, barr) bind(C)
        import; type(c_ptr), value :: h; integer(c_int32_t) :: nint

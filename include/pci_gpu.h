@@ -176,6 +176,23 @@ int pci_gpu_csf_counts(pci_gpu_t *h, int32_t *per_conf);
  * determinant vectors. */
 int pci_gpu_csf_to_det(pci_gpu_t *h, const double *Y, int32_t nv, double *X);
 
+/* Replaces: conf_pt's PTE (conf_pt.f90:751-952), second-order CI+PT, for PT
+ * spaces whose Hamiltonian the device holds: the resident determinant H
+ * (pci_gpu_form_h over the CI determinants followed by the PT ones) and the
+ * CI vectors X0 over the first nd0 determinants (nd0 x nv column-major,
+ * host; nd0 <= nd1 <= Nd, both at configuration ends).  For every
+ * determinant i > nd1: x = sum_(k <= nd0) H_ik X0_kn, dE[n] += x^2 /
+ * (E[n] - H_ii), and Xpt (Nd x nv column-major, may be NULL; rows <= nd1
+ * zero) receives c_in = x / (E[n] - H_ii).  E are the levels' energies as
+ * eigenvalues of H; dE is negative for a lowest level (the reference's
+ * Ey(n) is -dE[n] in its binding convention).  avg_diag = 1 applies
+ * average_diag as the reference does (conf_pt.f90:710-724: the mean goes to
+ * each PT configuration's last determinant).  H must be built with Gj = 0
+ * (conf_pt's Hmltn has no J^2 term; its energies E take the Gj shift off,
+ * conf_pt.f90:737). */
+int pci_gpu_pt2(pci_gpu_t *h, int64_t nd1, int64_t nd0, const double *X0, int32_t nv, const double *E,
+                int32_t avg_diag, double *dE, double *Xpt);
+
 /* No counterpart in the reference.  The J_av of pci_gpu_j_av for callers that
  * cannot allocate device memory (a host that owns all device memory through
  * its own pool or a framework's caching allocator, or a path where

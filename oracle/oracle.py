@@ -600,3 +600,29 @@ def csf_basis(sysm, J):
 def csf_hamiltonian(H_dense, C):
     """formh_sym (src/csf.f90:538-964): the CSF-basis H = C^T H C."""
     return C.T @ H_dense @ C
+
+
+def pt2(H_dense, nd1, nd0, X0, E, conf_sizes=None, avg_diag=False):
+    """PTE (src/conf_pt.f90:751-952) densely, in the engine's convention: for
+    every determinant i beyond nd1, x = sum_(k < nd0) H_ik X0_kn, dE_n +=
+    x^2 / (E_n - e_i) and c_in = x / (E_n - e_i), e_i = H_ii; average_diag
+    (conf_pt.f90:710-724) puts each PT configuration's mean on its last
+    determinant (the position the reference writes).  conf_sizes: the
+    determinants of each configuration (needed for avg_diag)."""
+    nd = H_dense.shape[0]
+    X0 = np.asarray(X0, np.float64).reshape(nd0, -1)
+    E = np.asarray(E, np.float64)
+    diag = np.diag(H_dense).copy()
+    if avg_diag:
+        starts = np.concatenate([[0], np.cumsum(conf_sizes)])
+        for a, b in zip(starts[:-1], starts[1:]):
+            if a >= nd1 and b > a:
+                diag[b - 1] = diag[a:b].mean()
+    dE = np.zeros(len(E))
+    C = np.zeros((nd, len(E)))
+    for i in range(nd1, nd):
+        x = H_dense[i, :nd0] @ X0
+        dl = E - diag[i]
+        dE += x * x / dl
+        C[i] = x / dl
+    return dE, C

@@ -33,7 +33,7 @@ NE_MAX = 8
 UNITS = [("hbuild", "hbuild.cu", NOFMA)] + \
     [(f"hbuild_ne{n}", "hbuild_ne.cu", NOFMA + [f"-DPCI_NE={n}"]) for n in range(1, NE_MAX + 1)] + \
     [("spmm", "spmm.cu", []), ("davidson", "davidson.cu", []), ("pci_gpu", "pci_gpu.cu", []),
-     ("noalloc", "noalloc.cu", []), ("pci_io", "pci_io.cpp", []), ("mlp", "mlp.cu", []), ("lsj", "lsj.cu", NOFMA), ("csf", "csf.cu", []),
+     ("noalloc", "noalloc.cu", []), ("pci_io", "pci_io.cpp", []), ("mlp", "mlp.cu", []), ("lsj", "lsj.cu", NOFMA), ("csf", "csf.cu", []), ("pt", "pt.cu", []),
      ("batch", "batch.cu", [])]
 HEADERS = ["pci_internal.h", "hbuild_impl.cuh", "mlp_tc.cuh", os.path.join("..", "..", "include", "pci_gpu.h"),
            os.path.join("..", "..", "include", "pci_io.h"), os.path.join("..", "..", "include", "pci_batch.h")]

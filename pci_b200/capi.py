@@ -22,7 +22,7 @@ PCI_DVD_FP64, PCI_DVD_FP32, PCI_DVD_LEARNED = 0, 1, 2
 EXPORTS = ["pci_gpu_create", "pci_gpu_set_basis", "pci_gpu_set_integrals", "pci_gpu_form_h",
            "pci_gpu_form_j", "pci_gpu_csr_info", "pci_gpu_get_csr", "pci_gpu_set_csr",
            "pci_gpu_davidson", "pci_gpu_j_av", "pci_gpu_j_av_noalloc", "pci_gpu_lsj", "pci_gpu_form_csf", "pci_gpu_csf_counts",
-           "pci_gpu_csf_to_det", "pci_gpu_jterms", "pci_gpu_stats",
+           "pci_gpu_csf_to_det", "pci_gpu_pt2", "pci_gpu_jterms", "pci_gpu_stats",
            "pci_gpu_last_error", "pci_gpu_destroy", "pci_mlp_create", "pci_mlp_num_params", "pci_mlp_set_params",
            "pci_mlp_get_params", "pci_mlp_forward", "pci_mlp_loss_grad", "pci_mlp_train", "pci_mlp_last_error",
            "pci_mlp_destroy", "pci_gpu_set_correction_model", "pci_gpu_davidson_harvest", "pci_mlp_forward_occ",
@@ -86,6 +86,7 @@ def load(path: str = LIB):
     L.pci_gpu_form_csf.argtypes = [P, P, P]
     L.pci_gpu_csf_counts.argtypes = [P, P]
     L.pci_gpu_csf_to_det.argtypes = [P, P, i32, P]
+    L.pci_gpu_pt2.argtypes = [P, i64, i64, P, i32, P, i32, P, P]
     L.pci_gpu_j_av_noalloc.argtypes = [P, P, P, i64, P, i64, i32, i64, P, P, C.c_char_p, i32]
     L.pci_mlp_create.argtypes = [i32, i32, i32, C.POINTER(P)]
     L.pci_mlp_num_params.argtypes = [P]
@@ -329,6 +330,22 @@ class Engine:
         out = np.zeros((nv, self._nd))
         self._check(self.L.pci_gpu_csf_to_det(self.h, _p(yc), nv, _p(out)))
         return out.T
+
+    def pt2(self, nd1, X0, E, avg_diag=False, want_vectors=False):
+        """Second-order CI+PT (conf_pt's PTE) on the resident H: X0 (nd0 x nv)
+        the CI vectors over the first nd0 determinants, E their energies;
+        returns dE (and the first-order coefficients, Nd x nv)."""
+        X0 = np.asarray(X0, np.float64)
+        if X0.ndim == 1:
+            X0 = X0[:, None]
+        nd0, nv = X0.shape
+        xc = np.ascontiguousarray(X0.T)
+        e = np.ascontiguousarray(E, np.float64)
+        de = np.zeros(nv)
+        xpt = np.zeros((nv, self._nd)) if want_vectors else None
+        self._check(self.L.pci_gpu_pt2(self.h, nd1, nd0, _p(xc), nv, _p(e), 1 if avg_diag else 0, _p(de),
+                                       _p(xpt) if xpt is not None else None))
+        return (de, xpt.T) if want_vectors else de
 
     def set_correction_model(self, mlp):
         """Attach a trained Mlp for mode=PCI_DVD_LEARNED (None detaches)."""

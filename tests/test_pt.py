@@ -1,0 +1,91 @@
+"""Second-order CI+PT (conf_pt's PTE, src/conf_pt.f90:751-952).
+
+CPU (oracle restatement): on a two-block matrix [[A, l B], [l B^T, D]] the
+second-order energy reproduces the exact lowest eigenvalue to O(l^4) (the
+third order vanishes when the coupling is off-diagonal), and scales as l^2;
+average_diag changes only each PT configuration's last diagonal element.
+GPU: pci_gpu_pt2 on the resident H of a CI + PT determinant list against the
+oracle, with and without average_diag."""
+import numpy as np
+import pytest
+
+from conftest import get_system, oracle_h
+
+
+def test_pt2_oracle_known_answer():
+    import oracle as O
+    rng = np.random.default_rng(5)
+    nci, npt = 20, 30
+    A = rng.standard_normal((nci, nci)); A = (A + A.T) / 2
+    D = rng.standard_normal((npt, npt)); D = (D + D.T) / 2 + 8 * np.eye(npt)   # PT space above the CI levels
+    B = rng.standard_normal((nci, npt))
+    w, V = np.linalg.eigh(A)
+    errs = []
+    for lam in (1e-2, 5e-3):
+        H = np.block([[A, lam * B], [lam * B.T, np.diag(np.diag(D))]])
+        dE, C = O.pt2(H, nci, nci, V[:, :1], w[:1])
+        exact = np.linalg.eigvalsh(H)[0]
+        errs.append(abs(exact - (w[0] + dE[0])))
+        assert dE[0] < 0
+        assert abs(dE[0] / lam**2 - O.pt2(np.block([[A, B], [B.T, np.diag(np.diag(D))]]), nci, nci,
+                                          V[:, :1], w[:1])[0][0]) < 1e-9
+    assert errs[0] < 1e-6 and errs[1] < errs[0] / 8          # fourth order in the coupling
+
+
+def test_pt2_oracle_average_diag_last_determinant():
+    import oracle as O
+    s = get_system("small3")
+    (rp, col, val, *_), _ = oracle_h("small3")
+    H = O.csr_to_dense(s.nd, rp, col, val)
+    cs = np.concatenate([[0], np.cumsum(s.ndc)])
+    nd1 = int(cs[len(cs) // 2])
+    X0 = np.linalg.eigh(H[:nd1, :nd1])[1][:, :2]
+    E = np.linalg.eigvalsh(H[:nd1, :nd1])[:2]
+    d0, c0 = O.pt2(H, nd1, nd1, X0, E)
+    d1, c1 = O.pt2(H, nd1, nd1, X0, E, s.ndc, avg_diag=True)
+    changed = np.flatnonzero(np.any(c0 != c1, axis=1))
+    last = set((cs[1:] - 1)[cs[1:] > nd1].tolist())
+    assert set(changed.tolist()) <= last
+
+
+def _ci_pt(name, k_ci):
+    import oracle as O
+    s = get_system(name)
+    (rp, col, val, *_), _ = oracle_h(name)
+    H = O.csr_to_dense(s.nd, rp, col, val)
+    cs = np.concatenate([[0], np.cumsum(s.ndc)])
+    nd1 = int(cs[k_ci])
+    w, V = np.linalg.eigh(H[:nd1, :nd1])
+    return s, H, cs, nd1, V[:, :4], w[:4]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,frac", [("cfg1", 0.3), ("small3", 0.5), ("small4", 0.4)])
+@pytest.mark.parametrize("avg", [False, True])
+def test_pt2_gpu_matches_oracle(name, frac, avg):
+    import oracle as O
+    from pci_b200.capi import Engine
+    s0 = get_system(name)
+    s, H, cs, nd1, X0, E = _ci_pt(name, max(1, int(frac * len(s0.ndc))))
+    k0 = max(1, int(np.searchsorted(cs, nd1)) // 2)
+    nd0 = int(cs[k0])                                  # a smaller zero-order space
+    want_de, want_c = O.pt2(H, nd1, nd0, X0[:nd0], E, s.ndc, avg_diag=avg)
+    with Engine(0) as e:
+        e.load_system(s)
+        e.form_h(64)
+        de, c = e.pt2(nd1, X0[:nd0], E, avg_diag=avg, want_vectors=True)
+    assert np.allclose(de, want_de, rtol=1e-10, atol=1e-13)
+    assert np.allclose(c, want_c, rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.gpu
+def test_pt2_gpu_errors():
+    from pci_b200.capi import Engine, PciError
+    s, H, cs, nd1, X0, E = _ci_pt("small3", 10)
+    with Engine(0) as e:
+        e.load_system(s)
+        e.form_h(64)
+        with pytest.raises(PciError):
+            e.pt2(nd1 + 1, X0, E)                      # Nd1 inside a configuration
+        with pytest.raises(PciError):
+            e.pt2(nd1, np.zeros((nd1 + 1, 1)), E[:1])  # Nd0 > Nd1
