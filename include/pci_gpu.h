@@ -160,6 +160,16 @@ int pci_gpu_j_av(pci_gpu_t *h, const double *X, int32_t nv, int64_t nlim, double
  * passed to pci_gpu_set_basis (PCI_E_STATE without them). */
 int pci_gpu_lsj(pci_gpu_t *h, const double *X, int32_t nv, double *xj, double *xl, double *xs);
 
+/* Replaces: the density-matrix pass of pdtm's FormDM (pdtm.f90:1134-1336):
+ * for each vector of X (Nd x nv column-major, host) the one-particle density
+ * matrix over the m-states, from the determinant pairs n >= k whose
+ * relativistic configurations differ by at most one orbital and whose
+ * coefficients satisfy |b_n| > trd and |b_n b_k| > trd (pdtm's Trd, default
+ * 1e-10).  Ro (Nst x Nst x nv, column-major per vector, host) receives
+ * Ro(i, j) for 1-based m-states i, j at Ro[(v*Nst + j-1)*Nst + i-1]; the
+ * reference's Ro is this shifted by Npo (the core m-states). */
+int pci_gpu_density(pci_gpu_t *h, const double *X, int32_t nv, double trd, double *Ro);
+
 /* Replaces: the kCSF = 1 path, jbasis + formh_sym (csf.f90:17-407, 538-1006;
  * pconf.F90:146-148, 211-214).  From the resident FP64 determinant H
  * (pci_gpu_form_h(64)) and J^2 (pci_gpu_form_j): each configuration's CSFs

@@ -78,6 +78,7 @@ def lib():
         L.orc_hint.argtypes = [C.POINTER(OrcSys), C.c_int, C.c_int]
         L.orc_hint.restype = C.c_double
         L.orc_lsj.argtypes = [C.POINTER(OrcSys), P, C.c_int, C.c_int, C.c_int, P]
+        L.orc_density.argtypes = [C.POINTER(OrcSys), P, C.c_double, P]
         _lib = L
     return _lib
 
@@ -206,6 +207,15 @@ class Oracle:
         t = self.lsj_sums(X)
         x = 0.5 * (np.sqrt(t + 1) - 1)
         return x[0], x[1], x[2]
+
+    def density(self, b, trd=1e-10):
+        """FormDM's density matrix (src/pdtm.f90:1254-1310) of vector b:
+        [Nst, Nst] with entry [i, j] = Ro(i+1, j+1)."""
+        b = np.ascontiguousarray(b, np.float64)
+        nst = self.sys.nst
+        ro = np.zeros(nst * nst)
+        lib().orc_density(C.byref(self.s), _ptr(b), float(trd), _ptr(ro))
+        return ro.reshape(nst, nst).T
 
     def form_j(self):
         L = lib()

@@ -833,3 +833,51 @@ void orc_lsj(const orc_sys *s, const double *X, int nv, int ic_lo, int ic_hi, do
     free(start);
     free(nh0);
 }
+
+/* ------------------------------------------------------ density matrix --- */
+
+/* FormDM's density pass, src/pdtm.f90:1254-1310, one vector b (length nd):
+ * ro[(j-1)*nst + i-1] = Ro(i, j) over 1-based m-states (Npo = 0). */
+void orc_density(const orc_sys *s, const double *b, double trd, double *ro)
+{
+    int ne = s->ne, nst = s->nst;
+    int32_t c1[8], c2[8];
+    for (int64_t q = 0; q < (int64_t)nst * nst; q++) ro[q] = 0.0;
+    int64_t n = 0;
+    for (int ic1 = 1; ic1 <= s->nc; ic1++) {
+        int64_t n2 = s->ndc[ic1 - 1];
+        for (int64_t n1 = 1; n1 <= n2; n1++) {
+            n++;
+            double bn = b[n - 1];
+            if (!(fabs(bn) > trd)) continue;
+            const int32_t *d1 = s->iarr + (n - 1) * ne;
+            int64_t k = 0;
+            for (int ic2 = 1; ic2 <= ic1; ic2++) {
+                int64_t kx = s->ndc[ic2 - 1];
+                if (ic1 == ic2) kx = n1;
+                const int32_t *d2 = s->iarr + k * ne;
+                for (int e = 0; e < ne; e++) { c1[e] = s->nh[d1[e] - 1]; c2[e] = s->nh[d2[e] - 1]; }
+                if (orc_compd(c1, c2, ne) > 1) { k += kx; continue; }
+                for (int64_t k1 = 1; k1 <= kx; k1++) {
+                    k++;
+                    double bk = b[k - 1];
+                    if (!(fabs(bn * bk) > trd)) continue;
+                    int is, nf, ii[3], jj[3];
+                    orc_rspq(d1, s->iarr + (k - 1) * ne, ne, &is, &nf, ii, jj);
+                    if (nf == 0) {
+                        int nn = n == k ? 1 : 2;
+                        for (int iq = 0; iq < ne; iq++) {
+                            int i1 = d1[iq];
+                            ro[(int64_t)(i1 - 1) * nst + i1 - 1] += bn * bk * is * nn;
+                        }
+                    }
+                    if (nf == 1) {
+                        int j1 = ii[1], j2 = jj[1];
+                        ro[(int64_t)(j2 - 1) * nst + j1 - 1] += bn * bk * is;
+                        ro[(int64_t)(j1 - 1) * nst + j2 - 1] = ro[(int64_t)(j2 - 1) * nst + j1 - 1];
+                    }
+                }
+            }
+        }
+    }
+}

@@ -21,7 +21,7 @@ PCI_DVD_FP64, PCI_DVD_FP32, PCI_DVD_LEARNED = 0, 1, 2
 
 EXPORTS = ["pci_gpu_create", "pci_gpu_set_basis", "pci_gpu_set_integrals", "pci_gpu_form_h",
            "pci_gpu_form_j", "pci_gpu_csr_info", "pci_gpu_get_csr", "pci_gpu_set_csr",
-           "pci_gpu_davidson", "pci_gpu_j_av", "pci_gpu_j_av_noalloc", "pci_gpu_lsj", "pci_gpu_form_csf", "pci_gpu_csf_counts",
+           "pci_gpu_davidson", "pci_gpu_j_av", "pci_gpu_j_av_noalloc", "pci_gpu_lsj", "pci_gpu_density", "pci_gpu_form_csf", "pci_gpu_csf_counts",
            "pci_gpu_csf_to_det", "pci_gpu_pt2", "pci_gpu_jterms", "pci_gpu_stats",
            "pci_gpu_last_error", "pci_gpu_destroy", "pci_mlp_create", "pci_mlp_num_params", "pci_mlp_set_params",
            "pci_mlp_get_params", "pci_mlp_forward", "pci_mlp_loss_grad", "pci_mlp_train", "pci_mlp_last_error",
@@ -83,6 +83,7 @@ def load(path: str = LIB):
     L.pci_gpu_davidson.argtypes = [P, C.POINTER(DvdParams), P, P, P, P, P, C.POINTER(i32), P]
     L.pci_gpu_j_av.argtypes = [P, P, i32, i64, P]
     L.pci_gpu_lsj.argtypes = [P, P, i32, P, P, P]
+    L.pci_gpu_density.argtypes = [P, P, i32, f64, P]
     L.pci_gpu_form_csf.argtypes = [P, P, P]
     L.pci_gpu_csf_counts.argtypes = [P, P]
     L.pci_gpu_csf_to_det.argtypes = [P, P, i32, P]
@@ -185,6 +186,7 @@ class Engine:
                                       _p(k["ll"]), _p(k["jj"]), sysm.nc, _p(k["ndc"]), float(sysm.gj))
         self._check(rc)
         self._nd = int(sysm.nd)
+        self._nst = int(sysm.nst)
 
     def set_integrals(self, sysm):
         hl = np.ascontiguousarray(sysm.hint_lut, np.float64)
@@ -305,6 +307,19 @@ class Engine:
         xj, xl, xs = np.zeros(nv), np.zeros(nv), np.zeros(nv)
         self._check(self.L.pci_gpu_lsj(self.h, _p(xc), nv, _p(xj), _p(xl), _p(xs)))
         return xj, xl, xs
+
+    def density(self, X, trd=1e-10):
+        """FormDM's one-particle density matrix of each column of X: [nv, Nst, Nst]
+        with entry [v, i, j] = Ro(i+1, j+1)."""
+        X = np.asarray(X, np.float64)
+        if X.ndim == 1:
+            X = X[:, None]
+        nd, nv = X.shape
+        xc = np.ascontiguousarray(X.T)
+        nst = self._nst
+        ro = np.zeros((nv, nst, nst))
+        self._check(self.L.pci_gpu_density(self.h, _p(xc), nv, float(trd), _p(ro)))
+        return np.transpose(ro, (0, 2, 1))             # column-major per vector -> [v, i, j]
 
     def form_csf(self):
         """jbasis + formh_sym on the device: the CSF Hamiltonian replaces the

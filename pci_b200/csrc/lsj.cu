@@ -1,3 +1,5 @@
+// LSJ and one-particle density matrices of CI vectors.
+//
 // LSJ: per-level <J^2>, <L^2>, <S^2> of CI vectors in the determinant basis,
 // as pconf's lsj / calcLSJ / lsj_det compute them (src/pconf.F90:2672-2962)
 // for kLSJ = 1, returned as J, L, S (x = (sqrt(<X^2> + 1) - 1) / 2).
@@ -280,6 +282,77 @@ __global__ void __launch_bounds__(128) k_lsj(const uint16_t *__restrict__ occ, c
     }
 }
 
+// FormDM (src/pdtm.f90:1134-1336): the one-particle density matrix of each
+// level over the determinant pairs n >= k whose relativistic configurations
+// differ by at most one orbital, both coefficients and their product above
+// trd.  One warp per FormH adjacency entry (c1, c2 <= c1, skipped unless
+// CompD <= 1); ro[(v * nst + j) * nst + i] = Ro(i, j) (0-based m-states,
+// column-major per level).  The reference adds b_n b_k is to Ro(a, b) and
+// then sets Ro(b, a) = Ro(a, b), which leaves the running total in both:
+// adding the term to both entries gives the same matrix.
+template <int NE>
+__global__ void __launch_bounds__(128) k_dm(const uint16_t *__restrict__ occ, const int64_t *__restrict__ conf_start,
+                                            const uint16_t *__restrict__ conf_orb, const int64_t *__restrict__ adj_ptr,
+                                            const int32_t *__restrict__ adj, int nc, const double *__restrict__ X,
+                                            int64_t nd, int nv, int nst, double trd, double *ro)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t nitems = adj_ptr[nc];
+    for (int64_t w = warp; w < nitems; w += nwarps) {
+        // row configuration of adjacency entry w (adj_ptr is ascending)
+        int lo = 0, hi = nc - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (adj_ptr[mid] <= w) lo = mid; else hi = mid - 1;
+        }
+        const int c1 = lo, c2 = adj[w];
+        uint16_t o1[NE], o2[NE];
+#pragma unroll
+        for (int e = 0; e < NE; e++) { o1[e] = conf_orb[(int64_t)c1 * NE + e]; o2[e] = conf_orb[(int64_t)c2 * NE + e]; }
+        int i = 0, j = 0, ni = 0, nj = 0;
+        while (i < NE && j < NE) {
+            if (o1[i] == o2[j]) { i++; j++; }
+            else if (o1[i] > o2[j]) { nj++; j++; }
+            else { ni++; i++; }
+        }
+        if (max(ni + NE - i, nj + NE - j) > 1) continue;   // CompC > 1
+        const int64_t n0 = conf_start[c1], nr = conf_start[c1 + 1] - n0;
+        const int64_t k0 = conf_start[c2], nk = conf_start[c2 + 1] - k0;
+        for (int64_t p = lane; p < nr * nk; p += 32) {
+            const int64_t a = p / nk, b = p - a * nk;
+            const int64_t n = n0 + a, k = k0 + b;
+            if (k > n) continue;
+            uint16_t d1[NE], d2[NE];
+#pragma unroll
+            for (int e = 0; e < NE; e++) { d1[e] = occ[n * NE + e]; d2[e] = occ[k * NE + e]; }
+            const LDiff<NE> df = l_diff<NE>(d1, d2);
+            if (df.nf > 1) continue;
+            for (int v = 0; v < nv; v++) {
+                const double bn = X[(int64_t)v * nd + n], bk = X[(int64_t)v * nd + k];
+                if (!(fabs(bn) > trd) || !(fabs(bn * bk) > trd)) continue;
+                double *r = ro + (int64_t)v * nst * nst;
+                if (df.nf == 0) {
+#pragma unroll
+                    for (int e = 0; e < NE; e++) atomicAdd(&r[(int64_t)d1[e] * nst + d1[e]], bn * bk);
+                } else {
+                    const double t = bn * bk * df.is;
+                    atomicAdd(&r[(int64_t)df.j2 * nst + df.i2], t);
+                    atomicAdd(&r[(int64_t)df.i2 * nst + df.j2], t);
+                }
+            }
+        }
+    }
+}
+
+template <int NE>
+void launch_dm(int blocks, cudaStream_t st, const DevSys &S, const int64_t *adj_ptr, const int32_t *adj,
+               const double *X, int nv, double trd, double *ro)
+{
+    k_dm<NE><<<blocks, 128, 0, st>>>(S.occ, S.conf_start, S.conf_orb, adj_ptr, adj, S.nc, X, S.nd, nv, S.nst, trd, ro);
+}
+
 template <int NE>
 void launch_lsj(int blocks, cudaStream_t st, const DevSys &S, const int8_t *orb_n, const int2 *items, int64_t nitems,
                 const double *X, int nv, int v0, double *out)
@@ -385,6 +458,45 @@ int pci_gpu_lsj(pci_gpu_t *h, const double *X, int32_t nv, double *xj, double *x
         xl[v] = 0.5 * (sqrt(sums[nv + v] + 1) - 1);
         xs[v] = 0.5 * (sqrt(sums[2 * nv + v] + 1) - 1);
     }
+    return PCI_OK;
+}
+
+int pci_gpu_density(pci_gpu_t *h, const double *X, int32_t nv, double trd, double *Ro)
+{
+    if (!h) return PCI_E_INPUT;
+    cudaSetDevice(h->device);
+    if (!X || !Ro) return set_err(h, PCI_E_INPUT, "null array");
+    if (!h->have_basis) return set_err(h, PCI_E_STATE, "density before set_basis");
+    if (nv < 1 || nv > 64) return set_err(h, PCI_E_INPUT, "density: nv must be 1..64");
+    int rc = 0;
+    if (!h->d_adj && (rc = hb_build_adjacency(h))) return rc;   // FormH's configuration adjacency
+    const int64_t nd = h->nd, nst = h->nst;
+    LsjBuf d_x, d_ro;
+    d_x.p = dev_alloc(h, (size_t)nd * nv * 8, &rc);
+    if (rc) return rc;
+    d_ro.p = dev_alloc(h, (size_t)nst * nst * nv * 8, &rc);
+    if (rc) return rc;
+    PCI_CUDA(h, cudaMemcpyAsync(d_x.p, X, (size_t)nd * nv * 8, cudaMemcpyHostToDevice, h->st));
+    PCI_CUDA(h, cudaMemsetAsync(d_ro.p, 0, (size_t)nst * nst * nv * 8, h->st));
+    const DevSys S = make_devsys(h);
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+    const int blocks = nsm * 8;
+    const double *x = (const double *)d_x.p;
+    double *r = (double *)d_ro.p;
+    switch (h->ne) {
+    case 1: launch_dm<1>(blocks, h->st, S, h->d_adj_ptr, h->d_adj, x, nv, trd, r); break;
+    case 2: launch_dm<2>(blocks, h->st, S, h->d_adj_ptr, h->d_adj, x, nv, trd, r); break;
+    case 3: launch_dm<3>(blocks, h->st, S, h->d_adj_ptr, h->d_adj, x, nv, trd, r); break;
+    case 4: launch_dm<4>(blocks, h->st, S, h->d_adj_ptr, h->d_adj, x, nv, trd, r); break;
+    case 5: launch_dm<5>(blocks, h->st, S, h->d_adj_ptr, h->d_adj, x, nv, trd, r); break;
+    case 6: launch_dm<6>(blocks, h->st, S, h->d_adj_ptr, h->d_adj, x, nv, trd, r); break;
+    case 7: launch_dm<7>(blocks, h->st, S, h->d_adj_ptr, h->d_adj, x, nv, trd, r); break;
+    default: launch_dm<8>(blocks, h->st, S, h->d_adj_ptr, h->d_adj, x, nv, trd, r); break;
+    }
+    PCI_CUDA(h, cudaGetLastError());
+    PCI_CUDA(h, cudaMemcpyAsync(Ro, d_ro.p, (size_t)nst * nst * nv * 8, cudaMemcpyDeviceToHost, h->st));
+    PCI_CUDA(h, cudaStreamSynchronize(h->st));
     return PCI_OK;
 }
 
