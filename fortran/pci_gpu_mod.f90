@@ -78,6 +78,11 @@ module pci_gpu_mod
        real(c_double) :: X0(*), E(*), dE(*); integer(c_int32_t), value :: nv, avg_diag
        type(c_ptr), value :: Xpt
      end function
+     ! pdtm FormDM density pass: Ro(Nst, Nst, nv) of X(Nd, nv)
+     integer(c_int) function pci_gpu_density(h, X, nv, trd, Ro) bind(C)
+       import; type(c_ptr), value :: h; real(c_double) :: X(*), Ro(*)
+       integer(c_int32_t), value :: nv; real(c_double), value :: trd
+     end function
      ! FormBarr: Barr(nint, Nd) of the basis (barr may be c_null_ptr)
      integer(c_int) function pci_gpu_form_barr(h, nint, barr) bind(C)
        import; type(c_ptr), value :: h; integer(c_int32_t) :: nint
