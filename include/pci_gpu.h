@@ -170,6 +170,17 @@ int pci_gpu_lsj(pci_gpu_t *h, const double *X, int32_t nv, double *xj, double *x
  * reference's Ro is this shifted by Npo (the core m-states). */
 int pci_gpu_density(pci_gpu_t *h, const double *X, int32_t nv, double trd, double *Ro);
 
+/* Replaces: the transition-density pass of pdtm's FormTM (pdtm.f90:
+ * 1538-1605) for one initial level (vector bi over the basis of handle hi)
+ * and one final level (bf over the basis of hf; the two bases share Ne and
+ * the m-states, e.g. opposite parities): the determinant pairs whose
+ * relativistic configurations differ by at most one orbital, |b_n| > trd
+ * and |b_n b_k| > trd.  Ro (Nst x Nst column-major, host) receives Ro(i, j)
+ * with i the initial determinant's m-state and j the final's (1-based, at
+ * Ro[(j-1)*Nst + i-1]). */
+int pci_gpu_transition_density(pci_gpu_t *hi, pci_gpu_t *hf, const double *bi, const double *bf, double trd,
+                               double *Ro);
+
 /* Replaces: the kCSF = 1 path, jbasis + formh_sym (csf.f90:17-407, 538-1006;
  * pconf.F90:146-148, 211-214).  From the resident FP64 determinant H
  * (pci_gpu_form_h(64)) and J^2 (pci_gpu_form_j): each configuration's CSFs

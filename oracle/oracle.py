@@ -79,6 +79,7 @@ def lib():
         L.orc_hint.restype = C.c_double
         L.orc_lsj.argtypes = [C.POINTER(OrcSys), P, C.c_int, C.c_int, C.c_int, P]
         L.orc_density.argtypes = [C.POINTER(OrcSys), P, C.c_double, P]
+        L.orc_transition_density.argtypes = [C.POINTER(OrcSys), C.POINTER(OrcSys), P, P, C.c_double, P]
         _lib = L
     return _lib
 
@@ -215,6 +216,17 @@ class Oracle:
         nst = self.sys.nst
         ro = np.zeros(nst * nst)
         lib().orc_density(C.byref(self.s), _ptr(b), float(trd), _ptr(ro))
+        return ro.reshape(nst, nst).T
+
+    def transition_density(self, initial, b_initial, b_final, trd=1e-10):
+        """FormTM's transition density (src/pdtm.f90:1538-1605) from a level of
+        `initial` (another Oracle) to a level of this system: [Nst, Nst] with
+        entry [i, j] = Ro(i+1, j+1), i the initial m-state."""
+        bi = np.ascontiguousarray(b_initial, np.float64)
+        bf = np.ascontiguousarray(b_final, np.float64)
+        nst = self.sys.nst
+        ro = np.zeros(nst * nst)
+        lib().orc_transition_density(C.byref(initial.s), C.byref(self.s), _ptr(bi), _ptr(bf), float(trd), _ptr(ro))
         return ro.reshape(nst, nst).T
 
     def form_j(self):

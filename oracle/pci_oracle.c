@@ -881,3 +881,43 @@ void orc_density(const orc_sys *s, const double *b, double trd, double *ro)
         }
     }
 }
+
+/* FormTM's transition density, src/pdtm.f90:1538-1605: final-state vector
+ * bf over system f, initial-state bi over system si (same m-states);
+ * ro[(j-1)*nst + i-1] = Ro(i, j), i the initial determinant's m-state. */
+void orc_transition_density(const orc_sys *si, const orc_sys *f, const double *bi, const double *bf, double trd,
+                            double *ro)
+{
+    int ne = f->ne, nst = f->nst;
+    int32_t c1[8], c2[8];
+    for (int64_t q = 0; q < (int64_t)nst * nst; q++) ro[q] = 0.0;
+    for (int64_t n = 1; n <= f->nd; n++) {                 /* final state */
+        double bn = bf[n - 1];
+        if (!(fabs(bn) > trd)) continue;
+        const int32_t *d2 = f->iarr + (n - 1) * ne;
+        int64_t k = 0;
+        for (int ic = 1; ic <= si->nc; ic++) {
+            int64_t kx = si->ndc[ic - 1];
+            const int32_t *d1 = si->iarr + k * ne;
+            for (int e = 0; e < ne; e++) { c1[e] = f->nh[d2[e] - 1]; c2[e] = si->nh[d1[e] - 1]; }
+            if (orc_compd(c1, c2, ne) > 1) { k += kx; continue; }
+            for (int64_t k1 = 1; k1 <= kx; k1++) {
+                k++;                                        /* initial state */
+                double bk = bi[k - 1];
+                if (!(fabs(bk * bn) > trd)) continue;
+                const int32_t *dk = si->iarr + (k - 1) * ne;
+                int is, nf, ii[3], jj[3];
+                orc_rspq(d2, dk, ne, &is, &nf, ii, jj);
+                if (nf == 0)
+                    for (int iq = 0; iq < ne; iq++) {
+                        int i1 = dk[iq];
+                        ro[(int64_t)(i1 - 1) * nst + i1 - 1] += bn * bk * is;
+                    }
+                if (nf == 1) {
+                    int j1 = jj[1], j2 = ii[1];                 /* initial, final */
+                    ro[(int64_t)(j2 - 1) * nst + j1 - 1] += bn * bk * is;
+                }
+            }
+        }
+    }
+}

@@ -21,7 +21,7 @@ PCI_DVD_FP64, PCI_DVD_FP32, PCI_DVD_LEARNED = 0, 1, 2
 
 EXPORTS = ["pci_gpu_create", "pci_gpu_set_basis", "pci_gpu_set_integrals", "pci_gpu_form_h",
            "pci_gpu_form_j", "pci_gpu_csr_info", "pci_gpu_get_csr", "pci_gpu_set_csr",
-           "pci_gpu_davidson", "pci_gpu_j_av", "pci_gpu_j_av_noalloc", "pci_gpu_lsj", "pci_gpu_density", "pci_gpu_form_csf", "pci_gpu_csf_counts",
+           "pci_gpu_davidson", "pci_gpu_j_av", "pci_gpu_j_av_noalloc", "pci_gpu_lsj", "pci_gpu_density", "pci_gpu_transition_density", "pci_gpu_form_csf", "pci_gpu_csf_counts",
            "pci_gpu_csf_to_det", "pci_gpu_pt2", "pci_gpu_jterms", "pci_gpu_stats",
            "pci_gpu_last_error", "pci_gpu_destroy", "pci_mlp_create", "pci_mlp_num_params", "pci_mlp_set_params",
            "pci_mlp_get_params", "pci_mlp_forward", "pci_mlp_loss_grad", "pci_mlp_train", "pci_mlp_last_error",
@@ -84,6 +84,7 @@ def load(path: str = LIB):
     L.pci_gpu_j_av.argtypes = [P, P, i32, i64, P]
     L.pci_gpu_lsj.argtypes = [P, P, i32, P, P, P]
     L.pci_gpu_density.argtypes = [P, P, i32, f64, P]
+    L.pci_gpu_transition_density.argtypes = [P, P, P, P, f64, P]
     L.pci_gpu_form_csf.argtypes = [P, P, P]
     L.pci_gpu_csf_counts.argtypes = [P, P]
     L.pci_gpu_csf_to_det.argtypes = [P, P, i32, P]
@@ -320,6 +321,16 @@ class Engine:
         ro = np.zeros((nv, nst, nst))
         self._check(self.L.pci_gpu_density(self.h, _p(xc), nv, float(trd), _p(ro)))
         return np.transpose(ro, (0, 2, 1))             # column-major per vector -> [v, i, j]
+
+    def transition_density(self, initial, b_initial, b_final, trd=1e-10):
+        """FormTM's transition density from a level of `initial` (another
+        Engine holding the initial basis) to a level of this engine's basis:
+        [Nst, Nst] with entry [i, j] = Ro(i+1, j+1), i the initial m-state."""
+        bi = np.ascontiguousarray(b_initial, np.float64)
+        bf = np.ascontiguousarray(b_final, np.float64)
+        ro = np.zeros(self._nst * self._nst)
+        self._check(self.L.pci_gpu_transition_density(initial.h, self.h, _p(bi), _p(bf), float(trd), _p(ro)))
+        return ro.reshape(self._nst, self._nst).T
 
     def form_csf(self):
         """jbasis + formh_sym on the device: the CSF Hamiltonian replaces the

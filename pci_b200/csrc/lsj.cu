@@ -346,6 +346,79 @@ __global__ void __launch_bounds__(128) k_dm(const uint16_t *__restrict__ occ, co
     }
 }
 
+// FormTM's transition density (src/pdtm.f90:1538-1605): final-state
+// determinants n (basis F) against initial-state determinants k (basis I)
+// whose relativistic configurations differ by at most one orbital,
+// |b_n| > trd and |b_n b_k| > trd; Rspq takes the final determinant first.
+// Equal determinants add b_n b_k to Ro(i, i) for each occupied m-state, one
+// differing m-state adds b_n b_k is to Ro(initial's, final's).  One warp per
+// final configuration finds the initial configurations within one orbital
+// (32 at a time, a ballot of the lanes' CompD), then its lanes take the
+// determinant pairs of each.
+template <int NE>
+__global__ void __launch_bounds__(128) k_tdm(const uint16_t *__restrict__ occ_f, const int64_t *__restrict__ cs_f,
+                                             const uint16_t *__restrict__ orb_f, int nc_f,
+                                             const uint16_t *__restrict__ occ_i, const int64_t *__restrict__ cs_i,
+                                             const uint16_t *__restrict__ orb_i, int nc_i,
+                                             const double *__restrict__ bf, const double *__restrict__ bi, int nst,
+                                             double trd, double *ro)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t cf = warp; cf < nc_f; cf += nwarps) {
+        uint16_t of[NE];
+#pragma unroll
+        for (int e = 0; e < NE; e++) of[e] = orb_f[cf * NE + e];
+        const int64_t n0 = cs_f[cf], nr = cs_f[cf + 1] - n0;
+        for (int c0 = 0; c0 < nc_i; c0 += 32) {
+            const int ci = c0 + lane;
+            bool near = false;
+            if (ci < nc_i) {
+                int i = 0, j = 0, ni = 0, nj = 0;
+                while (i < NE && j < NE) {
+                    const uint16_t a = of[i], b = orb_i[(int64_t)ci * NE + j];
+                    if (a == b) { i++; j++; }
+                    else if (a > b) { nj++; j++; }
+                    else { ni++; i++; }
+                }
+                near = max(ni + NE - i, nj + NE - j) <= 1;
+            }
+            unsigned m = __ballot_sync(0xffffffffu, near);
+            while (m) {
+                const int c = c0 + __ffs(m) - 1;
+                m &= m - 1;
+                const int64_t k0 = cs_i[c], nk = cs_i[c + 1] - k0;
+                for (int64_t p = lane; p < nr * nk; p += 32) {
+                    const int64_t a = p / nk, b = p - a * nk;
+                    const int64_t n = n0 + a, k = k0 + b;
+                    const double bn = bf[n], bk = bi[k];
+                    if (!(fabs(bn) > trd) || !(fabs(bk * bn) > trd)) continue;
+                    uint16_t d2[NE], d1[NE];
+#pragma unroll
+                    for (int e = 0; e < NE; e++) { d2[e] = occ_f[n * NE + e]; d1[e] = occ_i[k * NE + e]; }
+                    const LDiff<NE> df = l_diff<NE>(d2, d1);
+                    if (df.nf == 0) {
+#pragma unroll
+                        for (int e = 0; e < NE; e++) atomicAdd(&ro[(int64_t)d1[e] * nst + d1[e]], bn * bk * df.is);
+                    } else if (df.nf == 1) {
+                        // Ro(j1, j2): j1 the initial determinant's m-state, j2 the final's
+                        atomicAdd(&ro[(int64_t)df.i2 * nst + df.j2], bn * bk * df.is);
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <int NE>
+void launch_tdm(int blocks, cudaStream_t st, const pci_gpu *f, const pci_gpu *i, const double *bf, const double *bi,
+                double trd, double *ro)
+{
+    k_tdm<NE><<<blocks, 128, 0, st>>>(f->d_occ, f->d_conf_start, f->d_conf_orb, f->nc, i->d_occ, i->d_conf_start,
+                                      i->d_conf_orb, i->nc, bf, bi, f->nst, trd, ro);
+}
+
 template <int NE>
 void launch_dm(int blocks, cudaStream_t st, const DevSys &S, const int64_t *adj_ptr, const int32_t *adj,
                const double *X, int nv, double trd, double *ro)
@@ -458,6 +531,51 @@ int pci_gpu_lsj(pci_gpu_t *h, const double *X, int32_t nv, double *xj, double *x
         xl[v] = 0.5 * (sqrt(sums[nv + v] + 1) - 1);
         xs[v] = 0.5 * (sqrt(sums[2 * nv + v] + 1) - 1);
     }
+    return PCI_OK;
+}
+
+int pci_gpu_transition_density(pci_gpu_t *hi, pci_gpu_t *hf, const double *bi, const double *bf, double trd,
+                               double *Ro)
+{
+    if (!hi || !hf) return PCI_E_INPUT;
+    cudaSetDevice(hf->device);
+    if (!bi || !bf || !Ro) return set_err(hf, PCI_E_INPUT, "null array");
+    if (!hi->have_basis || !hf->have_basis) return set_err(hf, PCI_E_STATE, "transition density before set_basis");
+    if (hi->device != hf->device) return set_err(hf, PCI_E_INPUT, "the two bases are on different devices");
+    if (hi->ne != hf->ne || hi->nst != hf->nst || hi->h_nh != hf->h_nh || hi->h_jz != hf->h_jz)
+        return set_err(hf, PCI_E_INPUT, "the two bases must share Ne and the m-states");
+    int rc = 0;
+    const int64_t nst = hf->nst;
+    LsjBuf d_bi, d_bf, d_ro;
+    d_bi.p = dev_alloc(hf, (size_t)hi->nd * 8, &rc);
+    if (rc) return rc;
+    d_bf.p = dev_alloc(hf, (size_t)hf->nd * 8, &rc);
+    if (rc) return rc;
+    d_ro.p = dev_alloc(hf, (size_t)nst * nst * 8, &rc);
+    if (rc) return rc;
+    cudaStream_t st = hf->st;
+    PCI_CUDA(hf, cudaStreamSynchronize(hi->st));
+    PCI_CUDA(hf, cudaMemcpyAsync(d_bi.p, bi, (size_t)hi->nd * 8, cudaMemcpyHostToDevice, st));
+    PCI_CUDA(hf, cudaMemcpyAsync(d_bf.p, bf, (size_t)hf->nd * 8, cudaMemcpyHostToDevice, st));
+    PCI_CUDA(hf, cudaMemsetAsync(d_ro.p, 0, (size_t)nst * nst * 8, st));
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, hf->device);
+    const int blocks = nsm * 8;
+    const double *xb = (const double *)d_bf.p, *xa = (const double *)d_bi.p;
+    double *r = (double *)d_ro.p;
+    switch (hf->ne) {
+    case 1: launch_tdm<1>(blocks, st, hf, hi, xb, xa, trd, r); break;
+    case 2: launch_tdm<2>(blocks, st, hf, hi, xb, xa, trd, r); break;
+    case 3: launch_tdm<3>(blocks, st, hf, hi, xb, xa, trd, r); break;
+    case 4: launch_tdm<4>(blocks, st, hf, hi, xb, xa, trd, r); break;
+    case 5: launch_tdm<5>(blocks, st, hf, hi, xb, xa, trd, r); break;
+    case 6: launch_tdm<6>(blocks, st, hf, hi, xb, xa, trd, r); break;
+    case 7: launch_tdm<7>(blocks, st, hf, hi, xb, xa, trd, r); break;
+    default: launch_tdm<8>(blocks, st, hf, hi, xb, xa, trd, r); break;
+    }
+    PCI_CUDA(hf, cudaGetLastError());
+    PCI_CUDA(hf, cudaMemcpyAsync(Ro, d_ro.p, (size_t)nst * nst * 8, cudaMemcpyDeviceToHost, st));
+    PCI_CUDA(hf, cudaStreamSynchronize(st));
     return PCI_OK;
 }
 

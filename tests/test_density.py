@@ -61,3 +61,42 @@ def test_density_gpu_matches_oracle(name):
     for v in range(3):
         want = o.density(X[:, v])
         assert np.allclose(ro[v], want, rtol=1e-11, atol=1e-13)
+
+
+def _flipped(name):
+    from pci_b200 import system as S
+    kw = dict(S.CONFIGS[name]())
+    kw["parity"] = 1 - kw["parity"]
+    return S.make_system(**kw)
+
+
+def test_transition_density_oracle_same_level_is_density():
+    """FormTM from a level to itself in the same basis equals FormDM."""
+    import oracle as O
+    s, X = _vectors("small3")
+    o = O.Oracle(s)
+    for v in range(2):
+        tm = o.transition_density(o, X[:, v], X[:, v], trd=0.0)
+        assert np.allclose(tm, o.density(X[:, v], trd=0.0), atol=1e-13)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["small3", "cfg1", "small4"])
+def test_transition_density_gpu_matches_oracle(name):
+    """Initial levels over one parity's basis, final levels over the other's."""
+    import oracle as O
+    from pci_b200.capi import Engine
+    si, sf = get_system(name), _flipped(name)
+    rng = np.random.default_rng(8)
+    bi = rng.standard_normal(si.nd); bi /= np.linalg.norm(bi)
+    bf = rng.standard_normal(sf.nd); bf /= np.linalg.norm(bf)
+    want = O.Oracle(sf).transition_density(O.Oracle(si), bi, bf)
+    with Engine(0) as ei, Engine(0) as ef:
+        ei.load_system(si)
+        ef.load_system(sf)
+        got = ef.transition_density(ei, bi, bf)
+        same = ei.transition_density(ei, bi, bi, trd=0.0)
+        dm = ei.density(bi, trd=0.0)[0]
+    assert np.abs(want).max() > 0
+    assert np.allclose(got, want, rtol=1e-11, atol=1e-13)
+    assert np.allclose(same, dm, atol=1e-12)
