@@ -83,6 +83,11 @@ module pci_gpu_mod
        import; type(c_ptr), value :: h; real(c_double) :: X(*), Ro(*)
        integer(c_int32_t), value :: nv; real(c_double), value :: trd
      end function
+     ! pdtm FormTM transition density: initial level B1 (handle hi), final level B2 (handle hf)
+     integer(c_int) function pci_gpu_transition_density(hi, hf, B1, B2, trd, Ro) bind(C)
+       import; type(c_ptr), value :: hi, hf; real(c_double) :: B1(*), B2(*), Ro(*)
+       real(c_double), value :: trd
+     end function
      ! FormBarr: Barr(nint, Nd) of the basis (barr may be c_null_ptr)
      integer(c_int) function pci_gpu_form_barr(h, nint, barr) bind(C)
        import; type(c_ptr), value :: h; integer(c_int32_t) :: nint
