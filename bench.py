@@ -316,6 +316,11 @@ def run_ours(args):
     }
     if not args.no_lsj:
         line["lsj"] = lsj_section(args, eng, sysm)
+        for key, fn in (("density", density_section), ("pt2", pt2_section)):
+            try:
+                line[key] = fn(args, eng, sysm)
+            except Exception as exc:   # an optional section must not cost the bench line
+                line[key] = {"error": str(exc)[:300]}
 
     if args.davidson_iters > 0:
         eng.form_j()
@@ -417,6 +422,38 @@ def lsj_section(args, eng, sysm):
                                "sample": f"oracle calcLSJ over configurations 1..{k} of {sysm.nc} "
                                          f"({tc:.1f} s), scaled by determinants x later configurations"}
     return out
+
+
+def density_section(args, eng, sysm):
+    """pdtm's FormDM density pass (pci_gpu_density) for 10 normalised random
+    vectors of the configuration, through the host call."""
+    rng = np.random.default_rng(23)
+    X = rng.standard_normal((sysm.nd, 10))
+    X /= np.linalg.norm(X, axis=0)
+    t0 = time.perf_counter()
+    ro = eng.density(X)
+    t = time.perf_counter() - t0
+    tr = np.trace(ro, axis1=1, axis2=2)
+    return {"workload": f"{args.config}: one-particle density matrices of 10 vectors (Nd={sysm.nd}, "
+                        f"Nst={sysm.nst})", "gpu_ms": 1e3 * t,
+            "trace_range": [float(tr.min()), float(tr.max())], "ne": int(sysm.ne)}
+
+
+def pt2_section(args, eng, sysm):
+    """conf_pt's second-order step (pci_gpu_pt2) with the first tenth of the
+    determinants (whole configurations) as the CI space and 10 normalised
+    random CI vectors; the rest of the list is the PT space."""
+    cs = np.concatenate([[0], np.cumsum(sysm.ndc)])
+    nd1 = int(cs[np.searchsorted(cs, sysm.nd // 10)])
+    rng = np.random.default_rng(29)
+    X0 = rng.standard_normal((nd1, 10))
+    X0 /= np.linalg.norm(X0, axis=0)
+    E = np.full(10, -50.0)                               # below every diagonal element
+    t0 = time.perf_counter()
+    de = eng.pt2(nd1, X0, E)
+    t = time.perf_counter() - t0
+    return {"workload": f"{args.config}: CI space {nd1} determinants, PT space {sysm.nd - nd1}, 10 vectors",
+            "gpu_ms": 1e3 * t, "dE_range": [float(de.min()), float(de.max())]}
 
 
 def csf_section(args, local, e, sysm):
