@@ -321,6 +321,8 @@ def run_ours(args):
                 line[key] = fn(args, eng, sysm)
             except Exception as exc:   # an optional section must not cost the bench line
                 line[key] = {"error": str(exc)[:300]}
+        if "pt_block" in line.get("pt2", {}):
+            line["pt2"]["pt_block"]["numh_whole"] = int(numh)
 
     if args.davidson_iters > 0:
         eng.form_j()
@@ -442,7 +444,10 @@ def density_section(args, eng, sysm):
 def pt2_section(args, eng, sysm):
     """conf_pt's second-order step (pci_gpu_pt2) with the first tenth of the
     determinants (whole configurations) as the CI space and 10 normalised
-    random CI vectors; the rest of the list is the PT space."""
+    random CI vectors; the rest of the list is the PT space.  First on the
+    resident whole H, then on the PT block alone (pci_gpu_form_h_pt: PT rows
+    against the CI columns, conf_pt's own FormH), after which the whole FP64
+    H is formed again for the sections that follow."""
     cs = np.concatenate([[0], np.cumsum(sysm.ndc)])
     nd1 = int(cs[np.searchsorted(cs, sysm.nd // 10)])
     rng = np.random.default_rng(29)
@@ -452,8 +457,20 @@ def pt2_section(args, eng, sysm):
     t0 = time.perf_counter()
     de = eng.pt2(nd1, X0, E)
     t = time.perf_counter() - t0
-    return {"workload": f"{args.config}: CI space {nd1} determinants, PT space {sysm.nd - nd1}, 10 vectors",
-            "gpu_ms": 1e3 * t, "dE_range": [float(de.min()), float(de.max())]}
+    out = {"workload": f"{args.config}: CI space {nd1} determinants, PT space {sysm.nd - nd1}, 10 vectors",
+           "gpu_ms": 1e3 * t, "dE_range": [float(de.min()), float(de.max())]}
+    try:
+        numh_pt = eng.form_h_pt(nd1, nd1)
+        st = eng.stats()
+        t0 = time.perf_counter()
+        de_pt = eng.pt2(nd1, X0, E)
+        t_pt = time.perf_counter() - t0
+        out["pt_block"] = {"numh": int(numh_pt),
+                           "formh_pt_ms": st["formh_ms"], "pt2_ms": 1e3 * t_pt,
+                           "max_rel_dE_vs_whole": float(np.max(np.abs(de_pt - de) / np.abs(de)))}
+    finally:
+        eng.form_h(64)
+    return out
 
 
 def csf_section(args, local, e, sysm):

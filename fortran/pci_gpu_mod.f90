@@ -78,6 +78,11 @@ module pci_gpu_mod
        real(c_double) :: X0(*), E(*), dE(*); integer(c_int32_t), value :: nv, avg_diag
        type(c_ptr), value :: Xpt
      end function
+     ! conf_pt FormH (conf_pt.f90:1319-1351): the PT block (rows > nd1, columns <= nd0) in place of H
+     integer(c_int) function pci_gpu_form_h_pt(h, nd1, nd0, value_prec, NumH) bind(C)
+       import; type(c_ptr), value :: h; integer(c_int64_t), value :: nd1, nd0
+       integer(c_int32_t), value :: value_prec; integer(c_int64_t) :: NumH
+     end function
      ! pdtm FormDM density pass: Ro(Nst, Nst, nv) of X(Nd, nv)
      integer(c_int) function pci_gpu_density(h, X, nv, trd, Ro) bind(C)
        import; type(c_ptr), value :: h; real(c_double) :: X(*), Ro(*)

@@ -214,6 +214,20 @@ int pci_gpu_csf_to_det(pci_gpu_t *h, const double *Y, int32_t nv, double *X);
 int pci_gpu_pt2(pci_gpu_t *h, int64_t nd1, int64_t nd0, const double *X0, int32_t nv, const double *E,
                 int32_t avg_diag, double *dE, double *Xpt);
 
+/* Replaces: conf_pt's own FormH (conf_pt.f90:1319-1351), which forms for
+ * each PT determinant only its row against the first nd0 determinants.
+ * Builds, in place of H, the block pci_gpu_pt2 reads: the rows of the
+ * determinants beyond nd1 against columns below nd0, plus each PT
+ * configuration's own diagonal block (for H_ii); rows up to nd1 stay empty
+ * and the PT x PT block between different configurations is not formed, so
+ * the stored elements grow with the PT space times the zero-order space's
+ * neighbours instead of the PT space squared.  Elements are bit-identical to
+ * the same positions of pci_gpu_form_h's H.  nd0 <= nd1 <= Nd, both at
+ * configuration ends; value_prec 64 or 32.  pci_gpu_pt2 must then be called
+ * with the same nd1 and nd0; the Davidson entry points, the batched solver
+ * and pci_gpu_form_csf refuse this matrix. */
+int pci_gpu_form_h_pt(pci_gpu_t *h, int64_t nd1, int64_t nd0, int32_t value_prec, int64_t *NumH);
+
 /* No counterpart in the reference.  The J_av of pci_gpu_j_av for callers that
  * cannot allocate device memory (a host that owns all device memory through
  * its own pool or a framework's caching allocator, or a path where

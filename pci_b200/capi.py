@@ -22,7 +22,7 @@ PCI_DVD_FP64, PCI_DVD_FP32, PCI_DVD_LEARNED = 0, 1, 2
 EXPORTS = ["pci_gpu_create", "pci_gpu_set_basis", "pci_gpu_set_integrals", "pci_gpu_form_h",
            "pci_gpu_form_j", "pci_gpu_csr_info", "pci_gpu_get_csr", "pci_gpu_set_csr",
            "pci_gpu_davidson", "pci_gpu_j_av", "pci_gpu_j_av_noalloc", "pci_gpu_lsj", "pci_gpu_density", "pci_gpu_transition_density", "pci_gpu_form_csf", "pci_gpu_csf_counts",
-           "pci_gpu_csf_to_det", "pci_gpu_pt2", "pci_gpu_jterms", "pci_gpu_stats",
+           "pci_gpu_csf_to_det", "pci_gpu_pt2", "pci_gpu_form_h_pt", "pci_gpu_jterms", "pci_gpu_stats",
            "pci_gpu_last_error", "pci_gpu_destroy", "pci_mlp_create", "pci_mlp_num_params", "pci_mlp_set_params",
            "pci_mlp_get_params", "pci_mlp_forward", "pci_mlp_loss_grad", "pci_mlp_train", "pci_mlp_last_error",
            "pci_mlp_destroy", "pci_gpu_set_correction_model", "pci_gpu_davidson_harvest", "pci_mlp_forward_occ",
@@ -89,6 +89,7 @@ def load(path: str = LIB):
     L.pci_gpu_csf_counts.argtypes = [P, P]
     L.pci_gpu_csf_to_det.argtypes = [P, P, i32, P]
     L.pci_gpu_pt2.argtypes = [P, i64, i64, P, i32, P, i32, P, P]
+    L.pci_gpu_form_h_pt.argtypes = [P, i64, i64, i32, P]
     L.pci_gpu_j_av_noalloc.argtypes = [P, P, P, i64, P, i64, i32, i64, P, P, C.c_char_p, i32]
     L.pci_mlp_create.argtypes = [i32, i32, i32, C.POINTER(P)]
     L.pci_mlp_num_params.argtypes = [P]
@@ -356,6 +357,13 @@ class Engine:
         out = np.zeros((nv, self._nd))
         self._check(self.L.pci_gpu_csf_to_det(self.h, _p(yc), nv, _p(out)))
         return out.T
+
+    def form_h_pt(self, nd1: int, nd0: int, value_prec: int = 64) -> int:
+        """conf_pt's PT block (rows beyond nd1 against the first nd0
+        columns) in place of H; returns the stored element count."""
+        n = C.c_int64()
+        self._check(self.L.pci_gpu_form_h_pt(self.h, nd1, nd0, value_prec, C.byref(n)))
+        return n.value
 
     def pt2(self, nd1, X0, E, avg_diag=False, want_vectors=False):
         """Second-order CI+PT (conf_pt's PTE) on the resident H: X0 (nd0 x nv)

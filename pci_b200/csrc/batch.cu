@@ -1507,6 +1507,7 @@ int pci_batch_add_block(pci_batch_t *b, pci_gpu_t *h, int32_t *index)
     pci_gpu *c = &b->core;
     if (h->device != c->device) return set_err(c, PCI_E_INPUT, "block handle is on another device");
     if (!h->H.rowptr) return set_err(c, PCI_E_STATE, "the handle holds no Hamiltonian");
+    if (h->h_pt_nd1 >= 0) return set_err(c, PCI_E_STATE, "the handle holds conf_pt's PT block, not a Hamiltonian");
     if (b->blocks.size() >= (size_t)INT32_MAX) return set_err(c, PCI_E_INPUT, "too many blocks");
     if (b->rows + h->H.nrows >= (int64_t)1 << 40) return set_err(c, PCI_E_INPUT, "too many rows");
     cudaSetDevice(c->device);

@@ -401,6 +401,7 @@ int pci_gpu_form_csf(pci_gpu_t *h, int64_t *ncsf_out, int64_t *numh_out)
     csr_free(h->Hfull);
     h->H = out;
     h->h_from_tiles = false;
+    h->h_pt_nd1 = -1;
     h->hmin = hmin;
     h->numh = nnz;
     h->h_csf_start = csf_start;

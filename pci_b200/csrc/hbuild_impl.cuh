@@ -326,15 +326,20 @@ __device__ __forceinline__ int d_compd(const uint16_t *a, const uint16_t *b)
 
 // One warp per configuration c1: list c2 <= c1 (non-empty) with CompD <= 2.
 // The count pass also records the work of c1 (pairs its rows will visit).
+// With a window (w_c1 >= 0) only the rows of configurations c1 >= w_c1 get
+// entries, and only c2 < w_c0 and c2 = c1 (conf_pt's rows of the PT space
+// against the zero-order space, plus each PT configuration's own diagonal
+// block for H_ii); c1 stays the last entry of its list either way.
 template <int NE, int FILL>
 __global__ void __launch_bounds__(256) k_adjacency(DevSys S, const int32_t *ndc, int64_t *cnt, int32_t *adj,
-                                                   unsigned long long *work)
+                                                   unsigned long long *work, int w_c1, int w_c0)
 {
     int lane = threadIdx.x & 31;
     int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const bool win = w_c1 >= 0;
     for (int64_t c1 = warp; c1 < S.nc; c1 += nwarps) {
-        if (ndc[c1] == 0) {
+        if (ndc[c1] == 0 || (win && c1 < w_c1)) {
             if (!FILL && lane == 0) { cnt[c1] = 0; work[c1] = 0; }
             continue;
         }
@@ -343,10 +348,14 @@ __global__ void __launch_bounds__(256) k_adjacency(DevSys S, const int32_t *ndc,
         for (int e = 0; e < NE; e++) a[e] = S.conf_orb[c1 * NE + e];
         int64_t base = FILL ? cnt[c1] : 0, c = 0;
         unsigned long long wsum = 0;
-        for (int64_t c2b = 0; c2b <= c1; c2b += 32) {
-            int64_t c2 = c2b + lane;
+        // candidates t < nlo are c2 = t; one more (t = nlo) is c1 itself when the window cuts it off
+        const int64_t nlo = (win && w_c0 < c1 + 1) ? (int64_t)w_c0 : c1 + 1;
+        const int64_t ncand = nlo + ((win && c1 >= w_c0) ? 1 : 0);
+        for (int64_t tb = 0; tb < ncand; tb += 32) {
+            const int64_t t = tb + lane;
+            const int64_t c2 = t < nlo ? t : c1;
             bool ok = false;
-            if (c2 <= c1 && ndc[c2] > 0) {
+            if (t < ncand && ndc[c2] > 0) {
                 uint16_t b[NE];
 #pragma unroll
                 for (int e = 0; e < NE; e++) b[e] = S.conf_orb[c2 * NE + e];
@@ -376,7 +385,7 @@ static int adjacency_impl(pci_gpu *h, DevSys S, const int32_t *d_ndc)
     if (rc) return rc;
     unsigned long long *work = (unsigned long long *)dev_alloc(h, (nc + 1) * 8, &rc);
     if (rc) { dev_free(cnt); return rc; }
-    k_adjacency<NE, 0><<<148 * 8, 256, 0, h->st>>>(S, d_ndc, cnt, nullptr, work);
+    k_adjacency<NE, 0><<<148 * 8, 256, 0, h->st>>>(S, d_ndc, cnt, nullptr, work, h->adj_win_c1, h->adj_win_c0);
     PCI_CUDA(h, cudaGetLastError());
     dev_free(h->d_adj_ptr);
     h->d_adj_ptr = (int64_t *)dev_alloc(h, (nc + 1) * 8, &rc);
@@ -395,7 +404,8 @@ static int adjacency_impl(pci_gpu *h, DevSys S, const int32_t *d_ndc)
     h->d_adj = (int32_t *)dev_alloc(h, std::max<int64_t>(nadj, 1) * 4, &rc);
     if (rc) { dev_free(cnt); dev_free(work); return rc; }
     S.adj_ptr = h->d_adj_ptr;
-    k_adjacency<NE, 1><<<148 * 8, 256, 0, h->st>>>(S, d_ndc, h->d_adj_ptr, h->d_adj, nullptr);
+    k_adjacency<NE, 1><<<148 * 8, 256, 0, h->st>>>(S, d_ndc, h->d_adj_ptr, h->d_adj, nullptr, h->adj_win_c1,
+                                                   h->adj_win_c0);
     PCI_CUDA(h, cudaGetLastError());
     PCI_CUDA(h, cudaStreamSynchronize(h->st));
     dev_free(cnt);
@@ -1076,7 +1086,7 @@ static inline void make_items(const pci_gpu *h, const std::vector<unsigned long 
     std::vector<std::pair<double, int4>> tmp;
     for (int c = 0; c < nc; c++) {
         int nr = h->h_ndc[c];
-        if (nr == 0) continue;
+        if (nr == 0 || rowwork[c] == 0) continue;   // no pairs: outside a windowed adjacency
         double w = std::max(1.0, (double)rowwork[c]);
         int R = (int)std::max(1.0, std::min((double)TR, std::floor(target / w)));
         for (int r = 0; r < nr; r += R) {

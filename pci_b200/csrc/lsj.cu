@@ -587,7 +587,8 @@ int pci_gpu_density(pci_gpu_t *h, const double *X, int32_t nv, double trd, doubl
     if (!h->have_basis) return set_err(h, PCI_E_STATE, "density before set_basis");
     if (nv < 1 || nv > 64) return set_err(h, PCI_E_INPUT, "density: nv must be 1..64");
     int rc = 0;
-    if (!h->d_adj && (rc = hb_build_adjacency(h))) return rc;   // FormH's configuration adjacency
+    // FormH's configuration adjacency, in full (a PT block's window lists too few pairs)
+    if ((!h->d_adj || h->adj_win_c1 >= 0) && (rc = hb_build_adjacency(h))) return rc;
     const int64_t nd = h->nd, nst = h->nst;
     LsjBuf d_x, d_ro;
     d_x.p = dev_alloc(h, (size_t)nd * nv * 8, &rc);

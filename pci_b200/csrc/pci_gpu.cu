@@ -387,6 +387,13 @@ int pci_gpu_form_h(pci_gpu_t *h, int32_t value_prec, int64_t *NumH, int64_t *num
     return hb_form_h(h, value_prec, NumH, numzero, Hmin);
 }
 
+int pci_gpu_form_h_pt(pci_gpu_t *h, int64_t nd1, int64_t nd0, int32_t value_prec, int64_t *NumH)
+{
+    if (!h) return PCI_E_INPUT;
+    cudaSetDevice(h->device);
+    return hb_form_h_pt(h, nd1, nd0, value_prec, NumH);
+}
+
 int pci_gpu_form_j(pci_gpu_t *h, int64_t *NumJ)
 {
     if (!h) return PCI_E_INPUT;
@@ -469,6 +476,7 @@ int pci_gpu_set_csr(pci_gpu_t *h, int32_t which, int64_t Nd, int64_t nnz, const 
     if (which != PCI_MAT_J2) {
         csr_free(h->Hfull);
         h->h_from_tiles = false;
+        h->h_pt_nd1 = -1;
     }
     int rc = 0;
     c.nrows = Nd;
@@ -503,6 +511,8 @@ int pci_gpu_davidson(pci_gpu_t *h, const pci_dvd_params *p, const double *X0, do
     cudaSetDevice(h->device);
     if (h->H.rowptr && h->H.nrows != h->nd)
         return set_err(h, PCI_E_STATE, "davidson: the resident matrix is the CSF one; solve it with the batched solver");
+    if (h->H.rowptr && h->h_pt_nd1 >= 0)
+        return set_err(h, PCI_E_STATE, "davidson: the resident matrix is conf_pt's PT block (pci_gpu_form_h_pt)");
     return dv_run(h, p, X0, Tk, Tj, Iconverge, X, iters, resid);
 }
 
@@ -512,6 +522,8 @@ int pci_gpu_davidson_harvest(pci_gpu_t *h, const pci_dvd_params *p, const double
     if (!h || !p || !count) return PCI_E_INPUT;
     cudaSetDevice(h->device);
     if (p->mode != PCI_DVD_FP64) return set_err(h, PCI_E_INPUT, "harvest runs the FP64 form");
+    if (h->H.rowptr && (h->H.nrows != h->nd || h->h_pt_nd1 >= 0))
+        return set_err(h, PCI_E_STATE, "harvest needs the determinant H of pci_gpu_form_h");
     DvdHarvest hv;
     hv.feat = feat;
     hv.target = target;

@@ -110,7 +110,7 @@ int pci_gpu_pt2(pci_gpu_t *h, int64_t nd1, int64_t nd0, const double *X0, int32_
     cudaSetDevice(h->device);
     if (!X0 || !E || !dE) return set_err(h, PCI_E_INPUT, "null array");
     if (!h->have_basis || !h->H.rowptr || h->H.nrows != h->nd)
-        return set_err(h, PCI_E_STATE, "pt2 needs the determinant H of pci_gpu_form_h over the CI + PT list");
+        return set_err(h, PCI_E_STATE, "pt2 needs the determinant H of pci_gpu_form_h or pci_gpu_form_h_pt");
     if (nv < 1 || nv > 64) return set_err(h, PCI_E_INPUT, "pt2: nv must be 1..64");
     // conf_pt's Hmltn (conf_pt.f90:1353-1398) has no Gj J^2 term
     if (h->gj != 0.0) return set_err(h, PCI_E_INPUT, "pt2: H must be built with Gj = 0, as conf_pt's Hmltn");
@@ -122,6 +122,8 @@ int pci_gpu_pt2(pci_gpu_t *h, int64_t nd1, int64_t nd0, const double *X0, int32_
     auto at_boundary = [&](int64_t n) { return std::binary_search(cs.begin(), cs.end(), n); };
     if (!at_boundary(nd1) || !at_boundary(nd0))
         return set_err(h, PCI_E_INPUT, "pt2: Nd1 and Nd0 must end a configuration");
+    if (h->h_pt_nd1 >= 0 && (h->h_pt_nd1 != nd1 || h->h_pt_nd0 != nd0))
+        return set_err(h, PCI_E_INPUT, "pt2: the resident PT block was built for another Nd1 / Nd0");
     const int cpt0 = (int)(std::lower_bound(cs.begin(), cs.end(), nd1) - cs.begin());   // first PT configuration
     int rc = 0;
     PtBuf d_x0, d_x, d_y, d_d, d_e, d_de, d_c;
@@ -149,7 +151,9 @@ int pci_gpu_pt2(pci_gpu_t *h, int64_t nd1, int64_t nd0, const double *X0, int32_
     PCI_CUDA(h, cudaMemsetAsync(d_de.p, 0, (size_t)nv * 8, st));
     k_pt_pack<<<148 * 4, 256, 0, st>>>((const double *)d_x0.p, nd0, nv, (double *)d_x.p);
     PCI_CUDA(h, cudaGetLastError());
-    if ((rc = sp_spmm(h, (const double *)d_x.p, nv, (double *)d_y.p, nv, nv, st))) return rc;
+    for (int v0 = 0; v0 < nv; v0 += 16)   // the SpMM takes up to 16 vectors per call
+        if ((rc = sp_spmm(h, (const double *)d_x.p + v0, nv, (double *)d_y.p + v0, nv, std::min(16, nv - v0), st)))
+            return rc;
     if (nd > nd1) {
         k_pt_diag<<<148 * 4, 256, 0, st>>>(h->H.rowptr, h->H.col, h->H.val, h->H.val_f32, nd1, nd, (double *)d_d.p);
         PCI_CUDA(h, cudaGetLastError());

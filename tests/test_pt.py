@@ -89,3 +89,92 @@ def test_pt2_gpu_errors():
             e.pt2(nd1 + 1, X0, E)                      # Nd1 inside a configuration
         with pytest.raises(PciError):
             e.pt2(nd1, np.zeros((nd1 + 1, 1)), E[:1])  # Nd0 > Nd1
+
+
+def _pt_mask(ndc, nd1, nd0):
+    """Positions of conf_pt's PT block in the symmetric dense H: rows beyond
+    nd1 against columns below nd0, and each PT configuration's own block."""
+    conf = np.repeat(np.arange(len(ndc)), ndc)
+    nd = conf.size
+    i = np.arange(nd)[:, None]
+    k = np.arange(nd)[None, :]
+    m = (i >= nd1) & ((k < nd0) | (conf[:, None] == conf[None, :]))
+    return m | m.T
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,frac", [("cfg1", 0.3), ("small3", 0.5), ("small4", 0.4)])
+def test_pt_block_is_the_pt_part_of_h(name, frac):
+    """pci_gpu_form_h_pt stores exactly the PT block's elements of the
+    oracle's H, bit for bit, and pt2 on it equals pt2 on the whole H and the
+    oracle."""
+    import oracle as O
+    from pci_b200.capi import Engine
+    s0 = get_system(name)
+    s, H, cs, nd1, X0, E = _ci_pt(name, max(1, int(frac * len(s0.ndc))))
+    nd0 = int(cs[max(1, int(np.searchsorted(cs, nd1)) // 2)])
+    want_de, want_c = O.pt2(H, nd1, nd0, X0[:nd0], E, s.ndc, avg_diag=True)
+    with Engine(0) as e:
+        e.load_system(s)
+        e.form_h(64)
+        de_full = e.pt2(nd1, X0[:nd0], E, avg_diag=True)
+        nnz = e.form_h_pt(nd1, nd0)
+        rp, col, val = e.get_csr(0)
+        de, c = e.pt2(nd1, X0[:nd0], E, avg_diag=True, want_vectors=True)
+    mask = _pt_mask(np.asarray(s.ndc), nd1, nd0)
+    want = np.where(mask, H, 0.0)
+    assert nnz == rp[-1] == np.count_nonzero(np.tril(want))
+    assert np.array_equal(O.csr_to_dense(s.nd, rp, col, val), want)
+    assert np.all(np.diff(rp)[:nd1] == 0)
+    assert np.allclose(de, de_full, rtol=1e-12, atol=1e-15)
+    assert np.allclose(de, want_de, rtol=1e-10, atol=1e-13)
+    assert np.allclose(c, want_c, rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.gpu
+def test_pt2_more_than_16_vectors():
+    """The SpMM takes 16 vectors a call; pt2 runs 20 in two."""
+    import oracle as O
+    from pci_b200.capi import Engine
+    s, H, cs, nd1, X0, E = _ci_pt("small3", 10)
+    nd0 = nd1
+    rng = np.random.default_rng(11)
+    Xr = rng.standard_normal((nd0, 20))
+    Er = np.diag(H).min() - 1.0 - np.arange(20) * 0.1
+    want_de, want_c = O.pt2(H, nd1, nd0, Xr, Er)
+    with Engine(0) as e:
+        e.load_system(s)
+        e.form_h_pt(nd1, nd0)
+        de, c = e.pt2(nd1, Xr, Er, want_vectors=True)
+    assert np.allclose(de, want_de, rtol=1e-10, atol=1e-13)
+    assert np.allclose(c, want_c, rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.gpu
+def test_pt_block_state():
+    """The PT block is for pt2 alone: the solvers refuse it, pt2 refuses
+    another Nd1 / Nd0, the density pass rebuilds the full adjacency, and
+    FormH afterwards gives the whole H again."""
+    from pci_b200.capi import Batch, Engine, PciError
+    s, H, cs, nd1, X0, E = _ci_pt("small3", 10)
+    nd0 = int(cs[5])
+    rng = np.random.default_rng(3)
+    Xd = rng.standard_normal((s.nd, 2))
+    Xd /= np.linalg.norm(Xd, axis=0)
+    with Engine(0) as e:
+        e.load_system(s)
+        nfull = e.form_h(64)[0]
+        ro_full = e.density(Xd)
+        e.form_h_pt(nd1, nd0)
+        with pytest.raises(PciError):
+            e.davidson(s.nd, Nlv=2)
+        with pytest.raises(PciError):
+            e.pt2(nd1, X0[:nd1], E)                # built for nd0, called with nd1
+        with pytest.raises(PciError):
+            e.form_h_pt(nd1 + 1, nd0)              # not a configuration end
+        ro_pt = e.density(Xd)
+        with Batch(0) as b:
+            with pytest.raises(PciError):
+                b.add_engine(e)
+        assert e.form_h(64)[0] == nfull
+    assert np.allclose(ro_pt, ro_full, rtol=0, atol=1e-13)   # atomics: summation order varies
