@@ -78,9 +78,21 @@ module pci_gpu_mod
        real(c_double) :: X0(*), E(*), dE(*); integer(c_int32_t), value :: nv, avg_diag
        type(c_ptr), value :: Xpt
      end function
+     ! PTE with dE(n,ic), dV(n,ic) of row groups (conf_pt.f90:871-872): dEg(nv, ngrp), dVg(nv, ngrp)
+     integer(c_int) function pci_gpu_pt2_groups(h, nd1, nd0, X0, nv, E, avg_diag, grp, ngrp, dE, dEg, dVg, Xpt) &
+         bind(C)
+       import; type(c_ptr), value :: h; integer(c_int64_t), value :: nd1, nd0
+       real(c_double) :: X0(*), E(*), dE(*), dEg(*), dVg(*); integer(c_int32_t), value :: nv, avg_diag, ngrp
+       integer(c_int64_t) :: grp(*); type(c_ptr), value :: Xpt
+     end function
      ! conf_pt FormH (conf_pt.f90:1319-1351): the PT block (rows > nd1, columns <= nd0) in place of H
      integer(c_int) function pci_gpu_form_h_pt(h, nd1, nd0, value_prec, NumH) bind(C)
        import; type(c_ptr), value :: h; integer(c_int64_t), value :: nd1, nd0
+       integer(c_int32_t), value :: value_prec; integer(c_int64_t) :: NumH
+     end function
+     ! the PT block for the PT rows row_lo+1..row_hi only (one share of the PT space)
+     integer(c_int) function pci_gpu_form_h_pt_rows(h, nd1, nd0, row_lo, row_hi, value_prec, NumH) bind(C)
+       import; type(c_ptr), value :: h; integer(c_int64_t), value :: nd1, nd0, row_lo, row_hi
        integer(c_int32_t), value :: value_prec; integer(c_int64_t) :: NumH
      end function
      ! pdtm FormDM density pass: Ro(Nst, Nst, nv) of X(Nd, nv)

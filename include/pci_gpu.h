@@ -214,6 +214,19 @@ int pci_gpu_csf_to_det(pci_gpu_t *h, const double *Y, int32_t nv, double *X);
 int pci_gpu_pt2(pci_gpu_t *h, int64_t nd1, int64_t nd0, const double *X0, int32_t nv, const double *E,
                 int32_t avg_diag, double *dE, double *Xpt);
 
+/* Replaces: PTE's contributions of the non-relativistic configurations
+ * (dE(n,ic), dV(n,ic), conf_pt.f90:871-872, from which it prints DEnr and
+ * DVnr).  pci_gpu_pt2 plus, for ngrp groups of PT rows given as ascending
+ * determinant offsets grp[0..ngrp] (group g holds rows grp[g]..grp[g+1]-1,
+ * all within nd1..Nd; NR_Init's non-relativistic configurations,
+ * conf_pt.f90:500-570, are the reference's groups), dEg[g*nv + n] = the
+ * group's sum of x^2 / (E[n] - H_ii) and dVg[g*nv + n] = its sum of c_in^2
+ * (both ngrp x nv, host).  On a PT block of pci_gpu_form_h_pt_rows the
+ * sums cover that block's rows. */
+int pci_gpu_pt2_groups(pci_gpu_t *h, int64_t nd1, int64_t nd0, const double *X0, int32_t nv, const double *E,
+                       int32_t avg_diag, const int64_t *grp, int32_t ngrp, double *dE, double *dEg, double *dVg,
+                       double *Xpt);
+
 /* Replaces: conf_pt's own FormH (conf_pt.f90:1319-1351), which forms for
  * each PT determinant only its row against the first nd0 determinants.
  * Builds, in place of H, the block pci_gpu_pt2 reads: the rows of the
@@ -222,11 +235,22 @@ int pci_gpu_pt2(pci_gpu_t *h, int64_t nd1, int64_t nd0, const double *X0, int32_
  * and the PT x PT block between different configurations is not formed, so
  * the stored elements grow with the PT space times the zero-order space's
  * neighbours instead of the PT space squared.  Elements are bit-identical to
- * the same positions of pci_gpu_form_h's H.  nd0 <= nd1 <= Nd, both at
+ * the same positions of pci_gpu_form_h's H.  nd0 <= nd1 < Nd, both at
  * configuration ends; value_prec 64 or 32.  pci_gpu_pt2 must then be called
  * with the same nd1 and nd0; the Davidson entry points, the batched solver
  * and pci_gpu_form_csf refuse this matrix. */
 int pci_gpu_form_h_pt(pci_gpu_t *h, int64_t nd1, int64_t nd0, int32_t value_prec, int64_t *NumH);
+
+/* No counterpart in the reference, whose PTE shares each PT configuration's
+ * determinants out over its MPI ranks and reduces the sums
+ * (conf_pt.f90:825-860); here a share is a range of whole PT configurations,
+ * so that each block holds whole diagonal blocks.  pci_gpu_form_h_pt for the PT rows
+ * row_lo..row_hi-1 only (nd1 <= row_lo < row_hi <= Nd, all at configuration
+ * ends): for a PT space whose whole PT block exceeds the device, or for one
+ * range per GPU.  pci_gpu_pt2 on it gives that range's share: the ranges' dE
+ * add up to the whole PT space's, and Xpt is zero outside the range. */
+int pci_gpu_form_h_pt_rows(pci_gpu_t *h, int64_t nd1, int64_t nd0, int64_t row_lo, int64_t row_hi,
+                           int32_t value_prec, int64_t *NumH);
 
 /* No counterpart in the reference.  The J_av of pci_gpu_j_av for callers that
  * cannot allocate device memory (a host that owns all device memory through

@@ -624,6 +624,31 @@ def csf_hamiltonian(H_dense, C):
     return C.T @ H_dense @ C
 
 
+def pt2_groups(H_dense, nd1, nd0, X0, E, groups, conf_sizes=None, avg_diag=False):
+    """PTE's contributions per group of PT rows (src/conf_pt.f90:825-875,
+    dE(n,ic) and dV(n,ic) over the determinants of NR configuration ic), in
+    the engine's convention: rows groups[g]..groups[g+1]-1."""
+    nd = H_dense.shape[0]
+    X0 = np.asarray(X0, np.float64).reshape(nd0, -1)
+    E = np.asarray(E, np.float64)
+    diag = np.diag(H_dense).copy()
+    if avg_diag:
+        starts = np.concatenate([[0], np.cumsum(conf_sizes)])
+        for a, b in zip(starts[:-1], starts[1:]):
+            if a >= nd1 and b > a:
+                diag[b - 1] = diag[a:b].mean()
+    ng = len(groups) - 1
+    dEg = np.zeros((ng, len(E)))
+    dVg = np.zeros((ng, len(E)))
+    for g in range(ng):
+        for i in range(int(groups[g]), int(groups[g + 1])):
+            x = H_dense[i, :nd0] @ X0
+            dl = E - diag[i]
+            dEg[g] += x * x / dl
+            dVg[g] += (x / dl) ** 2
+    return dEg, dVg
+
+
 def pt2(H_dense, nd1, nd0, X0, E, conf_sizes=None, avg_diag=False):
     """PTE (src/conf_pt.f90:751-952) densely, in the engine's convention: for
     every determinant i beyond nd1, x = sum_(k < nd0) H_ik X0_kn, dE_n +=

@@ -22,7 +22,7 @@ PCI_DVD_FP64, PCI_DVD_FP32, PCI_DVD_LEARNED = 0, 1, 2
 EXPORTS = ["pci_gpu_create", "pci_gpu_set_basis", "pci_gpu_set_integrals", "pci_gpu_form_h",
            "pci_gpu_form_j", "pci_gpu_csr_info", "pci_gpu_get_csr", "pci_gpu_set_csr",
            "pci_gpu_davidson", "pci_gpu_j_av", "pci_gpu_j_av_noalloc", "pci_gpu_lsj", "pci_gpu_density", "pci_gpu_transition_density", "pci_gpu_form_csf", "pci_gpu_csf_counts",
-           "pci_gpu_csf_to_det", "pci_gpu_pt2", "pci_gpu_form_h_pt", "pci_gpu_jterms", "pci_gpu_stats",
+           "pci_gpu_csf_to_det", "pci_gpu_pt2", "pci_gpu_pt2_groups", "pci_gpu_form_h_pt", "pci_gpu_form_h_pt_rows", "pci_gpu_jterms", "pci_gpu_stats",
            "pci_gpu_last_error", "pci_gpu_destroy", "pci_mlp_create", "pci_mlp_num_params", "pci_mlp_set_params",
            "pci_mlp_get_params", "pci_mlp_forward", "pci_mlp_loss_grad", "pci_mlp_train", "pci_mlp_last_error",
            "pci_mlp_destroy", "pci_gpu_set_correction_model", "pci_gpu_davidson_harvest", "pci_mlp_forward_occ",
@@ -89,7 +89,9 @@ def load(path: str = LIB):
     L.pci_gpu_csf_counts.argtypes = [P, P]
     L.pci_gpu_csf_to_det.argtypes = [P, P, i32, P]
     L.pci_gpu_pt2.argtypes = [P, i64, i64, P, i32, P, i32, P, P]
+    L.pci_gpu_pt2_groups.argtypes = [P, i64, i64, P, i32, P, i32, P, i32, P, P, P, P]
     L.pci_gpu_form_h_pt.argtypes = [P, i64, i64, i32, P]
+    L.pci_gpu_form_h_pt_rows.argtypes = [P, i64, i64, i64, i64, i32, P]
     L.pci_gpu_j_av_noalloc.argtypes = [P, P, P, i64, P, i64, i32, i64, P, P, C.c_char_p, i32]
     L.pci_mlp_create.argtypes = [i32, i32, i32, C.POINTER(P)]
     L.pci_mlp_num_params.argtypes = [P]
@@ -358,12 +360,51 @@ class Engine:
         self._check(self.L.pci_gpu_csf_to_det(self.h, _p(yc), nv, _p(out)))
         return out.T
 
-    def form_h_pt(self, nd1: int, nd0: int, value_prec: int = 64) -> int:
-        """conf_pt's PT block (rows beyond nd1 against the first nd0
-        columns) in place of H; returns the stored element count."""
+    def form_h_pt(self, nd1: int, nd0: int, value_prec: int = 64, rows=None) -> int:
+        """conf_pt's PT block (rows beyond nd1, or the PT rows rows[0] to
+        rows[1]-1, against the first nd0 columns) in place of H; returns the
+        stored element count."""
         n = C.c_int64()
-        self._check(self.L.pci_gpu_form_h_pt(self.h, nd1, nd0, value_prec, C.byref(n)))
+        if rows is None:
+            self._check(self.L.pci_gpu_form_h_pt(self.h, nd1, nd0, value_prec, C.byref(n)))
+        else:
+            self._check(self.L.pci_gpu_form_h_pt_rows(self.h, nd1, nd0, int(rows[0]), int(rows[1]), value_prec,
+                                                      C.byref(n)))
         return n.value
+
+    def pt2_groups(self, nd1, X0, E, groups, avg_diag=False):
+        """pt2 with PTE's sums per group of PT rows (groups: ascending
+        determinant offsets, e.g. pci_b200.system.nr_configurations): returns
+        dE [nv], dEg and dVg [ngroups, nv]."""
+        X0 = np.asarray(X0, np.float64)
+        if X0.ndim == 1:
+            X0 = X0[:, None]
+        nd0, nv = X0.shape
+        xc = np.ascontiguousarray(X0.T)
+        e = np.ascontiguousarray(E, np.float64)
+        g = np.ascontiguousarray(groups, np.int64)
+        ng = g.size - 1
+        de = np.zeros(nv)
+        deg = np.zeros((max(ng, 1), nv))
+        dvg = np.zeros((max(ng, 1), nv))
+        self._check(self.L.pci_gpu_pt2_groups(self.h, nd1, nd0, _p(xc), nv, _p(e), 1 if avg_diag else 0, _p(g), ng,
+                                              _p(de), _p(deg), _p(dvg), None))
+        return de, deg[:ng], dvg[:ng]
+
+    def pt2_ranges(self, nd1, X0, E, ranges, avg_diag=False, want_vectors=False):
+        """pt2 over the PT space in row ranges (pci_b200.system.pt_row_ranges),
+        one PT block at a time: the sums of the ranges' dE (and first-order
+        coefficients) are the whole PT space's."""
+        nd0 = np.asarray(X0).reshape(np.asarray(X0).shape[0], -1).shape[0]
+        de, c = None, None
+        for lo, hi in ranges:
+            self.form_h_pt(nd1, nd0, 64, rows=(lo, hi))
+            r = self.pt2(nd1, X0, E, avg_diag=avg_diag, want_vectors=want_vectors)
+            d_r, c_r = r if want_vectors else (r, None)
+            de = d_r if de is None else de + d_r
+            if want_vectors:
+                c = c_r if c is None else c + c_r
+        return (de, c) if want_vectors else de
 
     def pt2(self, nd1, X0, E, avg_diag=False, want_vectors=False):
         """Second-order CI+PT (conf_pt's PTE) on the resident H: X0 (nd0 x nv)

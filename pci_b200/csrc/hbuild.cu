@@ -250,11 +250,12 @@ int hb_compact(pci_gpu *h, const int64_t *pptr, const int64_t *rowptr, int64_t n
 PCI_DECL_NE(1) PCI_DECL_NE(2) PCI_DECL_NE(3) PCI_DECL_NE(4)
 PCI_DECL_NE(5) PCI_DECL_NE(6) PCI_DECL_NE(7) PCI_DECL_NE(8)
 
-int hb_build_adjacency(pci_gpu *h, int w_c1, int w_c0)
+int hb_build_adjacency(pci_gpu *h, int w_c1, int w_c0, int w_c2)
 {
     int rc = 0;
     h->adj_win_c1 = w_c1;
     h->adj_win_c0 = w_c0;
+    h->adj_win_c2 = w_c2;
     int32_t *d_ndc = (int32_t *)dev_alloc(h, (size_t)h->nc * 4, &rc);
     if (rc) return rc;
     PCI_CUDA(h, cudaMemcpyAsync(d_ndc, h->h_ndc.data(), (size_t)h->nc * 4, cudaMemcpyHostToDevice, h->st));
@@ -324,16 +325,20 @@ int hb_form_h(pci_gpu *h, int value_prec, int64_t *numh, int64_t *numzero, doubl
     return PCI_OK;
 }
 
-// conf_pt's PT block: the rows of the determinants beyond nd1 against the
-// first nd0 columns and their own configuration's diagonal block (for H_ii),
-// through the tile kernel over a windowed adjacency.  Rows below nd1 stay
-// empty, so the stored elements are those PTE (conf_pt.f90:751-952) reads
-// and none of the PT x PT block beyond the diagonal configurations.
-int hb_form_h_pt(pci_gpu *h, int64_t nd1, int64_t nd0, int value_prec, int64_t *numh)
+// conf_pt's PT block: the rows of the PT determinants row_lo..row_hi-1
+// (within nd1..Nd-1) against the first nd0 columns and their own
+// configuration's diagonal block (for H_ii), through the tile kernel over a
+// windowed adjacency.  Other rows stay empty, so the stored elements are
+// those PTE (conf_pt.f90:751-952) reads for these rows and none of the PT x PT
+// block beyond the diagonal configurations.
+int hb_form_h_pt(pci_gpu *h, int64_t nd1, int64_t nd0, int64_t row_lo, int64_t row_hi, int value_prec,
+                 int64_t *numh)
 {
     if (!h->have_basis || !h->have_ints) return set_err(h, PCI_E_STATE, "form_h_pt before set_basis/set_integrals");
     if (value_prec != 64 && value_prec != 32) return set_err(h, PCI_E_INPUT, "value_prec must be 64 or 32");
     if (nd0 < 1 || nd0 > nd1 || nd1 > h->nd) return set_err(h, PCI_E_INPUT, "form_h_pt: need 1 <= Nd0 <= Nd1 <= Nd");
+    if (row_lo < nd1 || row_hi <= row_lo || row_hi > h->nd)
+        return set_err(h, PCI_E_INPUT, "form_h_pt: need Nd1 <= row_lo < row_hi <= Nd");
     // configuration index at which determinant n starts (n must end a configuration)
     auto conf_at = [&](int64_t n) -> int {
         int64_t s = 0;
@@ -343,13 +348,14 @@ int hb_form_h_pt(pci_gpu *h, int64_t nd1, int64_t nd0, int value_prec, int64_t *
         }
         return s == n ? h->nc : -1;
     };
-    const int c1 = conf_at(nd1), c0 = conf_at(nd0);
-    if (c1 < 0 || c0 < 0) return set_err(h, PCI_E_INPUT, "form_h_pt: Nd1 and Nd0 must end a configuration");
+    const int c1 = conf_at(row_lo), c2 = conf_at(row_hi), c0 = conf_at(nd0);
+    if (conf_at(nd1) < 0 || c0 < 0 || c1 < 0 || c2 < 0)
+        return set_err(h, PCI_E_INPUT, "form_h_pt: Nd1, Nd0, row_lo and row_hi must end a configuration");
     int rc;
     cudaEvent_t a0, a1;
     cudaEventCreate(&a0); cudaEventCreate(&a1);
     cudaEventRecord(a0, h->st);
-    if ((rc = hb_build_adjacency(h, c1, c0))) { cudaEventDestroy(a0); cudaEventDestroy(a1); return rc; }
+    if ((rc = hb_build_adjacency(h, c1, c0, c2))) { cudaEventDestroy(a0); cudaEventDestroy(a1); return rc; }
     cudaEventRecord(a1, h->st);
     cudaEventSynchronize(a1);
     float tadj = 0;
@@ -367,6 +373,8 @@ int hb_form_h_pt(pci_gpu *h, int64_t nd1, int64_t nd0, int value_prec, int64_t *
     h->h_from_tiles = false;   // the adjacency is windowed; nothing else may walk it with this H
     h->h_pt_nd1 = nd1;
     h->h_pt_nd0 = nd0;
+    h->h_pt_lo = row_lo;
+    h->h_pt_hi = row_hi;
     h->numh = h->H.nnz;
     h->numzero = (int64_t)hs.numzero;
     h->hmin = hs.hmin;

@@ -326,20 +326,20 @@ __device__ __forceinline__ int d_compd(const uint16_t *a, const uint16_t *b)
 
 // One warp per configuration c1: list c2 <= c1 (non-empty) with CompD <= 2.
 // The count pass also records the work of c1 (pairs its rows will visit).
-// With a window (w_c1 >= 0) only the rows of configurations c1 >= w_c1 get
-// entries, and only c2 < w_c0 and c2 = c1 (conf_pt's rows of the PT space
-// against the zero-order space, plus each PT configuration's own diagonal
-// block for H_ii); c1 stays the last entry of its list either way.
+// With a window (w_c1 >= 0) only the rows of configurations w_c1 <= c1 <
+// w_c2 get entries, and only c2 < w_c0 and c2 = c1 (conf_pt's rows of the PT
+// space against the zero-order space, plus each PT configuration's own
+// diagonal block for H_ii); c1 stays the last entry of its list either way.
 template <int NE, int FILL>
 __global__ void __launch_bounds__(256) k_adjacency(DevSys S, const int32_t *ndc, int64_t *cnt, int32_t *adj,
-                                                   unsigned long long *work, int w_c1, int w_c0)
+                                                   unsigned long long *work, int w_c1, int w_c0, int w_c2)
 {
     int lane = threadIdx.x & 31;
     int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const bool win = w_c1 >= 0;
     for (int64_t c1 = warp; c1 < S.nc; c1 += nwarps) {
-        if (ndc[c1] == 0 || (win && c1 < w_c1)) {
+        if (ndc[c1] == 0 || (win && (c1 < w_c1 || c1 >= w_c2))) {
             if (!FILL && lane == 0) { cnt[c1] = 0; work[c1] = 0; }
             continue;
         }
@@ -385,7 +385,8 @@ static int adjacency_impl(pci_gpu *h, DevSys S, const int32_t *d_ndc)
     if (rc) return rc;
     unsigned long long *work = (unsigned long long *)dev_alloc(h, (nc + 1) * 8, &rc);
     if (rc) { dev_free(cnt); return rc; }
-    k_adjacency<NE, 0><<<148 * 8, 256, 0, h->st>>>(S, d_ndc, cnt, nullptr, work, h->adj_win_c1, h->adj_win_c0);
+    k_adjacency<NE, 0><<<148 * 8, 256, 0, h->st>>>(S, d_ndc, cnt, nullptr, work, h->adj_win_c1, h->adj_win_c0,
+                                                   h->adj_win_c2);
     PCI_CUDA(h, cudaGetLastError());
     dev_free(h->d_adj_ptr);
     h->d_adj_ptr = (int64_t *)dev_alloc(h, (nc + 1) * 8, &rc);
@@ -405,7 +406,7 @@ static int adjacency_impl(pci_gpu *h, DevSys S, const int32_t *d_ndc)
     if (rc) { dev_free(cnt); dev_free(work); return rc; }
     S.adj_ptr = h->d_adj_ptr;
     k_adjacency<NE, 1><<<148 * 8, 256, 0, h->st>>>(S, d_ndc, h->d_adj_ptr, h->d_adj, nullptr, h->adj_win_c1,
-                                                   h->adj_win_c0);
+                                                   h->adj_win_c0, h->adj_win_c2);
     PCI_CUDA(h, cudaGetLastError());
     PCI_CUDA(h, cudaStreamSynchronize(h->st));
     dev_free(cnt);

@@ -391,7 +391,16 @@ int pci_gpu_form_h_pt(pci_gpu_t *h, int64_t nd1, int64_t nd0, int32_t value_prec
 {
     if (!h) return PCI_E_INPUT;
     cudaSetDevice(h->device);
-    return hb_form_h_pt(h, nd1, nd0, value_prec, NumH);
+    if (!h->have_basis) return set_err(h, PCI_E_STATE, "form_h_pt before set_basis/set_integrals");
+    return hb_form_h_pt(h, nd1, nd0, nd1, h->nd, value_prec, NumH);
+}
+
+int pci_gpu_form_h_pt_rows(pci_gpu_t *h, int64_t nd1, int64_t nd0, int64_t row_lo, int64_t row_hi,
+                           int32_t value_prec, int64_t *NumH)
+{
+    if (!h) return PCI_E_INPUT;
+    cudaSetDevice(h->device);
+    return hb_form_h_pt(h, nd1, nd0, row_lo, row_hi, value_prec, NumH);
 }
 
 int pci_gpu_form_j(pci_gpu_t *h, int64_t *NumJ)

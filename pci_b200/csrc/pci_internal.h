@@ -90,9 +90,10 @@ struct pci_gpu {
     int64_t *d_adj_ptr = nullptr;
     int32_t *d_adj = nullptr;
     int64_t n_adj = 0;
-    // window of the adjacency in use: rows of configurations >= adj_win_c1
-    // against configurations < adj_win_c0 and themselves (-1: full lower triangle)
-    int adj_win_c1 = -1, adj_win_c0 = 0;
+    // window of the adjacency in use: rows of configurations adj_win_c1 <= c
+    // < adj_win_c2 against configurations < adj_win_c0 and themselves (-1:
+    // full lower triangle)
+    int adj_win_c1 = -1, adj_win_c0 = 0, adj_win_c2 = 0;
     int16_t *d_ms_orb = nullptr;
     int8_t *d_ms_jz = nullptr;
     uint8_t *d_ms_type = nullptr;
@@ -125,9 +126,9 @@ struct pci_gpu {
     double st_adj = 0, st_pairs = 0, st_scanned = 0, st_launches = 0;
     double st_formh_compact = 0, st_formh_padded = 0, st_formh_compact_launches = 0, st_formh_slots = 0;
     bool h_from_tiles = false;  // H was built here by form_h: its rows follow the adjacency tiles
-    // H is conf_pt's PT block of pci_gpu_form_h_pt (rows >= h_pt_nd1 against
-    // columns < h_pt_nd0); -1: H is not a PT block
-    int64_t h_pt_nd1 = -1, h_pt_nd0 = 0;
+    // H is conf_pt's PT block of pci_gpu_form_h_pt (rows h_pt_lo..h_pt_hi-1,
+    // all >= h_pt_nd1, against columns < h_pt_nd0); -1: H is not a PT block
+    int64_t h_pt_nd1 = -1, h_pt_nd0 = 0, h_pt_lo = 0, h_pt_hi = 0;
     pci_mlp *corr_model = nullptr;   // learned Davidson correction (not owned)
     int spmm_mode = 0;        // 0 auto, 1 full symmetric copy, 2 lower triangle (env PCI_SPMM)
     int spmm_lower_used = 0;
@@ -160,7 +161,7 @@ struct RowStatsOut {
 };
 int hb_build_hash(pci_gpu *h, int64_t ngint, int kbrt, int r2_is_f64, const void *rint2,
                   const int32_t *iint2, const int32_t *iint3);
-int hb_build_adjacency(pci_gpu *h, int w_c1 = -1, int w_c0 = 0);
+int hb_build_adjacency(pci_gpu *h, int w_c1 = -1, int w_c0 = 0, int w_c2 = 0);
 // Squeeze the padded rows of the single-evaluation FormH (row r's entries at
 // pptr[r], rowptr[r+1]-rowptr[r] of them) into plain CSR order in place,
 // through a buffer of `chunk` entries.
@@ -168,7 +169,7 @@ int hb_compact(pci_gpu *h, const int64_t *pptr, const int64_t *rowptr, int64_t n
                int vbytes, int64_t chunk);
 int hb_form_h(pci_gpu *h, int value_prec, int64_t *numh, int64_t *numzero, double *hmin);
 int hb_form_j(pci_gpu *h, int64_t *numj);
-int hb_form_h_pt(pci_gpu *h, int64_t nd1, int64_t nd0, int value_prec, int64_t *numh);
+int hb_form_h_pt(pci_gpu *h, int64_t nd1, int64_t nd0, int64_t row_lo, int64_t row_hi, int value_prec, int64_t *numh);
 double host_gaunt(int nlx, const double *lut, int64_t nlut, int k, double xj1, double xm1,
                   double xj2, double xm2);
 

@@ -68,16 +68,17 @@ __global__ void k_pt_avg(const int64_t *__restrict__ conf_start, int c0, int nc,
     }
 }
 
-// dE_v += y^2 / (E_v - H_ii) and c = y / (E_v - H_ii) for the PT rows.
+// dE_v += y^2 / (E_v - H_ii) and c = y / (E_v - H_ii) for the PT rows lo..hi-1
+// (d holds H_ii of rows nd1..Nd-1).
 __global__ void __launch_bounds__(256) k_pt_terms(const double *__restrict__ y, const double *__restrict__ d,
-                                                  const double *__restrict__ e, int64_t nd1, int64_t nd, int nv,
-                                                  double *de, double *cpt)
+                                                  const double *__restrict__ e, int64_t nd1, int64_t lo, int64_t hi,
+                                                  int64_t nd, int nv, double *de, double *cpt)
 {
     __shared__ double red[8][64];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     double acc[64];
     for (int v = 0; v < nv; v++) acc[v] = 0.0;
-    for (int64_t i = nd1 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nd;
+    for (int64_t i = lo + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < hi;
          i += (int64_t)gridDim.x * blockDim.x) {
         for (int v = 0; v < nv; v++) {
             const double x = y[i * nv + v];
@@ -99,15 +100,52 @@ __global__ void __launch_bounds__(256) k_pt_terms(const double *__restrict__ y, 
     }
 }
 
-}  // namespace
-
-extern "C" {
-
-int pci_gpu_pt2(pci_gpu_t *h, int64_t nd1, int64_t nd0, const double *X0, int32_t nv, const double *E,
-                int32_t avg_diag, double *dE, double *Xpt)
+// PTE's per-configuration sums (conf_pt.f90:871-872): for group g (rows
+// grp[g]..grp[g+1]-1, clipped to lo..hi-1), dEg[g * nv + v] = sum of
+// y^2 / (E_v - H_ii) and dVg[g * nv + v] = sum of (y / (E_v - H_ii))^2.  One
+// thread block per group.
+__global__ void __launch_bounds__(256) k_pt_groups(const double *__restrict__ y, const double *__restrict__ d,
+                                                   const double *__restrict__ e, const int64_t *__restrict__ grp,
+                                                   int ngrp, int64_t nd1, int64_t lo, int64_t hi, int nv, double *deg,
+                                                   double *dvg)
 {
-    if (!h) return PCI_E_INPUT;
-    cudaSetDevice(h->device);
+    __shared__ double red[2][8][64];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int g = blockIdx.x; g < ngrp; g += gridDim.x) {
+        const int64_t a = grp[g] > lo ? grp[g] : lo, b = grp[g + 1] < hi ? grp[g + 1] : hi;
+        double ae[64], av[64];
+        for (int v = 0; v < nv; v++) { ae[v] = 0.0; av[v] = 0.0; }
+        for (int64_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+            for (int v = 0; v < nv; v++) {
+                const double x = y[i * nv + v];
+                const double del = e[v] - d[i - nd1];
+                const double c = x / del;
+                ae[v] += x * x / del;
+                av[v] += c * c;
+            }
+        }
+        for (int v = 0; v < nv; v++) {
+            double s = ae[v], t = av[v];
+            for (int o = 16; o > 0; o >>= 1) {
+                s += __shfl_down_sync(0xffffffffu, s, o);
+                t += __shfl_down_sync(0xffffffffu, t, o);
+            }
+            if (lane == 0) { red[0][w][v] = s; red[1][w][v] = t; }
+        }
+        __syncthreads();
+        for (int v = threadIdx.x; v < nv; v += blockDim.x) {
+            double s = 0.0, t = 0.0;
+            for (int x = 0; x < (int)(blockDim.x >> 5); x++) { s += red[0][x][v]; t += red[1][x][v]; }
+            deg[(int64_t)g * nv + v] = s;
+            dvg[(int64_t)g * nv + v] = t;
+        }
+        __syncthreads();
+    }
+}
+
+int pt2_impl(pci_gpu *h, int64_t nd1, int64_t nd0, const double *X0, int32_t nv, const double *E, int32_t avg_diag,
+             const int64_t *grp, int32_t ngrp, double *dE, double *dEg, double *dVg, double *Xpt)
+{
     if (!X0 || !E || !dE) return set_err(h, PCI_E_INPUT, "null array");
     if (!h->have_basis || !h->H.rowptr || h->H.nrows != h->nd)
         return set_err(h, PCI_E_STATE, "pt2 needs the determinant H of pci_gpu_form_h or pci_gpu_form_h_pt");
@@ -125,8 +163,20 @@ int pci_gpu_pt2(pci_gpu_t *h, int64_t nd1, int64_t nd0, const double *X0, int32_
     if (h->h_pt_nd1 >= 0 && (h->h_pt_nd1 != nd1 || h->h_pt_nd0 != nd0))
         return set_err(h, PCI_E_INPUT, "pt2: the resident PT block was built for another Nd1 / Nd0");
     const int cpt0 = (int)(std::lower_bound(cs.begin(), cs.end(), nd1) - cs.begin());   // first PT configuration
+    if (ngrp < 0 || (ngrp > 0 && (!grp || !dEg || !dVg))) return set_err(h, PCI_E_INPUT, "pt2: bad groups");
+    for (int g = 0; g < ngrp; g++)
+        if (grp[g] < nd1 || grp[g + 1] < grp[g] || grp[g + 1] > nd)
+            return set_err(h, PCI_E_INPUT, "pt2: groups must be ascending determinant offsets within Nd1..Nd");
     int rc = 0;
-    PtBuf d_x0, d_x, d_y, d_d, d_e, d_de, d_c;
+    PtBuf d_x0, d_x, d_y, d_d, d_e, d_de, d_c, d_grp, d_eg, d_vg;
+    if (ngrp > 0) {
+        d_grp.p = dev_alloc(h, (size_t)(ngrp + 1) * 8, &rc);
+        if (rc) return rc;
+        d_eg.p = dev_alloc(h, (size_t)ngrp * nv * 8, &rc);
+        if (rc) return rc;
+        d_vg.p = dev_alloc(h, (size_t)ngrp * nv * 8, &rc);
+        if (rc) return rc;
+    }
     d_x0.p = dev_alloc(h, (size_t)nd0 * nv * 8, &rc);
     if (rc) return rc;
     d_x.p = dev_alloc(h, (size_t)nd * nv * 8, &rc);
@@ -161,14 +211,53 @@ int pci_gpu_pt2(pci_gpu_t *h, int64_t nd1, int64_t nd0, const double *X0, int32_
             k_pt_avg<<<148, 256, 0, st>>>(h->d_conf_start, cpt0, h->nc, nd1, (double *)d_d.p);
             PCI_CUDA(h, cudaGetLastError());
         }
+        // a PT block holds rows h_pt_lo..h_pt_hi-1 only; the others are another block's
+        const bool blk = h->h_pt_nd1 >= 0;
+        const int64_t lo = blk ? h->h_pt_lo : nd1, hi = blk ? h->h_pt_hi : nd;
         k_pt_terms<<<148 * 4, 256, 0, st>>>((const double *)d_y.p, (const double *)d_d.p, (const double *)d_e.p, nd1,
-                                            nd, nv, (double *)d_de.p, Xpt ? (double *)d_c.p : nullptr);
+                                            lo, hi, nd, nv, (double *)d_de.p, Xpt ? (double *)d_c.p : nullptr);
         PCI_CUDA(h, cudaGetLastError());
+        if (ngrp > 0) {
+            PCI_CUDA(h, cudaMemcpyAsync(d_grp.p, grp, (size_t)(ngrp + 1) * 8, cudaMemcpyHostToDevice, st));
+            k_pt_groups<<<std::min(ngrp, 148 * 8), 256, 0, st>>>((const double *)d_y.p, (const double *)d_d.p,
+                                                                 (const double *)d_e.p, (const int64_t *)d_grp.p,
+                                                                 ngrp, nd1, lo, hi, nv, (double *)d_eg.p,
+                                                                 (double *)d_vg.p);
+            PCI_CUDA(h, cudaGetLastError());
+        }
+    } else if (ngrp > 0) {
+        PCI_CUDA(h, cudaMemsetAsync(d_eg.p, 0, (size_t)ngrp * nv * 8, st));
+        PCI_CUDA(h, cudaMemsetAsync(d_vg.p, 0, (size_t)ngrp * nv * 8, st));
+    }
+    if (ngrp > 0) {
+        PCI_CUDA(h, cudaMemcpyAsync(dEg, d_eg.p, (size_t)ngrp * nv * 8, cudaMemcpyDeviceToHost, st));
+        PCI_CUDA(h, cudaMemcpyAsync(dVg, d_vg.p, (size_t)ngrp * nv * 8, cudaMemcpyDeviceToHost, st));
     }
     PCI_CUDA(h, cudaMemcpyAsync(dE, d_de.p, (size_t)nv * 8, cudaMemcpyDeviceToHost, st));
     if (Xpt) PCI_CUDA(h, cudaMemcpyAsync(Xpt, d_c.p, (size_t)nd * nv * 8, cudaMemcpyDeviceToHost, st));
     PCI_CUDA(h, cudaStreamSynchronize(st));
     return PCI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pci_gpu_pt2(pci_gpu_t *h, int64_t nd1, int64_t nd0, const double *X0, int32_t nv, const double *E,
+                int32_t avg_diag, double *dE, double *Xpt)
+{
+    if (!h) return PCI_E_INPUT;
+    cudaSetDevice(h->device);
+    return pt2_impl(h, nd1, nd0, X0, nv, E, avg_diag, nullptr, 0, dE, nullptr, nullptr, Xpt);
+}
+
+int pci_gpu_pt2_groups(pci_gpu_t *h, int64_t nd1, int64_t nd0, const double *X0, int32_t nv, const double *E,
+                       int32_t avg_diag, const int64_t *grp, int32_t ngrp, double *dE, double *dEg, double *dVg,
+                       double *Xpt)
+{
+    if (!h) return PCI_E_INPUT;
+    cudaSetDevice(h->device);
+    return pt2_impl(h, nd1, nd0, X0, nv, E, avg_diag, grp, ngrp, dE, dEg, dVg, Xpt);
 }
 
 }  // extern "C"

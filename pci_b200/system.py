@@ -572,6 +572,65 @@ def split_blocks(nds, world, rank):
     return mine
 
 
+def squeeze_config(basis, conf):
+    """conf_pt's Squeeze (src/conf_pt.f90:1266-1317): a configuration's shell
+    list with adjacent relativistic shells of the same (n, l) merged, their
+    occupations added: [((n, l), q), ...]."""
+    out = []
+    for ni, nq in conf:
+        key = (int(basis.nn[ni - 1]), int(basis.ll[ni - 1]))
+        if out and out[-1][0] == key:
+            out[-1] = (key, out[-1][1] + int(nq))
+        else:
+            out.append((key, int(nq)))
+    return out
+
+
+def nr_configurations(basis, configs, ndc, nd1=None):
+    """conf_pt's NR_Init (src/conf_pt.f90:500-570): consecutive relativistic
+    configurations with equal squeezed shell lists form one non-relativistic
+    configuration.  Returns the determinant offsets of the NR configurations
+    (Ncnr + 1 ascending entries, the reference's Ndic plus the end).  With
+    nd1, an NR configuration may not straddle the CI / PT boundary (NR_Init
+    stops with an error there); ValueError."""
+    ends = np.concatenate([[0], np.cumsum(np.asarray(ndc, np.int64))])
+    offs = [0]
+    prev = None
+    for ic, conf in enumerate(configs):
+        sq = squeeze_config(basis, conf)
+        if prev is not None and sq != prev:
+            offs.append(int(ends[ic]))
+        prev = sq
+    offs.append(int(ends[len(configs)]))
+    offs = np.asarray(offs, np.int64)
+    if nd1 is not None and int(nd1) not in set(offs.tolist()):
+        raise ValueError("a non-relativistic configuration straddles the CI / PT boundary")
+    return offs
+
+
+def pt_row_ranges(ndc, nd1, parts):
+    """conf_pt's PT space (the determinants from nd1, which ends a
+    configuration, to the end of the list) cut into `parts` contiguous
+    ranges of whole configurations with about equal determinant counts, as
+    (row_lo, row_hi) pairs; empty ranges are dropped.  The second-order sums
+    of the ranges add up to the whole PT space's (each PT row's terms are
+    independent), so the ranges go to separate PT-block builds on one GPU
+    or to separate ranks, with one sum of dE at the end."""
+    ends = np.cumsum(np.asarray(ndc, np.int64))
+    nd = int(ends[-1]) if len(ends) else 0
+    if nd1 != 0 and nd1 not in set(ends.tolist()):
+        raise ValueError("nd1 must end a configuration")
+    out, lo = [], int(nd1)
+    for p in range(1, parts + 1):
+        target = nd1 + (nd - nd1) * p / parts
+        k = int(np.searchsorted(ends, target))      # first end at or beyond the target
+        hi = nd if p == parts else int(ends[min(k, len(ends) - 1)])
+        if hi > lo:
+            out.append((lo, hi))
+            lo = hi
+    return out
+
+
 def make_batch(nblocks=64, seed0=1000, nd_lo=2000, nd_hi=400000, workers=None):
     """Every block of the batched workload as a CISystem, generated in a pool
     of spawned worker processes (safe to start after CUDA is initialised)."""

@@ -178,3 +178,104 @@ def test_pt_block_state():
                 b.add_engine(e)
         assert e.form_h(64)[0] == nfull
     assert np.allclose(ro_pt, ro_full, rtol=0, atol=1e-13)   # atomics: summation order varies
+
+
+def test_nr_configurations_known_answer():
+    """NR_Init's grouping: 2p-1 2p+1 and 2p+2 squeeze to the same 2p^2 and
+    are consecutive (one NR configuration); 2p-1 3p-1 differs; 2p-2 is 2p^2
+    again but not consecutive with the first group, so it starts a new one."""
+    from pci_b200 import system as S
+    b = S.make_basis([(2, 1), (3, 1)])                   # 2p-, 2p+, 3p-, 3p+
+    configs = [[(1, 1), (2, 1)], [(2, 2)], [(1, 1), (3, 1)], [(1, 2)]]
+    assert S.squeeze_config(b, configs[0]) == S.squeeze_config(b, configs[1]) == [((2, 1), 2)]
+    offs = S.nr_configurations(b, configs, [3, 2, 4, 1])
+    assert offs.tolist() == [0, 5, 9, 10]
+    assert S.nr_configurations(b, configs, [3, 2, 4, 1], nd1=5).tolist() == [0, 5, 9, 10]
+    with pytest.raises(ValueError):
+        S.nr_configurations(b, configs, [3, 2, 4, 1], nd1=3)   # inside the first NR configuration
+
+
+@pytest.mark.parametrize("name", ["small3", "cfg1"])
+def test_nr_configurations_partition(name):
+    from pci_b200 import system as S
+    s = get_system(name)
+    offs = S.nr_configurations(s.basis, s.configs, s.ndc)
+    ends = np.concatenate([[0], np.cumsum(s.ndc)])
+    assert offs[0] == 0 and offs[-1] == s.nd and np.all(np.diff(offs) > 0)
+    assert set(offs.tolist()) <= set(ends.tolist())
+    # within a group the squeezed lists agree; across a boundary they differ
+    conf_of = {int(e): i for i, e in enumerate(ends[:-1])}
+    for a, b in zip(offs[:-1], offs[1:]):
+        cs = [i for e, i in conf_of.items() if a <= e < b]
+        sq = {tuple(S.squeeze_config(s.basis, s.configs[i])) for i in cs}
+        assert len(sq) == 1
+
+
+def test_pt2_groups_oracle_sum_to_pt2():
+    import oracle as O
+    from pci_b200 import system as S
+    s, H, cs, nd1, X0, E = _ci_pt("small3", 10)
+    offs = S.nr_configurations(s.basis, s.configs, s.ndc)
+    groups = offs[offs >= nd1]
+    if groups[0] != nd1:
+        pytest.skip("CI / PT boundary inside an NR configuration")
+    dEg, dVg = O.pt2_groups(H, nd1, nd1, X0, E, groups, s.ndc, avg_diag=True)
+    dE, Cf = O.pt2(H, nd1, nd1, X0, E, s.ndc, avg_diag=True)
+    assert np.allclose(dEg.sum(axis=0), dE, rtol=1e-12, atol=1e-15)
+    assert np.allclose(dVg.sum(axis=0), (Cf ** 2).sum(axis=0), rtol=1e-12, atol=1e-15)
+
+
+def test_pt_row_ranges():
+    from pci_b200 import system as S
+    s = get_system("small3")
+    cs = np.concatenate([[0], np.cumsum(s.ndc)])
+    nd1 = int(cs[10])
+    for parts in (1, 2, 3, 7):
+        r = S.pt_row_ranges(s.ndc, nd1, parts)
+        assert r[0][0] == nd1 and r[-1][1] == s.nd
+        assert all(a[1] == b[0] for a, b in zip(r[:-1], r[1:]))
+        assert all(lo in set(cs.tolist()) and hi in set(cs.tolist()) for lo, hi in r)
+        assert len(r) <= parts
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["cfg1", "small3"])
+def test_pt2_groups_gpu_matches_oracle(name):
+    import oracle as O
+    from pci_b200 import system as S
+    from pci_b200.capi import Engine
+    s0 = get_system(name)
+    offs = S.nr_configurations(s0.basis, s0.configs, s0.ndc)
+    k = int(np.searchsorted(np.concatenate([[0], np.cumsum(s0.ndc)]), offs[len(offs) // 3]))
+    s, H, cs, nd1, X0, E = _ci_pt(name, k)                # the CI space ends an NR configuration
+    groups = offs[offs >= nd1]
+    want_eg, want_vg = O.pt2_groups(H, nd1, nd1, X0, E, groups, s.ndc, avg_diag=True)
+    with Engine(0) as e:
+        e.load_system(s)
+        e.form_h_pt(nd1, nd1)
+        de, eg, vg = e.pt2_groups(nd1, X0, E, groups, avg_diag=True)
+    assert np.allclose(eg, want_eg, rtol=1e-10, atol=1e-14)
+    assert np.allclose(vg, want_vg, rtol=1e-9, atol=1e-14)
+    assert np.allclose(eg.sum(axis=0), de, rtol=1e-12, atol=1e-15)
+
+
+@pytest.mark.gpu
+def test_pt2_row_ranges_add_up():
+    """PT blocks over row ranges: their dE, first-order coefficients and
+    group sums add up to the single block's."""
+    from pci_b200 import system as S
+    from pci_b200.capi import Engine
+    s, H, cs, nd1, X0, E = _ci_pt("small3", 10)
+    ranges = S.pt_row_ranges(s.ndc, nd1, 3)
+    assert len(ranges) == 3
+    with Engine(0) as e:
+        e.load_system(s)
+        e.form_h_pt(nd1, nd1)
+        de, c = e.pt2(nd1, X0, E, avg_diag=True, want_vectors=True)
+        de_r, c_r = e.pt2_ranges(nd1, X0, E, ranges, avg_diag=True, want_vectors=True)
+        groups = np.array([nd1, ranges[0][1], s.nd], np.int64)
+        e.form_h_pt(nd1, nd1, rows=ranges[0])
+        _, eg0, _ = e.pt2_groups(nd1, X0, E, groups)
+    assert np.allclose(de_r, de, rtol=1e-12, atol=1e-15)
+    assert np.allclose(c_r, c, rtol=1e-12, atol=1e-15)
+    assert np.all(eg0[1] == 0.0)                       # the other range's rows are not in this block
