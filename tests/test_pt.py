@@ -279,3 +279,43 @@ def test_pt2_row_ranges_add_up():
     assert np.allclose(de_r, de, rtol=1e-12, atol=1e-15)
     assert np.allclose(c_r, c, rtol=1e-12, atol=1e-15)
     assert np.all(eg0[1] == 0.0)                       # the other range's rows are not in this block
+
+
+def _pt_rank_worker(rank, port, q):
+    import os
+    import torch
+    import torch.distributed as dist
+    import oracle as O
+    from pci_b200 import system as S
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=2)
+    s, H, cs, nd1, X0, E = _ci_pt("small3", 10)
+    lo, hi = S.pt_row_ranges(s.ndc, nd1, 2)[rank]
+    eg, _ = O.pt2_groups(H, nd1, nd1, X0, E, [lo, hi], s.ndc, avg_diag=True)
+    t = torch.tensor(eg[0])
+    dist.all_reduce(t)                                  # the one exchange: dE summed over ranks
+    q.put((rank, t.numpy().copy()))
+    dist.destroy_process_group()
+
+
+def test_pt_ranges_two_gloo_ranks():
+    """Two ranks take one PT row range each (pt_row_ranges) and compute their
+    share with no exchange; one all-reduce of dE gives the whole PT space's."""
+    import multiprocessing as mp
+    import socket
+    import oracle as O
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    ps = [ctx.Process(target=_pt_rank_worker, args=(r, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    for p in ps:
+        p.join(120)
+    res = dict(q.get(timeout=10) for _ in range(2))
+    s, H, cs, nd1, X0, E = _ci_pt("small3", 10)
+    want, _ = O.pt2(H, nd1, nd1, X0, E, s.ndc, avg_diag=True)
+    assert np.allclose(res[0], res[1], rtol=0, atol=0)
+    assert np.allclose(res[0], want, rtol=1e-12, atol=1e-15)
