@@ -586,23 +586,38 @@ def squeeze_config(basis, conf):
     return out
 
 
-def nr_configurations(basis, configs, ndc, nd1=None):
+def nr_layout(basis, configs, ndc):
     """conf_pt's NR_Init (src/conf_pt.f90:500-570): consecutive relativistic
     configurations with equal squeezed shell lists form one non-relativistic
-    configuration.  Returns the determinant offsets of the NR configurations
-    (Ncnr + 1 ascending entries, the reference's Ndic plus the end).  With
-    nd1, an NR configuration may not straddle the CI / PT boundary (NR_Init
-    stops with an error there); ValueError."""
-    ends = np.concatenate([[0], np.cumsum(np.asarray(ndc, np.int64))])
-    offs = [0]
+    configuration.  Returns, per NR configuration (0-based), NRR (its first
+    relativistic configuration), NRN (how many), Ndcnr (its determinants),
+    Nvcnr (the shells of its relativistic configurations) and the
+    determinant offsets (Ncnr + 1 entries: the reference's Ndic plus the
+    end)."""
+    ndc = np.asarray(ndc, np.int64)
+    nrr, nrn, ndcnr, nvcnr = [], [], [], []
     prev = None
     for ic, conf in enumerate(configs):
         sq = squeeze_config(basis, conf)
-        if prev is not None and sq != prev:
-            offs.append(int(ends[ic]))
+        if prev is None or sq != prev:
+            nrr.append(ic)
+            nrn.append(0)
+            ndcnr.append(0)
+            nvcnr.append(0)
+        nrn[-1] += 1
+        ndcnr[-1] += int(ndc[ic])
+        nvcnr[-1] += len(conf)
         prev = sq
-    offs.append(int(ends[len(configs)]))
-    offs = np.asarray(offs, np.int64)
+    ndcnr = np.asarray(ndcnr, np.int64)
+    return {"nrr": np.asarray(nrr, np.int64), "nrn": np.asarray(nrn, np.int64), "ndcnr": ndcnr,
+            "nvcnr": np.asarray(nvcnr, np.int64), "offsets": np.concatenate([[0], np.cumsum(ndcnr)])}
+
+
+def nr_configurations(basis, configs, ndc, nd1=None):
+    """Determinant offsets of NR_Init's non-relativistic configurations
+    (nr_layout's offsets).  With nd1, an NR configuration may not straddle
+    the CI / PT boundary (NR_Init stops with an error there); ValueError."""
+    offs = nr_layout(basis, configs, ndc)["offsets"]
     if nd1 is not None and int(nd1) not in set(offs.tolist()):
         raise ValueError("a non-relativistic configuration straddles the CI / PT boundary")
     return offs
