@@ -1,14 +1,17 @@
-"""pdtm's reduction of a one-particle density matrix (RdcDM,
-src/pdtm.f90:2229-2441): the reduced density matrices of ranks 0, 1 and 2
-between the relativistic shells, the number of electrons and the occupation
-numbers of the (n, l) shells.
+"""pdtm's reductions of one-particle density and transition density
+matrices: RdcDM (src/pdtm.f90:2229-2441), the reduced density matrices of
+ranks 0, 1 and 2 between the relativistic shells, the number of electrons
+and the occupation numbers of the (n, l) shells; RdcTM (1681-2104), the
+reduced transition matrices of ranks 0 to 3 between two levels.
 
-The density matrix comes from the device (pci_gpu_density, pdtm's FormDM);
-this reduction is host work over O(shells^2 x 2j+1) numbers, as in the
-reference, which runs it on its master rank.  The hyperfine constants A and B
-and the g-factors that RdcDM forms next from these matrices need pdtm's
-radial integrals of the operators (DTM.INT, from the orbitals' radial
-functions); they are not formed here.
+The matrices come from the device (pci_gpu_density and
+pci_gpu_transition_density, pdtm's FormDM and FormTM); the reductions are
+host work over O(shells^2 x (2j+1)^2) numbers, as in the reference, which
+runs them on its master rank.  The amplitudes that pdtm forms next from the
+reduced matrices (hyperfine A and B, g-factors, E1/E2/E3/M1/M2/M3, EDM, PNC,
+anapole and magnetic-quadrupole amplitudes) need its radial integrals of
+the operators (DTM.INT, from the orbitals' radial functions); they are not
+formed here.
 
 Wigner 3j symbols are the exact ones of pci_b200.wigner (the reference's
 Fj3 evaluates the same quantity with log-factorials).
@@ -34,6 +37,12 @@ def _sgn(n: int) -> float:
 def _tj(j2a: int, k: int, j2b: int, m2: int) -> float:
     """(ja k jb; -m 0 m) with ja = j2a/2, jb = j2b/2, m = m2/2."""
     return three_j(j2a / 2, k, j2b / 2, -m2 / 2, 0, m2 / 2)
+
+
+@lru_cache(maxsize=None)
+def _tjq(j2a: int, k: int, j2b: int, ma2: int, q2: int, mb2: int) -> float:
+    """(ja k jb; -ma q mb) from doubled ja, jb, ma, q, mb."""
+    return three_j(j2a / 2, k, j2b / 2, -ma2 / 2, q2 / 2, mb2 / 2)
 
 
 def rdc_shells(nh, jz, jj, imin, imax):
@@ -116,3 +125,78 @@ def reduced_density(ro, basis, nh, jz, tj, mj2, imin=0, imax=None):
                     occ.append((nk, lk, r[k, k]))
         rro[rank] = r
     return {"shells": shells, "rro": rro, "nel": nel, "occ": occ, "J": tjr, "M": mj2 / 2}
+
+
+def transition_parity(ro, nh, ll, imin=0, imax=None):
+    """FormTM's parity of a transition (src/pdtm.f90:1614-1630): +1 or -1
+    from the orbitals of the largest |Ro| element (the first in row-major
+    order among equal ones)."""
+    ro = np.asarray(ro, np.float64)
+    if imax is None:
+        imax = ro.shape[0] - 1
+    sub = np.abs(ro[imin:imax + 1, imin:imax + 1])
+    if not sub.any():
+        raise ValueError("the transition density is zero")
+    i, k = np.unravel_index(int(np.argmax(sub)), sub.shape)
+    li, lk = int(ll[int(nh[imin + i]) - 1]), int(ll[int(nh[imin + k]) - 1])
+    return 1 - 2 * ((li + lk) % 2)
+
+
+def reduced_transition(ro, basis, nh, jz, tj1, mj1_2, tj2, mj2_2, parity=None, imin=0, imax=None):
+    """RdcTM for a transition from level 1 (J1 = tj1, 2 M1 = mj1_2) to level
+    2 (tj2, mj2_2): ro the transition density ([i, k] = Ro(initial m-state
+    i+1, final m-state k+1), pci_gpu_transition_density's layout); parity
+    +1 / -1 (None: transition_parity).  J values are rounded to
+    half-integers as RdcDM does.
+
+    For rank t = 0..3 and shells a (initial), b (final) whose l_a + l_b has
+    the transition's parity,
+    Rro_t(a, b) = sum over m_a, m_b of (-1)^(j_b - m_b) (j_b t j_a; -m_b q m_a)
+    Ro(a m_a, b m_b) / [(-1)^(J2 - M2) (J2 t J1; -M2 q M1)], q = M2 - M1,
+    each side times sqrt(2 j_a + 1), sqrt(2 J1 + 1) for t = 0; a rank whose
+    denominator vanishes is None.  Returns dict shells, rro ([4]), parity,
+    trace (of ro over imin..imax)."""
+    ro = np.asarray(ro, np.float64)
+    nh = np.asarray(nh)
+    jz = np.asarray(jz)
+    nn, ll, jj = basis.nn, basis.ll, basis.jj
+    if imax is None:
+        imax = ro.shape[0] - 1
+    if parity is None:
+        parity = transition_parity(ro, nh, ll, imin, imax)
+    j1 = int(tj1 + tj1 + 0.1)
+    j2 = int(tj2 + tj2 + 0.1)
+    q2 = mj2_2 - mj1_2
+    spans = rdc_shells(nh, jz, jj, imin, imax)
+    shells = []
+    for a, b in spans:
+        no = int(nh[a]) - 1
+        if int(nh[b]) - 1 != no or np.any(np.diff(jz[a:b + 1]) != 2):
+            raise ValueError(f"RdcTM: wrong definition of shell {len(shells)}")
+        shells.append((int(nn[no]), int(ll[no]), int(jj[no]), a, b))
+    want_odd = (1 - parity) // 2
+    rro = [None, None, None, None]
+    for rank in range(4):
+        c = _sgn((j2 - mj2_2) // 2) * _tjq(j2, rank, j1, mj2_2, q2, mj1_2)
+        if c == 0.0:
+            continue
+        if rank == 0:
+            c *= math.sqrt(j1 + 1)
+        r = np.zeros((len(shells), len(shells)))
+        for k, (nk, lk, jk, ik1, ik2) in enumerate(shells):
+            for q, (nq, lq, jq, il1, il2) in enumerate(shells):
+                if (lk + lq) % 2 != want_odd:
+                    continue
+                s = 0.0
+                for il in range(il1, il2 + 1):
+                    ml = int(jz[il])
+                    for ik in range(ik1, ik2 + 1):
+                        x = ro[ik, il]
+                        if x != 0.0:
+                            s += _sgn((jq - ml) // 2) * _tjq(jq, rank, jk, ml, q2, int(jz[ik])) * x
+                if rank == 0:
+                    s *= math.sqrt(jk + 1)
+                r[k, q] = s / c
+        rro[rank] = r
+    return {"shells": shells, "rro": rro, "parity": parity,
+            "trace": float(np.trace(ro[imin:imax + 1, imin:imax + 1]))}

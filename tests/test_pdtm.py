@@ -96,3 +96,85 @@ def test_reduction_of_device_density():
             assert got["rro"][rank] is None
         else:
             assert np.allclose(got["rro"][rank], want["rro"][rank], rtol=1e-10, atol=1e-12)
+
+
+def _sp_basis():
+    """2s, 2p1/2, 2p3/2 m-states."""
+    b = S.make_basis([(2, 0), (2, 1)])
+    nh = np.array([1, 1, 2, 2, 3, 3, 3, 3])
+    jz = np.array([-1, 1, -1, 1, -3, -1, 1, 3])
+    return b, nh, jz
+
+
+@pytest.mark.parametrize("ia,ib", [(1, 7), (1, 6), (1, 5), (2, 4), (0, 3), (6, 6), (5, 2)])
+def test_one_electron_transition_is_one(ia, ib):
+    """One electron from m-state ia to ib (2s, 2p1/2, 2p3/2 m-states): every
+    rank the 3j symbols allow (the parity of l_a + l_b selects the shell
+    pairs) reduces to 1 on that shell pair, the others are None."""
+    b, nh, jz = _sp_basis()
+    ma2, mb2 = int(jz[ia]), int(jz[ib])
+    ro = np.zeros((8, 8))
+    ro[ia, ib] = 1.0
+    ja, jb = b.jj[nh[ia] - 1] / 2, b.jj[nh[ib] - 1] / 2
+    r = D.reduced_transition(ro, b, nh, jz, ja, ma2, jb, mb2)
+    assert r["parity"] == (1 if (b.ll[nh[ia] - 1] + b.ll[nh[ib] - 1]) % 2 == 0 else -1)
+    ka = [k for k, sh in enumerate(r["shells"]) if sh[3] <= ia <= sh[4]][0]
+    kb = [k for k, sh in enumerate(r["shells"]) if sh[3] <= ib <= sh[4]][0]
+    nonzero = 0
+    for rank in range(4):
+        if r["rro"][rank] is None:
+            continue
+        nonzero += 1
+        want = np.zeros_like(r["rro"][rank])
+        want[ka, kb] = 1.0
+        assert np.allclose(r["rro"][rank], want, atol=1e-14), rank
+    assert nonzero >= 1
+
+
+@pytest.mark.parametrize("name", ["cfg1", "small3"])
+def test_transition_to_itself_reduces_as_the_density(name):
+    """RdcTM of a level to itself (q = 0, even parity) equals RdcDM's
+    matrices in ranks 0-2."""
+    import oracle as O
+    s = get_system(name)
+    (rp, col, val, *_), (jr, jc, jv) = oracle_h(name)
+    H = O.csr_to_dense(s.nd, rp, col, val)
+    w, V = np.linalg.eigh(H)
+    x = V[:, 1]
+    tj = O.j_av(jr, jc, jv, x, s.nd)
+    o = O.Oracle(s)
+    ro = o.density(x, trd=0.0)
+    tm = o.transition_density(o, x, x, trd=0.0)
+    dm = D.reduced_density(ro, s.basis, s.nh, s.jz, tj=tj, mj2=s.mj)
+    tr = D.reduced_transition(tm, s.basis, s.nh, s.jz, tj, s.mj, tj, s.mj)
+    assert tr["parity"] == 1
+    for rank in range(3):
+        if dm["rro"][rank] is None:
+            assert tr["rro"][rank] is None
+        else:
+            assert np.allclose(tr["rro"][rank], dm["rro"][rank], atol=1e-12)
+
+
+@pytest.mark.gpu
+def test_reduction_of_device_transition_density():
+    import oracle as O
+    from pci_b200.capi import Engine
+    from test_density import _flipped
+    si, sf = get_system("small3"), _flipped("small3")
+    rng = np.random.default_rng(8)
+    bi = rng.standard_normal(si.nd); bi /= np.linalg.norm(bi)
+    bf = rng.standard_normal(sf.nd); bf /= np.linalg.norm(bf)
+    want_ro = O.Oracle(sf).transition_density(O.Oracle(si), bi, bf)
+    with Engine(0) as ei, Engine(0) as ef:
+        ei.load_system(si)
+        ef.load_system(sf)
+        got_ro = ef.transition_density(ei, bi, bf)
+    args = (si.basis, si.nh, si.jz, 1.5, si.mj, 2.5, sf.mj)
+    want = D.reduced_transition(want_ro, *args)
+    got = D.reduced_transition(got_ro, *args)
+    assert got["parity"] == want["parity"] == -1
+    for rank in range(4):
+        if want["rro"][rank] is None:
+            assert got["rro"][rank] is None
+        else:
+            assert np.allclose(got["rro"][rank], want["rro"][rank], rtol=1e-10, atol=1e-12)
