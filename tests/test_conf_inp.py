@@ -1,0 +1,101 @@
+"""CONF.INP (src/conf_init.f90:37-135, 215-312; shell codes decoded as in
+src/pconf.F90:506-529) read and written by pci_b200/conf_inp.py, and
+conf_pt's CONF_new.INP (src/conf_pt.f90:1130-1264)."""
+import numpy as np
+import pytest
+
+from conftest import get_system, oracle_h
+
+from pci_b200 import conf_inp as C
+from pci_b200 import conf_pt as P
+from pci_b200 import system as S
+
+SAMPLE = """ Cs test
+Z = 55.0
+Am = 132.9
+J = 0.5
+Jm = 0.5
+Nso = 2
+Nc = 3
+Kv = 4
+Nlv = 5
+Ne = 3   # three valence electrons
+Kl4 = 1
+Nc4 = 2
+Crt4 = 0.0001
+
+    -0.1001     0.2102
+   1 0.2102    -0.2101
+   2 0.2101
+     0.3001     0.3101
+   3
+     0.3002    -0.3101
+"""
+
+
+def test_shell_codes():
+    assert C.decode_qnl(0.2102) == (2, 1, 3, -2, 2)          # 2p3/2, two electrons
+    assert C.decode_qnl(-0.2101) == (2, 1, 1, 1, 1)          # 2p1/2, one electron
+    assert C.decode_qnl(-0.1001) == (1, 0, -1, 0, 1)         # as pconf decodes a minus on an s shell
+    assert C.decode_qnl(0.4012) == (4, 0, 1, -1, 12)
+    for n, l, j2, q in [(2, 1, 3, 2), (3, 2, 3, 4), (5, 0, 1, 1), (4, 3, 7, 8)]:
+        assert C.decode_qnl(C.encode_qnl(n, l, j2, q))[:3] == (n, l, j2)
+        assert C.decode_qnl(C.encode_qnl(n, l, j2, q))[4] == q
+    with pytest.raises(ValueError):
+        C.encode_qnl(2, 1, 5, 1)
+
+
+def test_read_sample():
+    r = C.read_conf_inp(SAMPLE)
+    assert r["name"].strip() == "Cs test"
+    p = r["params"]
+    assert (p["Z"], p["NSO"], p["NC"], p["NE"], p["KL4"], p["NC4"]) == (55.0, 2, 3, 3, 1, 2)
+    assert p["CRT4"] == pytest.approx(1e-4) and p["KBRT"] == 0 and p["CUT0"] == pytest.approx(0.001)
+    assert r["core"] == [pytest.approx(-0.1001), pytest.approx(0.2102)]
+    # configuration 2 runs over two lines until it holds Ne = 3 electrons;
+    # configuration 3's first line is blank apart from its number
+    got = [[round(x, 4) for x in c] for c in r["configs"]]
+    assert got == [[0.2102, -0.2101], [0.2101, 0.3001, 0.3101], [0.3002, -0.3101]]
+
+
+def test_write_read_round_trip_of_a_system():
+    s = get_system("small3")
+    codes = C.configs_to_qnl(s.basis, s.configs)
+    params = {"Z": 55.0, "AM": 133.0, "J": 0.5, "JM": s.mj / 2, "NSO": 0, "NC": len(codes), "KV": 4,
+              "NLV": 6, "NE": s.ne}
+    r = C.read_conf_inp(C.write_conf_inp("small3", params, [], codes))
+    assert r["params"]["NC"] == s.nc and r["params"]["NE"] == s.ne
+    assert C.configs_from_qnl(s.basis, r["configs"]) == [[(int(a), int(b)) for a, b in c] for c in s.configs]
+
+
+def test_new_conf_inp_reads_back_as_the_new_ci_space():
+    import oracle as O
+    s = get_system("small3")
+    lay = S.nr_layout(s.basis, s.configs, s.ndc)
+    offs = lay["offsets"]
+    ncnrci = len(lay["nrn"]) // 3
+    nd1 = int(offs[ncnrci])
+    (rp, col, val, *_), _ = oracle_h("small3")
+    H = O.csr_to_dense(s.nd, rp, col, val)
+    w, V = np.linalg.eigh(H[:nd1, :nd1])
+    X = V[:, :3]
+    nd0 = P.weight_ci(X, lay["ndcnr"][:ncnrci], lay["nrn"][:ncnrci], cut0=1e-3)["nd0"]
+    dEg, dVg = O.pt2_groups(H, nd1, nd0, X[:nd0], w[:3], offs[ncnrci:], s.ndc)
+    sel = P.select_configurations(lay, ncnrci, s.ndc, X, dEg, dVg, cut0=1e-3, nc4=40)
+    codes = C.configs_to_qnl(s.basis, s.configs)
+    params = {"Z": 55.0, "AM": 133.0, "J": 0.5, "JM": s.mj / 2, "NSO": 0, "NC": s.nc, "KV": 4, "NLV": 6,
+              "NE": s.ne, "KL4": 1, "NC4": 40}
+    parsed = C.read_conf_inp(C.write_conf_inp("small3", params, [], codes))
+    text = C.new_conf_inp(parsed, sel, lay)
+    assert "<CI<" in text and "(reordered)" in text.splitlines()[0]
+    back = C.read_conf_inp(text)
+    assert back["name"].strip() == "small3"
+    assert back["params"]["NC"] == sel["nci"]
+    assert (back["params"]["KL4"], back["params"]["NC4"]) == (sel["kl4"], sel["nc4"])
+    want = [[(int(a), int(b)) for a, b in s.configs[ic]] for ic in sel["conf_order"][:sel["nci"]]]
+    assert C.configs_from_qnl(s.basis, back["configs"]) == want
+    # the whole list, read with Nc = all configurations, is every configuration in the new order
+    full = C.read_conf_inp(text.replace(f"NC = {sel['nci']}", f"NC = {s.nc}"))
+    assert len(full["configs"]) == s.nc
+    assert C.configs_from_qnl(s.basis, full["configs"]) == [[(int(a), int(b)) for a, b in s.configs[ic]]
+                                                           for ic in sel["conf_order"]]
