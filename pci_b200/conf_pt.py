@@ -182,6 +182,25 @@ def new_conf_list(order, w, nrr, nrn, ndc, nc_0, nc4, maxnd0, ncnrci):
             "weights": [10.0 ** w[k, 0] for k in order]}
 
 
+def pt_level_table(E, dE, J=None):
+    """PTE's result table (src/conf_pt.f90:909-925) in the reference's sign
+    convention: per level n, (n, J, Ev0, DEL0, dE(PT2), Ev(PT2), DEL) with
+    Ev0 = -E_n (E the engine's eigenvalues of H), dE(PT2) = -dE_n (the
+    engine's pt2 result), Ev(PT2) = Ev0 + dE(PT2), and the intervals from
+    the first level in cm^-1, DEL0 = (Ev0_1 - Ev0_n) 2 Ry and DEL = DEL0 +
+    (dE_1 - dE_n) 2 Ry with the reference's dE."""
+    from .conf_lsj import DPRY
+    en = -np.asarray(E, np.float64)
+    ey = -np.asarray(dE, np.float64)
+    J = np.full(len(en), np.nan) if J is None else np.asarray(J, np.float64)
+    rows = []
+    for n in range(len(en)):
+        des0 = (en[0] - en[n]) * 2 * DPRY
+        des = des0 + (ey[0] - ey[n]) * 2 * DPRY
+        rows.append((n + 1, float(J[n]), float(en[n]), float(des0), float(ey[n]), float(en[n] + ey[n]), float(des)))
+    return rows
+
+
 def select_configurations(layout, ncnrci, ndc, X_ci, dEg, dVg, cut0, ktf=5, kvar=1, nc4=None, maxnd0=3000):
     """conf_pt's selection end to end: Weight_CI on the CI vectors, the PT
     weights from pci_gpu_pt2_groups' sums over the PT NR configurations,
