@@ -305,7 +305,11 @@ int hb_form_h(pci_gpu *h, int value_prec, int64_t *numh, int64_t *numzero, doubl
     cudaEventElapsedTime(&tadj, a0, a1);
     cudaEventDestroy(a0); cudaEventDestroy(a1);
     RowStatsOut hs;
-    if ((rc = rows_dispatch(h, 0, value_prec, h->H, &hs))) return rc;
+    h->h_from_tiles = false;
+    if ((rc = rows_dispatch(h, 0, value_prec, h->H, &hs))) {
+        csr_free(h->H);   // no half-built matrix stays resident
+        return rc;
+    }
     h->st_adj = tadj;
     h->st_formh += tadj;
     h->st_pairs = (double)hs.pairs;
@@ -363,7 +367,11 @@ int hb_form_h_pt(pci_gpu *h, int64_t nd1, int64_t nd0, int64_t row_lo, int64_t r
     cudaEventDestroy(a0); cudaEventDestroy(a1);
     RowStatsOut hs;
     h->h_pt_nd1 = -1;
-    if ((rc = rows_dispatch(h, 0, value_prec, h->H, &hs))) return rc;
+    h->h_from_tiles = false;
+    if ((rc = rows_dispatch(h, 0, value_prec, h->H, &hs))) {
+        csr_free(h->H);   // no half-built matrix stays resident
+        return rc;
+    }
     h->st_adj = tadj;
     h->st_formh += tadj;
     h->st_pairs = (double)hs.pairs;
