@@ -99,3 +99,38 @@ def test_new_conf_inp_reads_back_as_the_new_ci_space():
     assert len(full["configs"]) == s.nc
     assert C.configs_from_qnl(s.basis, full["configs"]) == [[(int(a), int(b)) for a, b in s.configs[ic]]
                                                            for ic in sel["conf_order"]]
+
+
+def test_reference_documented_sample():
+    """The head of the CONF.INP that the reference's pconf documentation
+    shows (Ir17+, even parity; tests/golden/conf_inp_doc_head.txt, made by
+    make_conf_inp_fixture.py): header keys with comments, 14 core shells over
+    three lines, and eight configurations, each preceded by lines carrying
+    only a number (the reader takes them as empty).  Core and valence
+    electrons add up to Ir17+'s 60."""
+    import pathlib
+    text = (pathlib.Path(__file__).parent / "golden" / "conf_inp_doc_head.txt").read_text()
+    text = text.replace("Nc = 481", "Nc =   8")          # the documentation shows the first 8
+    r = C.read_conf_inp(text)
+    assert r["name"].strip() == "Ir17+_even"
+    p = r["params"]
+    assert (p["Z"], p["AM"], p["J"], p["JM"]) == (77.0, 193.0, 2.0, 2.0)
+    assert (p["NSO"], p["NC"], p["KV"], p["NLV"], p["NE"], p["KL4"], p["NC4"]) == (14, 8, 4, 5, 14, 1, 28)
+    assert (p["KOUT"], p["NCPT"], p["N_IT"], p["KBRT"], p["K_IS"]) == (0, 1132, 100, 1, 0)
+    assert p["CRT4"] == pytest.approx(1e-4) and p["CUT0"] == pytest.approx(1e-4)
+    assert p["GNUC"] == pytest.approx(1.07) and p["C_IS"] == 0.0
+    core = [C.decode_qnl(x) for x in r["core"]]
+    assert len(core) == 14
+    assert [(n, l, j2) for n, l, j2, _, _ in core[:4]] == [(1, 0, 1), (2, 0, 1), (2, 1, 1), (2, 1, 3)]
+    assert sum(q for *_, q in core) == 46
+    assert len(r["configs"]) == 8
+    for conf in r["configs"]:
+        assert sum(C.decode_qnl(x)[4] for x in conf) == p["NE"]
+    assert sum(q for *_, q in core) + p["NE"] == 77 - 17
+    # configuration 1 is 4f5/2^6 4f7/2^8; configuration 5 has a 5p1/2 electron
+    assert [C.decode_qnl(x)[:3] + (C.decode_qnl(x)[4],) for x in r["configs"][0]] == [(4, 3, 5, 6), (4, 3, 7, 8)]
+    assert C.decode_qnl(r["configs"][4][2])[:3] == (5, 1, 1)
+    # written back in this module's layout and read again: the same shells
+    again = C.read_conf_inp(C.write_conf_inp(r["name"], p, r["core"], r["configs"]))
+    assert again["configs"] == [[pytest.approx(x) for x in c] for c in r["configs"]]
+    assert again["core"] == [pytest.approx(x) for x in r["core"]]
