@@ -51,12 +51,32 @@ module pci_gpu_mod
        import; type(c_ptr), value :: h; integer(c_int32_t), value :: which
        integer(c_int64_t) :: nrows, nnz
      end function
+     ! WriteMatrixCSR's arrays (matrix_io.f90:689-799): the whole resident CSR of H or J^2
+     integer(c_int) function pci_gpu_get_csr(h, which, rowptr, col, val) bind(C)
+       import; type(c_ptr), value :: h; integer(c_int32_t), value :: which
+       integer(c_int64_t) :: rowptr(*); integer(c_int32_t) :: col(*); real(c_double) :: val(*)
+     end function
+     ! ReadMatrixCSR (matrix_io.f90:801-939), Kl = 1: a stored CSR and its Hmin made resident
+     integer(c_int) function pci_gpu_set_csr(h, which, Nd, nnz, rowptr, col, val, Hmin) bind(C)
+       import; type(c_ptr), value :: h; integer(c_int32_t), value :: which
+       integer(c_int64_t), value :: Nd, nnz
+       integer(c_int64_t) :: rowptr(*); integer(c_int32_t) :: col(*); real(c_double) :: val(*)
+       real(c_double), value :: Hmin
+     end function
      ! one rank's row range of H (which 0) or J^2 (which 1), as RedistributeHamCSR leaves it
      integer(c_int) function pci_gpu_get_csr_rows(h, which, row_lo, row_hi, rowptr, col, val) bind(C)
        import; type(c_ptr), value :: h; integer(c_int32_t), value :: which
        integer(c_int64_t), value :: row_lo, row_hi
        integer(c_int64_t) :: rowptr(*)
        type(c_ptr), value :: col, val
+     end function
+     ! Jterm's table (determinants.f90:227-325): returns Njd, up to cap 2J values in out
+     integer(c_int32_t) function pci_gpu_jterms(h, out, cap) bind(C)
+       import; type(c_ptr), value :: h; integer(c_int32_t) :: out(*); integer(c_int32_t), value :: cap
+     end function
+     ! timings and counters of the last calls (the list in pci_gpu.h); returns the number written
+     integer(c_int32_t) function pci_gpu_stats(h, out, n) bind(C)
+       import; type(c_ptr), value :: h; real(c_double) :: out(*); integer(c_int32_t), value :: n
      end function
      ! kLSJ = 1 (lsj, pconf.F90:2672-2962): J, L, S of nv vectors X(Nd, nv)
      integer(c_int) function pci_gpu_lsj(h, X, nv, xj, xl, xs) bind(C)
@@ -66,6 +86,10 @@ module pci_gpu_mod
      ! kCSF = 1: jbasis + formh_sym (csf.f90); the CSF H replaces H on the handle
      integer(c_int) function pci_gpu_form_csf(h, ncsf, numh) bind(C)
        import; type(c_ptr), value :: h; integer(c_int64_t) :: ncsf, numh
+     end function
+     ! CSFs of each configuration (jbasis's per-configuration counts): per_conf(Nc)
+     integer(c_int) function pci_gpu_csf_counts(h, per_conf) bind(C)
+       import; type(c_ptr), value :: h; integer(c_int32_t) :: per_conf(*)
      end function
      ! unsym (csf.f90:1088-1134): Y(Ncsf, nv) -> X(Nd, nv)
      integer(c_int) function pci_gpu_csf_to_det(h, Y, nv, X) bind(C)
