@@ -12,10 +12,10 @@ on each line its shells end at the first empty or zero field, so lines
 whose fields are blank (conf_pt's weight lines, its `<CI<` marker) add
 nothing.
 
-A shell code is +-0.nlqq (pconf's decoding, src/pconf.F90:506-529): n and l
-one digit each, qq the occupation, the sign + for j = l + 1/2 and - for
-j = l - 1/2; the orbital is the basis orbital with that n and
-kappa = -sign * (j + 1/2).
+A shell code is +-(n/10 + l/100 + qq/10000) (pconf's decoding,
+src/pconf.F90:506-529): 0.nlqq for n < 10 and 1.0lqq for n = 10, l one digit,
+qq the occupation, the sign + for j = l + 1/2 and - for j = l - 1/2; the
+orbital is the basis orbital with that n and kappa = -sign * (j + 1/2).
 """
 from __future__ import annotations
 
@@ -43,8 +43,8 @@ def decode_qnl(x: float):
 
 def encode_qnl(n: int, l: int, j2: int, q: int) -> float:
     """The shell code of q electrons in (n, l, j = j2/2)."""
-    if not (0 <= n <= 9 and 0 <= l <= 9 and 0 <= q <= 99):
-        raise ValueError("a shell code holds one digit of n and l and two of q")
+    if not (0 <= n <= 99 and 0 <= l <= 9 and 0 <= q <= 99):
+        raise ValueError("a shell code holds n < 100, one digit of l and two of q")
     if j2 not in (2 * l + 1, 2 * l - 1):
         raise ValueError("j must be l +- 1/2")
     sign = 1.0 if j2 == 2 * l + 1 else -1.0

@@ -134,3 +134,34 @@ def test_reference_documented_sample():
     again = C.read_conf_inp(C.write_conf_inp(r["name"], p, r["core"], r["configs"]))
     assert again["configs"] == [[pytest.approx(x) for x in c] for c in r["configs"]]
     assert again["core"] == [pytest.approx(x) for x in r["core"]]
+
+
+def test_reference_pylib_written_configurations():
+    """Configuration lines that the reference's own py-lib (orbitals.py, as
+    create_conf_inp.py uses it) wrote for six non-relativistic
+    configurations (tests/golden/conf_inp_pylib.txt, made by
+    make_conf_inp_pylib_fixture.py): the reader finds the 30 relativistic
+    configurations, each shell decodes to what py-lib's own decoder says
+    (n = 10 included), and NR_Init's grouping of them (squeeze of adjacent
+    shells of one n, l) gives py-lib's expansion groups back."""
+    import json
+    import pathlib
+    g = pathlib.Path(__file__).parent / "golden"
+    r = C.read_conf_inp((g / "conf_inp_pylib.txt").read_text())
+    want = json.loads((g / "conf_inp_pylib.json").read_text())
+    assert len(r["configs"]) == len(want["configs"]) == r["params"]["NC"] == 30
+    lname = "spdfghikl"
+    for conf, exp in zip(r["configs"], want["configs"]):
+        got = []
+        for x in conf:
+            n, l, j2, kappa, q = C.decode_qnl(x)
+            got.append([f"{n}{lname[l]}", f"{j2}/2", q])
+        assert got == exp
+        assert sum(q for *_, q in exp) == r["params"]["NE"]
+    basis = S.make_basis([(4, 3), (5, 2), (6, 0), (6, 1), (10, 0)])
+    configs = C.configs_from_qnl(basis, r["configs"])
+    lay = S.nr_layout(basis, configs, [1] * len(configs))
+    assert lay["nrn"].tolist() == want["group_sizes"]
+    # and this module writes the same shell codes back
+    again = C.read_conf_inp(C.write_conf_inp("again", r["params"], [], C.configs_to_qnl(basis, configs)))
+    assert again["configs"] == [[pytest.approx(x) for x in c] for c in r["configs"]]
