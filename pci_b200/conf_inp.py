@@ -19,6 +19,8 @@ orbital is the basis orbital with that n and kappa = -sign * (j + 1/2).
 """
 from __future__ import annotations
 
+import math
+
 # ReadConfInp's defaults of the optional keys (conf_init.f90:219-231)
 DEFAULTS = {"K_IS": 0, "C_IS": 0.0, "KLOW": 0, "KBRT": 0, "KOUT": 1, "GJ": 0.0, "N_IT": 20, "CUT0": 0.001,
             "NCPT": 0, "GNUC": 1.0, "QNUC": 1.0}
@@ -217,3 +219,58 @@ def new_conf_inp(parsed, selection, layout):
         pos += int(nrn[k])
     return write_conf_inp(parsed["name"].ljust(16)[:16] + " (reordered)", params, parsed["core"], parsed["configs"],
                           order=selection["conf_order"], ci_marker_at=marker, nr_lines=nr_lines)
+
+
+def system_from_files(conf_inp, conf_int, conf_gnt=None, name=None):
+    """A CISystem from the reference's input files, as pconf assembles it:
+    CONF.INP (text, or a path) for the configurations and the job keys;
+    CONF.INT for the orbital table (Nn, Kk, Ll, Jj of orbitals 1..Nsu, which
+    the reference's Rint reads over CONF.DAT's, src/integrals.f90:35-52), Nso,
+    the core energy and the radial integrals (Nx = sqrt(nrd)); CONF.GNT for
+    the Gaunt factors (the exact 3j table of pci_b200.wigner when absent).
+    Determinants are Dinit's over all orbitals' m-states (core included, as
+    the reference numbers them); configurations without a determinant of
+    2M = 2|Jm| are kept, as in the reference."""
+    import os
+
+    import numpy as np
+
+    from . import files, wigner
+    from .system import Basis, CISystem, enumerate_determinants, m_states
+
+    text = conf_inp
+    if "\n" not in str(conf_inp) and os.path.exists(str(conf_inp)):
+        with open(conf_inp) as f:
+            text = f.read()
+    parsed = read_conf_inp(text)
+    p = parsed["params"]
+    ci = files.read_int(conf_int)
+    h = ci.header
+    if int(h.nso) != p["NSO"]:
+        raise ValueError(f"CONF.INT has Nso = {h.nso}, CONF.INP {p['NSO']}")
+    orb = ci.orbitals
+    basis = Basis(nn=orb[:, 0].astype(np.int32), ll=orb[:, 2].astype(np.int32), kk=orb[:, 1].astype(np.int32),
+                  jj=orb[:, 3].astype(np.int32), nso=int(h.nso))
+    configs = configs_from_qnl(basis, parsed["configs"])
+    ne = p["NE"]
+    mj = int(2 * abs(p["JM"]) + 0.01)
+    iarr, ndc = enumerate_determinants(basis, configs, ne, mj)
+    nsu = max(ni for c in configs for ni, _ in c)
+    if nsu > basis.ns:
+        raise ValueError(f"the configurations reach orbital {nsu}; CONF.INT holds {basis.ns}")
+    jz, nh, _ = m_states(basis, nsu)
+    nx = int(round(math.sqrt(h.nrd)))
+    lut = files.hint_lut(ci.rint1, ci.iint1, nx)
+    if conf_gnt is not None:
+        nlx, per, gin, ggnt = files.read_gnt(conf_gnt)
+        glut = files.gaunt_lut(gin, ggnt)
+    else:
+        nlx, gin, ggnt, per = wigner.gaunt_table(int(basis.ll[:nsu].max()))
+        glut = wigner.gaunt_lut(gin, ggnt)
+    params = dict(Nlv=p.get("NLV", 6), N_it=p.get("N_IT", 20), Crt4=p.get("CRT4", 1e-4), Kl4=p.get("KL4", 1),
+                  Kv=p.get("KV", 4), MaxNd0=3000, Nc4=p.get("NC4", len(configs)), KXIJ=0, admix_crit=1e-6)
+    return CISystem(name=name or parsed["name"].strip(), basis=basis, ne=ne, mj=mj, configs=configs, iarr=iarr,
+                    ndc=ndc, jz=jz, nh=nh, nsu=nsu, nx=nx, hint_lut=lut, rint2=ci.rint2, iint2=ci.iint2,
+                    iint3=ci.iint3, kbrt=int(h.kbrt), nlx=nlx, gaunt_in=gin, gaunt_gnt=ggnt, gaunt_per_wave=per,
+                    gaunt_lut=glut, gj=float(p.get("GJ", 0.0)), xj_av=float(p.get("J", 0.0)),
+                    ecore=float(h.ecore), params=params)

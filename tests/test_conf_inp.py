@@ -165,3 +165,49 @@ def test_reference_pylib_written_configurations():
     # and this module writes the same shell codes back
     again = C.read_conf_inp(C.write_conf_inp("again", r["params"], [], C.configs_to_qnl(basis, configs)))
     assert again["configs"] == [[pytest.approx(x) for x in c] for c in r["configs"]]
+
+
+def _write_inputs(tmp_path, s, core_codes=(), nso=0):
+    """CONF.INP, CONF.INT and CONF.GNT of a system, as the reference's
+    programs would leave them."""
+    from pci_b200 import files
+    b = s.basis
+    nz = np.nonzero(s.hint_lut)[0]
+    orb = np.stack([b.nn[:s.nsu], b.kk[:s.nsu], b.ll[:s.nsu], b.jj[:s.nsu]], axis=1)
+    files.write_int(tmp_path / "CONF.INT", ns=s.nsu, nso=nso, nsp=len(core_codes) + 3, ecore=-7.5, orbitals=orb,
+                    rint1=s.hint_lut[nz], iint1=(nz + 1).astype(np.int32), rint2=s.rint2, iint2=s.iint2,
+                    iint3=s.iint3, kbrt=s.kbrt, nlist=4, nx=s.nx)
+    files.write_gnt(tmp_path / "CONF.GNT", s.nlx, s.gaunt_per_wave, s.gaunt_in, s.gaunt_gnt)
+    params = {"Z": 20.0, "AM": 40.0, "J": 0.5, "JM": s.mj / 2, "NSO": nso, "NC": s.nc, "KV": 4, "NLV": 6,
+              "NE": s.ne, "KL4": 1, "NC4": 5, "CRT4": 1e-6, "N_IT": 50, "GJ": 0.0}
+    text = C.write_conf_inp("from files", params, list(core_codes), C.configs_to_qnl(b, s.configs))
+    (tmp_path / "CONF.INP").write_text(text)
+
+
+@pytest.mark.parametrize("name", ["tiny", "small3"])
+def test_system_from_reference_files(tmp_path, name):
+    """A system written out as the reference's inputs (CONF.INP, CONF.INT,
+    CONF.GNT) and read back through system_from_files is the same system:
+    determinants, m-states, integrals and Gaunt factors equal."""
+    s = get_system(name)
+    _write_inputs(tmp_path, s)
+    r = C.system_from_files(tmp_path / "CONF.INP", tmp_path / "CONF.INT", tmp_path / "CONF.GNT")
+    assert (r.ne, r.mj, r.nsu, r.nx, r.kbrt) == (s.ne, s.mj, s.nsu, s.nx, s.kbrt)
+    assert np.array_equal(r.iarr, s.iarr) and np.array_equal(r.ndc, s.ndc)
+    assert np.array_equal(r.jz, s.jz) and np.array_equal(r.nh, s.nh)
+    assert np.array_equal(r.hint_lut, s.hint_lut) and np.array_equal(r.rint2, s.rint2)
+    assert np.array_equal(r.iint2, s.iint2) and np.array_equal(r.iint3, s.iint3)
+    assert np.array_equal(r.gaunt_lut, s.gaunt_lut)
+    assert r.ecore == -7.5 and r.params["Nc4"] == 5 and r.params["N_it"] == 50
+    # without CONF.GNT the exact 3j table stands in
+    r2 = C.system_from_files(tmp_path / "CONF.INP", tmp_path / "CONF.INT")
+    assert np.allclose(r2.gaunt_lut, s.gaunt_lut, rtol=0, atol=1e-15)
+
+
+def test_system_from_files_checks_nso(tmp_path):
+    s = get_system("tiny")
+    _write_inputs(tmp_path, s)
+    text = (tmp_path / "CONF.INP").read_text().replace("NSO = 0", "NSO = 1\n     0.1002", 1)
+    (tmp_path / "CONF.INP").write_text(text)
+    with pytest.raises(ValueError):
+        C.system_from_files(tmp_path / "CONF.INP", tmp_path / "CONF.INT")
