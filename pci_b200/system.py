@@ -321,16 +321,22 @@ def make_integrals(basis: Basis, nsu: int, seed: int, nx: int = NX_DEFAULT,
 def make_system(name: str, shells, ne: int, mj: int, parity: int, refs,
                 seed: int, level: int = 2, r2_dtype=np.float64, kbrt: int = 0,
                 orbitals=None, params=None, gj: float = 0.0, xj_av: float = 0.0,
-                drop_empty: bool = True, max_nd=None) -> CISystem:
+                drop_empty: bool = True, max_nd=None, nso: int = 0) -> CISystem:
     """Build a seeded synthetic system.
 
     ``refs`` holds reference configurations as lists of orbital indices, one per
     electron (1-based).  Configurations are all excitations up to ``level`` of
     the references with the given parity; determinants have 2M = mj.  With
     ``max_nd`` the configuration list is cut after the first configuration at
-    which the determinant count reaches ``max_nd``.
+    which the determinant count reaches ``max_nd``.  With ``nso`` the first
+    nso orbitals are closed core shells (pconf's Nso): their m-states are
+    numbered first, as Dinit numbers them, no determinant occupies them, and
+    the integrals are keyed from orbital Nso + 1.
     """
     basis = make_basis(shells)
+    basis.nso = int(nso)
+    if nso and orbitals is None:
+        orbitals = list(range(nso + 1, basis.ns + 1))
     configs = sd_excitations(basis, refs, parity, mj, level, orbitals)
     if max_nd is not None:
         configs = _truncate_configs(basis, configs, ne, mj, int(max_nd))

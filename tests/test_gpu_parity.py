@@ -371,3 +371,23 @@ def test_hij_streamed_from_device(engine, name, tmp_path):
         files.write_hij_from_engine(got, engine, which, rows_per_chunk=97)
         files.write_hij(want, np.asarray(r, np.int64), np.asarray(c, np.int32), np.asarray(v, np.float64))
         assert got.read_bytes() == want.read_bytes()
+
+
+def test_form_h_with_core_shells_bit_exact(engine):
+    """Closed core orbitals (Nso = 2, as every real CONF.INP has): the device
+    keys the integrals from orbital Nso + 1 and numbers the core m-states
+    first, as the oracle (checked against the second-quantised H) does."""
+    shells = [(1, 0), (2, 0)] + S._shells({0: (3, 4), 1: (3, 4), 2: (3, 3)})
+    s = S.make_system("core", shells, 3, 1, 1, [[3, 4, 5]], 5, level=2, params=dict(Nlv=3, MaxNd0=20), nso=2)
+    o = O.Oracle(s)
+    rp, col, val, nz, hmin, pairs = o.form_h()
+    jr, jc, jv = o.form_j()
+    _load(engine, s)
+    numh, numzero, ghmin = engine.form_h(64)
+    grp, gcol, gval = engine.get_csr(0)
+    assert numh == rp[-1] and numzero == nz and ghmin == hmin
+    assert np.array_equal(grp, rp) and np.array_equal(gcol, col)
+    assert np.array_equal(gval.view(np.int64), val.view(np.int64))
+    engine.form_j()
+    gjr, gjc, gjv = engine.get_csr(1)
+    assert np.array_equal(gjr, jr) and np.array_equal(gjc, jc) and np.array_equal(gjv, jv)

@@ -350,3 +350,20 @@ def test_davidson_kv3_rejects_zero_term_filter():
     p = dict(s.params, Kv=3, XJ_av=1.0, Nlv=3)
     with pytest.raises(ValueError, match="divides by zero"):
         O.diag4(s.nd, (rp, col, val), hmin, (jr, jc, jv), p, s.ndc, jt=O.j_terms(s.basis, s.configs, s.mj))
+
+
+@pytest.mark.parametrize("ne,parity,mj", [(2, 0, 0), (3, 1, 1)])
+def test_oracle_with_core_shells_matches_second_quantisation(ne, parity, mj):
+    """Closed core orbitals (Nso = 2: 1s and 2s in front of the valence
+    shells), as every real CONF.INP has: the m-states of the core come first,
+    determinants occupy none of them, and the radial-integral keys start at
+    orbital Nso + 1.  The oracle's H equals the second-quantised one."""
+    shells = [(1, 0), (2, 0)] + S._shells({0: (3, 4), 1: (3, 4), 2: (3, 3)})
+    refs = [[i for i in range(3, ne + 3)]]
+    s = S.make_system("core", shells, ne, mj, parity, refs, 5, level=2, params=dict(Nlv=3, MaxNd0=20), nso=2)
+    assert s.basis.nso == 2 and s.iarr.min() > 2                # the 1s, 2s m-states (1, 2) never occupied
+    assert 10 < s.nd < 600
+    rp, col, val, nz, hmin, pairs = O.Oracle(s).form_h()
+    A = O.csr_to_dense(s.nd, rp, col, val)
+    B = second_quantised_h(s)
+    assert np.max(np.abs(A - B)) < 1e-12 * max(1.0, np.max(np.abs(B)))
