@@ -201,6 +201,35 @@ def pt_level_table(E, dE, J=None):
     return rows
 
 
+def save_vectors(path, EnG, Xj, X_ci, Xpt, nd1):
+    """SaveVectors (src/conf_pt.f90:954-989): CONF_PT.XIJ, one record per
+    level (pci_io's CONF.XIJ layout) holding the CI vector over the first
+    nd1 determinants and the first-order coefficients beyond them, the whole
+    normalised.  EnG and Xj are the levels' energies and J as the CI run's
+    CONF.XIJ holds them (PT_Init adds 4 Gj J(J+1) to EnG and SaveVectors
+    takes it off again, so they are written back unchanged); X_ci is nd1 x
+    nlv; Xpt the engine's first-order coefficients (pci_gpu_pt2's Xpt, Nd x
+    nlv).  The reference's coefficients are x / (En + H_ii) with En = -E
+    (conf_pt.f90:865-874), the engine's x / (E - H_ii): the PT part is
+    written as -Xpt.  Returns the written vectors (Nd x nlv)."""
+    from . import files
+    X_ci = np.asarray(X_ci, np.float64)
+    if X_ci.ndim == 1:
+        X_ci = X_ci[:, None]
+    Xpt = np.asarray(Xpt, np.float64)
+    if Xpt.ndim == 1:
+        Xpt = Xpt[:, None]
+    nd, nlv = Xpt.shape
+    if X_ci.shape != (nd1, nlv):
+        raise ValueError("X_ci must be nd1 x nlv")
+    X = np.zeros((nd, nlv))
+    X[:nd1] = X_ci
+    X[nd1:] = -Xpt[nd1:]
+    X /= np.sqrt(np.sum(X * X, axis=0))
+    files.write_xij(path, np.asarray(EnG, np.float64)[:nlv], np.asarray(Xj, np.float64)[:nlv], X)
+    return X
+
+
 def select_configurations(layout, ncnrci, ndc, X_ci, dEg, dVg, cut0, ktf=5, kvar=1, nc4=None, maxnd0=3000):
     """conf_pt's selection end to end: Weight_CI on the CI vectors, the PT
     weights from pci_gpu_pt2_groups' sums over the PT NR configurations,

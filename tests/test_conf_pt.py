@@ -143,3 +143,33 @@ def test_select_configurations_from_device_sums():
         pytest.skip("a weight sits on the threshold")
     assert got["conf_order"] == want["conf_order"]
     assert (got["nci"], got["nc4"], got["kl4"]) == (want["nci"], want["nc4"], want["kl4"])
+
+
+def test_save_vectors_signs_and_layout(tmp_path):
+    """SaveVectors' CONF_PT.XIJ: CI part then first-order part, normalised,
+    energies and J as read; the PT part follows PTE's own formula
+    (ci = x / (e0 - ei), e0 = En, ei = -Diag(i), conf_pt.f90:865-874) with
+    the CONF.XIJ energy En = -E, which is -1 times the engine's
+    coefficient."""
+    import oracle as O
+    from pci_b200 import files
+    s = get_system("small3")
+    (rp, col, val, *_), _ = oracle_h("small3")
+    H = O.csr_to_dense(s.nd, rp, col, val)
+    cs = np.concatenate([[0], np.cumsum(s.ndc)])
+    nd1 = int(cs[10])
+    w, V = np.linalg.eigh(H[:nd1, :nd1])
+    X_ci, E = V[:, :2], w[:2]
+    dE, C = O.pt2(H, nd1, nd1, X_ci, E)
+    En = -E                                                 # CONF.XIJ's energies
+    ref = np.zeros((s.nd, 2))
+    for i in range(nd1, s.nd):
+        x = H[i, :nd1] @ X_ci
+        ref[i] = x / (En - (-H[i, i]))                      # PTE's ci
+    assert np.allclose(ref[nd1:], -C[nd1:], rtol=1e-12, atol=1e-15)
+    X = P.save_vectors(tmp_path / "CONF_PT.XIJ", En, [0.5, 1.5], X_ci, C, nd1)
+    Tk, Tj, Xr = files.read_xij(tmp_path / "CONF_PT.XIJ", s.nd)
+    assert np.allclose(Tk, En) and np.allclose(Tj, [0.5, 1.5])
+    assert np.allclose(Xr, X) and np.allclose(np.linalg.norm(Xr, axis=0), 1.0)
+    norm = np.sqrt(1.0 + np.sum(ref[nd1:] ** 2, axis=0))
+    assert np.allclose(Xr[:nd1] * norm, X_ci) and np.allclose(Xr[nd1:] * norm, ref[nd1:])
