@@ -244,6 +244,10 @@ def system_from_files(conf_inp, conf_int, conf_gnt=None, name=None):
             text = f.read()
     parsed = read_conf_inp(text)
     p = parsed["params"]
+    # pconf drops the isotope-shift operator when |C_is| < 1e-6 (pconf.F90:335-336);
+    # its terms in Hint / Gint (integrals.f90:141-143) are not part of this engine's H
+    if p.get("K_IS", 0) != 0 and abs(p.get("C_IS", 0.0)) >= 1e-6:
+        raise ValueError("CONF.INP asks for the isotope-shift operator (K_is, C_is), which this engine does not add to H")
     ci = files.read_int(conf_int)
     h = ci.header
     if int(h.nso) != p["NSO"]:

@@ -211,3 +211,17 @@ def test_system_from_files_checks_nso(tmp_path):
     (tmp_path / "CONF.INP").write_text(text)
     with pytest.raises(ValueError):
         C.system_from_files(tmp_path / "CONF.INP", tmp_path / "CONF.INT")
+
+
+def test_system_from_files_refuses_isotope_shift(tmp_path):
+    """K_is with a non-negligible C_is would add the reference's SMS / VS
+    terms to H, which this engine does not: refused, not silently dropped;
+    |C_is| < 1e-6 switches the operator off, as pconf does."""
+    s = get_system("tiny")
+    _write_inputs(tmp_path, s)
+    base = (tmp_path / "CONF.INP").read_text()
+    (tmp_path / "CONF.INP").write_text(base.replace("GJ = 0", "GJ = 0\nK_IS = 2\nC_IS = 1.0", 1))
+    with pytest.raises(ValueError):
+        C.system_from_files(tmp_path / "CONF.INP", tmp_path / "CONF.INT")
+    (tmp_path / "CONF.INP").write_text(base.replace("GJ = 0", "GJ = 0\nK_IS = 2\nC_IS = 0.0", 1))
+    assert C.system_from_files(tmp_path / "CONF.INP", tmp_path / "CONF.INT").nd == s.nd
