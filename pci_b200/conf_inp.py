@@ -252,6 +252,8 @@ def system_from_files(conf_inp, conf_int, conf_gnt=None, name=None):
     h = ci.header
     if int(h.nso) != p["NSO"]:
         raise ValueError(f"CONF.INT has Nso = {h.nso}, CONF.INP {p['NSO']}")
+    if int(h.kbrt) != p.get("KBRT", 0):   # Rint stops here too (integrals.f90:53-60)
+        raise ValueError(f"CONF.INT's integrals are for Kbrt = {h.kbrt}, CONF.INP asks for {p.get('KBRT', 0)}")
     orb = ci.orbitals
     basis = Basis(nn=orb[:, 0].astype(np.int32), ll=orb[:, 2].astype(np.int32), kk=orb[:, 1].astype(np.int32),
                   jj=orb[:, 3].astype(np.int32), nso=int(h.nso))

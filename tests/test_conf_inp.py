@@ -225,3 +225,14 @@ def test_system_from_files_refuses_isotope_shift(tmp_path):
         C.system_from_files(tmp_path / "CONF.INP", tmp_path / "CONF.INT")
     (tmp_path / "CONF.INP").write_text(base.replace("GJ = 0", "GJ = 0\nK_IS = 2\nC_IS = 0.0", 1))
     assert C.system_from_files(tmp_path / "CONF.INP", tmp_path / "CONF.INT").nd == s.nd
+
+
+def test_system_from_files_checks_kbrt(tmp_path):
+    """As the reference's Rint: CONF.INP's Kbrt must be the one CONF.INT's
+    integrals were made for."""
+    s = get_system("tiny")
+    _write_inputs(tmp_path, s)
+    base = (tmp_path / "CONF.INP").read_text()
+    (tmp_path / "CONF.INP").write_text(base.replace("GJ = 0", "GJ = 0\nKBRT = 1", 1))
+    with pytest.raises(ValueError):
+        C.system_from_files(tmp_path / "CONF.INP", tmp_path / "CONF.INT")
