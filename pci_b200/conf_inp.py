@@ -94,10 +94,11 @@ def read_conf_inp(text: str):
         val = val.strip()[:10]
         if "#" in val:
             val = val[:val.index("#")].strip()
+        num = val.replace("d", "e").replace("D", "e")   # Fortran's double-precision exponent
         if key in INT_KEYS:
-            params[key] = int(float(val))
+            params[key] = int(float(num))
         elif key in REAL_KEYS:
-            params[key] = float(val)
+            params[key] = float(num)
         p += 1
     if p < len(lines) and lines[p].strip() == "":
         p += 1

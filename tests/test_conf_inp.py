@@ -22,7 +22,8 @@ Nlv = 5
 Ne = 3   # three valence electrons
 Kl4 = 1
 Nc4 = 2
-Crt4 = 0.0001
+Crt4 = 1.d-4
+Cut0 = 2.5D-3
 
     -0.1001     0.2102
    1 0.2102    -0.2101
@@ -50,7 +51,7 @@ def test_read_sample():
     assert r["name"].strip() == "Cs test"
     p = r["params"]
     assert (p["Z"], p["NSO"], p["NC"], p["NE"], p["KL4"], p["NC4"]) == (55.0, 2, 3, 3, 1, 2)
-    assert p["CRT4"] == pytest.approx(1e-4) and p["KBRT"] == 0 and p["CUT0"] == pytest.approx(0.001)
+    assert p["CRT4"] == pytest.approx(1e-4) and p["KBRT"] == 0 and p["CUT0"] == pytest.approx(2.5e-3)
     assert r["core"] == [pytest.approx(-0.1001), pytest.approx(0.2102)]
     # configuration 2 runs over two lines until it holds Ne = 3 electrons;
     # configuration 3's first line is blank apart from its number
