@@ -23,7 +23,7 @@ from functools import lru_cache
 
 import numpy as np
 
-from .wigner import three_j
+from .wigner import six_j, three_j
 
 
 def _sgn(n: int) -> float:
@@ -200,3 +200,35 @@ def reduced_transition(ro, basis, nh, jz, tj1, mj1_2, tj2, mj2_2, parity=None, i
         rro[rank] = r
     return {"shells": shells, "rro": rro, "parity": parity,
             "trace": float(np.trace(ro[imin:imax + 1, imin:imax + 1]))}
+
+
+def e1_amplitude(rt, radial):
+    """RdcTM's reduced E1 amplitude in the length gauge (the l1 = 2 branch
+    for a transition of parity -1, src/pdtm.f90:1810-1818, with amp_ops'
+    AmpE1, src/amp_ops.f90): for each initial shell a and final shell b of
+    the rank-1 reduced transition matrix, Rro_1(a, b) * radial(b, a) *
+    (-1)^k * sqrt((2 j_b + 1)(2 j_a + 1) l_max) * {l_b j_b 1/2; j_a l_a 1},
+    k = floor(j_a + l_max + 1.51), summed.  rt is reduced_transition's
+    result; radial(final, initial) returns pdtm's E1 radial integral
+    (Fint(3, ...), from its DTM.INT tables, which this engine does not form)
+    for orbitals given as (n, l, 2j).  0 when the transition is not odd or
+    has no rank-1 matrix."""
+    r = rt["rro"][1]
+    if rt["parity"] != -1 or r is None:
+        return 0.0
+    shells = rt["shells"]
+    total = 0.0
+    for a, (na, la, ja2, *_) in enumerate(shells):
+        for b, (nb, lb, jb2, *_) in enumerate(shells):
+            tme = r[a, b]
+            if tme == 0.0:
+                continue
+            al = tme * radial((nb, lb, jb2), (na, la, ja2))
+            if al == 0.0:
+                continue
+            lx = max(la, lb)
+            k = int(ja2 / 2 + lx + 1.51)
+            sign = -1.0 if k % 2 else 1.0
+            c = math.sqrt((jb2 + 1) * (ja2 + 1) * lx) * six_j(lb, jb2 / 2, 0.5, ja2 / 2, la, 1)
+            total += sign * c * al
+    return total

@@ -22,7 +22,7 @@ from functools import lru_cache
 
 import numpy as np
 
-__all__ = ["three_j", "gaun", "gaunt_table", "gaunt_lut"]
+__all__ = ["three_j", "six_j", "gaun", "gaunt_table", "gaunt_lut"]
 
 
 def _is_int(x: Fraction) -> bool:
@@ -68,6 +68,50 @@ def three_j(j1, j2, j3, m1, m2, m3) -> float:
     if sign == 0:
         return 0.0
     # sqrt of an exact rational, correctly rounded via integer sqrt at 2^-120 scale
+    num, den = sq.numerator, sq.denominator
+    scale = 1 << 240
+    root = math.isqrt(num * scale // den)
+    return sign * (root / float(1 << 120))
+
+
+def _tri_sq(a, b, c):
+    """Delta(abc)^2 as a Fraction, or None when a, b, c break the triangle rule."""
+    if not (abs(a - b) <= c <= a + b) or not _is_int(a + b + c):
+        return None
+    f = math.factorial
+    return Fraction(f(int(a + b - c)) * f(int(a - b + c)) * f(int(-a + b + c)), f(int(a + b + c + 1)))
+
+
+@lru_cache(maxsize=None)
+def _six_j_exact(j1, j2, j3, j4, j5, j6):
+    tris = [_tri_sq(j1, j2, j3), _tri_sq(j1, j5, j6), _tri_sq(j4, j2, j6), _tri_sq(j4, j5, j3)]
+    if any(t is None for t in tris):
+        return 0, Fraction(0)
+    f = math.factorial
+    a = [int(j1 + j2 + j3), int(j1 + j5 + j6), int(j4 + j2 + j6), int(j4 + j5 + j3)]
+    b = [int(j1 + j2 + j4 + j5), int(j2 + j3 + j5 + j6), int(j3 + j1 + j6 + j4)]
+    s = Fraction(0)
+    for t in range(max(a), min(b) + 1):
+        den = 1
+        for x in a:
+            den *= f(t - x)
+        for y in b:
+            den *= f(y - t)
+        s += Fraction((-1) ** t * f(t + 1), den)
+    if s == 0:
+        return 0, Fraction(0)
+    pre = tris[0] * tris[1] * tris[2] * tris[3]
+    return (1 if s > 0 else -1), pre * s * s
+
+
+def six_j(j1, j2, j3, j4, j5, j6) -> float:
+    """Wigner 6j symbol {j1 j2 j3; j4 j5 j6}, Racah's closed formula over
+    exact rationals, rounded once (the reference's Fj6 evaluates the same
+    quantity in floating point)."""
+    args = tuple(Fraction(x).limit_denominator(2) for x in (j1, j2, j3, j4, j5, j6))
+    sign, sq = _six_j_exact(*args)
+    if sign == 0:
+        return 0.0
     num, den = sq.numerator, sq.denominator
     scale = 1 << 240
     root = math.isqrt(num * scale // den)

@@ -178,3 +178,51 @@ def test_reduction_of_device_transition_density():
             assert got["rro"][rank] is None
         else:
             assert np.allclose(got["rro"][rank], want["rro"][rank], rtol=1e-10, atol=1e-12)
+
+
+def test_six_j_known_values():
+    from pci_b200 import wigner as W
+    # {a b c; 0 c b} = (-1)^(a+b+c) / sqrt((2b+1)(2c+1))
+    for a, b, c in [(1, 1, 1), (0.5, 1, 0.5), (2, 1.5, 2.5), (1, 2, 2)]:
+        want = (-1) ** int(round(a + b + c)) / np.sqrt((2 * b + 1) * (2 * c + 1))
+        assert W.six_j(a, b, c, 0, c, b) == pytest.approx(want, abs=1e-15)
+    assert W.six_j(0.5, 0.5, 1, 0.5, 0.5, 0) == pytest.approx(0.5, abs=1e-15)
+    assert W.six_j(1, 0.5, 0.5, 2.5, 2, 1) == 0.0              # triangle (1/2 5/2 1) broken
+    # orthogonality: sum_x (2x+1)(2f+1) {a b x; c d f}{a b x; c d f'} = delta(f, f')
+    a, b, c, d = 1.5, 1, 1.5, 1
+    for f in (0.5, 1.5, 2.5):
+        for g in (0.5, 1.5, 2.5):
+            s = sum((2 * x + 1) * (2 * f + 1) * W.six_j(a, b, x, c, d, f) * W.six_j(a, b, x, c, d, g)
+                    for x in (0.5, 1.5, 2.5))
+            assert s == pytest.approx(1.0 if f == g else 0.0, abs=1e-14)
+
+
+def _c1_reduced(ja, la, jb, lb):
+    """<jb lb || C^1 || ja la> from a 3j symbol: (-1)^(jb+1/2) sqrt((2jb+1)(2ja+1))
+    (jb 1 ja; -1/2 0 1/2), zero unless la + lb is odd."""
+    from pci_b200 import wigner as W
+    if (la + lb) % 2 == 0:
+        return 0.0
+    return (-1) ** int(round(jb + 0.5)) * np.sqrt((2 * jb + 1) * (2 * ja + 1)) * W.three_j(jb, 1, ja, -0.5, 0, 0.5)
+
+
+@pytest.mark.parametrize("ia,ib", [(1, 3), (1, 6), (3, 1), (6, 1), (0, 5)])
+def test_one_electron_e1_amplitude_is_the_c1_reduced_element(ia, ib):
+    """One electron between s1/2 and p1/2 / p3/2: the rank-1 reduced
+    transition matrix is 1 on the pair, so with a unit radial integral the
+    E1 amplitude's size is the single-particle <j_b||C^1||j_a>, computed
+    here independently from a 3j symbol."""
+    b, nh, jz = _sp_basis()
+    ro = np.zeros((8, 8))
+    ro[ia, ib] = 1.0
+    ja2, jb2 = int(b.jj[nh[ia] - 1]), int(b.jj[nh[ib] - 1])
+    la, lb = int(b.ll[nh[ia] - 1]), int(b.ll[nh[ib] - 1])
+    rt = D.reduced_transition(ro, b, nh, jz, ja2 / 2, int(jz[ia]), jb2 / 2, int(jz[ib]))
+    if rt["rro"][1] is None:
+        pytest.skip("rank 1 not allowed by the 3j denominator for these M")
+    amp = D.e1_amplitude(rt, lambda f, i: 1.0)
+    assert abs(amp) == pytest.approx(abs(_c1_reduced(ja2 / 2, la, jb2 / 2, lb)), rel=1e-13)
+    # the radial integral scales it, and an even transition has none
+    assert D.e1_amplitude(rt, lambda f, i: 2.5) == pytest.approx(2.5 * amp)
+    even = dict(rt, parity=1)
+    assert D.e1_amplitude(even, lambda f, i: 1.0) == 0.0
