@@ -232,3 +232,34 @@ def e1_amplitude(rt, radial):
             c = math.sqrt((jb2 + 1) * (ja2 + 1) * lx) * six_j(lb, jb2 / 2, 0.5, ja2 / 2, la, 1)
             total += sign * c * al
     return total
+
+
+def e2_amplitude(rt, radial):
+    """RdcTM's reduced E2 amplitude (the l1 = 3 branch of an even
+    transition, src/pdtm.f90:1849-1851, with amp_ops' AmpE2): for initial
+    shell a and final shell b with |j_b - j_a| <= 2 <= j_a + j_b, minus the
+    sum of Rro_2(a, b) * radial(b, a) * (-1)^floor(j_a + 0.51) *
+    sqrt((2j_b+1)(2j_a+1)(2l_b+1)(2l_a+1)) * (l_b l_a 2; 0 0 0) *
+    {j_b j_a 2; l_a l_b 1/2}.  radial(final, initial) is pdtm's E2 radial
+    integral (Fint(10, ...)) for orbitals given as (n, l, 2j).  0 when the
+    transition is not even or has no rank-2 matrix."""
+    r = rt["rro"][2]
+    if rt["parity"] != 1 or r is None:
+        return 0.0
+    shells = rt["shells"]
+    total = 0.0
+    for a, (na, la, ja2, *_) in enumerate(shells):
+        for b, (nb, lb, jb2, *_) in enumerate(shells):
+            if abs(jb2 - ja2) > 4 or jb2 + ja2 < 4:
+                continue
+            tme = r[a, b]
+            if tme == 0.0:
+                continue
+            ae = tme * radial((nb, lb, jb2), (na, la, ja2))
+            if ae == 0.0:
+                continue
+            sign = -1.0 if int(ja2 / 2 + 0.51) % 2 else 1.0
+            ae *= sign * math.sqrt((jb2 + 1) * (ja2 + 1) * (2 * lb + 1) * (2 * la + 1)) \
+                * three_j(lb, la, 2, 0, 0, 0) * six_j(jb2 / 2, ja2 / 2, 2, la, lb, 0.5)
+            total -= ae
+    return total

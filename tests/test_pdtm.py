@@ -226,3 +226,38 @@ def test_one_electron_e1_amplitude_is_the_c1_reduced_element(ia, ib):
     assert D.e1_amplitude(rt, lambda f, i: 2.5) == pytest.approx(2.5 * amp)
     even = dict(rt, parity=1)
     assert D.e1_amplitude(even, lambda f, i: 1.0) == 0.0
+
+
+def _c2_reduced(ja, la, jb, lb):
+    """<jb lb || C^2 || ja la> from a 3j symbol, zero unless la + lb is even."""
+    from pci_b200 import wigner as W
+    if (la + lb) % 2:
+        return 0.0
+    return (-1) ** int(round(jb + 0.5)) * np.sqrt((2 * jb + 1) * (2 * ja + 1)) * W.three_j(jb, 2, ja, -0.5, 0, 0.5)
+
+
+@pytest.mark.parametrize("ia,ib", [(3, 6), (6, 3), (4, 6), (3, 5), (2, 5), (6, 2)])
+def test_one_electron_e2_amplitude_is_the_c2_reduced_element(ia, ib):
+    """One electron within 2p (p1/2 <-> p3/2, p3/2 <-> p3/2): with a unit
+    radial integral the E2 amplitude's size is <j_b||C^2||j_a> from a 3j
+    symbol; the odd s-p transitions and j = 1/2 pairs have none."""
+    b, nh, jz = _sp_basis()
+    ro = np.zeros((8, 8))
+    ro[ia, ib] = 1.0
+    ja2, jb2 = int(b.jj[nh[ia] - 1]), int(b.jj[nh[ib] - 1])
+    la, lb = int(b.ll[nh[ia] - 1]), int(b.ll[nh[ib] - 1])
+    rt = D.reduced_transition(ro, b, nh, jz, ja2 / 2, int(jz[ia]), jb2 / 2, int(jz[ib]))
+    want = abs(_c2_reduced(ja2 / 2, la, jb2 / 2, lb))
+    if rt["rro"][2] is None:
+        pytest.skip("rank 2 not allowed by the 3j denominator for these M")
+    amp = D.e2_amplitude(rt, lambda f, i: 1.0)
+    assert abs(amp) == pytest.approx(want, rel=1e-13)
+    assert want > 0
+
+
+def test_e2_amplitude_of_odd_transition_is_zero():
+    b, nh, jz = _sp_basis()
+    ro = np.zeros((8, 8))
+    ro[1, 6] = 1.0                                       # 2s -> 2p3/2
+    rt = D.reduced_transition(ro, b, nh, jz, 0.5, 1, 1.5, 1)
+    assert D.e2_amplitude(rt, lambda f, i: 1.0) == 0.0
