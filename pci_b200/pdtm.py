@@ -263,3 +263,43 @@ def e2_amplitude(rt, radial):
                 * three_j(lb, la, 2, 0, 0, 0) * six_j(jb2 / 2, ja2 / 2, 2, la, lb, 0.5)
             total -= ae
     return total
+
+
+def _gj1(x, l):
+    """pdtm's Gj1 (src/pdtm.f90:1664-1671)."""
+    return (x + 0.5) * math.sqrt((2 * x + 1) * (4 * x - 2 * l + 1) / (2 * l + 1))
+
+
+def _gjj(kx, l):
+    """pdtm's Gjj (src/pdtm.f90:1673-1679), kx = 2j."""
+    return _sgn((kx + 1) // 2 + l) * math.sqrt(2.0 * l * (l + 1) / (2 * l + 1))
+
+
+def g_factor_nr(rd, overlap=None):
+    """RdcDM's non-relativistic M1 g-factor (K_M1 = 1, src/pdtm.f90:2340-2352
+    and 2392): over the rank-1 reduced density matrix, for shells a, b of
+    one l that are the same orbital or spin-orbit partners (j_a /= j_b),
+    Rro_1(a, b) * overlap(b, a) * (Gj1(j_a, l) when j_a = j_b, else Gjj(2 j_b,
+    l)), summed and divided by sqrt(J(J+1)(2J+1)).  overlap(b, a) is pdtm's
+    radial overlap (Fint(9, ...)) of orbitals given as (n, l, 2j); by default
+    1 for equal n and 0 otherwise.  rd is reduced_density's result; 0 when
+    its rank-1 matrix is absent."""
+    r = rd["rro"][1]
+    if r is None:
+        return 0.0
+    if overlap is None:
+        overlap = lambda b, a: 1.0 if b[0] == a[0] and b[1] == a[1] else 0.0
+    shells = rd["shells"]
+    g = 0.0
+    for a, (na, la, ja2, fa, _) in enumerate(shells):
+        for b, (nb, lb, jb2, fb, _) in enumerate(shells):
+            if la != lb:
+                continue
+            same = (na, la, ja2) == (nb, lb, jb2)
+            if not (same or ja2 != jb2):
+                continue
+            g1 = r[a, b] * overlap((nb, lb, jb2), (na, la, ja2))
+            g1 *= _gj1(ja2 / 2, la) if ja2 == jb2 else _gjj(jb2, lb)
+            g += g1
+    J = rd["J"]
+    return g / math.sqrt(J * (J + 1) * (2 * J + 1)) if g != 0.0 else 0.0

@@ -261,3 +261,25 @@ def test_e2_amplitude_of_odd_transition_is_zero():
     ro[1, 6] = 1.0                                       # 2s -> 2p3/2
     rt = D.reduced_transition(ro, b, nh, jz, 0.5, 1, 1.5, 1)
     assert D.e2_amplitude(rt, lambda f, i: 1.0) == 0.0
+
+
+@pytest.mark.parametrize("shells,orb,m2,want", [
+    ([(2, 0)], 1, 1, 2.0),                    # s1/2
+    ([(2, 1)], 1, -1, 2 / 3),                 # p1/2
+    ([(2, 1)], 2, 3, 4 / 3),                  # p3/2
+    ([(3, 2)], 1, 1, 4 / 5),                  # d3/2
+    ([(3, 2)], 2, -3, 6 / 5),                 # d5/2
+])
+def test_g_factor_of_one_electron_is_lande(shells, orb, m2, want):
+    """One electron in (n, l, j), J = j: RdcDM's non-relativistic g-factor
+    is Lande's g_j = 1 + (j(j+1) - l(l+1) + 3/4) / (2j(j+1))."""
+    b = S.make_basis(shells)
+    jz, nh, _ = S.m_states(b, b.ns)
+    ro = np.zeros((jz.size, jz.size))
+    i = [k for k in range(jz.size) if nh[k] == orb and jz[k] == m2][0]
+    ro[i, i] = 1.0
+    j = b.jj[orb - 1] / 2
+    rd = D.reduced_density(ro, b, nh, jz, tj=j, mj2=m2)
+    assert D.g_factor_nr(rd) == pytest.approx(want, rel=1e-13)
+    l = b.ll[orb - 1]
+    assert want == pytest.approx(1 + (j * (j + 1) - l * (l + 1) + 0.75) / (2 * j * (j + 1)))
