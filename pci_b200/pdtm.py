@@ -303,3 +303,21 @@ def g_factor_nr(rd, overlap=None):
             g += g1
     J = rd["J"]
     return g / math.sqrt(J * (J + 1) * (2 * J + 1)) if g != 0.0 else 0.0
+
+
+# Hartree in cm^-1 as pdtm writes it (src/pdtm.f90:1704)
+HARTREE_CM = 219474.63
+
+
+def e1_rate(ae1, e1, e2, tj1, tj2):
+    """RdcTM's E1 transition rate (src/pdtm.f90:1933-1949): the wavelength
+    wl = |1e7 / dE| nm with dE = (e2 - e1) * 219474.63 cm^-1 and A =
+    2.02613e18 AE1^2 / ((2J_u + 1) (10 wl)^3) s^-1, J_u the upper level's J
+    (level 1 when e2 > e1).  Energies in the sign convention of CONF.XIJ
+    (binding energies: the larger is the lower level).  Returns (wl, A)."""
+    de = (e2 - e1) * HARTREE_CM
+    if de == 0.0:
+        raise ValueError("the two levels have the same energy")
+    wl = abs(1e7 / de)
+    ju = tj1 if e2 > e1 else tj2
+    return wl, 2.02613e18 / ((2 * ju + 1) * (wl * 10) ** 3) * ae1 ** 2

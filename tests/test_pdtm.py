@@ -283,3 +283,16 @@ def test_g_factor_of_one_electron_is_lande(shells, orb, m2, want):
     assert D.g_factor_nr(rd) == pytest.approx(want, rel=1e-13)
     l = b.ll[orb - 1]
     assert want == pytest.approx(1 + (j * (j + 1) - l * (l + 1) + 0.75) / (2 * j * (j + 1)))
+
+
+def test_e1_rate():
+    # level 1 at 0.30 Ha binding, level 2 at 0.40 (more bound): 1 is the upper level
+    wl, a = D.e1_rate(2.0, 0.30, 0.40, 1.5, 0.5)
+    de = 0.10 * 219474.63
+    assert wl == pytest.approx(1e7 / de)
+    assert a == pytest.approx(2.02613e18 * 4.0 / (4 * (10 * wl) ** 3))
+    # the other way round the upper level is 2
+    wl2, a2 = D.e1_rate(2.0, 0.40, 0.30, 1.5, 0.5)
+    assert wl2 == pytest.approx(wl) and a2 == pytest.approx(2.02613e18 * 4.0 / (2 * (10 * wl) ** 3))
+    with pytest.raises(ValueError):
+        D.e1_rate(1.0, 0.3, 0.3, 0.5, 0.5)
