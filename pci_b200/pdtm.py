@@ -321,3 +321,59 @@ def e1_rate(ae1, e1, e2, tj1, tj2):
     wl = abs(1e7 / de)
     ju = tj1 if e2 > e1 else tj2
     return wl, 2.02613e18 / ((2 * ju + 1) * (wl * 10) ** 3) * ae1 ** 2
+
+
+# physical constants the reference uses (src/params.f90:14-21)
+DPCL = 137.0359922594      # speed of light, a.u.
+DPAU = 6.5796839e15        # a.u. of energy in Hz
+DPMP = 1836.153            # proton mass, a.u.
+DPRB = 0.529177249e-8      # Bohr radius, cm
+
+
+def _hfs_a_angular(jb2, ja2, la):
+    """HfsA's factor (src/amp_ops.f90) for column shell b (j_b) and row shell a
+    (j_a, l_a): the sign (-1)^floor(j_a + l_a + 1.51) times
+    sqrt((2j_b+1)(2j_a+1)/(min(j_a, j_b)+1)) between spin-orbit partners and
+    (2j+1) sqrt((2j+1)/(j(j+1))) within one j."""
+    jb, ja = jb2 / 2, ja2 / 2
+    sign = -1.0 if int(ja + la + 1.51) % 2 else 1.0
+    if abs(ja - jb) > 0.1:
+        return sign * math.sqrt((2 * jb + 1) * (2 * ja + 1) / (min(ja, jb) + 1))
+    return sign * (2 * jb + 1) * math.sqrt((2 * jb + 1) / (jb * (jb + 1)))
+
+
+def hfs_constants(rd, radial_a, radial_b=None, gnuc=1.0, qnuc=1.0):
+    """RdcDM's hyperfine constants A and B in MHz (src/pdtm.f90:2325-2392
+    with amp_ops' HfsA and HfsB): A sums Rro_1(a, b) * radial_a(b, a) * HfsA's
+    angular factor over shell pairs, B sums Rro_2(a, b) * radial_b(b, a) *
+    (-1)^floor(j_a + 0.51) * sqrt((2j_b+1)(2j_a+1)(2l_b+1)(2l_a+1)) *
+    (l_b l_a 2; 0 0 0) * {j_b j_a 2; l_a l_b 1/2}; then
+    A = -gnuc / (4 c m_p) / sqrt(J(J+1)(2J+1)) * sum * au[Hz] * 1e-6 and
+    B = -2 qnuc sqrt(J(2J-1) / ((J+1)(2J+1)(2J+3))) * sum * au[Hz] / r_B^2 *
+    1e-30.  radial_a / radial_b(b, a) are pdtm's hyperfine radial integrals
+    (Fint(1, ...), Fint(2, ...)) for orbitals given as (n, l, 2j); gnuc and
+    qnuc the nuclear g-factor and quadrupole moment of CONF.INP (Gnuc,
+    Qnuc).  Returns (A, B)."""
+    shells = rd["shells"]
+    J = rd["J"]
+    a_sum = b_sum = 0.0
+    r1, r2 = rd["rro"][1], rd["rro"][2]
+    for a, (na, la, ja2, *_) in enumerate(shells):
+        for b, (nb, lb, jb2, *_) in enumerate(shells):
+            if r1 is not None and r1[a, b] != 0.0:
+                v = r1[a, b] * radial_a((nb, lb, jb2), (na, la, ja2))
+                if v != 0.0:
+                    a_sum += v * _hfs_a_angular(jb2, ja2, la)
+            if radial_b is not None and r2 is not None and r2[a, b] != 0.0:
+                v = r2[a, b] * radial_b((nb, lb, jb2), (na, la, ja2))
+                if v != 0.0:
+                    sign = -1.0 if int(ja2 / 2 + 0.51) % 2 else 1.0
+                    b_sum += v * sign * math.sqrt((jb2 + 1) * (ja2 + 1) * (2 * lb + 1) * (2 * la + 1)) \
+                        * three_j(lb, la, 2, 0, 0, 0) * six_j(jb2 / 2, ja2 / 2, 2, la, lb, 0.5)
+    A = B = 0.0
+    if a_sum != 0.0:
+        A = -gnuc / (DPCL * 4 * DPMP) / math.sqrt(J * (J + 1) * (2 * J + 1)) * a_sum * DPAU * 1e-6
+    if b_sum != 0.0:
+        B = -2 * qnuc * math.sqrt(J * (2 * J - 1) / ((J + 1) * (2 * J + 1) * (2 * J + 3))) * b_sum \
+            * DPAU / (DPRB * DPRB) * 1e-30
+    return A, B

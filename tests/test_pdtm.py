@@ -296,3 +296,32 @@ def test_e1_rate():
     assert wl2 == pytest.approx(wl) and a2 == pytest.approx(2.02613e18 * 4.0 / (2 * (10 * wl) ** 3))
     with pytest.raises(ValueError):
         D.e1_rate(1.0, 0.3, 0.3, 0.5, 0.5)
+
+
+@pytest.mark.parametrize("shells,orb", [([(2, 0)], 1), ([(2, 1)], 1), ([(2, 1)], 2), ([(3, 2)], 1), ([(3, 2)], 2)])
+def test_hfs_a_of_one_electron(shells, orb):
+    """One electron in (n, l, j), M = J = j, unit radial integral: RdcDM's A
+    sum over sqrt(j(j+1)(2j+1)) is 2|kappa| / (j(j+1)) in size, twice the
+    textbook single-particle kappa / (j(j+1)) (pdtm's radial integral is
+    the one of P Q, the textbook's of P Q + Q P); A follows with the
+    reference's constants."""
+    b = S.make_basis(shells)
+    jz, nh, _ = S.m_states(b, b.ns)
+    j2 = int(b.jj[orb - 1])
+    ro = np.zeros((jz.size, jz.size))
+    i = [k for k in range(jz.size) if nh[k] == orb and jz[k] == j2][0]
+    ro[i, i] = 1.0
+    j = j2 / 2
+    rd = D.reduced_density(ro, b, nh, jz, tj=j, mj2=j2)
+    A, B = D.hfs_constants(rd, lambda f, i_: 1.0, lambda f, i_: 1.0, gnuc=1.0, qnuc=1.0)
+    kappa = int(b.kk[orb - 1])
+    per = abs(A) / (1.0 / (D.DPCL * 4 * D.DPMP) * D.DPAU * 1e-6)
+    assert per == pytest.approx(2 * abs(kappa) / (j * (j + 1)), rel=1e-13)
+    if j < 1:
+        assert B == 0.0                        # no quadrupole constant for J = 1/2
+    else:
+        # B's angular sum is <j||C^2||j> in size
+        bsum = abs(B) / (2 * np.sqrt(j * (2 * j - 1) / ((j + 1) * (2 * j + 1) * (2 * j + 3)))
+                         * D.DPAU / D.DPRB ** 2 * 1e-30)
+        l = int(b.ll[orb - 1])
+        assert bsum == pytest.approx(abs(_c2_reduced(j, l, j, l)), rel=1e-13)
