@@ -258,10 +258,7 @@ def e2_amplitude(rt, radial):
             ae = tme * radial((nb, lb, jb2), (na, la, ja2))
             if ae == 0.0:
                 continue
-            sign = -1.0 if int(ja2 / 2 + 0.51) % 2 else 1.0
-            ae *= sign * math.sqrt((jb2 + 1) * (ja2 + 1) * (2 * lb + 1) * (2 * la + 1)) \
-                * three_j(lb, la, 2, 0, 0, 0) * six_j(jb2 / 2, ja2 / 2, 2, la, lb, 0.5)
-            total -= ae
+            total -= ae * _ek_angular(2, jb2, ja2, lb, la)
     return total
 
 
@@ -367,9 +364,7 @@ def hfs_constants(rd, radial_a, radial_b=None, gnuc=1.0, qnuc=1.0):
             if radial_b is not None and r2 is not None and r2[a, b] != 0.0:
                 v = r2[a, b] * radial_b((nb, lb, jb2), (na, la, ja2))
                 if v != 0.0:
-                    sign = -1.0 if int(ja2 / 2 + 0.51) % 2 else 1.0
-                    b_sum += v * sign * math.sqrt((jb2 + 1) * (ja2 + 1) * (2 * lb + 1) * (2 * la + 1)) \
-                        * three_j(lb, la, 2, 0, 0, 0) * six_j(jb2 / 2, ja2 / 2, 2, la, lb, 0.5)
+                    b_sum += v * _ek_angular(2, jb2, ja2, lb, la)
     A = B = 0.0
     if a_sum != 0.0:
         A = -gnuc / (DPCL * 4 * DPMP) / math.sqrt(J * (J + 1) * (2 * J + 1)) * a_sum * DPAU * 1e-6
@@ -377,3 +372,34 @@ def hfs_constants(rd, radial_a, radial_b=None, gnuc=1.0, qnuc=1.0):
         B = -2 * qnuc * math.sqrt(J * (2 * J - 1) / ((J + 1) * (2 * J + 1) * (2 * J + 3))) * b_sum \
             * DPAU / (DPRB * DPRB) * 1e-30
     return A, B
+
+
+def _ek_angular(k, jb2, ja2, lb, la):
+    """AmpE2 / AmpE3 / HfsB's factor for rank k, final (column) shell b and
+    initial (row) shell a: (-1)^floor(j_a + 0.51) *
+    sqrt((2j_b+1)(2j_a+1)(2l_b+1)(2l_a+1)) * (l_b l_a k; 0 0 0) *
+    {j_b j_a k; l_a l_b 1/2}."""
+    sign = -1.0 if int(ja2 / 2 + 0.51) % 2 else 1.0
+    return sign * math.sqrt((jb2 + 1) * (ja2 + 1) * (2 * lb + 1) * (2 * la + 1)) \
+        * three_j(lb, la, k, 0, 0, 0) * six_j(jb2 / 2, ja2 / 2, k, la, lb, 0.5)
+
+
+def e3_amplitude(rt, radial):
+    """RdcTM's reduced E3 amplitude (the l1 = 4 branch of an odd transition,
+    src/pdtm.f90:1822-1826, with amp_ops' AmpE3): over initial shell a and
+    final shell b with |j_b - j_a| <= 3 <= j_a + j_b, the sum of
+    Rro_3(a, b) * radial(b, a) * the rank-3 factor of AmpE2's form.
+    radial(final, initial) is pdtm's E3 radial integral (Fint(11, ...)) for
+    orbitals given as (n, l, 2j)."""
+    r = rt["rro"][3]
+    if rt["parity"] != -1 or r is None:
+        return 0.0
+    total = 0.0
+    for a, (na, la, ja2, *_) in enumerate(rt["shells"]):
+        for b, (nb, lb, jb2, *_) in enumerate(rt["shells"]):
+            if abs(jb2 - ja2) > 6 or jb2 + ja2 < 6 or r[a, b] == 0.0:
+                continue
+            v = r[a, b] * radial((nb, lb, jb2), (na, la, ja2))
+            if v != 0.0:
+                total += v * _ek_angular(3, jb2, ja2, lb, la)
+    return total

@@ -325,3 +325,35 @@ def test_hfs_a_of_one_electron(shells, orb):
                          * D.DPAU / D.DPRB ** 2 * 1e-30)
         l = int(b.ll[orb - 1])
         assert bsum == pytest.approx(abs(_c2_reduced(j, l, j, l)), rel=1e-13)
+
+
+def _c3_reduced(ja, la, jb, lb):
+    from pci_b200 import wigner as W
+    if (la + lb) % 2 == 0:
+        return 0.0
+    return (-1) ** int(round(jb + 0.5)) * np.sqrt((2 * jb + 1) * (2 * ja + 1)) * W.three_j(jb, 3, ja, -0.5, 0, 0.5)
+
+
+@pytest.mark.parametrize("orb_a,orb_b", [(2, 4), (4, 2), (2, 3), (1, 4)])
+def test_one_electron_e3_amplitude_is_the_c3_reduced_element(orb_a, orb_b):
+    """One electron between 2p and 3d shells: with a unit radial integral
+    the E3 amplitude's size is <j_b||C^3||j_a> from a 3j symbol (zero for
+    p1/2 <-> d3/2, where j_a + j_b < 3)."""
+    b = S.make_basis([(2, 1), (3, 2)])                      # 2p1/2 2p3/2 3d3/2 3d5/2
+    jz, nh, _ = S.m_states(b, b.ns)
+    ja2, jb2 = int(b.jj[orb_a - 1]), int(b.jj[orb_b - 1])
+    la, lb = int(b.ll[orb_a - 1]), int(b.ll[orb_b - 1])
+    want = abs(_c3_reduced(ja2 / 2, la, jb2 / 2, lb))
+    found = False
+    for ia in range(jz.size):
+        for ib in range(jz.size):
+            if nh[ia] != orb_a or nh[ib] != orb_b:
+                continue
+            ro = np.zeros((jz.size, jz.size))
+            ro[ia, ib] = 1.0
+            rt = D.reduced_transition(ro, b, nh, jz, ja2 / 2, int(jz[ia]), jb2 / 2, int(jz[ib]))
+            if rt["rro"][3] is None:
+                continue
+            found = True
+            assert abs(D.e3_amplitude(rt, lambda f, i: 1.0)) == pytest.approx(want, rel=1e-13, abs=1e-15)
+    assert found or want == 0.0
